@@ -1,0 +1,212 @@
+/*
+ * pikgpu: B200 (sm_100a) implementation of the google/pik decoder's
+ * reconstruction path, exposed as a plain C ABI.
+ *
+ * The path is the one the reference runs after entropy decoding:
+ *   dequantisation of AC/DC integers (Quantizer, quant field, quant_weights
+ *   per AcStrategy) + chroma-from-luma -> DC smoothing -> LF/HF prediction ->
+ *   variable-size IDCT (2x2 .. 32x32, IDENTITY, LINES) -> gaborish ->
+ *   edge-preserving filter (EPF) + DCT-domain clamp -> gaborish ->
+ *   XYB -> linear RGB (and optionally 8-bit sRGB).
+ *
+ * Reference interfaces this ABI replaces (reference paths are relative to the
+ * google/pik checkout):
+ *   Dequant<first>::DoAC            pik/compressed_image.cc:586-707
+ *   ReconOpsinImage                 pik/compressed_image.h:93-98
+ *   FinalizeFrameDecoding           pik/compressed_image.h:104-110
+ *   DequantDC + AdaptiveDCReconstruction
+ *                                   pik/compressed_dc.cc:181-231,
+ *                                   pik/adaptive_reconstruction.cc:300-332
+ * Their callers are PikGroupToPixels (pik/pik_frame.cc:925-928) and
+ * PikPassToPixels (pik/pik_frame.cc:1149-1152).
+ *
+ * Conventions
+ *  - Every entry point returns an int status: 0 = OK, negative = error
+ *    (PIKGPU_ERR_*). Nothing aborts; the reason is in pikgpu_last_error().
+ *  - Images are planar. "blocks" are 8x8 pixel cells; Bx = ceil(xsize/8),
+ *    By = ceil(ysize/8). "colour tiles" are 64x64 pixels:
+ *    Tx = ceil(xsize/64), Ty = ceil(ysize/64).
+ *  - Host buffers stay owned by the caller. A context owns its device memory
+ *    and one CUDA stream; contexts are independent.
+ */
+#ifndef PIKGPU_H_
+#define PIKGPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIKGPU_OK 0
+#define PIKGPU_ERR_INVALID_ARG (-1) /* bad pointer, size or field value */
+#define PIKGPU_ERR_UNSUPPORTED (-2) /* feature the reference path has but
+                                       this build rejects (see below) */
+#define PIKGPU_ERR_CUDA (-3)        /* a CUDA call failed */
+#define PIKGPU_ERR_STATE (-4)       /* call out of order */
+#define PIKGPU_ERR_NO_MEMORY (-5)   /* device allocation failed */
+
+/* GaborishStrength (pik/pik_params.h:39-49). */
+#define PIKGPU_GABORISH_OFF 0
+#define PIKGPU_GABORISH_500 1
+#define PIKGPU_GABORISH_750 2
+#define PIKGPU_GABORISH_875 3
+#define PIKGPU_GABORISH_1000 4
+
+/* Number of QuantKind values (pik/quant_weights.h:25-34). */
+#define PIKGPU_NUM_QUANT_KINDS 7
+/* kMaxQuantControlFieldValue (pik/quant_weights.h:268). */
+#define PIKGPU_MAX_QUANT_CONTROL_FIELD 16
+
+/*
+ * Frame-level side information. Mirrors what PikPassToPixels holds after
+ * decoding the frame header and DC groups (pik/pik_frame.cc:1028-1065):
+ * FrameHeader subset, Quantizer scalars, DequantMatrices, dequant control
+ * field + map, ColorCorrelationMap, AcStrategyImage, raw quant field,
+ * EPF LUT ids and the quantized DC.
+ */
+typedef struct pikgpu_frame_params {
+  uint32_t xsize, ysize; /* pixels */
+
+  /* FrameHeader (pik/headers.h:202-232). */
+  uint32_t flags;    /* FrameHeader::flags; any set bit is UNSUPPORTED */
+  uint32_t gaborish; /* PIKGPU_GABORISH_* */
+  uint32_t predict_lf, predict_hf;
+  uint32_t have_adaptive_reconstruction;
+  /* EpfParams (pik/epf.h:19-40); used iff have_adaptive_reconstruction. */
+  uint32_t epf_enable_adaptive; /* 0 (fixed sigma) is UNSUPPORTED */
+  uint32_t epf_sigma;
+  uint32_t epf_use_sharpened;
+
+  /* Quantizer (pik/quantizer.h:111-389; Decode pik/quantizer.cc:63-71). */
+  int32_t global_scale; /* [1, 32768] */
+  int32_t quant_dc;     /* [1, 256] */
+
+  /* DequantMatrices (pik/quant_weights.h:202-266): the flat table and
+   * offsets[(table * 7 + kind) * 3 + c] into it. */
+  const float* dequant_table;
+  uint32_t dequant_table_size; /* floats */
+  const uint32_t* dequant_offsets;
+  uint32_t num_dequant_tables;
+  const uint8_t* dequant_control_field; /* Tx * Ty */
+  const uint8_t* dequant_map;           /* 16 * 256: [cf][qf - 1] -> table */
+
+  /* ColorCorrelationMap (pik/color_correlation.h:44-89). */
+  const int32_t* ytox_map; /* Tx * Ty */
+  const int32_t* ytob_map; /* Tx * Ty */
+  int32_t ytox_dc, ytob_dc;
+
+  /* Per-block fields, Bx * By each. */
+  const uint8_t* ac_strategy;     /* raw byte: type << 4 | sub-block index */
+  const int32_t* raw_quant_field; /* [1, 256] */
+  const uint8_t* ar_sigma_lut_ids;
+
+  /* Quantized DC after DC-prediction expansion (ExpandDC), 3 planes of
+   * Bx * By int16, plane-major (X, Y, B). */
+  const int16_t* quantized_dc;
+} pikgpu_frame_params;
+
+typedef struct pikgpu_ctx pikgpu_ctx;
+
+/* Creates a context on CUDA device `device`. */
+int pikgpu_ctx_create(int device, pikgpu_ctx** out);
+int pikgpu_ctx_destroy(pikgpu_ctx* ctx);
+/* Message of the last failed call on this context (never NULL). */
+const char* pikgpu_last_error(const pikgpu_ctx* ctx);
+
+/* Starts a frame: validates `params` (see "Errors"), sizes device buffers
+ * and uploads the side information. Replaces the frame-level state that
+ * PikPassToPixels builds before its group loop (pik/pik_frame.cc:1040-1065).
+ * Errors: INVALID_ARG for strategy > 8 (pik/ac_strategy.h:95-97), sub-block
+ * indices inconsistent with the strategy, qf outside [1,256]
+ * (pik/quantizer.h:125-128), LUT id > 1, dequant_map entries >= the number
+ * of tables, offsets past the table; UNSUPPORTED for any FrameHeader flag
+ * (noise, gradient map, grayscale, ...) and fixed-sigma EPF. */
+int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* params);
+
+/* Supplies the whole frame's quantized AC after entropy decoding and
+ * coefficient un-scattering (pik/compressed_image.cc:780-801): per plane,
+ * By rows of Bx * 64 int16 in the GroupDecCache::ac layout
+ * (pik/compressed_image_fwd.h:206). `stride` is in elements. Host memory. */
+int pikgpu_frame_set_ac(pikgpu_ctx* ctx, const int16_t* const planes[3],
+                        size_t stride);
+
+/* Same for one 512x512 group (group_index = gy * ceil(xsize/512) + gx),
+ * i.e. what DecodeFromBitstream decodes for that group
+ * (pik/compressed_image.cc:720-813). Groups may be supplied from different
+ * host threads concurrently; each writes a disjoint staging region. */
+int pikgpu_frame_set_group_ac(pikgpu_ctx* ctx, uint32_t group_index,
+                              const int16_t* const planes[3], size_t stride);
+
+/* Device-resident variant of pikgpu_frame_set_ac: `planes` are device
+ * pointers on the context's device; no host copy is made. */
+int pikgpu_frame_set_ac_device(pikgpu_ctx* ctx, const int16_t* const planes[3],
+                               size_t stride);
+
+/* Runs the whole reconstruction: the per-group Dequant::DoAC +
+ * ReconOpsinImage work and then FinalizeFrameDecoding
+ * (pik/compressed_image.cc:1144-1181). Outputs (either may be NULL):
+ *  out_linear: 3 planes of ysize rows x xsize floats, linear RGB on the
+ *     reference's 0..255 scale, row stride `linear_stride` floats.
+ *  out_srgb8: interleaved RGB bytes, row stride `srgb8_stride` bytes,
+ *     sRGB-encoded (TF_SRGB, pik/color_management.cc:323-345) and rounded
+ *     like ExternalImage::CopyTo (pik/external_image.cc:1205).
+ * If `outputs_on_device` is nonzero both pointers are device pointers and no
+ * host copy is made; otherwise they are host pointers. Blocks until done. */
+int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
+                       size_t linear_stride, uint8_t* out_srgb8,
+                       size_t srgb8_stride, int outputs_on_device);
+
+/* Intermediate planes for stage-by-stage parity checks, valid after
+ * pikgpu_reconstruct. Each is 3 planes in host memory. */
+#define PIKGPU_STAGE_DC 0          /* Bx x By: DC after AdaptiveDCRecon. */
+#define PIKGPU_STAGE_IDCT 1        /* padded frame: ReconOpsinImage output */
+#define PIKGPU_STAGE_SMOOTHED 2    /* gaborish #1 (EPF guide source) */
+#define PIKGPU_STAGE_EPF 3         /* EPF output before the DCT clamp */
+#define PIKGPU_STAGE_AR 4          /* after AdaptiveReconstruction clamp */
+#define PIKGPU_STAGE_PRE_OPSIN 5   /* after gaborish #2, before opsin */
+#define PIKGPU_STAGE_DEQUANT_AC 6  /* Bx*64 x By: DoAC output */
+int pikgpu_get_stage(pikgpu_ctx* ctx, int stage, float* const planes[3],
+                     size_t stride, size_t xsize, size_t ysize);
+
+/* Average device time in milliseconds of each kernel of the last
+ * pikgpu_reconstruct call, written to `ms` (up to `n` entries); returns the
+ * number of kernels or an error. Names via pikgpu_kernel_name. */
+int pikgpu_last_kernel_times(pikgpu_ctx* ctx, float* ms, int n);
+const char* pikgpu_kernel_name(int index);
+
+/* Checks `params` exactly as pikgpu_frame_begin does, without a device.
+ * Writes the reason for a failure into `msg` (may be NULL). */
+int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
+                    size_t msg_size);
+
+/* Options (set before pikgpu_frame_begin):
+ *  KEEP_STAGES: keep the dequantised AC, EPF and pre-opsin planes for
+ *               pikgpu_get_stage (costs extra device memory and copies);
+ *  PROFILE:     time each kernel group with CUDA events
+ *               (pikgpu_last_kernel_times). */
+#define PIKGPU_OPT_KEEP_STAGES 1
+#define PIKGPU_OPT_PROFILE 2
+int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value);
+
+/* Verification hooks for the EPF's discrete decisions, which make two
+ * implementations comparable on arithmetic alone: the u8 guide (3 planes of
+ * (8By + 12) x (8Bx + 12), the padded frame with the filter's 6-pixel
+ * mirrored border) and the per-block sigma (By x Bx int32), as computed by
+ * MakeGuide / SigmaFromQuant (pik/epf_target.cc:1009-1111). `set` replaces
+ * the computed values for the current frame (NULL restores computing them);
+ * `get` exports the values of the last pikgpu_reconstruct. Host memory. */
+int pikgpu_set_epf_decisions(pikgpu_ctx* ctx, const uint8_t* guide,
+                             const int32_t* sigma);
+int pikgpu_get_epf_decisions(pikgpu_ctx* ctx, uint8_t* guide, int32_t* sigma);
+
+/* Sets the CUDA stream (a cudaStream_t passed as void*) the context launches
+ * on; NULL restores the context's own stream. */
+int pikgpu_set_stream(pikgpu_ctx* ctx, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIKGPU_H_ */

@@ -1,0 +1,103 @@
+// Device kernels of the reconstruction path (sm_100a).
+//
+// Arithmetic is IEEE single precision with every multiply and add rounded
+// separately (this translation unit is compiled with -fmad=false) and sums
+// taken in a fixed order; transforms are separable matrix products with the
+// matrices of tables.h. This makes the plain FP32 form deterministic and
+// reproducible run to run.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tables.h"
+
+namespace pikgpu {
+
+
+// AcStrategy types (pik/ac_strategy.h:51-70).
+enum : int {
+  kDCT = 0, kIDENTITY = 1, kDCT2X2 = 2, kDCT4X4 = 3, kDCT16X16 = 4,
+  kDCT32X32 = 5, kLINES = 6, kDCT_NOHF = 7, kDCT4X4_NOHF = 8
+};
+
+__host__ __device__ inline int Covered(int type) {
+  return type == kDCT32X32 ? 4 : type == kDCT16X16 ? 2 : 1;
+}
+__host__ __device__ inline int QuantKindOf(int type) {
+  return type == kDCT_NOHF ? 0 : type == kDCT4X4_NOHF ? 3 : type;
+}
+__host__ __device__ inline bool PredictHFOf(int type) {
+  return type != kDCT2X2 && type != kIDENTITY && type != kDCT_NOHF &&
+         type != kDCT4X4_NOHF && type != kLINES;
+}
+__device__ inline float ARQuantScaleOf(int type) {
+  if (type == kDCT32X32) return 1.2282996852328099f;
+  if (type == kDCT16X16) return 1.1423171621463439f;
+  if (type == kDCT4X4 || type == kDCT4X4_NOHF) return 1.2f;
+  if (type == kDCT2X2) return 1.0098134203870499f;
+  return 1.0f;
+}
+
+// Mirror with the edge sample repeated once (pik/image_ops.h:217-227),
+// reflecting repeatedly for overshoots larger than the size.
+__host__ __device__ inline int MirrorIdx(int x, int size) {
+  while (x < 0 || x >= size) {
+    x = x < 0 ? -x - 1 : 2 * size - 1 - x;
+  }
+  return x;
+}
+
+// Frame geometry.
+struct Geo {
+  int W, H;       // pixels
+  int Bx, By;     // blocks
+  int PW, PH;     // padded pixels (8 Bx, 8 By)
+  int Tx, Ty;     // 64-pixel tiles
+  int Gx, Gy;     // 512-pixel groups
+  int ac_stride;  // Bx * 64
+};
+
+// Per-group bordered arrays: llf (66 x 66) and 2x2 images (132 x 132).
+constexpr int kGB = 66;
+constexpr int kG2 = 132;
+constexpr size_t kLlfGroupFloats = size_t(3) * kGB * kGB;
+constexpr size_t kG2GroupFloats = size_t(3) * kG2 * kG2;
+
+struct FrameScalars {
+  float inv_global_scale;  // Quantizer::InvGlobalScale
+  float inv_quant_dc;      // Quantizer::inv_quant_dc (decoder form)
+  float mul_dc[3];         // DequantMatrix(0, DCT8, c)[0] * inv_quant_dc
+  float ytox_dc, ytob_dc;  // YtoX(1, ytox_dc), YtoB(1, ytob_dc)
+  int gaborish;
+  int predict_lf, predict_hf;
+  int have_ar;
+  int use_sharpened;
+  int quant_dc;
+};
+
+// Device pointers of one frame.
+struct DevFrame {
+  const uint8_t* acs;
+  const int32_t* qf;
+  const uint8_t* lut;
+  const uint8_t* dq_cf;
+  const uint8_t* dq_map;
+  const int32_t* ytox;
+  const int32_t* ytob;
+  const float* table;
+  const uint32_t* offsets;
+  const int16_t* qdc;
+  const int16_t* qac;
+  float* dc;          // 3 x By x Bx
+  float* ac;          // 3 x By x ac_stride
+  float* llf_g;       // groups x 3 x 66 x 66
+  float* lf2x2_g;     // groups x 3 x 132 x 132
+  float* pred2x2_g;   // groups x 3 x 132 x 132
+  float* tmp2x2_g;    // groups x 3 x 132 x 132
+  float* idct;        // 3 x PH x PW
+  float* smoothed;    // 3 x PH x PW
+  float* filt;        // 3 x PH x PW
+};
+
+}  // namespace pikgpu

@@ -1,0 +1,946 @@
+// C ABI of the B200 reconstruction path (include/pikgpu.h): validation,
+// device memory, uploads and the launch sequence that replaces
+// Dequant::DoAC + ReconOpsinImage (per group) + FinalizeFrameDecoding
+// (pik/compressed_image.cc:586-707, 936-1106, 1144-1181) and
+// DequantDC + AdaptiveDCReconstruction (pik/compressed_dc.cc:181-231,
+// pik/adaptive_reconstruction.cc:300-332).
+//
+// Single translation unit: the kernels are included so that the
+// __constant__ tables need no relocatable device code.
+
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pikgpu.h"
+#include "recon_kernels.cu"
+#include "tables.cc"
+
+using namespace pikgpu;
+
+namespace {
+
+// Block classes launched by separate kernels.
+enum Class { kC8 = 0, kC16, kC32, kC4, kCSmall, kNumClasses };
+int ClassOf(int type) {
+  switch (type) {
+    case kDCT:
+    case kDCT_NOHF:
+      return kC8;
+    case kDCT16X16:
+      return kC16;
+    case kDCT32X32:
+      return kC32;
+    case kDCT4X4:
+    case kDCT4X4_NOHF:
+      return kC4;
+    default:
+      return kCSmall;
+  }
+}
+
+// Kernel groups timed with events when profiling is on.
+enum Timed {
+  kTDc = 0, kTLf, kTDequant, kTIdct, kTGab1, kTEpf, kTAr, kTFinal, kNumTimed
+};
+const char* kTimedNames[kNumTimed] = {
+    "dc_dequant_epf", "lf_prediction", "dequant_ac_lf_update", "hf_idct",
+    "gaborish1_minmax", "epf", "ar_clamp", "gaborish2_opsin_srgb"};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+std::mutex g_table_mutex;
+bool g_tables_uploaded[64] = {};
+
+}  // namespace
+
+struct pikgpu_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  bool have_frame = false, have_ac = false, have_result = false;
+  bool keep_stages = false, profile = false;
+  Geo g{};
+  FrameScalars s{};
+  // host copies needed after begin
+  std::vector<uint32_t> lists[kNumClasses];
+  // device buffers
+  DevBuf acs, qf, lut, dq_cf, dq_map, ytox, ytob, table, offsets;
+  DevBuf qdc, qac, dc, dcpad, dcfilt, ac, llf_g, lf2x2_g, pred2x2_g, tmp2x2_g;
+  DevBuf idct, smoothed, filt, mm, sigma, dc_sigma, list[kNumClasses];
+  DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr;
+  DevBuf sigma_ovr;
+  bool use_guide_ovr = false, use_sigma_ovr = false;
+  cudaEvent_t ev[kNumTimed + 1] = {};
+  float times[kNumTimed] = {};
+  float dc_half_step[3] = {};
+};
+
+namespace {
+
+int Fail(pikgpu_ctx* ctx, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                 \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) {                                                \
+      return Fail(ctx, PIKGPU_ERR_CUDA, "%s: %s", #call,                    \
+                  cudaGetErrorString(e_));                                  \
+    }                                                                       \
+  } while (0)
+
+int Ensure(pikgpu_ctx* ctx, DevBuf* b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b->cap >= bytes) return PIKGPU_OK;
+  if (b->p) cudaFree(b->p);
+  b->p = nullptr;
+  b->cap = 0;
+  const cudaError_t e = cudaMalloc(&b->p, bytes);
+  if (e != cudaSuccess) {
+    return Fail(ctx, PIKGPU_ERR_NO_MEMORY, "cudaMalloc(%zu): %s", bytes,
+                cudaGetErrorString(e));
+  }
+  b->cap = bytes;
+  return PIKGPU_OK;
+}
+
+void FreeBuf(DevBuf* b) {
+  if (b->p) cudaFree(b->p);
+  b->p = nullptr;
+  b->cap = 0;
+}
+
+template <typename T>
+T* P(const DevBuf& b) {
+  return static_cast<T*>(b.p);
+}
+
+constexpr int kRequiredSize[7] = {1, 1, 1, 1, 2, 4, 1};
+
+// Host-side validation shared by pikgpu_frame_begin and pikgpu_validate.
+int Validate(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
+  if (!p) return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "params is NULL");
+  if (p->xsize == 0 || p->ysize == 0) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "empty image %ux%u", p->xsize,
+                p->ysize);
+  }
+  if (p->xsize > (1u << 18) || p->ysize > (1u << 18)) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "image %ux%u too large",
+                p->xsize, p->ysize);
+  }
+  if (!p->dequant_table || !p->dequant_offsets || !p->dequant_control_field ||
+      !p->dequant_map || !p->ytox_map || !p->ytob_map || !p->ac_strategy ||
+      !p->raw_quant_field || !p->ar_sigma_lut_ids || !p->quantized_dc) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "NULL array in params");
+  }
+  if (p->flags != 0) {
+    return Fail(ctx, PIKGPU_ERR_UNSUPPORTED,
+                "FrameHeader flags 0x%x (noise/gradient/grayscale/...) are "
+                "not supported",
+                p->flags);
+  }
+  if (p->gaborish > PIKGPU_GABORISH_1000) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "gaborish strength %u",
+                p->gaborish);
+  }
+  if (p->have_adaptive_reconstruction && !p->epf_enable_adaptive) {
+    return Fail(ctx, PIKGPU_ERR_UNSUPPORTED, "fixed-sigma EPF");
+  }
+  if (p->global_scale < 1 || p->global_scale > 32768) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "global_scale %d",
+                p->global_scale);
+  }
+  if (p->quant_dc < 1 || p->quant_dc > 256) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "quant_dc %d", p->quant_dc);
+  }
+  if (p->num_dequant_tables < 1 || p->num_dequant_tables > 256) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "num_dequant_tables %u",
+                p->num_dequant_tables);
+  }
+  for (uint32_t t = 0; t < p->num_dequant_tables; ++t) {
+    for (int k = 0; k < 7; ++k) {
+      for (int c = 0; c < 3; ++c) {
+        const uint64_t off = p->dequant_offsets[(t * 7 + k) * 3 + c];
+        const uint64_t need = 64ull * kRequiredSize[k] * kRequiredSize[k];
+        if (off + need > p->dequant_table_size) {
+          return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                      "dequant offset %llu (table %u kind %d c %d) beyond "
+                      "table of %u floats",
+                      (unsigned long long)off, t, k, c,
+                      p->dequant_table_size);
+        }
+      }
+    }
+  }
+  const int bx = (p->xsize + 7) / 8, by = (p->ysize + 7) / 8;
+  const int tx = (p->xsize + 63) / 64, ty = (p->ysize + 63) / 64;
+  for (int i = 0; i < tx * ty; ++i) {
+    if (p->dequant_control_field[i] >= PIKGPU_MAX_QUANT_CONTROL_FIELD) {
+      return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "dequant control field %u",
+                  p->dequant_control_field[i]);
+    }
+  }
+  for (int i = 0; i < 16 * 256; ++i) {
+    if (p->dequant_map[i] >= p->num_dequant_tables) {
+      return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "dequant_map entry %u >= %u",
+                  p->dequant_map[i], p->num_dequant_tables);
+    }
+  }
+  // AcStrategyImage consistency (pik/ac_strategy.h:95-97, 315-356).
+  std::vector<uint8_t> expect(size_t(bx) * by, 0xFF);
+  for (int y = 0; y < by; ++y) {
+    for (int x = 0; x < bx; ++x) {
+      const uint8_t a = p->ac_strategy[y * bx + x];
+      const int type = a >> 4, blk = a & 0xF;
+      if (type > 8) {
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                    "invalid AcStrategy %d at block (%d, %d)", type, x, y);
+      }
+      const int q = p->raw_quant_field[y * bx + x];
+      if (q < 1 || q > 256) {
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                    "quant field %d at block (%d, %d) outside [1, 256]", q, x,
+                    y);
+      }
+      if (p->ar_sigma_lut_ids[y * bx + x] > 1) {
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "EPF LUT id %u at (%d, %d)",
+                    p->ar_sigma_lut_ids[y * bx + x], x, y);
+      }
+      if (blk != 0) continue;
+      const int cov = Covered(type);
+      if (cov > 1 && ((x % cov) != 0 || (y % cov) != 0)) {
+        return Fail(ctx, PIKGPU_ERR_UNSUPPORTED,
+                    "%dx%d transform at block (%d, %d) is not aligned to its "
+                    "size",
+                    8 * cov, 8 * cov, x, y);
+      }
+      if (x + cov > bx || y + cov > by) {
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                    "transform at (%d, %d) extends past the image", x, y);
+      }
+      for (int iy = 0; iy < cov; ++iy) {
+        for (int ix = 0; ix < cov; ++ix) {
+          uint8_t& e = expect[size_t(y + iy) * bx + x + ix];
+          if (e != 0xFF) {
+            return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                        "overlapping transforms at block (%d, %d)", x + ix,
+                        y + iy);
+          }
+          e = uint8_t((type << 4) | (iy * cov + ix));
+        }
+      }
+    }
+  }
+  for (size_t i = 0; i < expect.size(); ++i) {
+    if (expect[i] != p->ac_strategy[i]) {
+      return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                  "AcStrategy sub-block index inconsistent at block (%zu, "
+                  "%zu)",
+                  i % bx, i / bx);
+    }
+  }
+  return PIKGPU_OK;
+}
+
+void ComputeScalars(const pikgpu_frame_params* p, FrameScalars* s) {
+  // Quantizer::RecomputeFromGlobalScale + Decode (pik/quantizer.h:130-135,
+  // pik/quantizer.cc:63-71).
+  s->inv_global_scale = static_cast<float>(1.0 * 65536 / p->global_scale);
+  s->inv_quant_dc = s->inv_global_scale / p->quant_dc;
+  for (int c = 0; c < 3; ++c) {
+    s->mul_dc[c] =
+        p->dequant_table[p->dequant_offsets[c]] * s->inv_quant_dc;
+  }
+  s->ytox_dc = 1.0f * float(p->ytox_dc - 128) * (1.0f / 256);
+  s->ytob_dc = 1.0f * float(p->ytob_dc) * (1.0f / 128);
+  s->gaborish = p->gaborish;
+  s->predict_lf = p->predict_lf ? 1 : 0;
+  s->predict_hf = p->predict_hf ? 1 : 0;
+  s->have_ar = p->have_adaptive_reconstruction ? 1 : 0;
+  s->use_sharpened = p->epf_use_sharpened ? 1 : 0;
+  s->quant_dc = p->quant_dc;
+}
+
+int UploadTables(pikgpu_ctx* ctx) {
+  std::lock_guard<std::mutex> lock(g_table_mutex);
+  if (ctx->device < 64 && g_tables_uploaded[ctx->device]) return PIKGPU_OK;
+  DevTables t;
+  BuildTables(&t);
+  CUDA_TRY(ctx, cudaMemcpyToSymbol(c_t, &t, sizeof(t)));
+  if (ctx->device < 64) g_tables_uploaded[ctx->device] = true;
+  return PIKGPU_OK;
+}
+
+inline int Blocks(size_t n, int t) { return int((n + t - 1) / t); }
+
+void Mark(pikgpu_ctx* ctx, int i) {
+  if (ctx->profile) cudaEventRecord(ctx->ev[i], ctx->stream);
+}
+
+// The frame EPF or the DC EPF: minmax of the guide source is expected in
+// ctx->mm already; sigma per block into `sig`.
+int RunEpf(pikgpu_ctx* ctx, const float* in, const float* guide_src, int w,
+           int h, const int32_t* sig, float* out, const uint8_t* guide_ovr) {
+  dim3 grid(Blocks(w, kEpfTile), Blocks(h, kEpfTile));
+  k_epf<<<grid, 256, 0, ctx->stream>>>(in, guide_src, guide_ovr, w, h,
+                                       P<uint32_t>(ctx->mm), sig, out);
+  return PIKGPU_OK;
+}
+
+int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
+              size_t rgb8_stride) {
+  const Geo& g = ctx->g;
+  const FrameScalars& s = ctx->s;
+  cudaStream_t st = ctx->stream;
+  DevFrame f;
+  f.acs = P<uint8_t>(ctx->acs);
+  f.qf = P<int32_t>(ctx->qf);
+  f.lut = P<uint8_t>(ctx->lut);
+  f.dq_cf = P<uint8_t>(ctx->dq_cf);
+  f.dq_map = P<uint8_t>(ctx->dq_map);
+  f.ytox = P<int32_t>(ctx->ytox);
+  f.ytob = P<int32_t>(ctx->ytob);
+  f.table = P<float>(ctx->table);
+  f.offsets = P<uint32_t>(ctx->offsets);
+  f.qdc = P<int16_t>(ctx->qdc);
+  f.qac = P<int16_t>(ctx->qac);
+  f.dc = P<float>(ctx->dc);
+  f.ac = P<float>(ctx->ac);
+  f.llf_g = P<float>(ctx->llf_g);
+  f.lf2x2_g = P<float>(ctx->lf2x2_g);
+  f.pred2x2_g = P<float>(ctx->pred2x2_g);
+  f.tmp2x2_g = P<float>(ctx->tmp2x2_g);
+  f.idct = P<float>(ctx->idct);
+  f.smoothed = P<float>(ctx->smoothed);
+  f.filt = P<float>(ctx->filt);
+  uint32_t* mm = P<uint32_t>(ctx->mm);
+
+  Mark(ctx, kTDc);
+  // DC: dequant, EPF on the 8-padded DC image, clamp.
+  k_dequant_dc<<<Blocks(size_t(g.Bx) * g.By, 256), 256, 0, st>>>(g, f, s);
+  const int dpw = (g.Bx + 7) / 8 * 8, dph = (g.By + 7) / 8 * 8;
+  float* dcpad = P<float>(ctx->dcpad);
+  float* dcfilt = P<float>(ctx->dcfilt);
+  {
+    dim3 b(32, 8), gr(Blocks(dpw, 32), Blocks(dph, 8), 3);
+    k_pad_replicate<<<gr, b, 0, st>>>(f.dc, g.Bx, g.By, dcpad, dpw, dph);
+    k_minmax_init<<<1, 32, 0, st>>>(mm);
+    k_minmax<<<dim3(Blocks(size_t(dpw) * dph, 256 * 8), 3), 256, 0, st>>>(
+        dcpad, size_t(dpw) * dph, mm);
+    const int nb = (dpw / 8) * (dph / 8);
+    k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(
+        nb, nullptr, nullptr, nullptr, s.quant_dc / 2, mm,
+        P<int32_t>(ctx->dc_sigma));
+    RunEpf(ctx, dcpad, dcpad, dpw, dph, P<int32_t>(ctx->dc_sigma), dcfilt,
+           nullptr);
+    dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
+    k_dc_clamp<<<gr2, b, 0, st>>>(f.dc, dcfilt, g.Bx, g.By, dpw, dph,
+                                  ctx->dc_half_step[0], ctx->dc_half_step[1],
+                                  ctx->dc_half_step[2]);
+  }
+  Mark(ctx, kTLf);
+  // Per-group LF prediction.
+  const int ng = g.Gx * g.Gy;
+  {
+    dim3 b(16, 16), gr(Blocks(kGB, 16), Blocks(kGB, 16), 3 * ng);
+    k_llf<<<gr, b, 0, st>>>(g, f);
+    if (s.predict_lf) {
+      k_tmp2x2<<<gr, b, 0, st>>>(g, f);
+      dim3 gr2(Blocks(kG2, 16), Blocks(kG2, 16), 3 * ng);
+      k_lf_blur<<<gr2, b, 0, st>>>(g, f);
+      k_lf_from_2x2<<<gr, b, 0, st>>>(g, f);
+    }
+    if (s.predict_hf) {
+      k_pred_border<<<dim3(Blocks(4 * (kGB + 2), 128), 1, 3 * ng), 128, 0,
+                      st>>>(g, f, s.predict_lf);
+    }
+  }
+  Mark(ctx, kTDequant);
+  {
+    dim3 b(64, 4), gr(Blocks(g.Bx, 4), g.By);
+    k_dequant_ac<<<gr, b, 0, st>>>(g, f, s);
+    if (ctx->keep_stages) {
+      cudaMemcpyAsync(ctx->dbg_dequant.p, f.ac,
+                      sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
+                      cudaMemcpyDeviceToDevice, st);
+    }
+    dim3 b2(32, 8), gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
+    k_lf_update<<<gr2, b2, 0, st>>>(g, f, s.predict_lf, s.predict_hf);
+  }
+  Mark(ctx, kTIdct);
+  {
+    const uint32_t* L[kNumClasses];
+    int n[kNumClasses];
+    for (int k = 0; k < kNumClasses; ++k) {
+      L[k] = P<uint32_t>(ctx->list[k]);
+      n[k] = int(ctx->lists[k].size());
+    }
+    if (n[kC8]) k_square_idct<8><<<Blocks(n[kC8], 4), 256, 0, st>>>(
+        g, f, L[kC8], n[kC8], s.predict_hf);
+    if (n[kC16]) k_square_idct<16><<<n[kC16], 256, 0, st>>>(
+        g, f, L[kC16], n[kC16], s.predict_hf);
+    if (n[kC32]) k_square_idct<32><<<n[kC32], 256, 0, st>>>(
+        g, f, L[kC32], n[kC32], s.predict_hf);
+    if (n[kC4]) k_dct4_idct<<<Blocks(n[kC4], 16), 256, 0, st>>>(
+        g, f, L[kC4], n[kC4], s.predict_hf);
+    if (n[kCSmall]) k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, st>>>(
+        g, f, L[kCSmall], n[kCSmall]);
+  }
+  const float* final_in = f.idct;
+  Mark(ctx, kTGab1);
+  if (s.have_ar) {
+    const size_t npx = size_t(g.PW) * g.PH;
+    const float* guide_src = f.idct;
+    k_minmax_init<<<1, 32, 0, st>>>(mm);
+    if (s.gaborish) {
+      dim3 b(32, 8), gr(Blocks(g.PW, 32), Blocks(g.PH, 8), 3);
+      k_gaborish_minmax<<<gr, b, 0, st>>>(f.idct, g.PW, g.PH, s.gaborish,
+                                          f.smoothed,
+                                          s.use_sharpened ? nullptr : mm);
+      if (!s.use_sharpened) guide_src = f.smoothed;
+    }
+    if (guide_src == f.idct) {
+      k_minmax<<<dim3(Blocks(npx, 256 * 8), 3), 256, 0, st>>>(f.idct, npx,
+                                                               mm);
+    }
+    Mark(ctx, kTEpf);
+    const int nb = g.Bx * g.By;
+    int32_t* sig = P<int32_t>(ctx->sigma);
+    if (ctx->use_sigma_ovr) {
+      cudaMemcpyAsync(sig, ctx->sigma_ovr.p, sizeof(int32_t) * nb,
+                      cudaMemcpyDeviceToDevice, st);
+    } else {
+      k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, f.qf, f.acs, f.lut, 0,
+                                                   mm, sig);
+    }
+    RunEpf(ctx, f.idct, guide_src, g.PW, g.PH, sig, f.filt,
+           ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr);
+    if (ctx->keep_stages) {
+      cudaMemcpyAsync(ctx->dbg_epf.p, f.filt, sizeof(float) * 3 * npx,
+                      cudaMemcpyDeviceToDevice, st);
+    }
+    Mark(ctx, kTAr);
+    const uint32_t* L[kNumClasses];
+    int n[kNumClasses];
+    for (int k = 0; k < kNumClasses; ++k) {
+      L[k] = P<uint32_t>(ctx->list[k]);
+      n[k] = int(ctx->lists[k].size());
+    }
+    if (n[kC8]) k_square_ar<8><<<Blocks(n[kC8], 4), 256, 0, st>>>(
+        g, f, s, L[kC8], n[kC8]);
+    if (n[kC16]) k_square_ar<16><<<n[kC16], 256, 0, st>>>(g, f, s, L[kC16],
+                                                          n[kC16]);
+    if (n[kC32]) k_square_ar<32><<<n[kC32], 256, 0, st>>>(g, f, s, L[kC32],
+                                                          n[kC32]);
+    if (n[kC4]) k_dct4_ar<<<Blocks(n[kC4], 16), 256, 0, st>>>(
+        g, f, s, L[kC4], n[kC4]);
+    if (n[kCSmall]) k_small_ar<<<Blocks(n[kCSmall], 64), 64, 0, st>>>(
+        g, f, s, L[kCSmall], n[kCSmall]);
+    final_in = f.filt;
+  } else {
+    Mark(ctx, kTEpf);
+    Mark(ctx, kTAr);
+  }
+  Mark(ctx, kTFinal);
+  {
+    dim3 b(32, 8), gr(Blocks(g.W, 32), Blocks(g.H, 8));
+    k_final<<<gr, b, 0, st>>>(final_in, g.PW, g.PH, g.W, g.H, s.gaborish,
+                              ctx->keep_stages ? P<float>(ctx->dbg_pre)
+                                               : nullptr,
+                              lin, lin_stride, rgb8, rgb8_stride);
+  }
+  Mark(ctx, kNumTimed);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return PIKGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
+                    size_t msg_size) {
+  pikgpu_ctx tmp;
+  const int rc = Validate(&tmp, params);
+  if (msg && msg_size) {
+    snprintf(msg, msg_size, "%s", rc == PIKGPU_OK ? "" : tmp.err.c_str());
+  }
+  return rc;
+}
+
+int pikgpu_ctx_create(int device, pikgpu_ctx** out) {
+  if (!out) return PIKGPU_ERR_INVALID_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    return PIKGPU_ERR_CUDA;
+  }
+  pikgpu_ctx* ctx = new pikgpu_ctx;
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) !=
+          cudaSuccess) {
+    delete ctx;
+    return PIKGPU_ERR_CUDA;
+  }
+  ctx->stream = ctx->own_stream;
+  for (auto& e : ctx->ev) cudaEventCreate(&e);
+  if (UploadTables(ctx) != PIKGPU_OK) {
+    pikgpu_ctx_destroy(ctx);
+    return PIKGPU_ERR_CUDA;
+  }
+  *out = ctx;
+  return PIKGPU_OK;
+}
+
+int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
+  if (!ctx) return PIKGPU_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  DevBuf* bufs[] = {&ctx->acs,     &ctx->qf,        &ctx->lut,
+                    &ctx->dq_cf,   &ctx->dq_map,    &ctx->ytox,
+                    &ctx->ytob,    &ctx->table,     &ctx->offsets,
+                    &ctx->qdc,     &ctx->qac,       &ctx->dc,
+                    &ctx->dcpad,   &ctx->dcfilt,    &ctx->ac,
+                    &ctx->llf_g,   &ctx->lf2x2_g,   &ctx->pred2x2_g,
+                    &ctx->tmp2x2_g, &ctx->idct,     &ctx->smoothed,
+                    &ctx->filt,    &ctx->mm,        &ctx->sigma,
+                    &ctx->dc_sigma, &ctx->out_lin,  &ctx->out_rgb8,
+                    &ctx->dbg_dequant, &ctx->dbg_epf, &ctx->dbg_pre,
+                    &ctx->guide_ovr, &ctx->sigma_ovr};
+  for (DevBuf* b : bufs) FreeBuf(b);
+  for (auto& b : ctx->list) FreeBuf(&b);
+  for (auto& e : ctx->ev) {
+    if (e) cudaEventDestroy(e);
+  }
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return PIKGPU_OK;
+}
+
+const char* pikgpu_last_error(const pikgpu_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : "NULL context";
+}
+
+int pikgpu_set_stream(pikgpu_ctx* ctx, void* stream) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return PIKGPU_OK;
+}
+
+int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  switch (option) {
+    case PIKGPU_OPT_KEEP_STAGES:
+      ctx->keep_stages = value != 0;
+      return PIKGPU_OK;
+    case PIKGPU_OPT_PROFILE:
+      ctx->profile = value != 0;
+      return PIKGPU_OK;
+  }
+  return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "unknown option %d", option);
+}
+
+int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  ctx->have_frame = ctx->have_ac = ctx->have_result = false;
+  int rc = Validate(ctx, p);
+  if (rc != PIKGPU_OK) return rc;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  Geo& g = ctx->g;
+  g.W = p->xsize;
+  g.H = p->ysize;
+  g.Bx = (g.W + 7) / 8;
+  g.By = (g.H + 7) / 8;
+  g.PW = 8 * g.Bx;
+  g.PH = 8 * g.By;
+  g.Tx = (g.W + 63) / 64;
+  g.Ty = (g.H + 63) / 64;
+  g.Gx = (g.W + 511) / 512;
+  g.Gy = (g.H + 511) / 512;
+  g.ac_stride = g.Bx * 64;
+  ComputeScalars(p, &ctx->s);
+  for (int c = 0; c < 3; ++c) {
+    // AdaptiveDCReconstruction half step (pik/adaptive_reconstruction.cc:
+    // 319-322): inv_quant_dc * DequantMatrix(0, DCT8, c)[0] * 0.5f.
+    ctx->dc_half_step[c] = ctx->s.inv_quant_dc *
+                           p->dequant_table[p->dequant_offsets[c]] * 0.5f;
+  }
+  const size_t nb = size_t(g.Bx) * g.By, nt = size_t(g.Tx) * g.Ty;
+  const size_t npx = size_t(g.PW) * g.PH;
+  const size_t nac = size_t(g.ac_stride) * g.By;
+  const int ng = g.Gx * g.Gy;
+  const int dpw = (g.Bx + 7) / 8 * 8, dph = (g.By + 7) / 8 * 8;
+  struct {
+    DevBuf* b;
+    size_t bytes;
+  } allocs[] = {
+      {&ctx->acs, nb},
+      {&ctx->qf, 4 * nb},
+      {&ctx->lut, nb},
+      {&ctx->dq_cf, nt},
+      {&ctx->dq_map, 16 * 256},
+      {&ctx->ytox, 4 * nt},
+      {&ctx->ytob, 4 * nt},
+      {&ctx->table, 4 * size_t(p->dequant_table_size)},
+      {&ctx->offsets, 4 * size_t(p->num_dequant_tables) * 21},
+      {&ctx->qdc, 2 * 3 * nb},
+      {&ctx->qac, 2 * 3 * nac},
+      {&ctx->dc, 4 * 3 * nb},
+      {&ctx->dcpad, 4 * 3 * size_t(dpw) * dph},
+      {&ctx->dcfilt, 4 * 3 * size_t(dpw) * dph},
+      {&ctx->ac, 4 * 3 * nac},
+      {&ctx->llf_g, 4 * kLlfGroupFloats * ng},
+      {&ctx->lf2x2_g, 4 * kG2GroupFloats * ng},
+      {&ctx->pred2x2_g, 4 * kG2GroupFloats * ng},
+      {&ctx->tmp2x2_g, 4 * kG2GroupFloats * ng},
+      {&ctx->idct, 4 * 3 * npx},
+      {&ctx->smoothed, 4 * 3 * npx},
+      {&ctx->filt, 4 * 3 * npx},
+      {&ctx->mm, 64},
+      {&ctx->sigma, 4 * nb},
+      {&ctx->dc_sigma, 4 * size_t(dpw / 8) * (dph / 8)},
+  };
+  for (auto& a : allocs) {
+    rc = Ensure(ctx, a.b, a.bytes);
+    if (rc != PIKGPU_OK) return rc;
+  }
+  if (ctx->keep_stages) {
+    if ((rc = Ensure(ctx, &ctx->dbg_dequant, 4 * 3 * nac)) ||
+        (rc = Ensure(ctx, &ctx->dbg_epf, 4 * 3 * npx)) ||
+        (rc = Ensure(ctx, &ctx->dbg_pre, 4 * 3 * size_t(g.W) * g.H))) {
+      return rc;
+    }
+  }
+  // Block lists per transform class (first blocks only).
+  for (auto& l : ctx->lists) l.clear();
+  for (int y = 0; y < g.By; ++y) {
+    for (int x = 0; x < g.Bx; ++x) {
+      const uint8_t a = p->ac_strategy[y * g.Bx + x];
+      if (a & 0xF) continue;
+      ctx->lists[ClassOf(a >> 4)].push_back(uint32_t(x) | (uint32_t(y) << 16));
+    }
+  }
+  cudaStream_t st = ctx->stream;
+  for (int k = 0; k < kNumClasses; ++k) {
+    rc = Ensure(ctx, &ctx->list[k], 4 * ctx->lists[k].size());
+    if (rc != PIKGPU_OK) return rc;
+    if (!ctx->lists[k].empty()) {
+      CUDA_TRY(ctx, cudaMemcpyAsync(ctx->list[k].p, ctx->lists[k].data(),
+                                    4 * ctx->lists[k].size(),
+                                    cudaMemcpyHostToDevice, st));
+    }
+  }
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->acs.p, p->ac_strategy, nb,
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->qf.p, p->raw_quant_field, 4 * nb,
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->lut.p, p->ar_sigma_lut_ids, nb,
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dq_cf.p, p->dequant_control_field, nt,
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dq_map.p, p->dequant_map, 16 * 256,
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ytox.p, p->ytox_map, 4 * nt,
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ytob.p, p->ytob_map, 4 * nt,
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->table.p, p->dequant_table,
+                                4 * size_t(p->dequant_table_size),
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->offsets.p, p->dequant_offsets,
+                                4 * size_t(p->num_dequant_tables) * 21,
+                                cudaMemcpyHostToDevice, st));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->qdc.p, p->quantized_dc, 2 * 3 * nb,
+                                cudaMemcpyHostToDevice, st));
+  ctx->have_frame = true;
+  return PIKGPU_OK;
+}
+
+int pikgpu_frame_set_ac(pikgpu_ctx* ctx, const int16_t* const planes[3],
+                        size_t stride) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
+  if (!planes || stride < size_t(ctx->g.ac_stride)) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "bad AC planes/stride");
+  }
+  const Geo& g = ctx->g;
+  for (int c = 0; c < 3; ++c) {
+    if (!planes[c]) return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "NULL AC plane");
+    int16_t* dst = P<int16_t>(ctx->qac) + size_t(c) * g.ac_stride * g.By;
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, 2 * size_t(g.ac_stride), planes[c],
+                                    2 * stride, 2 * size_t(g.ac_stride), g.By,
+                                    cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->have_ac = true;
+  return PIKGPU_OK;
+}
+
+int pikgpu_frame_set_group_ac(pikgpu_ctx* ctx, uint32_t group_index,
+                              const int16_t* const planes[3], size_t stride) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
+  const Geo& g = ctx->g;
+  if (group_index >= uint32_t(g.Gx * g.Gy)) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "group %u of %d", group_index,
+                g.Gx * g.Gy);
+  }
+  const int x0 = (group_index % g.Gx) * 64, y0 = (group_index / g.Gx) * 64;
+  const int gxs = std::min(64, g.Bx - x0), gys = std::min(64, g.By - y0);
+  if (!planes || stride < size_t(gxs) * 64) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "bad AC planes/stride");
+  }
+  for (int c = 0; c < 3; ++c) {
+    if (!planes[c]) return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "NULL AC plane");
+    int16_t* dst = P<int16_t>(ctx->qac) + size_t(c) * g.ac_stride * g.By +
+                   size_t(y0) * g.ac_stride + size_t(x0) * 64;
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, 2 * size_t(g.ac_stride), planes[c],
+                                    2 * stride, 2 * size_t(gxs) * 64, gys,
+                                    cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->have_ac = true;
+  return PIKGPU_OK;
+}
+
+int pikgpu_frame_set_ac_device(pikgpu_ctx* ctx, const int16_t* const planes[3],
+                               size_t stride) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
+  if (!planes || stride < size_t(ctx->g.ac_stride)) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "bad AC planes/stride");
+  }
+  const Geo& g = ctx->g;
+  for (int c = 0; c < 3; ++c) {
+    if (!planes[c]) return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "NULL AC plane");
+    int16_t* dst = P<int16_t>(ctx->qac) + size_t(c) * g.ac_stride * g.By;
+    CUDA_TRY(ctx, cudaMemcpy2DAsync(dst, 2 * size_t(g.ac_stride), planes[c],
+                                    2 * stride, 2 * size_t(g.ac_stride), g.By,
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  ctx->have_ac = true;
+  return PIKGPU_OK;
+}
+
+int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
+                       size_t linear_stride, uint8_t* out_srgb8,
+                       size_t srgb8_stride, int outputs_on_device) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->have_frame || !ctx->have_ac) {
+    return Fail(ctx, PIKGPU_ERR_STATE, "frame or AC not supplied");
+  }
+  const Geo& g = ctx->g;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (out_linear) {
+    for (int c = 0; c < 3; ++c) {
+      if (!out_linear[c]) {
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "NULL output plane");
+      }
+    }
+    if (linear_stride < size_t(g.W)) {
+      return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "linear stride too small");
+    }
+  }
+  if (out_srgb8 && srgb8_stride < 3 * size_t(g.W)) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "sRGB-8 stride too small");
+  }
+  float* lin = nullptr;
+  size_t lin_stride = size_t(g.W);
+  uint8_t* rgb8 = nullptr;
+  size_t rgb8_stride = 3 * size_t(g.W);
+  int rc;
+  // The kernel writes three planes at lin + c * lin_stride * H; device
+  // outputs must be laid out that way (checked below), host outputs go
+  // through a dense device buffer.
+  if (out_linear) {
+    if (outputs_on_device) {
+      const size_t plane = linear_stride * g.H;
+      if (out_linear[1] != out_linear[0] + plane ||
+          out_linear[2] != out_linear[0] + 2 * plane) {
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                    "device output planes must be consecutive (plane = "
+                    "stride * ysize)");
+      }
+      lin = out_linear[0];
+      lin_stride = linear_stride;
+    } else {
+      if ((rc = Ensure(ctx, &ctx->out_lin, 4 * 3 * size_t(g.W) * g.H))) {
+        return rc;
+      }
+      lin = P<float>(ctx->out_lin);
+    }
+  }
+  if (out_srgb8) {
+    if (outputs_on_device) {
+      rgb8 = out_srgb8;
+      rgb8_stride = srgb8_stride;
+    } else {
+      if ((rc = Ensure(ctx, &ctx->out_rgb8, 3 * size_t(g.W) * g.H))) return rc;
+      rgb8 = P<uint8_t>(ctx->out_rgb8);
+    }
+  }
+  rc = LaunchAll(ctx, lin, lin_stride, rgb8, rgb8_stride);
+  if (rc != PIKGPU_OK) return rc;
+  if (!outputs_on_device) {
+    if (out_linear) {
+      for (int c = 0; c < 3; ++c) {
+        CUDA_TRY(ctx, cudaMemcpy2DAsync(
+                          out_linear[c], 4 * linear_stride,
+                          lin + size_t(c) * g.W * g.H, 4 * size_t(g.W),
+                          4 * size_t(g.W), g.H, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+      }
+    }
+    if (out_srgb8) {
+      CUDA_TRY(ctx, cudaMemcpy2DAsync(out_srgb8, srgb8_stride, rgb8,
+                                      3 * size_t(g.W), 3 * size_t(g.W), g.H,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->profile) {
+    for (int i = 0; i < kNumTimed; ++i) {
+      cudaEventElapsedTime(&ctx->times[i], ctx->ev[i], ctx->ev[i + 1]);
+    }
+  }
+  ctx->have_result = true;
+  return PIKGPU_OK;
+}
+
+int pikgpu_get_stage(pikgpu_ctx* ctx, int stage, float* const planes[3],
+                     size_t stride, size_t xsize, size_t ysize) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->have_result) return Fail(ctx, PIKGPU_ERR_STATE, "no result");
+  const Geo& g = ctx->g;
+  const float* src = nullptr;
+  size_t w = 0, h = 0;
+  switch (stage) {
+    case PIKGPU_STAGE_DC:
+      src = P<float>(ctx->dc), w = g.Bx, h = g.By;
+      break;
+    case PIKGPU_STAGE_IDCT:
+      src = P<float>(ctx->idct), w = g.PW, h = g.PH;
+      break;
+    case PIKGPU_STAGE_SMOOTHED:
+      src = P<float>(ctx->smoothed), w = g.PW, h = g.PH;
+      break;
+    case PIKGPU_STAGE_EPF:
+      src = P<float>(ctx->dbg_epf), w = g.PW, h = g.PH;
+      break;
+    case PIKGPU_STAGE_AR:
+      src = P<float>(ctx->filt), w = g.PW, h = g.PH;
+      break;
+    case PIKGPU_STAGE_PRE_OPSIN:
+      src = P<float>(ctx->dbg_pre), w = g.W, h = g.H;
+      break;
+    case PIKGPU_STAGE_DEQUANT_AC:
+      src = P<float>(ctx->dbg_dequant), w = g.ac_stride, h = g.By;
+      break;
+    default:
+      return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "stage %d", stage);
+  }
+  const bool debug_stage = stage == PIKGPU_STAGE_EPF ||
+                           stage == PIKGPU_STAGE_PRE_OPSIN ||
+                           stage == PIKGPU_STAGE_DEQUANT_AC;
+  if (debug_stage && !ctx->keep_stages) {
+    return Fail(ctx, PIKGPU_ERR_STATE,
+                "stage %d needs PIKGPU_OPT_KEEP_STAGES before frame_begin",
+                stage);
+  }
+  if (!planes || xsize != w || ysize != h || stride < w) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                "stage %d is %zux%zu (got %zux%zu, stride %zu)", stage, w, h,
+                xsize, ysize, stride);
+  }
+  for (int c = 0; c < 3; ++c) {
+    CUDA_TRY(ctx, cudaMemcpy2D(planes[c], 4 * stride, src + c * w * h, 4 * w,
+                               4 * w, h, cudaMemcpyDeviceToHost));
+  }
+  return PIKGPU_OK;
+}
+
+int pikgpu_set_epf_decisions(pikgpu_ctx* ctx, const uint8_t* guide,
+                             const int32_t* sigma) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
+  const Geo& g = ctx->g;
+  int rc;
+  ctx->use_guide_ovr = guide != nullptr;
+  ctx->use_sigma_ovr = sigma != nullptr;
+  if (guide) {
+    const size_t n = 3 * size_t(g.PW + 12) * (g.PH + 12);
+    if ((rc = Ensure(ctx, &ctx->guide_ovr, n))) return rc;
+    CUDA_TRY(ctx, cudaMemcpy(ctx->guide_ovr.p, guide, n,
+                             cudaMemcpyHostToDevice));
+  }
+  if (sigma) {
+    const size_t n = 4 * size_t(g.Bx) * g.By;
+    if ((rc = Ensure(ctx, &ctx->sigma_ovr, n))) return rc;
+    CUDA_TRY(ctx, cudaMemcpy(ctx->sigma_ovr.p, sigma, n,
+                             cudaMemcpyHostToDevice));
+  }
+  return PIKGPU_OK;
+}
+
+int pikgpu_get_epf_decisions(pikgpu_ctx* ctx, uint8_t* guide,
+                             int32_t* sigma) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->have_result || !ctx->s.have_ar) {
+    return Fail(ctx, PIKGPU_ERR_STATE, "no EPF result");
+  }
+  const Geo& g = ctx->g;
+  if (sigma) {
+    CUDA_TRY(ctx, cudaMemcpy(sigma, ctx->sigma.p, 4 * size_t(g.Bx) * g.By,
+                             cudaMemcpyDeviceToHost));
+  }
+  if (guide) {
+    const size_t n = 3 * size_t(g.PW + 12) * (g.PH + 12);
+    DevBuf tmp;
+    int rc = Ensure(ctx, &tmp, n);
+    if (rc) return rc;
+    const float* src = (ctx->s.gaborish && !ctx->s.use_sharpened)
+                           ? P<float>(ctx->smoothed)
+                           : P<float>(ctx->idct);
+    dim3 b(32, 8), gr(Blocks(g.PW + 12, 32), Blocks(g.PH + 12, 8), 3);
+    k_export_guide<<<gr, b, 0, ctx->stream>>>(src, g.PW, g.PH,
+                                              P<uint32_t>(ctx->mm),
+                                              P<uint8_t>(tmp));
+    cudaStreamSynchronize(ctx->stream);
+    const cudaError_t e =
+        cudaMemcpy(guide, tmp.p, n, cudaMemcpyDeviceToHost);
+    FreeBuf(&tmp);
+    if (e != cudaSuccess) {
+      return Fail(ctx, PIKGPU_ERR_CUDA, "guide copy: %s",
+                  cudaGetErrorString(e));
+    }
+  }
+  return PIKGPU_OK;
+}
+
+int pikgpu_last_kernel_times(pikgpu_ctx* ctx, float* ms, int n) {
+  if (!ctx || !ms) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->profile) return Fail(ctx, PIKGPU_ERR_STATE, "profiling is off");
+  for (int i = 0; i < n && i < kNumTimed; ++i) ms[i] = ctx->times[i];
+  return kNumTimed;
+}
+
+const char* pikgpu_kernel_name(int index) {
+  return index >= 0 && index < kNumTimed ? kTimedNames[index] : "";
+}
+
+}  // extern "C"

@@ -1,0 +1,1451 @@
+// Included by pikgpu.cu (single translation unit, so the __constant__
+// tables need no relocatable device code).
+//
+// Reconstruction kernels: DC, dequantisation, LF/HF prediction, the
+// variable-size inverse transforms, gaborish, EPF, the DCT-domain clamp and
+// XYB -> linear RGB / sRGB-8. Each kernel names the reference function it
+// implements (paths relative to the google/pik checkout).
+
+#include "kernels.cuh"
+
+
+namespace pikgpu {
+
+__constant__ DevTables c_t;
+
+namespace {
+
+__device__ __forceinline__ const float* IdctMat(int n) {
+  return c_t.idct + MatOffset(n);
+}
+__device__ __forceinline__ const float* DctMat(int n) {
+  return c_t.dct + MatOffset(n);
+}
+
+// ---------------------------------------------------------------------------
+// Single-thread transforms used by the small LF kernels (n <= 8).
+
+// tsIDCT (pik/dct.h:441-507): out = A C^T A^T (C row = horizontal freq).
+__device__ void TsIdct1(int n, const float* in, int is, float* out, int os) {
+  const float* a = IdctMat(n);
+  float tmp[64];
+  for (int k = 0; k < n; ++k) {
+    for (int v = 0; v < n; ++v) {
+      float s = 0.f;
+      for (int l = 0; l < n; ++l) s += in[k * is + l] * a[v * n + l];
+      tmp[k * n + v] = s;
+    }
+  }
+  for (int v = 0; v < n; ++v) {
+    for (int u = 0; u < n; ++u) {
+      float s = 0.f;
+      for (int k = 0; k < n; ++k) s += a[u * n + k] * tmp[k * n + v];
+      out[v * os + u] = s;
+    }
+  }
+}
+
+// tsDCT with ScaleToBlock (pik/dct.h:362-428, pik/block.h:103-132).
+__device__ void TsDct1(int n, const float* in, int is, float* out, int os) {
+  const float* b = DctMat(n);
+  float tmp[64];
+  for (int k = 0; k < n; ++k) {
+    for (int y = 0; y < n; ++y) {
+      float s = 0.f;
+      for (int x = 0; x < n; ++x) s += b[k * n + x] * in[y * is + x];
+      tmp[k * n + y] = s;
+    }
+  }
+  const float scale = 1.0f / float(n * n);
+  for (int k = 0; k < n; ++k) {
+    for (int l = 0; l < n; ++l) {
+      float s = 0.f;
+      for (int y = 0; y < n; ++y) s += tmp[k * n + y] * b[l * n + y];
+      out[k * os + l] = s * scale;
+    }
+  }
+}
+
+// ReinterpretingDCT / ReinterpretingIDCT (pik/ac_strategy.cc:270-311).
+__device__ void ReinterpDct(int dctn, int n, const float* in, int is,
+                            float* out, int os) {
+  float block[64], res[64];
+  for (int y = 0; y < n; ++y) {
+    for (int x = 0; x < n; ++x) block[y * n + x] = in[y * is + x];
+  }
+  TsDct1(n, block, n, res, n);
+  const int sn = SizeIndex(n), sd = SizeIndex(dctn);
+  for (int y = 0; y < n; ++y) {
+    for (int x = 0; x < n; ++x) {
+      out[y * os + x] = res[y * n + x] * c_t.total_scale[sn][y][x] *
+                        c_t.inv_total_scale[sd][y][x];
+    }
+  }
+}
+__device__ void ReinterpIdct(int dctn, int lf, int n, const float* in, int is,
+                             float* out, int os) {
+  float block[64];
+  for (int i = 0; i < n * n; ++i) block[i] = 0.f;
+  const int sn = SizeIndex(n), sd = SizeIndex(dctn);
+  for (int y = 0; y < lf; ++y) {
+    for (int x = 0; x < lf; ++x) {
+      block[y * n + x] = in[y * is + x] * c_t.inv_total_scale[sn][y][x] *
+                         c_t.total_scale[sd][y][x];
+    }
+  }
+  TsIdct1(n, block, n, out, os);
+}
+
+// AcStrategy LLF/LF helpers (pik/ac_strategy.cc:850-1056).
+__device__ void LowestFreqFromDC(int type, const float* dc, int ds, float* llf,
+                                 int ls) {
+  if (type == kDCT16X16) {
+    float t[4];
+    ReinterpDct(16, 2, dc, ds, t, 2);
+    for (int y = 0; y < 2; ++y)
+      for (int x = 0; x < 2; ++x) llf[y * ls + x] = t[y * 2 + x];
+  } else if (type == kDCT32X32) {
+    float t[16];
+    ReinterpDct(32, 4, dc, ds, t, 4);
+    for (int y = 0; y < 4; ++y)
+      for (int x = 0; x < 4; ++x) llf[y * ls + x] = t[y * 4 + x];
+  } else {
+    llf[0] = dc[0];
+  }
+}
+
+__device__ void DC2x2FromLowestFreq(int type, const float* llf, int ls,
+                                    float* d, int dstr) {
+  if (type == kDCT || type == kDCT_NOHF || type == kLINES) {
+    ReinterpIdct(8, 1, 2, llf, 0, d, dstr);
+  } else if (type == kDCT16X16) {
+    float dest[16];
+    for (int i = 0; i < 16; ++i) dest[i] = 0.f;
+    dest[0] = llf[0];
+    dest[1] = llf[1];
+    dest[4] = llf[ls];
+    dest[5] = llf[ls + 1];
+    ReinterpIdct(16, 2, 4, dest, 4, d, dstr);
+  } else if (type == kDCT32X32) {
+    float dest[64];
+    for (int i = 0; i < 64; ++i) dest[i] = 0.f;
+    for (int iy = 0; iy < 4; ++iy)
+      for (int ix = 0; ix < 4; ++ix) dest[iy * 8 + ix] = llf[iy * ls + ix];
+    ReinterpIdct(32, 4, 8, dest, 8, d, dstr);
+  } else {
+    d[0] = llf[0];
+    d[1] = llf[0];
+    d[dstr] = llf[0];
+    d[dstr + 1] = llf[0];
+  }
+}
+
+// `blk(i)` reads element i of the block's coefficient matrix.
+template <class Blk>
+__device__ void DC2x2FromLowFreq(int type, const Blk& blk, float* d,
+                                 int dstr) {
+  if (type == kDCT || type == kDCT_NOHF || type == kLINES) {
+    float in[4] = {blk(0), blk(1), blk(8), blk(9)};
+    ReinterpIdct(8, 2, 2, in, 2, d, dstr);
+  } else if (type == kDCT16X16) {
+    float dest[16];
+    for (int y = 0; y < 4; ++y)
+      for (int x = 0; x < 4; ++x) dest[4 * y + x] = blk(16 * y + x);
+    ReinterpIdct(16, 4, 4, dest, 4, d, dstr);
+  } else if (type == kDCT32X32) {
+    float dest[64];
+    for (int y = 0; y < 8; ++y)
+      for (int x = 0; x < 8; ++x) dest[8 * y + x] = blk(32 * y + x);
+    ReinterpIdct(32, 8, 8, dest, 8, d, dstr);
+  } else {
+    const float b00 = blk(0), b01 = blk(1), b10 = blk(8), b11 = blk(9);
+    d[0] = b00 + b01 + b10 + b11;
+    d[1] = b00 + b01 - b10 - b11;
+    d[dstr] = b00 - b01 + b10 - b11;
+    d[dstr + 1] = b00 - b01 - b10 + b11;
+  }
+}
+
+__device__ void LowFreqFromDC2x2(int type, float* d, int dstr) {
+  if (type == kDCT || type == kDCT_NOHF || type == kLINES) {
+    float out[4];
+    ReinterpDct(8, 2, d, dstr, out, 2);
+    d[0] = out[0];
+    d[1] = out[1];
+    d[dstr] = out[2];
+    d[dstr + 1] = out[3];
+  } else if (type == kDCT16X16) {
+    float out[16];
+    ReinterpDct(16, 4, d, dstr, out, 4);
+    for (int y = 0; y < 4; ++y)
+      for (int x = 0; x < 4; ++x) d[dstr * y + x] = out[y * 4 + x];
+  } else if (type == kDCT32X32) {
+    float out[64];
+    ReinterpDct(32, 8, d, dstr, out, 8);
+    for (int y = 0; y < 8; ++y)
+      for (int x = 0; x < 8; ++x) d[dstr * y + x] = out[y * 8 + x];
+  } else {
+    const float b00 = d[0], b01 = d[1], b10 = d[dstr], b11 = d[dstr + 1];
+    d[0] = (b00 + b01 + b10 + b11) * 0.25f;
+    d[1] = (b00 + b01 - b10 - b11) * 0.25f;
+    d[dstr] = (b00 - b01 + b10 - b11) * 0.25f;
+    d[dstr + 1] = (b00 - b01 - b10 + b11) * 0.25f;
+  }
+}
+
+__device__ __forceinline__ void GroupDims(const Geo& g, int gi, int* x0,
+                                          int* y0, int* gxs, int* gys) {
+  const int gx = gi % g.Gx, gy = gi / g.Gx;
+  *x0 = gx * 64;
+  *y0 = gy * 64;
+  *gxs = min(64, g.Bx - *x0);
+  *gys = min(64, g.By - *y0);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// DC: DequantDC (pik/compressed_dc.cc:181-231).
+__global__ void k_dequant_dc(Geo g, DevFrame f, FrameScalars s) {
+  const int n = g.Bx * g.By;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float y = float(f.qdc[n + i]) * s.mul_dc[1];
+  f.dc[n + i] = y;
+  f.dc[i] = s.ytox_dc * y + float(f.qdc[i]) * s.mul_dc[0];
+  f.dc[2 * n + i] = s.ytob_dc * y + float(f.qdc[2 * n + i]) * s.mul_dc[2];
+}
+
+// PadImageToMultiple(dc, 8) (pik/image.cc:45-77): replicate the last
+// column/row. out: 3 x ph x pw.
+__global__ void k_pad_replicate(const float* in, int w, int h, float* out,
+                                int pw, int ph) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = blockIdx.z;
+  if (x >= pw || y >= ph) return;
+  out[(size_t(c) * ph + y) * pw + x] =
+      in[(size_t(c) * h + min(y, h - 1)) * w + min(x, w - 1)];
+}
+
+// AdaptiveDCReconstruction's final clamp (pik/adaptive_reconstruction.cc:
+// 319-331): dc = max(dc - step, min(denoised, dc + step)).
+__global__ void k_dc_clamp(float* dc, const float* den, int w, int h, int pw,
+                           int ph, float hs0, float hs1, float hs2) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = blockIdx.z;
+  if (x >= w || y >= h) return;
+  const float hs = c == 0 ? hs0 : c == 1 ? hs1 : hs2;
+  float& v = dc[(size_t(c) * h + y) * w + x];
+  const float d = den[(size_t(c) * ph + y) * pw + x];
+  const float lo = v - hs, hi = v + hs;
+  const float m = d < hi ? d : hi;
+  v = lo < m ? m : lo;
+}
+
+// ---------------------------------------------------------------------------
+// Min/max of 3 planes (MinMax, pik/epf_target.cc:980-1006): ordered-integer
+// atomics. mm[0..2] = min, mm[3..5] = max (encoded).
+__device__ __forceinline__ uint32_t OrderedBits(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__host__ __device__ inline float FromOrderedBits(uint32_t u) {
+  const uint32_t b = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(b);
+#else
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+#endif
+}
+
+__global__ void k_minmax_init(uint32_t* mm) {
+  if (threadIdx.x < 3) mm[threadIdx.x] = 0xFFFFFFFFu;
+  else if (threadIdx.x < 6) mm[threadIdx.x] = 0u;
+}
+
+__global__ void k_minmax(const float* planes, size_t n, uint32_t* mm) {
+  const int c = blockIdx.y;
+  const float* p = planes + size_t(c) * n;
+  uint32_t lo = 0xFFFFFFFFu, hi = 0u;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t o = OrderedBits(p[i]);
+    lo = min(lo, o);
+    hi = max(hi, o);
+  }
+  for (int off = 16; off; off >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, off));
+    hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&mm[c], lo);
+    atomicMax(&mm[3 + c], hi);
+  }
+}
+
+// Stretch and guide multiplier from the min/max (AdaptiveFilter and
+// MakeGuide, pik/epf_target.cc:1040-1047, 1140-1151).
+__device__ __forceinline__ void GuideParams(const uint32_t* mm, float* all_min,
+                                            float* mul, float* stretch) {
+  const float mn0 = FromOrderedBits(mm[0]), mn1 = FromOrderedBits(mm[1]),
+              mn2 = FromOrderedBits(mm[2]);
+  const float mx0 = FromOrderedBits(mm[3]), mx1 = FromOrderedBits(mm[4]),
+              mx2 = FromOrderedBits(mm[5]);
+  const float amax = fmaxf(fmaxf(mx0, mx1), mx2);
+  const float amin = fminf(fminf(mn0, mn1), mn2);
+  const float range = amax - amin;
+  *all_min = amin;
+  *mul = range == 0.0f ? 1.0f : 255.0f / range;
+  *stretch = amin == amax ? 1.0f : 255.0f / range;
+}
+
+// SigmaFromQuant (pik/epf_target.cc:1072-1111) per 8x8 block.
+// If qf == nullptr, every block uses `const_qf` with a DCT strategy and LUT 0
+// (AdaptiveDCReconstruction, pik/adaptive_reconstruction.cc:300-318).
+__global__ void k_epf_sigma(int nb, const int32_t* qf, const uint8_t* acs,
+                            const uint8_t* lut, int const_qf,
+                            const uint32_t* mm, int32_t* sigma) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  float amin, mul, stretch;
+  GuideParams(mm, &amin, &mul, &stretch);
+  const float ac_q = float(qf ? qf[i] : const_qf);
+  const float scale = qf ? ARQuantScaleOf(acs[i] >> 4) : 1.0f;
+  const int lut_id = qf ? lut[i] : 0;
+  const float quant = ac_q * scale * 0.039324273f;
+  float unscaled;
+  const float* l = c_t.sigma_lut[lut_id];
+  if (quant <= 0.022156f) {
+    unscaled = l[0];
+  } else if (quant >= 0.531738f) {
+    unscaled = l[15];
+  } else {
+    const float pos = (quant - 0.022156f) * 29.435892f;
+    const int trunc = int(pos);
+    const float frac = pos - float(trunc);
+    unscaled = frac * l[trunc + 1] + (1.0f - frac) * l[trunc];
+  }
+  const int s = int(unscaled * stretch + 0.5182760822018414f);
+  sigma[i] = min(s, kMaxSigma);
+}
+
+// EPF filter (AdaptiveFilter + WeightedSum, pik/epf_target.cc:526-801,
+// 1113-1278): 16x16 output pixels per CTA, one per thread.
+constexpr int kEpfTile = 16;
+constexpr int kGuideW = kEpfTile + 10;  // x - 4 .. x + 6
+constexpr int kGuideH = kEpfTile + 8;   // y - 4 .. y + 4
+constexpr int kInW = kEpfTile + 7;      // x - 3 .. x + 4
+constexpr int kInH = kEpfTile + 6;      // y - 3 .. y + 3
+
+__device__ __forceinline__ float WeightFast(int mul, int sad) {
+  const int clamped = min(sad, 507);
+  const int prescaled = int(int16_t(clamped << 6));
+  const int unbiased = (prescaled * mul) >> 16;
+  const int biased = int(int16_t(unbiased + (127 << 7)));
+  return __uint_as_float(uint32_t(uint16_t(biased)) << 16);
+}
+
+__global__ void __launch_bounds__(256)
+    k_epf(const float* in, const float* guide_src, const uint8_t* guide_ovr,
+          int w, int h, const uint32_t* mm, const int32_t* sigma,
+          float* out) {
+  __shared__ uint8_t sg[3][kGuideH][kGuideW];
+  __shared__ float si[3][kInH][kInW];
+  const int x0 = blockIdx.x * kEpfTile, y0 = blockIdx.y * kEpfTile;
+  const int tid = threadIdx.x;
+  float amin, mul, stretch;
+  GuideParams(mm, &amin, &mul, &stretch);
+  const size_t plane = size_t(w) * h;
+  const int gw = w + 12;
+  for (int i = tid; i < 3 * kGuideH * kGuideW; i += 256) {
+    const int c = i / (kGuideH * kGuideW);
+    const int r = (i / kGuideW) % kGuideH, col = i % kGuideW;
+    const int gx = x0 - 4 + col, gy = y0 - 4 + r;
+    uint8_t v;
+    if (guide_ovr) {
+      // Positions beyond the 6-pixel border are never used by valid pixels.
+      const bool inside = gx >= -6 && gx < w + 6 && gy >= -6 && gy < h + 6;
+      v = inside ? guide_ovr[(size_t(c) * (h + 12) + gy + 6) * gw + gx + 6]
+                 : uint8_t(0);
+    } else {
+      const float s = guide_src[c * plane + size_t(MirrorIdx(gy, h)) * w +
+                                MirrorIdx(gx, w)];
+      const float scaled = (s - amin) * mul;
+      v = uint8_t(uint32_t(__float2int_rz(scaled)));
+    }
+    sg[c][r][col] = v;
+  }
+  for (int i = tid; i < 3 * kInH * kInW; i += 256) {
+    const int c = i / (kInH * kInW);
+    const int r = (i / kInW) % kInH, col = i % kInW;
+    const int gx = x0 - 3 + col, gy = y0 - 3 + r;
+    si[c][r][col] =
+        in[c * plane + size_t(MirrorIdx(gy, h)) * w + MirrorIdx(gx, w)];
+  }
+  __syncthreads();
+  const int lx = tid % kEpfTile, ly = tid / kEpfTile;
+  const int x = x0 + lx, y = y0 + ly;
+  if (x >= w || y >= h) return;
+  const int bw = w / 8;
+  const int sg_ = sigma[(y / 8) * bw + x / 8];
+  if (sg_ < kMinSigma) {
+    for (int c = 0; c < 3; ++c) out[c * plane + size_t(y) * w + x] =
+        si[c][ly + 3][lx + 3];
+    return;
+  }
+  const int m = c_t.mul_table[sg_];
+  // Reference patch (3 x 4 around the pixel, top-left at (-1, -1)).
+  int ref[3][3][4];
+  for (int c = 0; c < 3; ++c)
+    for (int py = 0; py < 3; ++py)
+      for (int px = 0; px < 4; ++px)
+        ref[c][py][px] = sg[c][ly + 4 + py - 1][lx + 4 + px - 1];
+  float ws0 = 0.f, ws1 = 0.f, ws2 = 0.f, sw = 0.f;
+  for (int cy = -3; cy <= 3; ++cy) {
+    for (int cx = -3; cx <= 4; ++cx) {
+      int sad_max = 0;
+      for (int c = 0; c < 3; ++c) {
+        int sad = 0;
+#pragma unroll
+        for (int py = 0; py < 3; ++py) {
+#pragma unroll
+          for (int px = 0; px < 4; ++px) {
+            sad += abs(ref[c][py][px] -
+                       int(sg[c][ly + 4 + cy + py - 1][lx + 4 + cx + px - 1]));
+          }
+        }
+        sad_max = max(sad_max, sad);
+      }
+      float wgt = WeightFast(m, sad_max);
+      if (!(wgt >= 0.05f)) wgt = 0.0f;
+      ws0 += si[0][ly + 3 + cy][lx + 3 + cx] * wgt;
+      ws1 += si[1][ly + 3 + cy][lx + 3 + cx] * wgt;
+      ws2 += si[2][ly + 3 + cy][lx + 3 + cx] * wgt;
+      sw += wgt;
+    }
+  }
+  out[size_t(y) * w + x] = ws0 / sw;
+  out[plane + size_t(y) * w + x] = ws1 / sw;
+  out[2 * plane + size_t(y) * w + x] = ws2 / sw;
+}
+
+// Guide decision export (verification hook): u8 guide with the 6-pixel
+// mirrored border, 3 x (h + 12) x (w + 12).
+__global__ void k_export_guide(const float* src, int w, int h,
+                               const uint32_t* mm, uint8_t* guide) {
+  const int gx = blockIdx.x * blockDim.x + threadIdx.x - 6;
+  const int gy = blockIdx.y * blockDim.y + threadIdx.y - 6;
+  const int c = blockIdx.z;
+  if (gx >= w + 6 || gy >= h + 6) return;
+  float amin, mul, stretch;
+  GuideParams(mm, &amin, &mul, &stretch);
+  const float s = src[(size_t(c) * h + MirrorIdx(gy, h)) * w + MirrorIdx(gx, w)];
+  guide[(size_t(c) * (h + 12) + gy + 6) * (w + 12) + gx + 6] =
+      uint8_t(uint32_t(__float2int_rz((s - amin) * mul)));
+}
+
+// ---------------------------------------------------------------------------
+// Gaborish / symmetric 3x3 convolution with mirrored borders
+// (ConvolveT<Symmetric3>, pik/convolve.h:500-629).
+__device__ __forceinline__ float Sym3(const float* p, int w, int h, int x,
+                                      int y, float w0, float w1, float w2) {
+  const float* t = p + size_t(MirrorIdx(y - 1, h)) * w;
+  const float* m = p + size_t(y) * w;
+  const float* b = p + size_t(MirrorIdx(y + 1, h)) * w;
+  const int xl = MirrorIdx(x - 1, w), xr = MirrorIdx(x + 1, w);
+  const float sum_tb = t[x] + b[x];
+  const float mul0 = m[x] * w0;
+  const float sum_lr = m[xl] + m[xr];
+  const float x1 = sum_tb + sum_lr;
+  const float mul1 = x1 * w1 + mul0;
+  const float sum_t2 = t[xl] + t[xr];
+  const float sum_b2 = b[xl] + b[xr];
+  const float x2 = sum_t2 + sum_b2;
+  return x2 * w2 + mul1;
+}
+
+// ConvolveGaborish (pik/gaborish.cc:137-159) plus min/max of the result.
+__global__ void k_gaborish_minmax(const float* in, int w, int h, int strength,
+                                  float* out, uint32_t* mm) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = blockIdx.z;
+  const size_t plane = size_t(w) * h;
+  uint32_t o = 0;
+  bool valid = x < w && y < h;
+  if (valid) {
+    const float* wt = c_t.gaborish[strength];
+    const float v = Sym3(in + c * plane, w, h, x, y, wt[0], wt[1], wt[2]);
+    out[c * plane + size_t(y) * w + x] = v;
+    o = OrderedBits(v);
+  }
+  uint32_t lo = valid ? o : 0xFFFFFFFFu, hi = valid ? o : 0u;
+  for (int off = 16; off; off >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, off));
+    hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, off));
+  }
+  if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == 0 && mm) {
+    atomicMin(&mm[c], lo);
+    atomicMax(&mm[3 + c], hi);
+  }
+}
+
+// Final stage: gaborish #2 (or copy), ShrinkTo(xsize, ysize), XybToRgb
+// (pik/opsin_inverse.cc:38-123), optional sRGB-8 (TF_SRGB +
+// ExternalImage::CopyTo rounding). Also writes the pre-opsin planes for the
+// stage export when `pre` != nullptr.
+__device__ __forceinline__ uint8_t Srgb8(float lin255) {
+  const float x = lin255 * (1.0f / 255);
+  const float a = fabsf(x);
+  float mag;
+  if (a > 0.0031308f) {
+    const float s = sqrtf(a);
+    float yp = c_t.srgb_p[4], yq = c_t.srgb_q[4];
+    for (int i = 3; i >= 0; --i) {
+      yp = yp * s + c_t.srgb_p[i];
+      yq = yq * s + c_t.srgb_q[i];
+    }
+    mag = yp / yq;
+  } else {
+    mag = a * 12.92f;
+  }
+  const float e = copysignf(mag, x);
+  const float cl = fminf(fmaxf(0.0f, e), 1.0f);
+  const float sample = cl * 255.0f + 0.0f;
+  return uint8_t(int(sample + 0.5f));
+}
+
+__global__ void k_final(const float* in, int pw, int ph, int w, int h,
+                        int strength, float* pre, float* lin, size_t lin_stride,
+                        uint8_t* rgb8, size_t rgb8_stride) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const size_t plane = size_t(pw) * ph;
+  float v[3];
+  for (int c = 0; c < 3; ++c) {
+    if (strength) {
+      const float* wt = c_t.gaborish[strength];
+      v[c] = Sym3(in + c * plane, pw, ph, x, y, wt[0], wt[1], wt[2]);
+    } else {
+      v[c] = in[c * plane + size_t(y) * pw + x];
+    }
+    if (pre) pre[(size_t(c) * h + y) * w + x] = v[c];
+  }
+  const float* m = c_t.opsin_inv;
+  const float gr = 1.0f * (v[1] + v[0]);
+  const float gg = 1.0f * (v[1] - v[0]);
+  const float gb = v[2];
+  const float mr = gr * gr * gr + c_t.opsin_neg_bias[0];
+  const float mg = gg * gg * gg + c_t.opsin_neg_bias[1];
+  const float mb = gb * gb * gb + c_t.opsin_neg_bias[2];
+  float lr = m[0] * mr, lg = m[3] * mr, lb = m[6] * mr;
+  const float tr = m[1] * mg, tg = m[4] * mg, tb = m[7] * mg;
+  lr = m[2] * mb + lr;
+  lg = m[5] * mb + lg;
+  lb = m[8] * mb + lb;
+  const float r = lr + tr, g = lg + tg, b = lb + tb;
+  if (lin) {
+    lin[0 * lin_stride * h + size_t(y) * lin_stride + x] = r;
+    lin[1 * lin_stride * h + size_t(y) * lin_stride + x] = g;
+    lin[2 * lin_stride * h + size_t(y) * lin_stride + x] = b;
+  }
+  if (rgb8) {
+    uint8_t* o = rgb8 + size_t(y) * rgb8_stride + 3 * size_t(x);
+    o[0] = Srgb8(r);
+    o[1] = Srgb8(g);
+    o[2] = Srgb8(b);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// AC dequantisation + chroma from luma (Dequant<true>::DoAC,
+// pik/compressed_image.cc:586-707), one thread per (block, coefficient).
+__global__ void k_dequant_ac(Geo g, DevFrame f, FrameScalars s) {
+  const int k = threadIdx.x;  // 0..63
+  const int bx = blockIdx.x * (blockDim.y) + threadIdx.y;
+  const int by = blockIdx.y;
+  if (bx >= g.Bx) return;
+  const int cell = by * g.Bx + bx;
+  const int qf = f.qf[cell];
+  const float scaled = qf == 0 ? 1E10f : s.inv_global_scale / float(qf);
+  const int tx = bx >> 3, ty = by >> 3;
+  const int cf = f.dq_cf[ty * g.Tx + tx];
+  const int table = f.dq_map[cf * 256 + (qf - 1)];
+  const int a = f.acs[cell];
+  const int kind = QuantKindOf(a >> 4);
+  const int blk = a & 0xF;
+  const float x_cc = 1.0f * float(f.ytox[ty * g.Tx + tx] - 128) * (1.0f / 256);
+  const float b_cc = 1.0f * float(f.ytob[ty * g.Tx + tx]) * (1.0f / 128);
+  const size_t pos = size_t(by) * g.ac_stride + size_t(bx) * 64 + k;
+  const size_t plane = size_t(g.ac_stride) * g.By;
+  float dq[3];
+  for (int c = 0; c < 3; ++c) {
+    const float m = f.table[f.offsets[(table * 7 + kind) * 3 + c] + blk * 64 +
+                            k];
+    const float mulc = m * scaled;
+    const float q = float(f.qac[c * plane + pos]);
+    const float qa = fabsf(q);
+    float adj;
+    if (qa >= 1.5f) {
+      adj = q - 0.145f / q;
+    } else if (qa >= 0.5f) {
+      adj = copysignf(1.0f - c_t.one_bias[c], q);
+    } else {
+      adj = q;
+    }
+    dq[c] = adj * mulc;
+  }
+  f.ac[plane + pos] = dq[1];
+  f.ac[pos] = x_cc * dq[1] + dq[0];
+  f.ac[2 * plane + pos] = b_cc * dq[1] + dq[2];
+}
+
+// ---------------------------------------------------------------------------
+// Per-group LF prediction (ComputeLlf, PredictLf, pik/ac_predictions.cc:
+// 380-470), one thread per bordered cell. Group-local cell (bx, by) in
+// [0, gxs+2) x [0, gys+2); border ring acts as DCT8; DC from the frame with
+// mirroring (InitializeDecCache, pik/compressed_dc.cc:530-556).
+__global__ void k_llf(Geo g, DevFrame f) {
+  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
+  int x0, y0, gxs, gys;
+  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int by = blockIdx.y * blockDim.y + threadIdx.y;
+  if (bx >= gxs + 2 || by >= gys + 2) return;
+  const bool border = bx == 0 || by == 0 || bx == gxs + 1 || by == gys + 1;
+  const int a = border ? 0 : f.acs[(y0 + by - 1) * g.Bx + x0 + bx - 1];
+  if (a & 0xF) return;
+  const int type = a >> 4, cov = Covered(type);
+  float dc[16];
+  for (int iy = 0; iy < cov; ++iy)
+    for (int ix = 0; ix < cov; ++ix)
+      dc[iy * 4 + ix] =
+          f.dc[(size_t(c) * g.By + MirrorIdx(y0 + by - 1 + iy, g.By)) * g.Bx +
+               MirrorIdx(x0 + bx - 1 + ix, g.Bx)];
+  float* llf = f.llf_g + gi * kLlfGroupFloats + c * kGB * kGB;
+  LowestFreqFromDC(type, dc, 4, llf + by * kGB + bx, kGB);
+}
+
+__global__ void k_tmp2x2(Geo g, DevFrame f) {
+  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
+  int x0, y0, gxs, gys;
+  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int by = blockIdx.y * blockDim.y + threadIdx.y;
+  if (bx >= gxs + 2 || by >= gys + 2) return;
+  const bool border = bx == 0 || by == 0 || bx == gxs + 1 || by == gys + 1;
+  const int a = border ? 0 : f.acs[(y0 + by - 1) * g.Bx + x0 + bx - 1];
+  if (a & 0xF) return;
+  const float* llf = f.llf_g + gi * kLlfGroupFloats + c * kGB * kGB;
+  float* tmp = f.tmp2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  DC2x2FromLowestFreq(a >> 4, llf + by * kGB + bx, kGB,
+                      tmp + 2 * by * kG2 + 2 * bx, kG2);
+}
+
+// LFPredictionBlur over the group's 2x2 image (ConvolveT<Symmetric3>).
+__global__ void k_lf_blur(Geo g, DevFrame f) {
+  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
+  int x0, y0, gxs, gys;
+  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
+  const int w2 = 2 * (gxs + 2), h2 = 2 * (gys + 2);
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w2 || y >= h2) return;
+  const float* tmp = f.tmp2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  float* lf = f.lf2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  const float* t = tmp + MirrorIdx(y - 1, h2) * kG2;
+  const float* m = tmp + y * kG2;
+  const float* b = tmp + MirrorIdx(y + 1, h2) * kG2;
+  const int xl = MirrorIdx(x - 1, w2), xr = MirrorIdx(x + 1, w2);
+  const float w0 = c_t.lf_blur[0], w1 = c_t.lf_blur[1], w2_ = c_t.lf_blur[2];
+  const float sum_tb = t[x] + b[x];
+  const float mul0 = m[x] * w0;
+  const float sum_lr = m[xl] + m[xr];
+  const float x1 = sum_tb + sum_lr;
+  const float mul1 = x1 * w1 + mul0;
+  const float sum_t2 = t[xl] + t[xr];
+  const float sum_b2 = b[xl] + b[xr];
+  const float x2 = sum_t2 + sum_b2;
+  lf[y * kG2 + x] = x2 * w2_ + mul1;
+}
+
+__global__ void k_lf_from_2x2(Geo g, DevFrame f) {
+  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
+  int x0, y0, gxs, gys;
+  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int by = blockIdx.y * blockDim.y + threadIdx.y;
+  if (bx >= gxs + 2 || by >= gys + 2) return;
+  const bool border = bx == 0 || by == 0 || bx == gxs + 1 || by == gys + 1;
+  const int a = border ? 0 : f.acs[(y0 + by - 1) * g.Bx + x0 + bx - 1];
+  if (a & 0xF) return;
+  float* lf = f.lf2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  LowFreqFromDC2x2(a >> 4, lf + 2 * by * kG2 + 2 * bx, kG2);
+}
+
+// Border ring of pred2x2 (pik/compressed_image.cc:978-1039).
+__global__ void k_pred_border(Geo g, DevFrame f, int predict_lf) {
+  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
+  int x0, y0, gxs, gys;
+  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // Ring cells: 2 columns of (gys + 2) then 2 rows of (gxs + 2).
+  int x, y;
+  if (i < 2 * (gys + 2)) {
+    x = (i & 1) ? gxs + 1 : 0;
+    y = i >> 1;
+  } else if (i < 2 * (gys + 2) + 2 * (gxs + 2)) {
+    const int j = i - 2 * (gys + 2);
+    y = (j & 1) ? gys + 1 : 0;
+    x = j >> 1;
+  } else {
+    return;
+  }
+  const float* llf = f.llf_g + gi * kLlfGroupFloats + c * kGB * kGB;
+  const float* lf = f.lf2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  if (predict_lf) {
+    float blk[10];
+    blk[0] = llf[y * kGB + x];
+    blk[1] = lf[2 * y * kG2 + 2 * x + 1];
+    blk[8] = lf[(2 * y + 1) * kG2 + 2 * x];
+    blk[9] = lf[(2 * y + 1) * kG2 + 2 * x + 1];
+    DC2x2FromLowFreq(kDCT, [&](int k) { return blk[k]; },
+                     pred + 2 * y * kG2 + 2 * x, kG2);
+  } else {
+    DC2x2FromLowestFreq(kDCT, llf + y * kGB + x, kGB,
+                        pred + 2 * y * kG2 + 2 * x, kG2);
+  }
+}
+
+// UpdateLfForDecoder (pik/ac_predictions.cc:560-635) over first blocks:
+// writes the LLF into the coefficients, adds the LF prediction and forms the
+// block's pred2x2 cells.
+__global__ void k_lf_update(Geo g, DevFrame f, int predict_lf,
+                            int predict_hf) {
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int by = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = blockIdx.z;
+  if (bx >= g.Bx || by >= g.By) return;
+  const int a = f.acs[by * g.Bx + bx];
+  if (a & 0xF) return;
+  const int type = a >> 4, cov = Covered(type);
+  const int gi = (by >> 6) * g.Gx + (bx >> 6);
+  const int lbx = bx & 63, lby = by & 63;
+  const float* llf = f.llf_g + gi * kLlfGroupFloats + c * kGB * kGB;
+  const float* lf = f.lf2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  float* base = f.ac + size_t(c) * g.ac_stride * g.By +
+                size_t(by) * g.ac_stride + size_t(bx) * 64;
+  const int chunk = 64 * cov;
+  auto at = [&](int i) -> float& {
+    return base[(i / chunk) * size_t(g.ac_stride) + i % chunk];
+  };
+  for (int y = 0; y < cov; ++y)
+    for (int x = 0; x < cov; ++x)
+      at(cov * 8 * y + x) = llf[(lby + 1 + y) * kGB + lbx + 1 + x];
+  if (predict_lf) {
+    for (int y = 0; y < 2 * cov; ++y) {
+      const int start = y < cov ? cov : 0;
+      for (int x = start; x < 2 * cov; ++x) {
+        at(y * cov * 8 + x) += lf[(2 * (lby + 1) + y) * kG2 + 2 * (lbx + 1) + x];
+      }
+    }
+  }
+  if (predict_hf) {
+    DC2x2FromLowFreq(type, [&](int i) { return at(i); },
+                     pred + 2 * (lby + 1) * kG2 + 2 * (lbx + 1), kG2);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cooperative batched transforms in shared memory. `nb` blocks of n x n,
+// contiguous in smem; T threads; every thread calls __syncthreads.
+__device__ void CoopTsIdct(int n, int nb, const float* a, const float* in,
+                           float* tmp, float* out) {
+  const int nn = n * n;
+  for (int i = threadIdx.x; i < nb * nn; i += blockDim.x) {
+    const int b = i / nn, r = i % nn, k = r / n, v = r % n;
+    const float* src = in + b * nn + k * n;
+    float s = 0.f;
+    for (int l = 0; l < n; ++l) s += src[l] * a[v * n + l];
+    tmp[b * nn + k * n + v] = s;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb * nn; i += blockDim.x) {
+    const int b = i / nn, r = i % nn, v = r / n, u = r % n;
+    const float* t = tmp + b * nn;
+    float s = 0.f;
+    for (int k = 0; k < n; ++k) s += a[u * n + k] * t[k * n + v];
+    out[b * nn + v * n + u] = s;
+  }
+  __syncthreads();
+}
+
+__device__ void CoopTsDct(int n, int nb, const float* bm, const float* in,
+                          float* tmp, float* out) {
+  const int nn = n * n;
+  for (int i = threadIdx.x; i < nb * nn; i += blockDim.x) {
+    const int b = i / nn, r = i % nn, k = r / n, y = r % n;
+    const float* src = in + b * nn + y * n;
+    float s = 0.f;
+    for (int x = 0; x < n; ++x) s += bm[k * n + x] * src[x];
+    tmp[b * nn + k * n + y] = s;
+  }
+  __syncthreads();
+  const float scale = 1.0f / float(nn);
+  for (int i = threadIdx.x; i < nb * nn; i += blockDim.x) {
+    const int b = i / nn, r = i % nn, k = r / n, l = r % n;
+    const float* t = tmp + b * nn + k * n;
+    float s = 0.f;
+    for (int y = 0; y < n; ++y) s += t[y] * bm[l * n + y];
+    out[b * nn + k * n + l] = s * scale;
+  }
+  __syncthreads();
+}
+
+// Upsampled-blurred HF prediction pixel (UpSample4x4BlurDCT,
+// pik/ac_predictions.cc:263-374) at group-local pixel (X, Y).
+__device__ __forceinline__ float Upsample(const float* pred, int X, int Y) {
+  const int r = Y >> 2, q = X >> 2, ix = X & 3, iy = Y & 3;
+  float bx[3];
+  for (int j = 0; j < 3; ++j) {
+    const float* row = pred + (r + j + 1) * kG2;
+    const float v0 = row[q + 1], v1 = row[q + 2], v2 = row[q + 3];
+    bx[j] = v0 * c_t.ub4[0][ix] + v1 * c_t.ub4[1][ix] + v2 * c_t.ub4[2][ix];
+  }
+  return bx[0] * c_t.ub4[0][iy] + bx[1] * c_t.ub4[1][iy] +
+         bx[2] * c_t.ub4[2][iy];
+}
+
+// Square DCT blocks (DCT8, DCT_NOHF, DCT16, DCT32): HF prediction (if the
+// type predicts HF) + AddBlockExceptLFAndLLFTo + InverseIntegralTransform
+// (pik/compressed_image.cc:869-934). One CTA handles `nb` blocks of n x n.
+template <int N>
+__global__ void __launch_bounds__(256)
+    k_square_idct(Geo g, DevFrame f, const uint32_t* list, int count,
+                  int predict_hf) {
+  constexpr int NN = N * N;
+  constexpr int NB = NN >= 256 ? 1 : 256 / NN;
+  __shared__ float s_a[NN], s_b[NN];
+  __shared__ float s_c[NB * NN], s_t[NB * NN], s_p[NB * NN];
+  for (int i = threadIdx.x; i < NN; i += blockDim.x) {
+    s_a[i] = c_t.idct[MatOffset(N) + i];
+    s_b[i] = c_t.dct[MatOffset(N) + i];
+  }
+  const int first = blockIdx.x * NB;
+  const int nb = min(NB, count - first);
+  constexpr int cov = N / 8, chunk = 64 * cov;
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
+  const size_t plane_px = size_t(g.PW) * g.PH;
+  __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    // Load coefficients and, if predicting HF, the upsampled pixels.
+    for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
+      const int b = i / NN, e = i % NN;
+      const uint32_t pk = list[first + b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      const float* base = f.ac + c * plane_ac + size_t(by) * g.ac_stride +
+                          size_t(bx) * 64;
+      s_c[i] = base[(e / chunk) * size_t(g.ac_stride) + e % chunk];
+      if (predict_hf) {
+        const int gi = (by >> 6) * g.Gx + (bx >> 6);
+        const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+        const int X = (bx & 63) * 8 + e % N, Y = (by & 63) * 8 + e / N;
+        s_p[i] = Upsample(pred, X, Y);
+      }
+    }
+    __syncthreads();
+    if (predict_hf) {
+      CoopTsDct(N, nb, s_b, s_p, s_t, s_p);
+      for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
+        const int e = i % NN, y = e / N, x = e % N;
+        if (y < 2 * cov && x < 2 * cov) continue;
+        s_c[i] += s_p[i];
+      }
+      __syncthreads();
+    }
+    CoopTsIdct(N, nb, s_a, s_c, s_t, s_p);
+    for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
+      const int b = i / NN, e = i % NN;
+      const uint32_t pk = list[first + b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      f.idct[c * plane_px + size_t(by * 8 + e / N) * g.PW + bx * 8 + e % N] =
+          s_p[i];
+    }
+    __syncthreads();
+  }
+}
+
+// DCT4X4 (and _NOHF): four 4x4 transforms with interleaved coefficients
+// (AcStrategy::TransformFromPixels/ToPixels, pik/ac_strategy.cc:604-629,
+// 762-790). 16 blocks per CTA (64 sub-blocks of 4x4).
+__global__ void __launch_bounds__(256)
+    k_dct4_idct(Geo g, DevFrame f, const uint32_t* list, int count,
+                int predict_hf) {
+  constexpr int NB = 16;
+  __shared__ float s_a[16], s_b[16];
+  __shared__ float s_c[NB * 64], s_p[NB * 64], s_t[NB * 64], s_q[NB * 64];
+  if (threadIdx.x < 16) {
+    s_a[threadIdx.x] = c_t.idct[MatOffset(4) + threadIdx.x];
+    s_b[threadIdx.x] = c_t.dct[MatOffset(4) + threadIdx.x];
+  }
+  const int first = blockIdx.x * NB;
+  const int nb = min(NB, count - first);
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
+  const size_t plane_px = size_t(g.PW) * g.PH;
+  __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+      const int b = i / 64, e = i % 64;
+      const uint32_t pk = list[first + b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      s_c[i] = f.ac[c * plane_ac + size_t(by) * g.ac_stride + bx * 64 + e];
+      if (predict_hf && PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) {
+        // Sub-block-major pixel layout: sub-block (sy, sx), pixel (py, px).
+        const int sb = e / 16, py = (e % 16) / 4, px = e % 4;
+        const int sy = sb / 2, sx = sb % 2;
+        const int gi = (by >> 6) * g.Gx + (bx >> 6);
+        const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+        s_p[i] = Upsample(pred, (bx & 63) * 8 + sx * 4 + px,
+                          (by & 63) * 8 + sy * 4 + py);
+      } else {
+        s_p[i] = 0.f;
+      }
+    }
+    __syncthreads();
+    if (predict_hf) {
+      CoopTsDct(4, nb * 4, s_b, s_p, s_t, s_q);
+      // Scatter to interleaved coefficient positions, skipping the LF
+      // corner (positions 0, 1, 8, 9 hold the sub-block DCs).
+      for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+        const int b = i / 64, e = i % 64;
+        const int sb = e / 16, iy = (e % 16) / 4, ix = e % 4;
+        const int sy = sb / 2, sx = sb % 2;
+        const int pos = (sy + iy * 2) * 8 + sx + ix * 2;
+        if (pos == 0 || pos == 1 || pos == 8 || pos == 9) continue;
+        const uint32_t pk = list[first + b];
+        const int bx = pk & 0xFFFF, by = pk >> 16;
+        if (!PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) continue;
+        s_c[b * 64 + pos] += s_q[i];
+      }
+      __syncthreads();
+    }
+    // Gather sub-block inputs: DCs from the Hadamard of 0, 1, 8, 9.
+    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+      const int b = i / 64, e = i % 64;
+      const int sb = e / 16, iy = (e % 16) / 4, ix = e % 4;
+      const int sy = sb / 2, sx = sb % 2;
+      const float* cb = s_c + b * 64;
+      float v;
+      if (iy == 0 && ix == 0) {
+        const float b00 = cb[0], b01 = cb[1], b10 = cb[8], b11 = cb[9];
+        const float d[4] = {b00 + b01 + b10 + b11, b00 + b01 - b10 - b11,
+                            b00 - b01 + b10 - b11, b00 - b01 - b10 + b11};
+        v = d[sy * 2 + sx];
+      } else {
+        v = cb[(sy + iy * 2) * 8 + sx + ix * 2];
+      }
+      s_q[i] = v;
+    }
+    __syncthreads();
+    CoopTsIdct(4, nb * 4, s_a, s_q, s_t, s_p);
+    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+      const int b = i / 64, e = i % 64;
+      const int sb = e / 16, py = (e % 16) / 4, px = e % 4;
+      const int sy = sb / 2, sx = sb % 2;
+      const uint32_t pk = list[first + b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      f.idct[c * plane_px + size_t(by * 8 + sy * 4 + py) * g.PW + bx * 8 +
+             sx * 4 + px] = s_p[i];
+    }
+    __syncthreads();
+  }
+}
+
+// DCT2X2, IDENTITY and LINES: inverse transforms only (no HF prediction),
+// one thread per block and channel.
+__device__ void SmallInverse(int type, const float* cb, float* px, int ps) {
+  if (type == kDCT2X2) {
+    float co[64];
+    for (int i = 0; i < 64; ++i) co[i] = cb[i];
+    for (int s = 2; s <= 8; s *= 2) {  // IDCT2TopBlock<2>, <4>, <8>
+      float tmp[64];
+      const int h = s / 2;
+      for (int y = 0; y < h; ++y) {
+        for (int x = 0; x < h; ++x) {
+          const float c00 = co[y * 8 + x], c01 = co[y * 8 + h + x];
+          const float c10 = co[(y + h) * 8 + x], c11 = co[(y + h) * 8 + h + x];
+          tmp[y * 2 * 8 + x * 2] = c00 + c01 + c10 + c11;
+          tmp[y * 2 * 8 + x * 2 + 1] = c00 + c01 - c10 - c11;
+          tmp[(y * 2 + 1) * 8 + x * 2] = c00 - c01 + c10 - c11;
+          tmp[(y * 2 + 1) * 8 + x * 2 + 1] = c00 - c01 - c10 + c11;
+        }
+      }
+      for (int y = 0; y < s; ++y)
+        for (int x = 0; x < s; ++x) co[y * 8 + x] = tmp[y * 8 + x];
+    }
+    for (int y = 0; y < 8; ++y)
+      for (int x = 0; x < 8; ++x) px[y * ps + x] = co[y * 8 + x];
+  } else if (type == kIDENTITY) {
+    const float b00 = cb[0], b01 = cb[1], b10 = cb[8], b11 = cb[9];
+    const float dcs[4] = {b00 + b01 + b10 + b11, b00 + b01 - b10 - b11,
+                          b00 - b01 + b10 - b11, b00 - b01 - b10 + b11};
+    for (int y = 0; y < 2; ++y) {
+      for (int x = 0; x < 2; ++x) {
+        float residual_sum = 0.f;
+        for (int iy = 0; iy < 4; ++iy)
+          for (int ix = 0; ix < 4; ++ix)
+            if (ix != 0 || iy != 0)
+              residual_sum += cb[(y + iy * 2) * 8 + x + ix * 2];
+        const float ctr = dcs[y * 2 + x] - residual_sum * (1.0f / 16);
+        for (int iy = 0; iy < 4; ++iy)
+          for (int ix = 0; ix < 4; ++ix)
+            if (ix != 1 || iy != 1)
+              px[(y * 4 + iy) * ps + x * 4 + ix] =
+                  cb[(y + iy * 2) * 8 + x + ix * 2] + ctr;
+        px[(y * 4 + 1) * ps + x * 4 + 1] = ctr;
+        px[y * 4 * ps + x * 4] = cb[(y + 2) * 8 + x + 2] + ctr;
+      }
+    }
+  } else {  // LINES (pik/ac_strategy.cc:680-724)
+    const int8_t kP3[4][3] = {{6, 7, 15}, {5, 14, 23}, {40, 49, 58},
+                              {48, 56, 57}};
+    const int8_t kP4[4][4] = {{4, 13, 22, 31}, {3, 12, 30, 39},
+                              {24, 33, 51, 60}, {32, 41, 50, 59}};
+    const int8_t kP6[4][6] = {{2, 11, 20, 29, 38, 47},
+                              {1, 10, 19, 37, 46, 55},
+                              {8, 17, 26, 44, 53, 62},
+                              {16, 25, 34, 43, 52, 61}};
+    const int8_t kP8[8] = {0, 9, 18, 27, 36, 45, 54, 63};
+    const int8_t kC4[4][4] = {{4, 13, 22, 31}, {3, 12, 21, 30},
+                              {24, 33, 42, 51}, {32, 41, 50, 59}};
+    const int8_t kC6[4][6] = {{2, 11, 20, 29, 38, 47},
+                              {10, 19, 28, 37, 46, 55},
+                              {17, 26, 35, 44, 53, 62},
+                              {16, 25, 34, 43, 52, 61}};
+    const int8_t kC8[8] = {18, 27, 36, 45, 54, 39, 60, 63};
+    const int8_t kDc00[21] = {0,  8,  9,  16, 17, 18, 25, 26, 27, 34, 35,
+                              36, 43, 44, 45, 52, 53, 54, 61, 62, 63};
+    const int8_t kDc01[15] = {24, 32, 33, 40, 41, 42, 48, 49,
+                              50, 51, 56, 57, 58, 59, 60};
+    const int8_t kDc10[15] = {3,  4,  5,  6,  7,  12, 13, 14,
+                              15, 21, 22, 23, 30, 31, 39};
+    const int8_t kDc11[13] = {1, 2, 10, 11, 19, 20, 28, 29, 37, 38, 46, 47, 55};
+    auto cm = [](int i) { return (i & 7) * 8 + (i >> 3); };
+    float temp[64];
+    for (int i = 0; i < 64; ++i) temp[i] = 0.f;
+    auto idcts = [&](int n, const int8_t* ip, const int8_t* ic) {
+      float v[8];
+      for (int j = 0; j < n; ++j) v[j] = cb[cm(ic[j])];
+      for (int j = 0; j < n; ++j) {
+        float s = 0.f;
+        for (int k = 0; k < n; ++k) s += c_t.lines_inv[n][j][k] * v[k];
+        temp[cm(ip[j])] = s;
+      }
+    };
+    for (int i = 0; i < 4; ++i) idcts(3, kP3[i], kP3[i]);
+    for (int i = 0; i < 4; ++i) idcts(4, kP4[i], kC4[i]);
+    for (int i = 0; i < 4; ++i) idcts(6, kP6[i], kC6[i]);
+    idcts(8, kP8, kC8);
+    const float i0 = cb[0], i1 = cb[8], i2 = cb[1], i3 = cb[9];
+    const float d00 = i0 + i1 + i2 + i3, d01 = i0 - i1 + i2 - i3;
+    const float d10 = i0 + i1 - i2 - i3, d11 = i0 - i1 - i2 + i3;
+    for (int v : kDc00) temp[cm(v)] += d00;
+    for (int v : kDc01) temp[cm(v)] += d01;
+    for (int v : kDc10) temp[cm(v)] += d10;
+    for (int v : kDc11) temp[cm(v)] += d11;
+    temp[21] = (temp[12] + temp[30]) * 0.5f;
+    temp[28] = (temp[19] + temp[37]) * 0.5f;
+    temp[35] = (temp[26] + temp[44]) * 0.5f;
+    temp[42] = (temp[33] + temp[51]) * 0.5f;
+    for (int y = 0; y < 8; ++y)
+      for (int x = 0; x < 8; ++x) px[y * ps + x] = temp[y * 8 + x];
+  }
+}
+
+__global__ void k_small_idct(Geo g, DevFrame f, const uint32_t* list,
+                             int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * count) return;
+  const int b = i / 3, c = i % 3;
+  const uint32_t pk = list[b];
+  const int bx = pk & 0xFFFF, by = pk >> 16;
+  const int type = f.acs[by * g.Bx + bx] >> 4;
+  const float* cb = f.ac + c * size_t(g.ac_stride) * g.By +
+                    size_t(by) * g.ac_stride + bx * 64;
+  float* px = f.idct + c * size_t(g.PW) * g.PH + size_t(by * 8) * g.PW + bx * 8;
+  SmallInverse(type, cb, px, g.PW);
+}
+
+// ---------------------------------------------------------------------------
+// AdaptiveReconstruction's DCT-domain clamp (pik/adaptive_reconstruction.cc:
+// 72-244, 334-471): per first block, DCT of (filtered - original) per
+// channel, the clamp ratio of each coefficient to half a quantisation step
+// (LLF: to the DC step), the minimum over the three channels, then the
+// scaled correction is transformed back and added to the original.
+
+struct ArBlockInfo {
+  const float* dm[3];  // dequant matrix per channel
+  float inv_quant_ac;
+};
+
+__device__ __forceinline__ ArBlockInfo ArInfo(const Geo& g, const DevFrame& f,
+                                              const FrameScalars& s, int bx,
+                                              int by, int type) {
+  ArBlockInfo r;
+  const int qac = f.qf[by * g.Bx + bx];
+  r.inv_quant_ac = s.inv_global_scale / float(qac);
+  const int cf = f.dq_cf[(by >> 3) * g.Tx + (bx >> 3)];
+  const int table = f.dq_map[cf * 256 + (qac - 1)];
+  const int kind = QuantKindOf(type);
+  for (int c = 0; c < 3; ++c) {
+    r.dm[c] = f.table + f.offsets[(table * 7 + kind) * 3 + c];
+  }
+  return r;
+}
+
+// SymmetricClamp's ratio for one coefficient (only +0.0 counts as zero).
+__device__ __forceinline__ float ClampRatio(float corr, float interval) {
+  const float upper = 0.5f * interval;
+  const float lower = -0.5f * interval;
+  const float mx = lower < corr ? corr : lower;
+  const float clamped = mx < upper ? mx : upper;
+  const float divisor = __float_as_uint(corr) == 0u ? 1E-7f : corr;
+  return clamped / divisor;
+}
+
+__device__ __forceinline__ float LlfScale(int type, int x, int y) {
+  if (type == kDCT16X16) return c_t.ar_llf16[y][x];
+  if (type == kDCT32X32) return c_t.ar_llf32[y][x];
+  return 1.0f;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256)
+    k_square_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
+                int count) {
+  constexpr int NN = N * N;
+  constexpr int NB = NN >= 256 ? 1 : 256 / NN;
+  constexpr int cov = N / 8;
+  __shared__ float s_a[NN], s_b[NN];
+  __shared__ float s_blk[3][NB * NN];
+  __shared__ float s_r[NB * NN], s_t[NB * NN], s_p[NB * NN];
+  for (int i = threadIdx.x; i < NN; i += blockDim.x) {
+    s_a[i] = c_t.idct[MatOffset(N) + i];
+    s_b[i] = c_t.dct[MatOffset(N) + i];
+  }
+  const int first = blockIdx.x * NB;
+  const int nb = min(NB, count - first);
+  const size_t plane = size_t(g.PW) * g.PH;
+  __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
+      const int b = i / NN, e = i % NN;
+      const uint32_t pk = list[first + b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      const size_t o = c * plane + size_t(by * 8 + e / N) * g.PW + bx * 8 + e % N;
+      s_p[i] = f.filt[o] - f.idct[o];
+    }
+    __syncthreads();
+    CoopTsDct(N, nb, s_b, s_p, s_t, s_blk[c]);
+  }
+  for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
+    const int b = i / NN, e = i % NN, y = e / N, x = e % N;
+    const uint32_t pk = list[first + b];
+    const int bx = pk & 0xFFFF, by = pk >> 16;
+    const int type = f.acs[by * g.Bx + bx] >> 4;
+    const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
+    float mr = 1.0f;
+    for (int c = 0; c < 3; ++c) {
+      const float interval =
+          (y < cov && x < cov)
+              ? LlfScale(type, x, y) * s.mul_dc[c]
+              : info.dm[c][e] * info.inv_quant_ac;
+      const float r = ClampRatio(s_blk[c][i], interval);
+      mr = r < mr ? r : mr;
+    }
+    s_r[i] = mr;
+  }
+  __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
+      s_blk[c][i] = s_blk[c][i] * s_r[i];
+    }
+    __syncthreads();
+    CoopTsIdct(N, nb, s_a, s_blk[c], s_t, s_p);
+    for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
+      const int b = i / NN, e = i % NN;
+      const uint32_t pk = list[first + b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      const size_t o = c * plane + size_t(by * 8 + e / N) * g.PW + bx * 8 + e % N;
+      f.filt[o] = s_p[i] + f.idct[o];
+    }
+    __syncthreads();
+  }
+}
+
+// Clamp for DCT4X4 blocks.
+__global__ void __launch_bounds__(256)
+    k_dct4_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
+              int count) {
+  constexpr int NB = 16;
+  __shared__ float s_a[16], s_b[16];
+  __shared__ float s_blk[3][NB * 64];
+  __shared__ float s_r[NB * 64], s_t[NB * 64], s_p[NB * 64];
+  if (threadIdx.x < 16) {
+    s_a[threadIdx.x] = c_t.idct[MatOffset(4) + threadIdx.x];
+    s_b[threadIdx.x] = c_t.dct[MatOffset(4) + threadIdx.x];
+  }
+  const int first = blockIdx.x * NB;
+  const int nb = min(NB, count - first);
+  const size_t plane = size_t(g.PW) * g.PH;
+  __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    // Sub-block-major pixels.
+    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+      const int b = i / 64, e = i % 64;
+      const int sb = e / 16, py = (e % 16) / 4, px = e % 4;
+      const uint32_t pk = list[first + b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      const size_t o = c * plane + size_t(by * 8 + (sb / 2) * 4 + py) * g.PW +
+                       bx * 8 + (sb % 2) * 4 + px;
+      s_p[i] = f.filt[o] - f.idct[o];
+    }
+    __syncthreads();
+    CoopTsDct(4, nb * 4, s_b, s_p, s_t, s_r);
+    // Interleave into coefficient order, then the 2x2 DC Hadamard * 0.25.
+    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+      const int b = i / 64, e = i % 64;
+      const int sb = e / 16, iy = (e % 16) / 4, ix = e % 4;
+      const int pos = ((sb / 2) + iy * 2) * 8 + (sb % 2) + ix * 2;
+      s_blk[c][b * 64 + pos] = s_r[i];
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      float* cb = s_blk[c] + b * 64;
+      const float b00 = cb[0], b01 = cb[1], b10 = cb[8], b11 = cb[9];
+      cb[0] = (b00 + b01 + b10 + b11) * 0.25f;
+      cb[1] = (b00 + b01 - b10 - b11) * 0.25f;
+      cb[8] = (b00 - b01 + b10 - b11) * 0.25f;
+      cb[9] = (b00 - b01 - b10 + b11) * 0.25f;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+    const int b = i / 64, e = i % 64;
+    const uint32_t pk = list[first + b];
+    const int bx = pk & 0xFFFF, by = pk >> 16;
+    const int type = f.acs[by * g.Bx + bx] >> 4;
+    const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
+    float mr = 1.0f;
+    for (int c = 0; c < 3; ++c) {
+      const float interval =
+          e == 0 ? 1.0f * s.mul_dc[c] : info.dm[c][e] * info.inv_quant_ac;
+      const float r = ClampRatio(s_blk[c][i], interval);
+      mr = r < mr ? r : mr;
+    }
+    s_r[i] = mr;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+    for (int c = 0; c < 3; ++c) s_blk[c][i] = s_blk[c][i] * s_r[i];
+  }
+  __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+      const int b = i / 64, e = i % 64;
+      const int sb = e / 16, iy = (e % 16) / 4, ix = e % 4;
+      const int sy = sb / 2, sx = sb % 2;
+      const float* cb = s_blk[c] + b * 64;
+      float v;
+      if (iy == 0 && ix == 0) {
+        const float b00 = cb[0], b01 = cb[1], b10 = cb[8], b11 = cb[9];
+        const float d[4] = {b00 + b01 + b10 + b11, b00 + b01 - b10 - b11,
+                            b00 - b01 + b10 - b11, b00 - b01 - b10 + b11};
+        v = d[sy * 2 + sx];
+      } else {
+        v = cb[(sy + iy * 2) * 8 + sx + ix * 2];
+      }
+      s_t[i] = v;
+    }
+    __syncthreads();
+    CoopTsIdct(4, nb * 4, s_a, s_t, s_r, s_p);
+    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
+      const int b = i / 64, e = i % 64;
+      const int sb = e / 16, py = (e % 16) / 4, px = e % 4;
+      const uint32_t pk = list[first + b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      const size_t o = c * plane + size_t(by * 8 + (sb / 2) * 4 + py) * g.PW +
+                       bx * 8 + (sb % 2) * 4 + px;
+      f.filt[o] = s_p[i] + f.idct[o];
+    }
+    __syncthreads();
+  }
+}
+
+// Forward transforms of DCT2X2, IDENTITY and LINES (pik/ac_strategy.cc:
+// 531-603, 630-663), single thread.
+__device__ void SmallForward(int type, const float* px, int ps, float* co) {
+  if (type == kDCT2X2) {
+    float cur[64];
+    for (int y = 0; y < 8; ++y)
+      for (int x = 0; x < 8; ++x) cur[y * 8 + x] = px[y * ps + x];
+    for (int s = 8; s >= 2; s /= 2) {  // DCT2TopBlock<8>, <4>, <2>
+      float tmp[64];
+      const int h = s / 2;
+      for (int y = 0; y < h; ++y) {
+        for (int x = 0; x < h; ++x) {
+          const float c00 = cur[y * 2 * 8 + x * 2];
+          const float c01 = cur[y * 2 * 8 + x * 2 + 1];
+          const float c10 = cur[(y * 2 + 1) * 8 + x * 2];
+          const float c11 = cur[(y * 2 + 1) * 8 + x * 2 + 1];
+          tmp[y * 8 + x] = (c00 + c01 + c10 + c11) * 0.25f;
+          tmp[y * 8 + h + x] = (c00 + c01 - c10 - c11) * 0.25f;
+          tmp[(y + h) * 8 + x] = (c00 - c01 + c10 - c11) * 0.25f;
+          tmp[(y + h) * 8 + h + x] = (c00 - c01 - c10 + c11) * 0.25f;
+        }
+      }
+      for (int y = 0; y < s; ++y)
+        for (int x = 0; x < s; ++x) cur[y * 8 + x] = tmp[y * 8 + x];
+    }
+    for (int i = 0; i < 64; ++i) co[i] = cur[i];
+  } else if (type == kIDENTITY) {
+    for (int y = 0; y < 2; ++y) {
+      for (int x = 0; x < 2; ++x) {
+        float block_dc = 0.f;
+        for (int iy = 0; iy < 4; ++iy)
+          for (int ix = 0; ix < 4; ++ix)
+            block_dc += px[(y * 4 + iy) * ps + x * 4 + ix];
+        block_dc *= 1.0f / 16;
+        const float ctr = px[(y * 4 + 1) * ps + x * 4 + 1];
+        for (int iy = 0; iy < 4; ++iy)
+          for (int ix = 0; ix < 4; ++ix)
+            if (ix != 1 || iy != 1)
+              co[(y + iy * 2) * 8 + x + ix * 2] =
+                  px[(y * 4 + iy) * ps + x * 4 + ix] - ctr;
+        co[(y + 2) * 8 + x + 2] = co[y * 8 + x];
+        co[y * 8 + x] = block_dc;
+      }
+    }
+    const float b00 = co[0], b01 = co[1], b10 = co[8], b11 = co[9];
+    co[0] = (b00 + b01 + b10 + b11) * 0.25f;
+    co[1] = (b00 + b01 - b10 - b11) * 0.25f;
+    co[8] = (b00 - b01 + b10 - b11) * 0.25f;
+    co[9] = (b00 - b01 - b10 + b11) * 0.25f;
+  } else {  // LINES
+    const int8_t kP3[4][3] = {{6, 7, 15}, {5, 14, 23}, {40, 49, 58},
+                              {48, 56, 57}};
+    const int8_t kP4[4][4] = {{4, 13, 22, 31}, {3, 12, 30, 39},
+                              {24, 33, 51, 60}, {32, 41, 50, 59}};
+    const int8_t kP6[4][6] = {{2, 11, 20, 29, 38, 47},
+                              {1, 10, 19, 37, 46, 55},
+                              {8, 17, 26, 44, 53, 62},
+                              {16, 25, 34, 43, 52, 61}};
+    const int8_t kP8[8] = {0, 9, 18, 27, 36, 45, 54, 63};
+    const int8_t kC4[4][4] = {{4, 13, 22, 31}, {3, 12, 21, 30},
+                              {24, 33, 42, 51}, {32, 41, 50, 59}};
+    const int8_t kC6[4][6] = {{2, 11, 20, 29, 38, 47},
+                              {10, 19, 28, 37, 46, 55},
+                              {17, 26, 35, 44, 53, 62},
+                              {16, 25, 34, 43, 52, 61}};
+    const int8_t kC8[8] = {18, 27, 36, 45, 54, 39, 60, 63};
+    const int8_t kDc00[21] = {0,  8,  9,  16, 17, 18, 25, 26, 27, 34, 35,
+                              36, 43, 44, 45, 52, 53, 54, 61, 62, 63};
+    const int8_t kDc01[15] = {24, 32, 33, 40, 41, 42, 48, 49,
+                              50, 51, 56, 57, 58, 59, 60};
+    const int8_t kDc10[15] = {3,  4,  5,  6,  7,  12, 13, 14,
+                              15, 21, 22, 23, 30, 31, 39};
+    const int8_t kDc11[13] = {1, 2, 10, 11, 19, 20, 28, 29, 37, 38, 46, 47, 55};
+    auto cm = [](int i) { return (i & 7) * 8 + (i >> 3); };
+    float temp[64];
+    for (int y = 0; y < 8; ++y)
+      for (int x = 0; x < 8; ++x) temp[y * 8 + x] = px[y * ps + x];
+    for (int i = 0; i < 64; ++i) co[i] = 0.f;
+    auto dc_part = [&](const int8_t* idx, int num) {
+      float dc = 0.f;
+      for (int i = 0; i < num; ++i) dc += temp[cm(idx[i])];
+      dc /= float(num);
+      for (int i = 0; i < num; ++i) temp[cm(idx[i])] -= dc;
+      return dc;
+    };
+    const float d00 = dc_part(kDc00, 21), d01 = dc_part(kDc01, 15);
+    const float d10 = dc_part(kDc10, 15), d11 = dc_part(kDc11, 13);
+    co[0] = (d00 + d01 + d10 + d11) * 0.25f;
+    co[8] = (d00 - d01 + d10 - d11) * 0.25f;
+    co[1] = (d00 + d01 - d10 - d11) * 0.25f;
+    co[9] = (d00 - d01 - d10 + d11) * 0.25f;
+    auto dcts = [&](int n, const int8_t* ip, const int8_t* ic) {
+      for (int k = 0; k < n; ++k) {
+        float sum = 0.f;
+        for (int j = 0; j < n; ++j) sum += c_t.lines_fwd[n][k][j] * temp[cm(ip[j])];
+        co[cm(ic[k])] = sum;
+      }
+    };
+    for (int i = 0; i < 4; ++i) dcts(3, kP3[i], kP3[i]);
+    for (int i = 0; i < 4; ++i) dcts(4, kP4[i], kC4[i]);
+    for (int i = 0; i < 4; ++i) dcts(6, kP6[i], kC6[i]);
+    dcts(8, kP8, kC8);
+  }
+}
+
+__global__ void k_small_ar(Geo g, DevFrame f, FrameScalars s,
+                           const uint32_t* list, int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint32_t pk = list[i];
+  const int bx = pk & 0xFFFF, by = pk >> 16;
+  const int type = f.acs[by * g.Bx + bx] >> 4;
+  const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
+  const size_t plane = size_t(g.PW) * g.PH;
+  const size_t o0 = size_t(by * 8) * g.PW + bx * 8;
+  float blk[3][64];
+  float mr[64];
+  for (int k = 0; k < 64; ++k) mr[k] = 1.0f;
+  for (int c = 0; c < 3; ++c) {
+    float diff[64];
+    for (int y = 0; y < 8; ++y)
+      for (int x = 0; x < 8; ++x) {
+        const size_t o = c * plane + o0 + size_t(y) * g.PW + x;
+        diff[y * 8 + x] = f.filt[o] - f.idct[o];
+      }
+    SmallForward(type, diff, 8, blk[c]);
+    for (int k = 0; k < 64; ++k) {
+      const float interval = k == 0 ? 1.0f * s.mul_dc[c]
+                                    : info.dm[c][k] * info.inv_quant_ac;
+      const float r = ClampRatio(blk[c][k], interval);
+      mr[k] = r < mr[k] ? r : mr[k];
+    }
+  }
+  for (int c = 0; c < 3; ++c) {
+    for (int k = 0; k < 64; ++k) blk[c][k] = blk[c][k] * mr[k];
+    float px[64];
+    SmallInverse(type, blk[c], px, 8);
+    for (int y = 0; y < 8; ++y)
+      for (int x = 0; x < 8; ++x) {
+        const size_t o = c * plane + o0 + size_t(y) * g.PW + x;
+        f.filt[o] = px[y * 8 + x] + f.idct[o];
+      }
+  }
+}
+
+// Explicit instantiations.
+template __global__ void k_square_idct<8>(Geo, DevFrame, const uint32_t*, int,
+                                          int);
+template __global__ void k_square_idct<16>(Geo, DevFrame, const uint32_t*,
+                                           int, int);
+template __global__ void k_square_idct<32>(Geo, DevFrame, const uint32_t*,
+                                           int, int);
+template __global__ void k_square_ar<8>(Geo, DevFrame, FrameScalars,
+                                        const uint32_t*, int);
+template __global__ void k_square_ar<16>(Geo, DevFrame, FrameScalars,
+                                         const uint32_t*, int);
+template __global__ void k_square_ar<32>(Geo, DevFrame, FrameScalars,
+                                         const uint32_t*, int);
+
+}  // namespace pikgpu

@@ -1,0 +1,183 @@
+"""Python access to the native library (pik_b200/libpikgpu.so, the C ABI of
+include/pikgpu.h). Fails loudly when the library is missing: there is no
+fallback implementation."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import abi, layout
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                        "libpikgpu.so")
+
+OK = 0
+ERRORS = {-1: "INVALID_ARG", -2: "UNSUPPORTED", -3: "CUDA", -4: "STATE",
+          -5: "NO_MEMORY"}
+STAGES = {"dc": 0, "idct": 1, "smoothed": 2, "epf": 3, "ar": 4,
+          "pre_opsin": 5, "dequant_ac": 6}
+OPT_KEEP_STAGES = 1
+OPT_PROFILE = 2
+
+_lib = None
+
+
+class PikGpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -c 'import "
+            f"__graft_entry__ as g; g.build()'` (no fallback exists)")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    S = ctypes.c_size_t
+    L.pikgpu_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(P)]
+    L.pikgpu_ctx_destroy.argtypes = [P]
+    L.pikgpu_last_error.restype = ctypes.c_char_p
+    L.pikgpu_last_error.argtypes = [P]
+    L.pikgpu_validate.argtypes = [P, ctypes.c_char_p, S]
+    L.pikgpu_set_option.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.pikgpu_frame_begin.argtypes = [P, P]
+    L.pikgpu_frame_set_ac.argtypes = [P, ctypes.POINTER(P), S]
+    L.pikgpu_frame_set_group_ac.argtypes = [P, ctypes.c_uint32,
+                                            ctypes.POINTER(P), S]
+    L.pikgpu_frame_set_ac_device.argtypes = [P, ctypes.POINTER(P), S]
+    L.pikgpu_reconstruct.argtypes = [P, ctypes.POINTER(P), S, P, S,
+                                     ctypes.c_int]
+    L.pikgpu_get_stage.argtypes = [P, ctypes.c_int, ctypes.POINTER(P), S, S,
+                                   S]
+    L.pikgpu_set_epf_decisions.argtypes = [P, P, P]
+    L.pikgpu_get_epf_decisions.argtypes = [P, P, P]
+    L.pikgpu_last_kernel_times.argtypes = [P, P, ctypes.c_int]
+    L.pikgpu_kernel_name.restype = ctypes.c_char_p
+    L.pikgpu_kernel_name.argtypes = [ctypes.c_int]
+    L.pikgpu_set_stream.argtypes = [P, P]
+    _lib = L
+    return L
+
+
+def validate(frame: layout.Frame) -> tuple[int, str]:
+    """Host-only validation (no device needed)."""
+    packed = abi.PackedFrame(frame)
+    buf = ctypes.create_string_buffer(512)
+    rc = lib().pikgpu_validate(packed.ref, buf, 512)
+    return rc, buf.value.decode()
+
+
+def _planes(arrs) -> ctypes.Array:
+    return (ctypes.c_void_p * 3)(*[a.ctypes.data for a in arrs])
+
+
+class Context:
+    """One pikgpu context (device memory + stream)."""
+
+    def __init__(self, device: int = 0, *, keep_stages: bool = False,
+                 profile: bool = False):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        rc = self.L.pikgpu_ctx_create(device, ctypes.byref(h))
+        if rc != OK:
+            raise PikGpuError(rc, "pikgpu_ctx_create failed")
+        self.h = h
+        self._check(self.L.pikgpu_set_option(h, OPT_KEEP_STAGES,
+                                             int(keep_stages)))
+        self._check(self.L.pikgpu_set_option(h, OPT_PROFILE, int(profile)))
+        self.frame = None
+        self._packed = None
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.pikgpu_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        if rc < 0:
+            raise PikGpuError(rc, self.L.pikgpu_last_error(self.h).decode())
+
+    def begin(self, frame: layout.Frame) -> None:
+        self._packed = abi.PackedFrame(frame)
+        self.frame = frame
+        self._check(self.L.pikgpu_frame_begin(self.h, self._packed.ref))
+
+    def set_ac(self, ac: np.ndarray | None = None) -> None:
+        a = self._packed.ac if ac is None else np.ascontiguousarray(ac,
+                                                                    np.int16)
+        self._ac_keep = a
+        self._check(self.L.pikgpu_frame_set_ac(self.h, _planes(a),
+                                               a.shape[-1]))
+
+    def set_group_ac(self, group: int, planes: np.ndarray) -> None:
+        a = np.ascontiguousarray(planes, np.int16)
+        self._check(self.L.pikgpu_frame_set_group_ac(self.h, group,
+                                                     _planes(a), a.shape[-1]))
+
+    def reconstruct(self, *, linear: bool = True, srgb8: bool = False):
+        f = self.frame
+        lin = np.zeros((3, f.ysize, f.xsize), np.float32) if linear else None
+        rgb = np.zeros((f.ysize, f.xsize, 3), np.uint8) if srgb8 else None
+        self._check(self.L.pikgpu_reconstruct(
+            self.h, _planes(lin) if lin is not None else None, f.xsize,
+            rgb.ctypes.data if rgb is not None else None, 3 * f.xsize, 0))
+        return lin, rgb
+
+    def reconstruct_device(self, lin_ptr: int, lin_stride: int,
+                           rgb_ptr: int = 0, rgb_stride: int = 0) -> None:
+        """Outputs into device memory (three consecutive planes)."""
+        f = self.frame
+        planes = None
+        if lin_ptr:
+            plane = lin_stride * f.ysize * 4
+            planes = (ctypes.c_void_p * 3)(lin_ptr, lin_ptr + plane,
+                                           lin_ptr + 2 * plane)
+        self._check(self.L.pikgpu_reconstruct(self.h, planes, lin_stride,
+                                              rgb_ptr or None, rgb_stride, 1))
+
+    def stage(self, name: str) -> np.ndarray:
+        f = self.frame
+        by, bx = f.blocks
+        shape = {"dc": (by, bx), "dequant_ac": (by, bx * 64),
+                 "pre_opsin": (f.ysize, f.xsize)}.get(name, (by * 8, bx * 8))
+        out = np.zeros((3,) + shape, np.float32)
+        self._check(self.L.pikgpu_get_stage(self.h, STAGES[name],
+                                            _planes(out), shape[1], shape[1],
+                                            shape[0]))
+        return out
+
+    def set_decisions(self, guide: np.ndarray | None,
+                      sigma: np.ndarray | None) -> None:
+        g = None if guide is None else np.ascontiguousarray(guide, np.uint8)
+        s = None if sigma is None else np.ascontiguousarray(sigma, np.int32)
+        self._keep_dec = (g, s)
+        self._check(self.L.pikgpu_set_epf_decisions(
+            self.h, g.ctypes.data if g is not None else None,
+            s.ctypes.data if s is not None else None))
+
+    def decisions(self):
+        f = self.frame
+        by, bx = f.blocks
+        g = np.zeros((3, by * 8 + 12, bx * 8 + 12), np.uint8)
+        s = np.zeros((by, bx), np.int32)
+        self._check(self.L.pikgpu_get_epf_decisions(self.h, g.ctypes.data,
+                                                    s.ctypes.data))
+        return g, s
+
+    def kernel_times(self) -> dict:
+        ms = np.zeros(16, np.float32)
+        n = self.L.pikgpu_last_kernel_times(self.h, ms.ctypes.data, 16)
+        self._check(n)
+        return {self.L.pikgpu_kernel_name(i).decode(): float(ms[i])
+                for i in range(n)}

@@ -1,0 +1,158 @@
+"""Seeded synthetic workloads for the reconstruction path.
+
+Two generators:
+
+* ``make_image`` -- the test-image generator the benchmark configurations are
+  defined with: a sum of random 2-D sinusoids (period 4..64 px, random
+  orientation, phase and amplitude), random flat axis-aligned rectangles and
+  Gaussian noise, clipped to the 8-bit (or 16-bit) range. Images from it are
+  encoded by the reference encoder in the parity tests.
+
+* ``make_frame`` -- a synthetic *decoded frame*: the integer coefficients and
+  side information a pik bitstream carries for the reconstruction path
+  (AcStrategy layout with all nine transform types, raw quant field, EPF LUT
+  ids, colour-correlation maps, quantized DC and AC), drawn from seeded
+  distributions shaped like the reference encoder's output at
+  butteraugli distance ~1. It lets the benchmark build 4K/8K inputs on the
+  GPU host without running an encoder; its statistics are documented in
+  the design notes and compared against real encoder output in the tests.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import layout
+
+__all__ = ["make_image", "make_frame", "srgb8_to_linear255"]
+
+
+def make_image(xsize: int, ysize: int, *, seed: int = 0, sinusoids: int = 6,
+               rectangles: int = 3, noise_sigma: float = 4.0,
+               maxval: float = 255.0) -> np.ndarray:
+    """Returns a (3, ysize, xsize) float32 image in [0, maxval]."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:ysize, 0:xsize].astype(np.float32)
+    img = np.full((3, ysize, xsize), 0.5 * maxval, dtype=np.float32)
+    for _ in range(sinusoids):
+        period = rng.uniform(4.0, 64.0)
+        theta = rng.uniform(0.0, np.pi)
+        phase = rng.uniform(0.0, 2.0 * np.pi)
+        amp = rng.uniform(0.02, 0.12) * maxval * rng.uniform(0.3, 1.0, size=3)
+        arg = (2.0 * np.pi / period) * (np.cos(theta) * xx +
+                                        np.sin(theta) * yy) + phase
+        wave = np.sin(arg).astype(np.float32)
+        img += amp[:, None, None].astype(np.float32) * wave[None]
+    for _ in range(rectangles):
+        w = int(rng.integers(max(2, xsize // 16), max(3, xsize // 3)))
+        h = int(rng.integers(max(2, ysize // 16), max(3, ysize // 3)))
+        x0 = int(rng.integers(0, max(1, xsize - w)))
+        y0 = int(rng.integers(0, max(1, ysize - h)))
+        colour = rng.uniform(0.0, maxval, size=3).astype(np.float32)
+        img[:, y0:y0 + h, x0:x0 + w] = colour[:, None, None]
+    img += rng.normal(0.0, noise_sigma, size=img.shape).astype(np.float32)
+    return np.clip(img, 0.0, maxval).astype(np.float32)
+
+
+def srgb8_to_linear255(img: np.ndarray) -> np.ndarray:
+    """sRGB-encoded [0,255] -> linear on the reference's 0..255 scale
+    (IEC 61966-2-1 transfer function)."""
+    v = np.asarray(img, dtype=np.float64) / 255.0
+    lin = np.where(v <= 0.04045, v / 12.92, ((v + 0.055) / 1.055) ** 2.4)
+    return (lin * 255.0).astype(np.float32)
+
+
+# Shares of 8x8 cells covered by each transform type, shaped like the
+# reference encoder's choices on the generator images at distance ~1
+# (multi-block transforms are placed first, aligned to their size).
+_DEFAULT_SHARES = {
+    "DCT32X32": 0.18, "DCT16X16": 0.22, "DCT": 0.36, "DCT4X4": 0.08,
+    "DCT2X2": 0.04, "IDENTITY": 0.03, "LINES": 0.02, "DCT_NOHF": 0.04,
+    "DCT4X4_NOHF": 0.03,
+}
+
+
+def make_frame(xsize: int, ysize: int, *, seed: int = 0,
+               shares: dict | None = None, have_ar: bool = True,
+               gaborish: int = 2, global_scale: int = 2521,
+               quant_dc: int = 28, ac_scale: float = 1.0) -> "layout.Frame":
+    """Synthetic decoded frame of ``xsize`` x ``ysize`` pixels."""
+    rng = np.random.default_rng(seed)
+    shares = dict(_DEFAULT_SHARES if shares is None else shares)
+    bx, by = -(-xsize // 8), -(-ysize // 8)
+    tx, ty = -(-xsize // 64), -(-ysize // 64)
+    acs = np.full((by, bx), 0xFF, dtype=np.uint8)
+
+    def place(size: int, code: int, share: float) -> None:
+        if share <= 0:
+            return
+        cells = by * bx
+        target = int(share * cells / (size * size))
+        ys = np.arange(0, by - size + 1, size)
+        xs = np.arange(0, bx - size + 1, size)
+        if len(ys) == 0 or len(xs) == 0:
+            return
+        cand = np.stack(np.meshgrid(ys, xs, indexing="ij"), -1).reshape(-1, 2)
+        rng.shuffle(cand)
+        placed = 0
+        for y0, x0 in cand:
+            if placed >= target:
+                break
+            if np.all(acs[y0:y0 + size, x0:x0 + size] == 0xFF):
+                for iy in range(size):
+                    for ix in range(size):
+                        acs[y0 + iy, x0 + ix] = (code << 4) | (iy * size + ix
+                                                               if size > 1 else 0)
+                placed += 1
+
+    place(4, layout.ACS_TYPES["DCT32X32"], shares.pop("DCT32X32", 0.0))
+    place(2, layout.ACS_TYPES["DCT16X16"], shares.pop("DCT16X16", 0.0))
+    single = [(layout.ACS_TYPES[k], v) for k, v in shares.items()]
+    free = acs == 0xFF
+    codes = np.array([c for c, _ in single], dtype=np.uint8)
+    p = np.array([v for _, v in single], dtype=np.float64)
+    p = p / p.sum()
+    pick = rng.choice(codes, size=int(free.sum()), p=p)
+    acs[free] = (pick << 4).astype(np.uint8)
+
+    # Quant field: smooth log-normal around the median the encoder targets.
+    base = rng.normal(0.0, 0.25, size=(ty + 1, tx + 1))
+    qf = np.exp(np.kron(base, np.ones((8, 8)))[:by, :bx] +
+                rng.normal(0.0, 0.1, size=(by, bx)))
+    raw_qf = np.clip(np.round(qf * 5.0), 1, 256).astype(np.int32)
+    # Multi-block transforms share the first block's qf.
+    layout.broadcast_first_block(acs, raw_qf)
+    lut = np.zeros((by, bx), dtype=np.uint8)
+
+    # DC: smooth image in quantized units.
+    yy, xx = np.mgrid[0:by, 0:bx].astype(np.float32)
+    dc = np.zeros((3, by, bx), dtype=np.int16)
+    for c, (amp, off) in enumerate(((30.0, 0.0), (300.0, 600.0),
+                                    (200.0, 500.0))):
+        f = off + amp * np.sin(xx / (7.0 + 3 * c)) * np.cos(yy / (11.0 + c))
+        f += rng.normal(0.0, amp * 0.05, size=f.shape)
+        dc[c] = np.clip(np.round(f), -32000, 32000).astype(np.int16)
+
+    # AC: mostly zeros, Laplacian magnitudes falling with frequency.
+    k = np.arange(64)
+    freq = (k // 8) + (k % 8)
+    ac = np.zeros((3, by, bx * 64), dtype=np.int16)
+    for c, strength in enumerate((0.35, 1.2, 0.6)):
+        lam = ac_scale * strength * np.exp(-0.35 * freq)
+        lam = np.tile(lam, bx)[None, :]
+        mag = rng.exponential(1.0, size=(by, bx * 64)) * lam
+        sign = rng.choice(np.array([-1, 1], dtype=np.int16), size=mag.shape)
+        vals = np.floor(mag).astype(np.int16) * sign
+        ac[c] = vals
+    ac[:, :, 0::64] = 0  # DC slots are filled from the DC image
+    ytox = np.full((ty, tx), 128, dtype=np.int32) + rng.integers(
+        -6, 7, size=(ty, tx)).astype(np.int32)
+    ytob = np.full((ty, tx), 120, dtype=np.int32) + rng.integers(
+        -6, 7, size=(ty, tx)).astype(np.int32)
+    return layout.Frame(
+        xsize=xsize, ysize=ysize, gaborish=gaborish, predict_lf=1,
+        predict_hf=1, have_ar=int(have_ar), epf_enable_adaptive=1,
+        epf_sigma=0, epf_use_sharpened=0, global_scale=global_scale,
+        quant_dc=quant_dc, ytox_dc=128, ytob_dc=120, ytox_map=ytox,
+        ytob_map=ytob, ac_strategy=acs, raw_quant_field=raw_qf,
+        ar_sigma_lut_ids=lut, quantized_dc=dc, quantized_ac=ac)
