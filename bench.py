@@ -1,0 +1,361 @@
+"""Benchmark of the pik reconstruction path on B200.
+
+Workload (config 2 of the benchmark definition): a 3840x2160 generator image
+(12 sinusoids, 20 rectangles, noise sigma 3, seed 0) encoded by the
+reference encoder at butteraugli distance 1.0 -- mixed AcStrategy blocks,
+adaptive quant field, chroma-from-luma, gaborish and EPF on -- decoded to
+the reconstruction boundary by the reference's own decoding functions
+(tests/golden/c2_4k_d1_frame.npz, made by tests/golden/make_fixtures.py).
+One step = one full reconstruction of that frame (integer coefficients ->
+FP32 linear RGB), the reference's Dequant::DoAC + ReconOpsinImage over all
+groups + FinalizeFrameDecoding.
+
+  value  decoded MP/s with the inputs resident in device memory
+  e2e    the same through the C ABI with host buffers: each step uploads the
+         frame's side information and int16 coefficients from pinned host
+         memory and reads the FP32 linear planes back.
+
+`--impl reference` times the reference's own CPU implementation (built from
+its sources into oracle/_ref/, AVX2 flavour, all host threads) on the same
+frame. Multi-GPU: independent replicas (one frame per rank per step).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FRAME = os.path.join(ROOT, "tests", "golden", "c2_4k_d1_frame.npz")
+BITSTREAM = os.path.join(ROOT, "tests", "golden", "c2_4k_d1.pik")
+METRIC = ("decoded MP/s at 4K, split-BF16 vs FP32 form @<=2e-5 err; "
+          "% of HBM peak")
+# Algorithmic bytes per pixel of the path: int16 AC in (6), DC (0.1875),
+# side info (0.094), CfL maps (~0.002), FP32 linear RGB out (12).
+PATH_BYTES_PER_PX = 18.28
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples (every 100 ms) during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.path = f"/tmp/pik_b200_clocks_{os.getpid()}.csv"
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "100", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+            os.remove(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None,
+                    "reasons": ["no samples"]}
+
+        def num(v):
+            try:
+                return float(v.split()[0])
+            except (ValueError, IndexError):
+                return None
+        sm = [x for x in (num(r[0]) for r in rows) if x is not None]
+        mx = [x for x in (num(r[1]) for r in rows) if x is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reference_arm(args):
+    """The reference's CPU reconstruction on the same frame."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import refpy
+    if not refpy.available("avx2"):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference build oracle/_ref is "
+                          "missing (build() compiles it from the checkout)"}))
+        return
+    bs = open(BITSTREAM, "rb").read()
+    fz = refpy.Frozen(bs, flavour="avx2")
+    threads = os.cpu_count() or 1
+    px = fz.xsize * fz.ysize
+    for _ in range(args.warmup):
+        fz.run_stages(threads=threads, want=())
+    times = []
+    for _ in range(args.steps):
+        _, secs = fz.run_stages(threads=threads, want=())
+        times.append(secs)
+    t = sum(times)
+    value = px * args.steps / t / 1e6
+    sample = (f"{args.steps} full 3840x2160 reconstructions (DequantImageAC +"
+              f" ReconOpsinImage per group + FinalizeFrameDecoding stages)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 3),
+        "unit": "MP/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * t / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "c2: 3840x2160 generator image, reference-"
+                   "encoded at distance 1.0 (mixed blocks, EPF on)",
+                   "impl": "reference C++ (AVX2 build, ThreadPool)"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "MP/s",
+                         "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "MP/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def cpu_baseline(frame_px):
+    """Reference CPU path on a bounded sample: 2 reconstructions of the frame
+    with all host threads."""
+    try:
+        from oracle import refpy
+    except Exception as e:  # noqa: BLE001
+        return {"value": None, "unit": "MP/s", "cores": 0,
+                "kind": "reference", "sample": f"unavailable: {e}"}
+    if not refpy.available("avx2"):
+        return {"value": None, "unit": "MP/s", "cores": 0,
+                "kind": "reference", "sample": "unavailable: no oracle/_ref"}
+    bs = open(BITSTREAM, "rb").read()
+    fz = refpy.Frozen(bs, flavour="avx2")
+    threads = os.cpu_count() or 1
+    fz.run_stages(threads=threads, want=())
+    t = 0.0
+    n = 2
+    for _ in range(n):
+        _, s = fz.run_stages(threads=threads, want=())
+        t += s
+    return {"value": round(frame_px * n / t / 1e6, 3), "unit": "MP/s",
+            "cores": threads, "kind": "reference",
+            "sample": f"{n} full 4K reconstructions, AVX2 build"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    from pik_b200 import layout, native
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    frame = layout.Frame.load(FRAME)
+    px = frame.xsize * frame.ysize
+    by, bx = frame.blocks
+    dev = torch.device("cuda", local)
+
+    # Device-resident run: AC already in HBM, outputs into device buffers.
+    ctx = native.Context(local)
+    ctx.begin(frame)
+    ac_dev = torch.from_numpy(frame.quantized_ac).to(dev)
+    lin_dev = torch.empty((3, frame.ysize, frame.xsize), dtype=torch.float32,
+                          device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
+    import ctypes
+    planes = (ctypes.c_void_p * 3)(*[ac_dev[c].data_ptr() for c in range(3)])
+
+    def step():
+        ctx._check(ctx.L.pikgpu_frame_set_ac_device(ctx.h, planes, bx * 64))
+        ctx.reconstruct_device(lin_dev.data_ptr(), frame.xsize)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    launches = ctx.L.pikgpu_last_launch_count(ctx.h)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * px / (ms * 1e-3) / 1e6
+
+    # Per-kernel-group device times (CUDA events on the launching stream).
+    pctx = native.Context(local, profile=True)
+    pctx.begin(frame)
+    pctx.L.pikgpu_set_stream(pctx.h, stream.cuda_stream)
+    pctx._check(pctx.L.pikgpu_frame_set_ac_device(pctx.h, planes, bx * 64))
+    acc = {}
+    for i in range(3 + args.steps):
+        pctx.reconstruct_device(lin_dev.data_ptr(), frame.xsize)
+        if i >= 3:
+            for k, v in pctx.kernel_times().items():
+                acc[k] = acc.get(k, 0.0) + v / args.steps
+    pctx.close()
+
+    # End to end through the C ABI with pinned host buffers.
+    pin = {
+        "ac": torch.from_numpy(frame.quantized_ac).pin_memory(),
+        "lin": torch.empty((3, frame.ysize, frame.xsize),
+                           dtype=torch.float32).pin_memory(),
+    }
+    ac_planes = (ctypes.c_void_p * 3)(
+        *[pin["ac"][c].data_ptr() for c in range(3)])
+    lin_planes = (ctypes.c_void_p * 3)(
+        *[pin["lin"][c].data_ptr() for c in range(3)])
+    from pik_b200 import abi
+    packed = abi.PackedFrame(frame)
+    h2d = frame.quantized_ac.nbytes + sum(a.nbytes for a in
+                                          packed.arrays.values())
+    d2h = pin["lin"].numel() * 4
+
+    def e2e_step():
+        ctx._check(ctx.L.pikgpu_frame_begin(ctx.h, packed.ref))
+        ctx._check(ctx.L.pikgpu_frame_set_ac(ctx.h, ac_planes, bx * 64))
+        ctx._check(ctx.L.pikgpu_reconstruct(ctx.h, lin_planes, frame.xsize,
+                                            None, 0, 0))
+
+    for _ in range(max(3, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = ws * px / (e2e_ms * 1e-3) / 1e6
+    ctx.close()
+
+    peak, peak_kind = load_peaks()
+    top = max(acc, key=acc.get)
+    # Algorithmic bytes per pixel of each kernel group (design notes).
+    group_bytes = {
+        "epf": 3 * 4 + 3 * 4 + 3 * 4,          # in + guide source + out
+        "ar_clamp": 3 * 4 + 3 * 4 + 3 * 4,     # filtered + original + out
+        "hf_idct": 3 * 4 + 3 * 4,              # coefficients in, pixels out
+        "gaborish1_minmax": 3 * 4 + 3 * 4,
+        "gaborish2_opsin_srgb": 3 * 4 + 3 * 4,
+        "dequant_ac_lf_update": 3 * 2 + 3 * 4,
+        "lf_prediction": 0.5,
+        "dc_dequant_epf": 0.2,
+    }
+    top_bytes = group_bytes.get(top, 12) * px
+    achieved = top_bytes / (acc[top] * 1e-3) / 1e9
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 2), "unit": "MP/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": "c2: 3840x2160 generator image, reference-encoded"
+                            " at distance 1.0 (mixed blocks, adaptive qf, CfL,"
+                            " gaborish + EPF on)",
+                "form": "plain FP32 (CUDA cores)",
+                "l2": "working set > L2 (inputs 50 MB, planes 100 MB each)",
+                "parallelism": f"replicas x{ws}"},
+            "roofline": {"bound": "hbm", "kernel": top,
+                         "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": None, "peak_kind": peak_kind,
+                         "path_achieved": round(
+                             PATH_BYTES_PER_PX * px / (ms * 1e-3) / 1e9, 1),
+                         "path_frac": round(PATH_BYTES_PER_PX * px /
+                                            (ms * 1e-3) / 1e9 / peak, 4)},
+            "kernel_ms": {k: round(v, 4) for k, v in acc.items()},
+            "e2e": {"value": round(e2e, 2), "unit": "MP/s",
+                    "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu_baseline(px) if ws == 1 else None,
+        }
+        print(json.dumps(out))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

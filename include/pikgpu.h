@@ -175,6 +175,8 @@ int pikgpu_get_stage(pikgpu_ctx* ctx, int stage, float* const planes[3],
  * number of kernels or an error. Names via pikgpu_kernel_name. */
 int pikgpu_last_kernel_times(pikgpu_ctx* ctx, float* ms, int n);
 const char* pikgpu_kernel_name(int index);
+/* Number of kernels the last pikgpu_reconstruct launched. */
+int pikgpu_last_launch_count(const pikgpu_ctx* ctx);
 
 /* Checks `params` exactly as pikgpu_frame_begin does, without a device.
  * Writes the reason for a failure into `msg` (may be NULL). */

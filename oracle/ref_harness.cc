@@ -47,6 +47,7 @@
 #include "pik/headers.h"
 #include "pik/image.h"
 #include "pik/noise.h"
+#include "pik/opsin_image.h"
 #include "pik/opsin_inverse.h"
 #include "pik/opsin_params.h"
 #include "pik/pik.h"
@@ -661,6 +662,103 @@ int pikref_frozen_set_ac(void* h, const int16_t* planes, size_t nelems) {
     }
   }
   return 0;
+}
+
+// Encoder route of pik/compressed_image_test.cc:31-95 for an all-DCT8
+// frame with a uniform quant field: OpsinDynamicsImage + GaborishInverse,
+// InitializeFrameEncCache / InitializeEncCache / ComputeCoefficients with an
+// all-DCT AcStrategyImage. Returns a frozen frame holding the encoder's
+// integers and the decoder-side quantizer (Quantizer::Decode of its encoded
+// bytes), with EPF off; `gaborish` is the GaborishStrength in the header.
+void* pikref_frozen_encode_dct8(const float* planes, int xsize, int ysize,
+                                float quant, int gaborish) {
+  InitEpf();
+  CodecContext context;
+  CodecInOut io(&context);
+  Image3F img(xsize, ysize);
+  for (int c = 0; c < 3; ++c) {
+    for (int y = 0; y < ysize; ++y) {
+      memcpy(img.PlaneRow(c, y), planes + (size_t(c) * ysize + y) * xsize,
+             xsize * sizeof(float));
+    }
+  }
+  io.SetFromImage(std::move(img), context.c_linear_srgb[0]);
+  Image3F opsin =
+      PadImageToMultiple(OpsinDynamicsImage(&io, Rect(io.color())), kBlockDim);
+  FrameHeader header;
+  header.gaborish = GaborishStrength(gaborish);
+  header.have_adaptive_reconstruction = false;
+  if (header.gaborish != GaborishStrength::kOff) {
+    // Same pre-sharpening as PixelsToPikPass (pik/pik_frame.cc:529-532).
+    opsin = GaborishInverse(opsin, 0.92718927264540152);
+  }
+  const size_t xb = opsin.xsize() / kBlockDim, yb = opsin.ysize() / kBlockDim;
+  std::unique_ptr<Frozen> f(new Frozen);
+  f->xsize = xsize;
+  f->ysize = ysize;
+  f->xsize_blocks = xb;
+  f->ysize_blocks = yb;
+  f->header = header;
+  f->cmap = ColorCorrelationMap(opsin.xsize(), opsin.ysize());
+  f->fdc.reset(new FrameDecCache);
+  FrameDecCache& fdc = *f->fdc;
+  DequantMatrices dequant(/*need_inv_matrices=*/true);
+  Quantizer enc_q(&dequant, xb, yb);
+  enc_q.SetQuant(quant);
+  AcStrategyImage ac_strategy(xb, yb);
+  FrameEncCache fec;
+  fec.dequant_control_field =
+      ImageB(DivCeil(opsin.xsize(), kTileDim), DivCeil(opsin.ysize(), kTileDim));
+  ZeroFillImage(&fec.dequant_control_field);
+  BlockDictionary dictionary;
+  InitializeFrameEncCache(header, opsin, ac_strategy, enc_q, f->cmap,
+                          dictionary, nullptr, &fec, nullptr);
+  EncCache ec;
+  GroupHeader gh;
+  InitializeEncCache(header, gh, fec, Rect(opsin), &ec);
+  ec.ac_strategy = ac_strategy.Copy();
+  ComputeCoefficients(enc_q, f->cmap, Rect(f->cmap.ytob_map), nullptr, fec,
+                      &ec);
+  // Decoder-side state.
+  const std::string qbytes = enc_q.Encode(nullptr);
+  PaddedBytes qb(qbytes.size());
+  memcpy(qb.data(), qbytes.data(), qbytes.size());
+  BitReader br(qb.data(), qb.size());
+  f->quantizer.reset(new Quantizer(&fdc.matrices, 0, 0));
+  if (!f->quantizer->Decode(&br)) {
+    g_error = "quantizer decode failed";
+    return nullptr;
+  }
+  fdc.ac_strategy = ac_strategy.Copy();
+  fdc.raw_quant_field = CopyImage(ec.quant_field);
+  fdc.ar_sigma_lut_ids = ImageB(xb, yb);
+  ZeroFillImage(&fdc.ar_sigma_lut_ids);
+  fdc.dequant_control_field = CopyImage(fec.dequant_control_field);
+  f->quantized_dc = CopyImage(fec.dc);
+  f->quantized_ac = CopyImage(ec.ac);
+  // DequantDC (pik/compressed_dc.cc:181-231; not exported by the
+  // reference, restated here) + AdaptiveDCReconstruction.
+  float mul_dc[3];
+  for (int c = 0; c < 3; ++c) {
+    mul_dc[c] = f->quantizer->DequantMatrix(0, kQuantKindDCT8, c)[0] *
+                f->quantizer->inv_quant_dc();
+  }
+  const float ytox_dc = ColorCorrelationMap::YtoX(1.0f, f->cmap.ytox_dc);
+  const float ytob_dc = ColorCorrelationMap::YtoB(1.0f, f->cmap.ytob_dc);
+  Image3F dc(xb, yb);
+  for (size_t y = 0; y < yb; ++y) {
+    for (size_t x = 0; x < xb; ++x) {
+      const float vy = f->quantized_dc.ConstPlaneRow(1, y)[x] * mul_dc[1];
+      dc.PlaneRow(1, y)[x] = vy;
+      const float dx = f->quantized_dc.ConstPlaneRow(0, y)[x] * mul_dc[0];
+      dc.PlaneRow(0, y)[x] = ytox_dc * vy + dx;
+      const float db = f->quantized_dc.ConstPlaneRow(2, y)[x] * mul_dc[2];
+      dc.PlaneRow(2, y)[x] = ytob_dc * vy + db;
+    }
+  }
+  AdaptiveDCReconstruction(dc, *f->quantizer, nullptr);
+  f->dc_smoothed = std::move(dc);
+  return f.release();
 }
 
 // ---- Probes of single reference functions (for pinning the restatement).

@@ -56,6 +56,10 @@ def lib(flavour: str = "scalar") -> ctypes.CDLL:
                                     ctypes.POINTER(ctypes.c_void_p),
                                     ctypes.POINTER(ctypes.c_double)]
     L.pikref_frozen_set_ac.argtypes = [P, P, ctypes.c_size_t]
+    L.pikref_frozen_encode_dct8.restype = P
+    L.pikref_frozen_encode_dct8.argtypes = [P, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_float, ctypes.c_int]
+    L.pikref_opsin_inverse_matrix.argtypes = [P]
     L.pikref_transform.argtypes = [ctypes.c_int, ctypes.c_int, P,
                                    ctypes.c_size_t, P, ctypes.c_size_t]
     L.pikref_lf_helper.argtypes = [ctypes.c_int, ctypes.c_int, P,
@@ -104,18 +108,35 @@ def decode(bitstream: bytes, xsize: int, ysize: int, *, threads: int = 0,
     return out
 
 
+def encode_dct8(linear: np.ndarray, quant: float, *, gaborish: int = 2,
+                flavour: str = "scalar") -> "Frozen":
+    """All-DCT8, EPF-off frame from the reference encoder's coefficient stage
+    with a uniform quant field (the compressed_image_test route)."""
+    L = lib(flavour)
+    img = np.ascontiguousarray(linear, dtype=np.float32)
+    h = L.pikref_frozen_encode_dct8(_ptr(img), img.shape[2], img.shape[1],
+                                    float(quant), gaborish)
+    if not h:
+        raise RuntimeError(L.pikref_last_error().decode())
+    return Frozen(None, flavour=flavour, handle=h)
+
+
 class Frozen:
     """A bitstream decoded up to the reconstruction boundary by the
     reference's own decoding functions."""
 
-    def __init__(self, bitstream: bytes, *, override_ar: int = -1,
-                 override_gaborish: int = -1, flavour: str = "scalar"):
+    def __init__(self, bitstream: bytes | None, *, override_ar: int = -1,
+                 override_gaborish: int = -1, flavour: str = "scalar",
+                 handle=None):
         self.flavour = flavour
         self.L = lib(flavour)
-        buf = ctypes.create_string_buffer(bitstream, len(bitstream))
-        self.h = self.L.pikref_frozen_from_bitstream(
-            ctypes.cast(buf, ctypes.c_void_p), len(bitstream), override_ar,
-            override_gaborish)
+        if handle is not None:
+            self.h = handle
+        else:
+            buf = ctypes.create_string_buffer(bitstream, len(bitstream))
+            self.h = self.L.pikref_frozen_from_bitstream(
+                ctypes.cast(buf, ctypes.c_void_p), len(bitstream),
+                override_ar, override_gaborish)
         if not self.h:
             raise RuntimeError(self.L.pikref_last_error().decode())
         ints = np.zeros(32, np.int64)

@@ -77,11 +77,12 @@ struct pikgpu_ctx {
   DevBuf qdc, qac, dc, dcpad, dcfilt, ac, llf_g, lf2x2_g, pred2x2_g, tmp2x2_g;
   DevBuf idct, smoothed, filt, mm, sigma, dc_sigma, list[kNumClasses];
   DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr;
-  DevBuf sigma_ovr;
+  DevBuf sigma_ovr, counters, active[kNumClasses];
   bool use_guide_ovr = false, use_sigma_ovr = false;
   cudaEvent_t ev[kNumTimed + 1] = {};
   float times[kNumTimed] = {};
   float dc_half_step[3] = {};
+  int launches = 0;
 };
 
 namespace {
@@ -300,6 +301,7 @@ int RunEpf(pikgpu_ctx* ctx, const float* in, const float* guide_src, int w,
   dim3 grid(Blocks(w, kEpfTile), Blocks(h, kEpfTile));
   k_epf<<<grid, 256, 0, ctx->stream>>>(in, guide_src, guide_ovr, w, h,
                                        P<uint32_t>(ctx->mm), sig, out);
+  ++ctx->launches;
   return PIKGPU_OK;
 }
 
@@ -331,57 +333,58 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   f.filt = P<float>(ctx->filt);
   uint32_t* mm = P<uint32_t>(ctx->mm);
 
+  ctx->launches = 0;
   Mark(ctx, kTDc);
   // DC: dequant, EPF on the 8-padded DC image, clamp.
-  k_dequant_dc<<<Blocks(size_t(g.Bx) * g.By, 256), 256, 0, st>>>(g, f, s);
+  k_dequant_dc<<<Blocks(size_t(g.Bx) * g.By, 256), 256, 0, st>>>(g, f, s); ++ctx->launches;
   const int dpw = (g.Bx + 7) / 8 * 8, dph = (g.By + 7) / 8 * 8;
   float* dcpad = P<float>(ctx->dcpad);
   float* dcfilt = P<float>(ctx->dcfilt);
   {
     dim3 b(32, 8), gr(Blocks(dpw, 32), Blocks(dph, 8), 3);
-    k_pad_replicate<<<gr, b, 0, st>>>(f.dc, g.Bx, g.By, dcpad, dpw, dph);
-    k_minmax_init<<<1, 32, 0, st>>>(mm);
+    k_pad_replicate<<<gr, b, 0, st>>>(f.dc, g.Bx, g.By, dcpad, dpw, dph); ++ctx->launches;
+    k_minmax_init<<<1, 32, 0, st>>>(mm); ++ctx->launches;
     k_minmax<<<dim3(Blocks(size_t(dpw) * dph, 256 * 8), 3), 256, 0, st>>>(
-        dcpad, size_t(dpw) * dph, mm);
+        dcpad, size_t(dpw) * dph, mm); ++ctx->launches;
     const int nb = (dpw / 8) * (dph / 8);
     k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(
         nb, nullptr, nullptr, nullptr, s.quant_dc / 2, mm,
-        P<int32_t>(ctx->dc_sigma));
+        P<int32_t>(ctx->dc_sigma)); ++ctx->launches;
     RunEpf(ctx, dcpad, dcpad, dpw, dph, P<int32_t>(ctx->dc_sigma), dcfilt,
            nullptr);
     dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
     k_dc_clamp<<<gr2, b, 0, st>>>(f.dc, dcfilt, g.Bx, g.By, dpw, dph,
                                   ctx->dc_half_step[0], ctx->dc_half_step[1],
-                                  ctx->dc_half_step[2]);
+                                  ctx->dc_half_step[2]); ++ctx->launches;
   }
   Mark(ctx, kTLf);
   // Per-group LF prediction.
   const int ng = g.Gx * g.Gy;
   {
     dim3 b(16, 16), gr(Blocks(kGB, 16), Blocks(kGB, 16), 3 * ng);
-    k_llf<<<gr, b, 0, st>>>(g, f);
+    k_llf<<<gr, b, 0, st>>>(g, f); ++ctx->launches;
     if (s.predict_lf) {
-      k_tmp2x2<<<gr, b, 0, st>>>(g, f);
+      k_tmp2x2<<<gr, b, 0, st>>>(g, f); ++ctx->launches;
       dim3 gr2(Blocks(kG2, 16), Blocks(kG2, 16), 3 * ng);
-      k_lf_blur<<<gr2, b, 0, st>>>(g, f);
-      k_lf_from_2x2<<<gr, b, 0, st>>>(g, f);
+      k_lf_blur<<<gr2, b, 0, st>>>(g, f); ++ctx->launches;
+      k_lf_from_2x2<<<gr, b, 0, st>>>(g, f); ++ctx->launches;
     }
     if (s.predict_hf) {
       k_pred_border<<<dim3(Blocks(4 * (kGB + 2), 128), 1, 3 * ng), 128, 0,
-                      st>>>(g, f, s.predict_lf);
+                      st>>>(g, f, s.predict_lf); ++ctx->launches;
     }
   }
   Mark(ctx, kTDequant);
   {
     dim3 b(64, 4), gr(Blocks(g.Bx, 4), g.By);
-    k_dequant_ac<<<gr, b, 0, st>>>(g, f, s);
+    k_dequant_ac<<<gr, b, 0, st>>>(g, f, s); ++ctx->launches;
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_dequant.p, f.ac,
                       sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
                       cudaMemcpyDeviceToDevice, st);
     }
     dim3 b2(32, 8), gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
-    k_lf_update<<<gr2, b2, 0, st>>>(g, f, s.predict_lf, s.predict_hf);
+    k_lf_update<<<gr2, b2, 0, st>>>(g, f, s.predict_lf, s.predict_hf); ++ctx->launches;
   }
   Mark(ctx, kTIdct);
   {
@@ -391,12 +394,23 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       L[k] = P<uint32_t>(ctx->list[k]);
       n[k] = int(ctx->lists[k].size());
     }
-    if (n[kC8]) k_square_idct<8><<<Blocks(n[kC8], 4), 256, 0, st>>>(
-        g, f, L[kC8], n[kC8], s.predict_hf);
-    if (n[kC16]) k_square_idct<16><<<n[kC16], 256, 0, st>>>(
-        g, f, L[kC16], n[kC16], s.predict_hf);
-    if (n[kC32]) k_square_idct<32><<<n[kC32], 256, 0, st>>>(
-        g, f, L[kC32], n[kC32], s.predict_hf);
+    auto rows_grid = [](int items, int n) {
+      const int upw = 32 / n;
+      const int warps = (items + upw - 1) / upw;
+      return (warps * 32 + kSquareThreads - 1) / kSquareThreads;
+    };
+    if (n[kC8]) {
+      k_square_idct_rows<8><<<rows_grid(3 * n[kC8], 8), kSquareThreads, 0,
+                              st>>>(g, f, L[kC8], n[kC8], s.predict_hf);
+    }
+    if (n[kC16]) {
+      k_square_idct_rows<16><<<rows_grid(3 * n[kC16], 16), kSquareThreads, 0,
+                               st>>>(g, f, L[kC16], n[kC16], s.predict_hf);
+    }
+    if (n[kC32]) {
+      k_square_idct_rows<32><<<rows_grid(3 * n[kC32], 32), kSquareThreads, 0,
+                               st>>>(g, f, L[kC32], n[kC32], s.predict_hf);
+    }
     if (n[kC4]) k_dct4_idct<<<Blocks(n[kC4], 16), 256, 0, st>>>(
         g, f, L[kC4], n[kC4], s.predict_hf);
     if (n[kCSmall]) k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, st>>>(
@@ -407,17 +421,17 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   if (s.have_ar) {
     const size_t npx = size_t(g.PW) * g.PH;
     const float* guide_src = f.idct;
-    k_minmax_init<<<1, 32, 0, st>>>(mm);
+    k_minmax_init<<<1, 32, 0, st>>>(mm); ++ctx->launches;
     if (s.gaborish) {
       dim3 b(32, 8), gr(Blocks(g.PW, 32), Blocks(g.PH, 8), 3);
       k_gaborish_minmax<<<gr, b, 0, st>>>(f.idct, g.PW, g.PH, s.gaborish,
                                           f.smoothed,
-                                          s.use_sharpened ? nullptr : mm);
+                                          s.use_sharpened ? nullptr : mm); ++ctx->launches;
       if (!s.use_sharpened) guide_src = f.smoothed;
     }
     if (guide_src == f.idct) {
       k_minmax<<<dim3(Blocks(npx, 256 * 8), 3), 256, 0, st>>>(f.idct, npx,
-                                                               mm);
+                                                               mm); ++ctx->launches;
     }
     Mark(ctx, kTEpf);
     const int nb = g.Bx * g.By;
@@ -427,7 +441,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
                       cudaMemcpyDeviceToDevice, st);
     } else {
       k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, f.qf, f.acs, f.lut, 0,
-                                                   mm, sig);
+                                                   mm, sig); ++ctx->launches;
     }
     RunEpf(ctx, f.idct, guide_src, g.PW, g.PH, sig, f.filt,
            ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr);
@@ -442,16 +456,38 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       L[k] = P<uint32_t>(ctx->list[k]);
       n[k] = int(ctx->lists[k].size());
     }
-    if (n[kC8]) k_square_ar<8><<<Blocks(n[kC8], 4), 256, 0, st>>>(
-        g, f, s, L[kC8], n[kC8]);
-    if (n[kC16]) k_square_ar<16><<<n[kC16], 256, 0, st>>>(g, f, s, L[kC16],
-                                                          n[kC16]);
-    if (n[kC32]) k_square_ar<32><<<n[kC32], 256, 0, st>>>(g, f, s, L[kC32],
-                                                          n[kC32]);
+    // Only blocks the EPF filtered need the clamp (see k_active_blocks).
+    int* counters = P<int>(ctx->counters);
+    cudaMemsetAsync(counters, 0, sizeof(int) * kNumClasses, st);
+    for (int k = 0; k < kNumClasses; ++k) {
+      if (!n[k]) continue;
+      k_active_blocks<<<Blocks(n[k], 256), 256, 0, st>>>(
+          g, sig, f.acs, L[k], n[k], P<uint32_t>(ctx->active[k]),
+          counters + k);
+    }
+    auto rows_grid = [](int items, int nn) {
+      const int upw = 32 / nn;
+      const int warps = (items + upw - 1) / upw;
+      return (warps * 32 + kSquareThreads - 1) / kSquareThreads;
+    };
+    if (n[kC8]) {
+      k_square_ar_rows<8><<<rows_grid(n[kC8], 8), kSquareThreads, 0, st>>>(
+          g, f, s, P<uint32_t>(ctx->active[kC8]), counters + kC8);
+    }
+    if (n[kC16]) {
+      k_square_ar_rows<16><<<rows_grid(n[kC16], 16), kSquareThreads, 0,
+                             st>>>(g, f, s, P<uint32_t>(ctx->active[kC16]),
+                                   counters + kC16);
+    }
+    if (n[kC32]) {
+      k_square_ar_rows<32><<<rows_grid(n[kC32], 32), kSquareThreads, 0,
+                             st>>>(g, f, s, P<uint32_t>(ctx->active[kC32]),
+                                   counters + kC32);
+    }
     if (n[kC4]) k_dct4_ar<<<Blocks(n[kC4], 16), 256, 0, st>>>(
-        g, f, s, L[kC4], n[kC4]);
+        g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
     if (n[kCSmall]) k_small_ar<<<Blocks(n[kCSmall], 64), 64, 0, st>>>(
-        g, f, s, L[kCSmall], n[kCSmall]);
+        g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
     final_in = f.filt;
   } else {
     Mark(ctx, kTEpf);
@@ -463,7 +499,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     k_final<<<gr, b, 0, st>>>(final_in, g.PW, g.PH, g.W, g.H, s.gaborish,
                               ctx->keep_stages ? P<float>(ctx->dbg_pre)
                                                : nullptr,
-                              lin, lin_stride, rgb8, rgb8_stride);
+                              lin, lin_stride, rgb8, rgb8_stride); ++ctx->launches;
   }
   Mark(ctx, kNumTimed);
   CUDA_TRY(ctx, cudaGetLastError());
@@ -526,6 +562,8 @@ int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
                     &ctx->guide_ovr, &ctx->sigma_ovr};
   for (DevBuf* b : bufs) FreeBuf(b);
   for (auto& b : ctx->list) FreeBuf(&b);
+  for (auto& b : ctx->active) FreeBuf(&b);
+  FreeBuf(&ctx->counters);
   for (auto& e : ctx->ev) {
     if (e) cudaEventDestroy(e);
   }
@@ -560,6 +598,7 @@ int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
 int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
   ctx->have_frame = ctx->have_ac = ctx->have_result = false;
+  ctx->use_guide_ovr = ctx->use_sigma_ovr = false;
   int rc = Validate(ctx, p);
   if (rc != PIKGPU_OK) return rc;
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
@@ -638,8 +677,13 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
     }
   }
   cudaStream_t st = ctx->stream;
+  if ((rc = Ensure(ctx, &ctx->counters, sizeof(int) * kNumClasses))) {
+    return rc;
+  }
   for (int k = 0; k < kNumClasses; ++k) {
     rc = Ensure(ctx, &ctx->list[k], 4 * ctx->lists[k].size());
+    if (rc != PIKGPU_OK) return rc;
+    rc = Ensure(ctx, &ctx->active[k], 4 * ctx->lists[k].size());
     if (rc != PIKGPU_OK) return rc;
     if (!ctx->lists[k].empty()) {
       CUDA_TRY(ctx, cudaMemcpyAsync(ctx->list[k].p, ctx->lists[k].data(),
@@ -837,7 +881,10 @@ int pikgpu_get_stage(pikgpu_ctx* ctx, int stage, float* const planes[3],
       src = P<float>(ctx->idct), w = g.PW, h = g.PH;
       break;
     case PIKGPU_STAGE_SMOOTHED:
-      src = P<float>(ctx->smoothed), w = g.PW, h = g.PH;
+      // Without gaborish the EPF guide source is the IDCT output itself
+      // (DoAdaptiveReconstruction, pik/compressed_image.cc:1126-1132).
+      src = P<float>(ctx->s.gaborish ? ctx->smoothed : ctx->idct);
+      w = g.PW, h = g.PH;
       break;
     case PIKGPU_STAGE_EPF:
       src = P<float>(ctx->dbg_epf), w = g.PW, h = g.PH;
@@ -937,6 +984,10 @@ int pikgpu_last_kernel_times(pikgpu_ctx* ctx, float* ms, int n) {
   if (!ctx->profile) return Fail(ctx, PIKGPU_ERR_STATE, "profiling is off");
   for (int i = 0; i < n && i < kNumTimed; ++i) ms[i] = ctx->times[i];
   return kNumTimed;
+}
+
+int pikgpu_last_launch_count(const pikgpu_ctx* ctx) {
+  return ctx ? ctx->launches : PIKGPU_ERR_INVALID_ARG;
 }
 
 const char* pikgpu_kernel_name(int index) {

@@ -267,7 +267,9 @@ __global__ void k_minmax_init(uint32_t* mm) {
   else if (threadIdx.x < 6) mm[threadIdx.x] = 0u;
 }
 
-__global__ void k_minmax(const float* planes, size_t n, uint32_t* mm) {
+__global__ void __launch_bounds__(256)
+    k_minmax(const float* planes, size_t n, uint32_t* mm) {
+  __shared__ uint32_t s_lo[8], s_hi[8];
   const int c = blockIdx.y;
   const float* p = planes + size_t(c) * n;
   uint32_t lo = 0xFFFFFFFFu, hi = 0u;
@@ -282,6 +284,15 @@ __global__ void k_minmax(const float* planes, size_t n, uint32_t* mm) {
     hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, off));
   }
   if ((threadIdx.x & 31) == 0) {
+    s_lo[threadIdx.x >> 5] = lo;
+    s_hi[threadIdx.x >> 5] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < 8; ++i) {
+      lo = min(lo, s_lo[i]);
+      hi = max(hi, s_hi[i]);
+    }
     atomicMin(&mm[c], lo);
     atomicMax(&mm[3 + c], hi);
   }
@@ -357,9 +368,32 @@ __global__ void __launch_bounds__(256)
   __shared__ float si[3][kInH][kInW];
   const int x0 = blockIdx.x * kEpfTile, y0 = blockIdx.y * kEpfTile;
   const int tid = threadIdx.x;
+  const size_t plane = size_t(w) * h;
+  const int bw = w / 8;
+  {
+    // Tiles whose 2x2 blocks all have sigma < kMinSigma are plain copies
+    // (CopyOriginalBlock, pik/epf_target.cc:1228-1236).
+    bool any = false;
+    for (int i = 0; i < 4; ++i) {
+      const int bx = x0 / 8 + (i & 1), by = y0 / 8 + (i >> 1);
+      if (bx * 8 < w && by * 8 < h && sigma[by * bw + bx] >= kMinSigma) {
+        any = true;
+      }
+    }
+    if (!any) {
+      const int lx = tid % kEpfTile, ly = tid / kEpfTile;
+      const int x = x0 + lx, y = y0 + ly;
+      if (x < w && y < h) {
+        for (int c = 0; c < 3; ++c) {
+          out[c * plane + size_t(y) * w + x] =
+              in[c * plane + size_t(y) * w + x];
+        }
+      }
+      return;
+    }
+  }
   float amin, mul, stretch;
   GuideParams(mm, &amin, &mul, &stretch);
-  const size_t plane = size_t(w) * h;
   const int gw = w + 12;
   for (int i = tid; i < 3 * kGuideH * kGuideW; i += 256) {
     const int c = i / (kGuideH * kGuideW);
@@ -390,7 +424,6 @@ __global__ void __launch_bounds__(256)
   const int lx = tid % kEpfTile, ly = tid / kEpfTile;
   const int x = x0 + lx, y = y0 + ly;
   if (x >= w || y >= h) return;
-  const int bw = w / 8;
   const int sg_ = sigma[(y / 8) * bw + x / 8];
   if (sg_ < kMinSigma) {
     for (int c = 0; c < 3; ++c) out[c * plane + size_t(y) * w + x] =
@@ -468,27 +501,39 @@ __device__ __forceinline__ float Sym3(const float* p, int w, int h, int x,
   return x2 * w2 + mul1;
 }
 
-// ConvolveGaborish (pik/gaborish.cc:137-159) plus min/max of the result.
-__global__ void k_gaborish_minmax(const float* in, int w, int h, int strength,
-                                  float* out, uint32_t* mm) {
+// ConvolveGaborish (pik/gaborish.cc:137-159) plus min/max of the result,
+// reduced per CTA (256 threads) before one atomic per channel.
+__global__ void __launch_bounds__(256)
+    k_gaborish_minmax(const float* in, int w, int h, int strength, float* out,
+                      uint32_t* mm) {
+  __shared__ uint32_t s_lo[8], s_hi[8];
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int c = blockIdx.z;
   const size_t plane = size_t(w) * h;
-  uint32_t o = 0;
-  bool valid = x < w && y < h;
+  const bool valid = x < w && y < h;
+  uint32_t lo = 0xFFFFFFFFu, hi = 0u;
   if (valid) {
     const float* wt = c_t.gaborish[strength];
     const float v = Sym3(in + c * plane, w, h, x, y, wt[0], wt[1], wt[2]);
     out[c * plane + size_t(y) * w + x] = v;
-    o = OrderedBits(v);
+    lo = hi = OrderedBits(v);
   }
-  uint32_t lo = valid ? o : 0xFFFFFFFFu, hi = valid ? o : 0u;
   for (int off = 16; off; off >>= 1) {
     lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, off));
     hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, off));
   }
-  if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == 0 && mm) {
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  if ((t & 31) == 0) {
+    s_lo[t >> 5] = lo;
+    s_hi[t >> 5] = hi;
+  }
+  __syncthreads();
+  if (t == 0 && mm) {
+    for (int i = 1; i < 8; ++i) {
+      lo = min(lo, s_lo[i]);
+      hi = max(hi, s_hi[i]);
+    }
     atomicMin(&mm[c], lo);
     atomicMax(&mm[3 + c], hi);
   }
@@ -853,7 +898,10 @@ __global__ void __launch_bounds__(256)
       const float* base = f.ac + c * plane_ac + size_t(by) * g.ac_stride +
                           size_t(bx) * 64;
       s_c[i] = base[(e / chunk) * size_t(g.ac_stride) + e % chunk];
-      if (predict_hf) {
+      // DCT_NOHF shares this kernel with DCT but takes no HF prediction.
+      if (predict_hf && !PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) {
+        s_p[i] = 0.f;
+      } else if (predict_hf) {
         const int gi = (by >> 6) * g.Gx + (bx >> 6);
         const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
         const int X = (bx & 63) * 8 + e % N, Y = (by & 63) * 8 + e / N;
@@ -866,6 +914,10 @@ __global__ void __launch_bounds__(256)
       for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
         const int e = i % NN, y = e / N, x = e % N;
         if (y < 2 * cov && x < 2 * cov) continue;
+        const uint32_t pk = list[first + i / NN];
+        if (!PredictHFOf(f.acs[(pk >> 16) * g.Bx + (pk & 0xFFFF)] >> 4)) {
+          continue;
+        }
         s_c[i] += s_p[i];
       }
       __syncthreads();
@@ -1193,7 +1245,9 @@ __global__ void __launch_bounds__(256)
 // Clamp for DCT4X4 blocks.
 __global__ void __launch_bounds__(256)
     k_dct4_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
-              int count) {
+              const int* count_ptr) {
+  const int count = *count_ptr;
+  if (int(blockIdx.x) * 16 >= count) return;
   constexpr int NB = 16;
   __shared__ float s_a[16], s_b[16];
   __shared__ float s_blk[3][NB * 64];
@@ -1395,7 +1449,8 @@ __device__ void SmallForward(int type, const float* px, int ps, float* co) {
 }
 
 __global__ void k_small_ar(Geo g, DevFrame f, FrameScalars s,
-                           const uint32_t* list, int count) {
+                           const uint32_t* list, const int* count_ptr) {
+  const int count = *count_ptr;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const uint32_t pk = list[i];
@@ -1434,18 +1489,24 @@ __global__ void k_small_ar(Geo g, DevFrame f, FrameScalars s,
   }
 }
 
+}  // namespace pikgpu
+
+#include "square_kernels.cuh"
+
+namespace pikgpu {
+
 // Explicit instantiations.
-template __global__ void k_square_idct<8>(Geo, DevFrame, const uint32_t*, int,
-                                          int);
-template __global__ void k_square_idct<16>(Geo, DevFrame, const uint32_t*,
-                                           int, int);
-template __global__ void k_square_idct<32>(Geo, DevFrame, const uint32_t*,
-                                           int, int);
-template __global__ void k_square_ar<8>(Geo, DevFrame, FrameScalars,
-                                        const uint32_t*, int);
-template __global__ void k_square_ar<16>(Geo, DevFrame, FrameScalars,
-                                         const uint32_t*, int);
-template __global__ void k_square_ar<32>(Geo, DevFrame, FrameScalars,
-                                         const uint32_t*, int);
+template __global__ void k_square_idct_rows<8>(Geo, DevFrame, const uint32_t*,
+                                               int, int);
+template __global__ void k_square_idct_rows<16>(Geo, DevFrame,
+                                                const uint32_t*, int, int);
+template __global__ void k_square_idct_rows<32>(Geo, DevFrame,
+                                                const uint32_t*, int, int);
+template __global__ void k_square_ar_rows<8>(Geo, DevFrame, FrameScalars,
+                                             const uint32_t*, const int*);
+template __global__ void k_square_ar_rows<16>(Geo, DevFrame, FrameScalars,
+                                              const uint32_t*, const int*);
+template __global__ void k_square_ar_rows<32>(Geo, DevFrame, FrameScalars,
+                                              const uint32_t*, const int*);
 
 }  // namespace pikgpu

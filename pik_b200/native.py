@@ -63,6 +63,7 @@ def lib() -> ctypes.CDLL:
     L.pikgpu_kernel_name.restype = ctypes.c_char_p
     L.pikgpu_kernel_name.argtypes = [ctypes.c_int]
     L.pikgpu_set_stream.argtypes = [P, P]
+    L.pikgpu_last_launch_count.argtypes = [P]
     _lib = L
     return L
 
@@ -127,6 +128,9 @@ class Context:
 
     def reconstruct(self, *, linear: bool = True, srgb8: bool = False):
         f = self.frame
+        if f is None:  # let the library report the state error
+            self._check(self.L.pikgpu_reconstruct(self.h, None, 0, None, 0,
+                                                  0))
         lin = np.zeros((3, f.ysize, f.xsize), np.float32) if linear else None
         rgb = np.zeros((f.ysize, f.xsize, 3), np.uint8) if srgb8 else None
         self._check(self.L.pikgpu_reconstruct(

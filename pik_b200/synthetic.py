@@ -74,9 +74,17 @@ _DEFAULT_SHARES = {
 
 def make_frame(xsize: int, ysize: int, *, seed: int = 0,
                shares: dict | None = None, have_ar: bool = True,
-               gaborish: int = 2, global_scale: int = 2521,
-               quant_dc: int = 28, ac_scale: float = 1.0) -> "layout.Frame":
-    """Synthetic decoded frame of ``xsize`` x ``ysize`` pixels."""
+               gaborish: int = 2, global_scale: int = 3065,
+               quant_dc: int = 16, qf_median: float = 18.0,
+               qf_spread: float = 0.3, ac_scale: float = 1.0) -> "layout.Frame":
+    """Synthetic decoded frame of ``xsize`` x ``ysize`` pixels.
+
+    Defaults follow the reference encoder on the generator images at
+    butteraugli distance 1: global_scale 3065, quant_dc 16, raw quant field
+    log-normal around 18 (5th-95th percentile ~11-25), quantized DC of
+    X ~ -10 +- 20, Y ~ 240 +- 48, B ~ 0 +- 27, and sparse AC whose mean
+    magnitude falls off with frequency (Y dominant, X and B ~10x smaller).
+    """
     rng = np.random.default_rng(seed)
     shares = dict(_DEFAULT_SHARES if shares is None else shares)
     bx, by = -(-xsize // 8), -(-ysize // 8)
@@ -86,73 +94,77 @@ def make_frame(xsize: int, ysize: int, *, seed: int = 0,
     def place(size: int, code: int, share: float) -> None:
         if share <= 0:
             return
-        cells = by * bx
-        target = int(share * cells / (size * size))
+        target = int(share * by * bx / (size * size))
         ys = np.arange(0, by - size + 1, size)
         xs = np.arange(0, bx - size + 1, size)
-        if len(ys) == 0 or len(xs) == 0:
+        if len(ys) == 0 or len(xs) == 0 or target == 0:
             return
         cand = np.stack(np.meshgrid(ys, xs, indexing="ij"), -1).reshape(-1, 2)
         rng.shuffle(cand)
+        sub = (np.arange(size)[:, None] * size +
+               np.arange(size)[None, :]).astype(np.uint8)
         placed = 0
         for y0, x0 in cand:
             if placed >= target:
                 break
             if np.all(acs[y0:y0 + size, x0:x0 + size] == 0xFF):
-                for iy in range(size):
-                    for ix in range(size):
-                        acs[y0 + iy, x0 + ix] = (code << 4) | (iy * size + ix
-                                                               if size > 1 else 0)
+                acs[y0:y0 + size, x0:x0 + size] = (code << 4) | sub
                 placed += 1
 
     place(4, layout.ACS_TYPES["DCT32X32"], shares.pop("DCT32X32", 0.0))
     place(2, layout.ACS_TYPES["DCT16X16"], shares.pop("DCT16X16", 0.0))
-    single = [(layout.ACS_TYPES[k], v) for k, v in shares.items()]
+    single = [(layout.ACS_TYPES[k], v) for k, v in shares.items() if v > 0]
     free = acs == 0xFF
     codes = np.array([c for c, _ in single], dtype=np.uint8)
     p = np.array([v for _, v in single], dtype=np.float64)
-    p = p / p.sum()
-    pick = rng.choice(codes, size=int(free.sum()), p=p)
+    pick = rng.choice(codes, size=int(free.sum()), p=p / p.sum())
     acs[free] = (pick << 4).astype(np.uint8)
 
-    # Quant field: smooth log-normal around the median the encoder targets.
-    base = rng.normal(0.0, 0.25, size=(ty + 1, tx + 1))
-    qf = np.exp(np.kron(base, np.ones((8, 8)))[:by, :bx] +
-                rng.normal(0.0, 0.1, size=(by, bx)))
-    raw_qf = np.clip(np.round(qf * 5.0), 1, 256).astype(np.int32)
-    # Multi-block transforms share the first block's qf.
+    def smooth(shape, scale_blocks, amp):
+        sy, sx = shape
+        coarse = rng.normal(0.0, 1.0, size=(sy // scale_blocks + 2,
+                                            sx // scale_blocks + 2))
+        f = np.kron(coarse, np.ones((scale_blocks, scale_blocks)))[:sy, :sx]
+        return amp * f
+
+    qf = qf_median * np.exp(smooth((by, bx), 8, qf_spread) +
+                            rng.normal(0.0, 0.08, size=(by, bx)))
+    raw_qf = np.clip(np.round(qf), 6, 31).astype(np.int32)
     layout.broadcast_first_block(acs, raw_qf)
     lut = np.zeros((by, bx), dtype=np.uint8)
 
-    # DC: smooth image in quantized units.
-    yy, xx = np.mgrid[0:by, 0:bx].astype(np.float32)
     dc = np.zeros((3, by, bx), dtype=np.int16)
-    for c, (amp, off) in enumerate(((30.0, 0.0), (300.0, 600.0),
-                                    (200.0, 500.0))):
-        f = off + amp * np.sin(xx / (7.0 + 3 * c)) * np.cos(yy / (11.0 + c))
-        f += rng.normal(0.0, amp * 0.05, size=f.shape)
-        dc[c] = np.clip(np.round(f), -32000, 32000).astype(np.int16)
+    for c, (mean, sd) in enumerate(((-10.0, 20.0), (240.0, 48.0),
+                                    (0.0, 27.0))):
+        f = mean + smooth((by, bx), 16, sd * 0.8) + rng.normal(
+            0.0, sd * 0.3, size=(by, bx))
+        dc[c] = np.clip(np.round(f), -2000, 2000).astype(np.int16)
 
-    # AC: mostly zeros, Laplacian magnitudes falling with frequency.
+    # AC: per coefficient of each transform, mean magnitude falling with the
+    # coefficient's frequency (row + column, in 8-point units).
     k = np.arange(64)
-    freq = (k // 8) + (k % 8)
     ac = np.zeros((3, by, bx * 64), dtype=np.int16)
-    for c, strength in enumerate((0.35, 1.2, 0.6)):
-        lam = ac_scale * strength * np.exp(-0.35 * freq)
-        lam = np.tile(lam, bx)[None, :]
-        mag = rng.exponential(1.0, size=(by, bx * 64)) * lam
-        sign = rng.choice(np.array([-1, 1], dtype=np.int16), size=mag.shape)
-        vals = np.floor(mag).astype(np.int16) * sign
-        ac[c] = vals
-    ac[:, :, 0::64] = 0  # DC slots are filled from the DC image
-    ytox = np.full((ty, tx), 128, dtype=np.int32) + rng.integers(
-        -6, 7, size=(ty, tx)).astype(np.int32)
-    ytob = np.full((ty, tx), 120, dtype=np.int32) + rng.integers(
-        -6, 7, size=(ty, tx)).astype(np.int32)
+    freq = np.zeros((by, bx * 64), dtype=np.float32)
+    types = acs >> 4
+    blk = acs & 0xF
+    cov = np.where(types == 5, 4, np.where(types == 4, 2, 1))
+    # Position of each stored coefficient inside its (8c x 8c) matrix.
+    flat = blk[:, :, None].astype(np.int64) * 64 + k[None, None, :]
+    n = (8 * cov)[:, :, None]
+    row = flat // n
+    col = flat % n
+    freq = ((row + col) * 8.0 / n).reshape(by, bx * 64).astype(np.float32)
+    for c, amp in enumerate((0.12, 2.5, 0.25)):
+        mean = ac_scale * amp * np.exp(-freq / 1.6)
+        mag = np.floor(rng.exponential(1.0, size=freq.shape) * mean)
+        sign = np.where(rng.random(size=freq.shape) < 0.5, -1, 1)
+        ac[c] = np.clip(mag * sign, -2000, 2000).astype(np.int16)
+    ytox = (rng.integers(98, 129, size=(ty, tx))).astype(np.int32)
+    ytob = np.full((ty, tx), 120, dtype=np.int32)
     return layout.Frame(
         xsize=xsize, ysize=ysize, gaborish=gaborish, predict_lf=1,
         predict_hf=1, have_ar=int(have_ar), epf_enable_adaptive=1,
         epf_sigma=0, epf_use_sharpened=0, global_scale=global_scale,
-        quant_dc=quant_dc, ytox_dc=128, ytob_dc=120, ytox_map=ytox,
+        quant_dc=quant_dc, ytox_dc=130, ytob_dc=120, ytox_map=ytox,
         ytob_map=ytob, ac_strategy=acs, raw_quant_field=raw_qf,
         ar_sigma_lut_ids=lut, quantized_dc=dc, quantized_ac=ac)
