@@ -75,3 +75,32 @@ def frame_decisions(smoothed: np.ndarray, raw_qf: np.ndarray,
         scale[(acs >> 4) == t] = s
     quant = (raw_qf.astype(np.float32) * scale) * np.float32(0.039324273)
     return guide, sigma_from_quant(quant, stretch, lut_ids.astype(np.int64))
+
+
+def dc_decisions(frame):
+    """Decisions of AdaptiveDCReconstruction's EPF
+    (pik/adaptive_reconstruction.cc:300-318): guide over the dequantized DC
+    padded to a multiple of 8 by edge replication, one sigma for every block
+    (qf = quant_dc / 2, DCT strategy, LUT 0). The dequantized DC is formed
+    like DequantDC (pik/compressed_dc.cc:181-231) in float32."""
+    f32 = np.float32
+    inv_gs = f32(1.0 * 65536 / frame.global_scale)
+    inv_qdc = f32(inv_gs / f32(frame.quant_dc))
+    m0 = frame.dequant_table[frame.dequant_offsets[:3]].astype(np.float32)
+    mul = (m0 * inv_qdc).astype(np.float32)
+    q = frame.quantized_dc.astype(np.float32)
+    y = (q[1] * mul[1]).astype(np.float32)
+    ytox = f32(f32(frame.ytox_dc - 128) * f32(1.0 / 256))
+    ytob = f32(f32(frame.ytob_dc) * f32(1.0 / 128))
+    dc = np.stack([(ytox * y + (q[0] * mul[0]).astype(np.float32)),
+                   y, (ytob * y + (q[2] * mul[2]).astype(np.float32))]
+                  ).astype(np.float32)
+    by, bx = dc.shape[1:]
+    py, px = -(-by // 8) * 8, -(-bx // 8) * 8
+    pad = np.pad(dc, ((0, 0), (0, py - by), (0, px - bx)), mode="edge")
+    guide, stretch = guide_and_stretch(pad)
+    nb = (py // 8, px // 8)
+    quant = np.full(nb, np.float32(frame.quant_dc // 2), np.float32)
+    quant = (quant * np.float32(1.0)) * np.float32(0.039324273)
+    sigma = sigma_from_quant(quant, stretch, np.zeros(nb, np.int64))
+    return guide, sigma

@@ -298,9 +298,9 @@ void Mark(pikgpu_ctx* ctx, int i) {
 // ctx->mm already; sigma per block into `sig`.
 int RunEpf(pikgpu_ctx* ctx, const float* in, const float* guide_src, int w,
            int h, const int32_t* sig, float* out, const uint8_t* guide_ovr) {
-  dim3 grid(Blocks(w, kEpfTile), Blocks(h, kEpfTile));
-  k_epf<<<grid, 256, 0, ctx->stream>>>(in, guide_src, guide_ovr, w, h,
-                                       P<uint32_t>(ctx->mm), sig, out);
+  dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
+  k_epf_box<<<grid, kEpfThreads, 0, ctx->stream>>>(
+      in, guide_src, guide_ovr, w, h, P<uint32_t>(ctx->mm), sig, out);
   ++ctx->launches;
   return PIKGPU_OK;
 }

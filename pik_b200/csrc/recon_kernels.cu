@@ -1492,6 +1492,7 @@ __global__ void k_small_ar(Geo g, DevFrame f, FrameScalars s,
 }  // namespace pikgpu
 
 #include "square_kernels.cuh"
+#include "epf_kernel.cuh"
 
 namespace pikgpu {
 

@@ -167,9 +167,12 @@ def test_errors_leave_context_usable():
 
 @pytest.mark.skipif(not refpy.available("scalar"),
                     reason="reference build (oracle/_ref) not present")
-def test_4k_real_frame_against_reference():
+def test_4k_real_frame_against_reference_and_fp64():
     """The config-2 workload itself (3840x2160, reference-encoded at
-    distance 1) against the reference's reconstruction at full size."""
+    distance 1) at full size. With the reference's own EPF decisions the GPU
+    is within 2e-5 of the FP64 oracle everywhere; its few differences from
+    the reference beyond 2e-5 are pixels where the reference's FP32 result
+    is itself further than 2e-5 from FP64."""
     frame = layout.Frame.load(os.path.join(golden_cases.GOLDEN,
                                            "c2_4k_d1_frame.npz"))
     bs = open(os.path.join(golden_cases.GOLDEN, "c2_4k_d1.pik"), "rb").read()
@@ -182,8 +185,16 @@ def test_4k_real_frame_against_reference():
     g, s = decisions.frame_decisions(st["smoothed"], frame.raw_quant_field,
                                      frame.ac_strategy,
                                      frame.ar_sigma_lut_ids)
+    dg, ds = decisions.dc_decisions(frame)
     gpu2 = run_gpu(frame, guide=g, sigma=s, keep=False)
-    assert np.abs(gpu2["linear"] - st["linear"]).max() / 255 <= 2e-5
+    o64 = oraclepy.run(frame, precision=64, want=("linear",), guide=g,
+                       sigma=s, dc_guide=dg, dc_sigma=ds)["linear"]
+    err_gpu = np.abs(gpu2["linear"] - o64) / 255
+    err_ref = np.abs(st["linear"] - o64) / 255
+    assert err_gpu.max() <= 2e-5
+    diff = np.abs(gpu2["linear"] - st["linear"]) / 255
+    assert np.quantile(diff, 0.99999) <= 2e-5
+    assert np.all(err_ref[diff > 2e-5] > 2e-5)
     lsb = np.abs(gpu2["srgb8"].transpose(2, 0, 1).astype(np.int32) -
-                 golden_cases.srgb8_exact(st["linear"]))
+                 golden_cases.srgb8_exact(o64))
     assert lsb.max() <= 1
