@@ -18,8 +18,7 @@ NVCC_FLAGS = [
     "-fmad=false",
 ]
 SOURCES = ["pikgpu.cu"]
-DEPS = ["pikgpu.cu", "recon_kernels.cu", "kernels.cuh", "tables.h",
-        "tables.cc"]
+DEPS_EXT = (".cu", ".cuh", ".h", ".cc")
 
 
 def _nvcc() -> str:
@@ -33,7 +32,8 @@ def needs_build() -> bool:
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, d) for d in DEPS]
+    deps = [os.path.join(CSRC, d) for d in os.listdir(CSRC)
+            if d.endswith(DEPS_EXT)]
     deps.append(os.path.join(ROOT, "include", "pikgpu.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
