@@ -402,19 +402,28 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     if (n[kC8]) {
       k_square_idct_rows<8><<<rows_grid(3 * n[kC8], 8), kSquareThreads, 0,
                               st>>>(g, f, L[kC8], n[kC8], s.predict_hf);
+      ++ctx->launches;
     }
     if (n[kC16]) {
       k_square_idct_rows<16><<<rows_grid(3 * n[kC16], 16), kSquareThreads, 0,
                                st>>>(g, f, L[kC16], n[kC16], s.predict_hf);
+      ++ctx->launches;
     }
     if (n[kC32]) {
       k_square_idct_rows<32><<<rows_grid(3 * n[kC32], 32), kSquareThreads, 0,
                                st>>>(g, f, L[kC32], n[kC32], s.predict_hf);
+      ++ctx->launches;
     }
-    if (n[kC4]) k_dct4_idct<<<Blocks(n[kC4], 16), 256, 0, st>>>(
-        g, f, L[kC4], n[kC4], s.predict_hf);
-    if (n[kCSmall]) k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, st>>>(
-        g, f, L[kCSmall], n[kCSmall]);
+    if (n[kC4]) {
+      k_dct4_idct<<<Blocks(n[kC4], 16), 256, 0, st>>>(g, f, L[kC4], n[kC4],
+                                                      s.predict_hf);
+      ++ctx->launches;
+    }
+    if (n[kCSmall]) {
+      k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, st>>>(
+          g, f, L[kCSmall], n[kCSmall]);
+      ++ctx->launches;
+    }
   }
   const float* final_in = f.idct;
   Mark(ctx, kTGab1);
@@ -464,6 +473,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       k_active_blocks<<<Blocks(n[k], 256), 256, 0, st>>>(
           g, sig, f.acs, L[k], n[k], P<uint32_t>(ctx->active[k]),
           counters + k);
+      ++ctx->launches;
     }
     auto rows_grid = [](int items, int nn) {
       const int upw = 32 / nn;
@@ -473,21 +483,30 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     if (n[kC8]) {
       k_square_ar_rows<8><<<rows_grid(n[kC8], 8), kSquareThreads, 0, st>>>(
           g, f, s, P<uint32_t>(ctx->active[kC8]), counters + kC8);
+      ++ctx->launches;
     }
     if (n[kC16]) {
       k_square_ar_rows<16><<<rows_grid(n[kC16], 16), kSquareThreads, 0,
                              st>>>(g, f, s, P<uint32_t>(ctx->active[kC16]),
                                    counters + kC16);
+      ++ctx->launches;
     }
     if (n[kC32]) {
       k_square_ar_rows<32><<<rows_grid(n[kC32], 32), kSquareThreads, 0,
                              st>>>(g, f, s, P<uint32_t>(ctx->active[kC32]),
                                    counters + kC32);
+      ++ctx->launches;
     }
-    if (n[kC4]) k_dct4_ar<<<Blocks(n[kC4], 16), 256, 0, st>>>(
-        g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
-    if (n[kCSmall]) k_small_ar<<<Blocks(n[kCSmall], 64), 64, 0, st>>>(
-        g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
+    if (n[kC4]) {
+      k_dct4_ar<<<Blocks(n[kC4], 16), 256, 0, st>>>(
+          g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
+      ++ctx->launches;
+    }
+    if (n[kCSmall]) {
+      k_small_ar<<<Blocks(n[kCSmall], 64), 64, 0, st>>>(
+          g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
+      ++ctx->launches;
+    }
     final_in = f.filt;
   } else {
     Mark(ctx, kTEpf);
