@@ -319,6 +319,14 @@ def main():
         "lf_prediction": 0.5,
         "dc_dequant_epf": 0.2,
     }
+    # DRAM bytes per launch of the 4K workload measured with ncu
+    # (dram__bytes_read.sum + dram__bytes_write.sum, one cold launch each).
+    ncu_traffic_4k = {
+        "epf": 155.10e6 + 68.46e6,
+        "gaborish1_minmax": 99.54e6 + 64.64e6,
+        "gaborish2_opsin_srgb": 99.55e6 + 63.85e6,
+    }
+    traffic = ncu_traffic_4k.get(top) if px == 3840 * 2160 else None
     top_bytes = group_bytes.get(top, 12) * px
     achieved = top_bytes / (acc[top] * 1e-3) / 1e9
     if rank == 0:
@@ -338,7 +346,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": top,
                          "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": None, "peak_kind": peak_kind,
+                         "traffic": traffic, "peak_kind": peak_kind,
                          "path_achieved": round(
                              PATH_BYTES_PER_PX * px / (ms * 1e-3) / 1e9, 1),
                          "path_frac": round(PATH_BYTES_PER_PX * px /

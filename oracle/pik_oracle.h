@@ -15,7 +15,7 @@
  *     another run so that only arithmetic error is measured.
  *
  * Parity is pinned against the reference compiled from its own sources
- * (oracle/_ref/libpikref_*.so; tests/test_oracle_vs_reference.py) and
+ * (oracle/_ref/libpikref_*.so; tests/test_oracle_golden.py) and
  * against golden fixtures generated from it (tests/golden/).
  */
 #ifndef PIK_ORACLE_H_
