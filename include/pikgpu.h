@@ -207,6 +207,34 @@ int pikgpu_get_epf_decisions(pikgpu_ctx* ctx, uint8_t* guide, int32_t* sigma);
  * on; NULL restores the context's own stream. */
 int pikgpu_set_stream(pikgpu_ctx* ctx, void* stream);
 
+/* Allocation-free DC reconstruction. No counterpart in the reference: its
+ * DequantDC + AdaptiveDCReconstruction (pik/compressed_dc.cc:181-231,
+ * pik/adaptive_reconstruction.cc:300-332) allocate their images as they go.
+ * This call gives the same result as the DC stage of pikgpu_reconstruct
+ * (PIKGPU_STAGE_DC) for callers that must not allocate device memory when
+ * they reconstruct: it calls no allocating routine and keeps its
+ * intermediates in a static device array of about 6 MiB per device.
+ *  quantized_dc: device, 3 planes (X, Y, B) of ysize_blocks x xsize_blocks
+ *                int16, contiguous;
+ *  dc:           device, 3 planes of ysize_blocks x xsize_blocks floats,
+ *                contiguous (output; must not overlap quantized_dc);
+ *  dc_dequant:   host, DequantMatrix(0, DCT, c)[0] for c = 0..2;
+ *  global_scale, quant_dc, ytox_dc, ytob_dc: as in pikgpu_frame_params.
+ * Limit: xsize_blocks, ysize_blocks <= 512 (images up to 4096 x 4096);
+ * larger sizes fail with PIKGPU_ERR_INVALID_ARG. Runs on the current device,
+ * asynchronously on `stream` (a cudaStream_t; NULL = default stream). The
+ * first call on a device does a one-time set-up (table upload, scratch
+ * address lookup) and should come before any stream capture on it. All
+ * calls on a device share the scratch: calls that overlap in time on one
+ * device race and must be ordered on one stream or serialised. Writes the
+ * reason for a failure into `msg` (may be NULL). */
+int pikgpu_dc_reconstruct_noalloc(const int16_t* quantized_dc,
+                                  uint32_t xsize_blocks, uint32_t ysize_blocks,
+                                  int32_t global_scale, int32_t quant_dc,
+                                  const float dc_dequant[3], int32_t ytox_dc,
+                                  int32_t ytob_dc, float* dc, void* stream,
+                                  char* msg, size_t msg_size);
+
 #ifdef __cplusplus
 }
 #endif

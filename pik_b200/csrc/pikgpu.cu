@@ -1014,3 +1014,5 @@ const char* pikgpu_kernel_name(int index) {
 }
 
 }  // extern "C"
+
+#include "dc_noalloc.cu"

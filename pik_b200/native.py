@@ -64,6 +64,9 @@ def lib() -> ctypes.CDLL:
     L.pikgpu_kernel_name.argtypes = [ctypes.c_int]
     L.pikgpu_set_stream.argtypes = [P, P]
     L.pikgpu_last_launch_count.argtypes = [P]
+    L.pikgpu_dc_reconstruct_noalloc.argtypes = [
+        P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
+        P, ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_char_p, S]
     _lib = L
     return L
 
@@ -74,6 +77,23 @@ def validate(frame: layout.Frame) -> tuple[int, str]:
     buf = ctypes.create_string_buffer(512)
     rc = lib().pikgpu_validate(packed.ref, buf, 512)
     return rc, buf.value.decode()
+
+
+def dc_reconstruct_noalloc(qdc_ptr: int, xsize_blocks: int,
+                           ysize_blocks: int, global_scale: int,
+                           quant_dc: int, dc_dequant, ytox_dc: int,
+                           ytob_dc: int, dc_ptr: int, stream: int = 0) -> None:
+    """pikgpu_dc_reconstruct_noalloc on device buffers (3 contiguous int16
+    planes in, 3 contiguous float planes out) on the current device."""
+    mul = np.ascontiguousarray(dc_dequant, np.float32)
+    assert mul.shape == (3,)
+    buf = ctypes.create_string_buffer(512)
+    rc = lib().pikgpu_dc_reconstruct_noalloc(
+        qdc_ptr or None, xsize_blocks, ysize_blocks, global_scale, quant_dc,
+        mul.ctypes.data, ytox_dc, ytob_dc, dc_ptr or None, stream or None,
+        buf, 512)
+    if rc != OK:
+        raise PikGpuError(rc, buf.value.decode())
 
 
 def _planes(arrs) -> ctypes.Array:
