@@ -26,7 +26,8 @@
 //    the min/max words with a kernel, then fully writes the padded images
 //    and sigmas before it reads them.
 //  * The first call on a device does the set-up, with that device current:
-//    it uploads the constant tables and looks up the scratch address. Make
+//    it uploads the constant tables, sets the EPF kernel's shared-memory
+//    limit and looks up the scratch address. Make
 //    that first call before any stream capture on the device.
 //  * All calls on one device share the scratch. Calls that overlap in time
 //    on the same device (other streams, or host threads without ordering)
@@ -164,8 +165,9 @@ int DcNoAlloc(pikgpu_ctx* ctx, const int16_t* quantized_dc, uint32_t bx,
       dcpad, size_t(dpw) * dph, mm);
   k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, nullptr, nullptr, nullptr,
                                                s.quant_dc / 2, mm, sig);
-  k_epf_box<<<dim3(Blocks(dpw, kEpfW), Blocks(dph, kEpfH)), kEpfThreads, 0,
-              st>>>(dcpad, dcpad, nullptr, dpw, dph, mm, sig, dcfilt);
+  k_epf_box<<<dim3(Blocks(dpw, kEpfW), Blocks(dph, kEpfH)), kEpfThreads,
+              kEpfSmemBytes, st>>>(dcpad, dcpad, nullptr, dpw, dph, mm, sig,
+                                   dcfilt);
   dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
   k_dc_clamp<<<gr2, b, 0, st>>>(dc, dcfilt, g.Bx, g.By, dpw, dph,
                                 half_step[0], half_step[1], half_step[2]);

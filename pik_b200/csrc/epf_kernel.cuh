@@ -1,69 +1,92 @@
 // Edge-preserving filter (AdaptiveFilter + WeightedSum,
-// pik/epf_target.cc:526-801, 1113-1278) with packed-byte box sums.
+// pik/epf_target.cc:526-801, 1113-1278) on packed guide bytes.
 //
-// One CTA filters a 64 x 32 pixel tile; each thread owns a 4 x 2 pixel
-// micro-tile (inside one 8 x 8 block, so sigma is uniform per thread). For
-// every displacement (cy, cx) of the 7 x 8 neighbourhood and every channel,
-// the 3 x 4 patch SADs of the micro-tile's 16 pixels are formed from packed
-// u8 guide words: byte-wise |ref - window| (__vabsdiffu4) over the 7
-// columns x-1 .. x+5 of the four patch rows, horizontal 4-sums by __dp4a on
-// funnel-shifted words, then vertical 3-sums. The SADs are exact integers;
-// weights and the weighted sums follow the reference's neighbour order
-// (cy = -3..3, cx = -3..4) with separately rounded products and sums, so
-// the output equals the per-pixel formulation bit for bit.
+// One CTA filters a 64 x 32 pixel tile with 8 warps. Lane l of warp w owns
+// the pixels (x0 + l + 32 i, y0 + 4 w + j), i = 0..1, j = 0..3: two columns
+// 32 apart (so the 32 lanes of a warp read 32 consecutive values of every
+// shared-memory row), four rows inside one 8x8 block row.
+//
+// The u8 guide is staged in shared memory as four copies, copy s holding at
+// word k the bytes 4k + s .. 4k + s + 3 of the row. The 4 guide bytes of a
+// patch row at any byte offset are then one 32-bit load, and the sum of
+// absolute differences against the centre pixel's patch row is one
+// __vsadu4. For every displacement (cy, cx) of the 7 x 8 neighbourhood and
+// every channel, a lane forms the 6 patch-row SADs of each of its columns and
+// sums them vertically into the 3 x 4 patch SADs of its 4 rows; the SAD is
+// the maximum over the channels. The SADs are exact integers; the weights
+// (WeightFast's bit construction) and the weighted sums follow the
+// reference's neighbour order (cy = -3..3, cx = -3..4) with separately
+// rounded products and sums, so the output equals the per-pixel formulation
+// bit for bit.
 // Included by recon_kernels.cu.
 #pragma once
 
 namespace pikgpu {
 
-constexpr int kEpfW = 64, kEpfH = 32;      // output tile
-constexpr int kEpfGW = kEpfW + 16;         // guide bytes: x0 - 8 .. x0 + 71
-constexpr int kEpfGWords = kEpfGW / 4;     // 20 words per guide row
-constexpr int kEpfGH = kEpfH + 8;          // guide rows: y0 - 4 .. y0 + 35
-constexpr int kEpfIW = kEpfW + 8;          // in cols: x0 - 3 .. x0 + 68
-constexpr int kEpfIH = kEpfH + 6;          // in rows: y0 - 3 .. y0 + 34
-constexpr int kEpfMH = 2;                  // micro-tile rows
-constexpr int kEpfThreads = 16 * (kEpfH / kEpfMH);
+constexpr int kEpfW = 64, kEpfH = 32;   // output tile
+constexpr int kEpfThreads = 256;
+constexpr int kEpfGH = kEpfH + 8;       // guide rows: y0 - 4 .. y0 + 35
+constexpr int kEpfGWords = 20;          // guide bytes x0 - 8 .. x0 + 71
+// Words per shifted copy; = 8 (mod 32), so that the 32 lanes' loads of 32
+// consecutive byte offsets fall in (at most one pair excepted) distinct banks.
+constexpr int kEpfCopyWords = kEpfGH * kEpfGWords + 8;
+constexpr int kEpfIW = kEpfW + 8;       // input cols: x0 - 3 .. x0 + 68
+constexpr int kEpfIH = kEpfH + 6;       // input rows: y0 - 3 .. y0 + 34
+constexpr size_t kEpfGuideWords = size_t(3) * 4 * kEpfCopyWords;
+constexpr size_t kEpfSmemBytes =
+    kEpfGuideWords * 4 + size_t(3) * kEpfIH * kEpfIW * 4;
 
-__device__ __forceinline__ uint32_t Shr8(uint32_t lo, uint32_t hi, int sh) {
-  // Bytes sh .. sh+3 of the 8-byte little-endian pair (hi:lo).
-  return sh == 0 ? lo : __funnelshift_r(lo, hi, 8 * sh);
+// WeightFast (pik/epf_target.cc:304-428) as 4 integer operations:
+// ((int16(min(sad, 507) << 6) * mul) >> 16 + (127 << 7)) in the high half of
+// a float equals ((min(sad, 507) * 64 mul) & 0xFFFF0000) + 0x3F800000 for
+// every sad >= 0 and -32768 <= mul < 0 (the product fits in int32).
+__device__ __forceinline__ float EpfWeight(int mul64, int sad) {
+  const int t = min(sad, 507) * mul64;
+  return __uint_as_float((uint32_t(t) & 0xFFFF0000u) + 0x3F800000u);
 }
 
-__global__ void __launch_bounds__(kEpfThreads)
+__global__ void __launch_bounds__(kEpfThreads, 2)
     k_epf_box(const float* in, const float* guide_src,
               const uint8_t* guide_ovr, int w, int h, const uint32_t* mm,
               const int32_t* sigma, float* out) {
-  // One spare word per row: the last window read may touch it (unused).
-  __shared__ uint32_t sg[3][kEpfGH][kEpfGWords + 1];
-  __shared__ float si[3][kEpfIH][kEpfIW];
+  extern __shared__ __align__(16) uint32_t epf_smem[];
+  uint32_t* sg = epf_smem;  // [3][4][kEpfCopyWords]
+  float(*si)[kEpfIH][kEpfIW] =
+      reinterpret_cast<float(*)[kEpfIH][kEpfIW]>(epf_smem + kEpfGuideWords);
   const int x0 = blockIdx.x * kEpfW, y0 = blockIdx.y * kEpfH;
   const int tid = threadIdx.x;
+  const int lane = tid & 31, wp = tid >> 5;
   const size_t plane = size_t(w) * h;
   const int bw = w / 8;
-  const int tx = tid & 15, ty = tid >> 4;  // micro-tile column / row
-  const int px = x0 + 4 * tx, py = y0 + kEpfMH * ty;
-  const bool inside = px < w && py < h;
-  const int sig = inside ? sigma[(py >> 3) * bw + (px >> 3)] : 0;
-  const bool filtered = sig >= kMinSigma;
+  const int py0 = y0 + 4 * wp;  // first row; w and h are multiples of 8
+  bool inside[2], filtered[2];
+  int sig[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int px = x0 + lane + 32 * i;
+    inside[i] = px < w && py0 < h;
+    sig[i] = inside[i] ? sigma[(py0 >> 3) * bw + (px >> 3)] : 0;
+    filtered[i] = sig[i] >= kMinSigma;
+  }
 
   // Tiles without filtered blocks are copies (CopyOriginalBlock).
-  if (!__syncthreads_or(filtered)) {
-    if (inside) {
-      for (int c = 0; c < 3; ++c) {
-        for (int j = 0; j < kEpfMH; ++j) {
-          const size_t o = c * plane + size_t(py + j) * w + px;
-          *reinterpret_cast<float4*>(out + o) =
-              *reinterpret_cast<const float4*>(in + o);
+  if (!__syncthreads_or(filtered[0] || filtered[1])) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      if (!inside[i]) continue;
+      const int px = x0 + lane + 32 * i;
+      for (int c = 0; c < 3; ++c)
+        for (int j = 0; j < 4; ++j) {
+          const size_t o = c * plane + size_t(py0 + j) * w + px;
+          out[o] = in[o];
         }
-      }
     }
     return;
   }
 
   float amin, mul, stretch;
   GuideParams(mm, &amin, &mul, &stretch);
-  // u8 guide (MakeGuide, pik/epf_target.cc:1009-1070), 4 bytes per word.
+  // u8 guide (MakeGuide, pik/epf_target.cc:1009-1070) into copy 0.
   for (int i = tid; i < 3 * kEpfGH * kEpfGWords; i += kEpfThreads) {
     const int c = i / (kEpfGH * kEpfGWords);
     const int r = (i / kEpfGWords) % kEpfGH, wd = i % kEpfGWords;
@@ -83,7 +106,7 @@ __global__ void __launch_bounds__(kEpfThreads)
       }
       word |= v << (8 * b);
     }
-    sg[c][r][wd] = word;
+    sg[(c * 4) * kEpfCopyWords + r * kEpfGWords + wd] = word;
   }
   for (int i = tid; i < 3 * kEpfIH * kEpfIW; i += kEpfThreads) {
     const int c = i / (kEpfIH * kEpfIW);
@@ -93,108 +116,118 @@ __global__ void __launch_bounds__(kEpfThreads)
         in[c * plane + size_t(MirrorIdx(gy, h)) * w + MirrorIdx(gx, w)];
   }
   __syncthreads();
+  // Copies 1..3: byte-shifted words of copy 0.
+  for (int i = tid; i < 3 * 3 * kEpfGH * kEpfGWords; i += kEpfThreads) {
+    const int c = i / (3 * kEpfGH * kEpfGWords);
+    const int s = 1 + (i / (kEpfGH * kEpfGWords)) % 3;
+    const int rk = i % (kEpfGH * kEpfGWords), k = rk % kEpfGWords;
+    const uint32_t* c0 = sg + (c * 4) * kEpfCopyWords;
+    const uint32_t lo = c0[rk];
+    const uint32_t hi = k + 1 < kEpfGWords ? c0[rk + 1] : 0u;
+    sg[(c * 4 + s) * kEpfCopyWords + rk] = __funnelshift_r(lo, hi, 8 * s);
+  }
+  __syncthreads();
 
-  // Warps (one block row of 8 blocks) without filtered blocks copy.
-  if (!__any_sync(0xFFFFFFFFu, filtered)) {
-    if (inside) {
-      for (int c = 0; c < 3; ++c) {
-        for (int j = 0; j < kEpfMH; ++j) {
-          float* o = out + c * plane + size_t(py + j) * w + px;
-          const float* s = &si[c][kEpfMH * ty + j + 3][4 * tx + 3];
-          o[0] = s[0], o[1] = s[1], o[2] = s[2], o[3] = s[3];
-        }
-      }
+  // Warps (half a block row of 8 blocks) without filtered blocks copy.
+  if (!__any_sync(0xFFFFFFFFu, filtered[0] || filtered[1])) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      if (!inside[i]) continue;
+      const int px = x0 + lane + 32 * i;
+      for (int c = 0; c < 3; ++c)
+        for (int j = 0; j < 4; ++j)
+          out[c * plane + size_t(py0 + j) * w + px] =
+              si[c][4 * wp + j + 3][lane + 32 * i + 3];
     }
     return;
   }
-  const int m = c_t.mul_table[filtered ? sig : kMinSigma];
+  int m64[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    m64[i] = c_t.mul_table[filtered[i] ? sig[i] : kMinSigma] * 64;
+  }
 
-  // Reference words: rows py-1 .. py+MH, bytes px-4 .. px+7 (words tx+1..3).
-  constexpr int R = kEpfMH + 2, NP = 4 * kEpfMH;
-  const int gr0 = kEpfMH * ty + 3;  // smem guide row of py - 1
-  uint32_t ref[3][R][3];
+  // Centre patch rows: guide rows py0 - 1 .. py0 + 4, bytes px - 1 .. px + 2.
+  const int gr0 = 4 * wp + 3;  // guide smem row of py0 - 1
+  uint32_t ref[3][6][2];
+  {
+    const int off = lane + 7;  // byte offset of px - 1 from x0 - 8 (i = 0)
+    const uint32_t* g = sg + (off & 3) * kEpfCopyWords + gr0 * kEpfGWords +
+                        (off >> 2);
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
+    for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int r = 0; r < R; ++r)
+      for (int r = 0; r < 6; ++r)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) ref[c][r][k] = sg[c][gr0 + r][tx + 1 + k];
+        for (int i = 0; i < 2; ++i)
+          ref[c][r][i] =
+              g[c * 4 * kEpfCopyWords + r * kEpfGWords + 8 * i];
+  }
 
-  float ws[3][NP], sw[NP];
+  float ws[3][8], sw[8];
 #pragma unroll
-  for (int p = 0; p < NP; ++p) {
+  for (int p = 0; p < 8; ++p) {
     ws[0][p] = ws[1][p] = ws[2][p] = 0.f;
     sw[p] = 0.f;
   }
 #pragma unroll 1
   for (int cy = -3; cy <= 3; ++cy) {
-#pragma unroll 2
+#pragma unroll 1
     for (int cx = -3; cx <= 4; ++cx) {
-      // Window byte offset of column px - 4 + cx from the row start.
-      const int o = 4 * tx + 4 + cx;
-      const int k = o >> 2;
-      const int sh = (cx + 4) & 3;
-      int sad[NP];
+      const int off = lane + 7 + cx;  // window byte offset (i = 0)
+      const uint32_t* g = sg + (off & 3) * kEpfCopyWords +
+                          (gr0 + cy) * kEpfGWords + (off >> 2);
+      int sad[8];  // [j * 2 + i]
 #pragma unroll
-      for (int p = 0; p < NP; ++p) sad[p] = 0;
+      for (int p = 0; p < 8; ++p) sad[p] = 0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        int hs[R][4];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const uint32_t* row = sg[c][gr0 + r + cy];
-          const uint32_t w0 = row[k], w1 = row[k + 1], w2 = row[k + 2],
-                         w3 = row[k + 3];
-          const uint32_t da = __vabsdiffu4(ref[c][r][0], Shr8(w0, w1, sh));
-          const uint32_t db = __vabsdiffu4(ref[c][r][1], Shr8(w1, w2, sh));
-          const uint32_t dc = __vabsdiffu4(ref[c][r][2], Shr8(w2, w3, sh));
-          hs[r][0] = (int)__dp4a((unsigned)__funnelshift_r(da, db, 24), 0x01010101u, 0u);
-          hs[r][1] = (int)__dp4a((unsigned)db, 0x01010101u, 0u);
-          hs[r][2] = (int)__dp4a((unsigned)__funnelshift_r(db, dc, 8), 0x01010101u, 0u);
-          hs[r][3] = (int)__dp4a((unsigned)__funnelshift_r(db, dc, 16), 0x01010101u, 0u);
-        }
+        for (int i = 0; i < 2; ++i) {
+          int hs[6];
 #pragma unroll
-        for (int j = 0; j < kEpfMH; ++j)
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int s = hs[j][i] + hs[j + 1][i] + hs[j + 2][i];
-            sad[j * 4 + i] = max(sad[j * 4 + i], s);
+          for (int r = 0; r < 6; ++r) {
+            hs[r] = int(__vsadu4(
+                ref[c][r][i],
+                g[c * 4 * kEpfCopyWords + r * kEpfGWords + 8 * i]));
           }
+          const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
+          sad[0 + i] = max(sad[0 + i], hs[0] + p12);
+          sad[2 + i] = max(sad[2 + i], p12 + hs[3]);
+          sad[4 + i] = max(sad[4 + i], hs[2] + p34);
+          sad[6 + i] = max(sad[6 + i], p34 + hs[5]);
+        }
       }
 #pragma unroll
-      for (int j = 0; j < kEpfMH; ++j) {
-        const int ir = kEpfMH * ty + j + 3 + cy;
-        const float* i0 = &si[0][ir][4 * tx + 3 + cx];
-        const float* i1 = &si[1][ir][4 * tx + 3 + cx];
-        const float* i2 = &si[2][ir][4 * tx + 3 + cx];
+      for (int j = 0; j < 4; ++j) {
+        const int ir = 4 * wp + j + 3 + cy;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int p = j * 4 + i;
-          float wgt = WeightFast(m, sad[p]);
+        for (int i = 0; i < 2; ++i) {
+          const int p = j * 2 + i;
+          const int col = lane + 32 * i + 3 + cx;
+          float wgt = EpfWeight(m64[i], sad[p]);
           if (!(wgt >= 0.05f)) wgt = 0.0f;
-          ws[0][p] += i0[i] * wgt;
-          ws[1][p] += i1[i] * wgt;
-          ws[2][p] += i2[i] * wgt;
+          ws[0][p] += si[0][ir][col] * wgt;
+          ws[1][p] += si[1][ir][col] * wgt;
+          ws[2][p] += si[2][ir][col] * wgt;
           sw[p] += wgt;
         }
       }
     }
   }
-  if (!inside) return;
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
+  for (int i = 0; i < 2; ++i) {
+    if (!inside[i]) continue;
+    const int px = x0 + lane + 32 * i;
 #pragma unroll
-    for (int j = 0; j < kEpfMH; ++j) {
-      float v[4];
+    for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int p = j * 4 + i;
-        v[i] = filtered ? ws[c][p] / sw[p]
-                        : si[c][kEpfMH * ty + j + 3][4 * tx + 3 + i];
+      for (int j = 0; j < 4; ++j) {
+        const int p = j * 2 + i;
+        out[c * plane + size_t(py0 + j) * w + px] =
+            filtered[i] ? ws[c][p] / sw[p]
+                        : si[c][4 * wp + j + 3][lane + 32 * i + 3];
       }
-      *reinterpret_cast<float4*>(out + c * plane + size_t(py + j) * w + px) =
-          make_float4(v[0], v[1], v[2], v[3]);
-    }
   }
 }
 

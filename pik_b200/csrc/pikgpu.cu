@@ -284,6 +284,9 @@ int UploadTables(pikgpu_ctx* ctx) {
   DevTables t;
   BuildTables(&t);
   CUDA_TRY(ctx, cudaMemcpyToSymbol(c_t, &t, sizeof(t)));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_epf_box, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(kEpfSmemBytes)));
   if (ctx->device < 64) g_tables_uploaded[ctx->device] = true;
   return PIKGPU_OK;
 }
@@ -299,7 +302,7 @@ void Mark(pikgpu_ctx* ctx, int i) {
 int RunEpf(pikgpu_ctx* ctx, const float* in, const float* guide_src, int w,
            int h, const int32_t* sig, float* out, const uint8_t* guide_ovr) {
   dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
-  k_epf_box<<<grid, kEpfThreads, 0, ctx->stream>>>(
+  k_epf_box<<<grid, kEpfThreads, kEpfSmemBytes, ctx->stream>>>(
       in, guide_src, guide_ovr, w, h, P<uint32_t>(ctx->mm), sig, out);
   ++ctx->launches;
   return PIKGPU_OK;
@@ -415,7 +418,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       ++ctx->launches;
     }
     if (n[kC4]) {
-      k_dct4_idct<<<Blocks(n[kC4], 16), 256, 0, st>>>(g, f, L[kC4], n[kC4],
+      k_dct4_idct<<<Blocks(n[kC4], kDct4Blocks), 256, 0, st>>>(g, f, L[kC4], n[kC4],
                                                       s.predict_hf);
       ++ctx->launches;
     }
@@ -432,10 +435,10 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     const float* guide_src = f.idct;
     k_minmax_init<<<1, 32, 0, st>>>(mm); ++ctx->launches;
     if (s.gaborish) {
-      dim3 b(32, 8), gr(Blocks(g.PW, 32), Blocks(g.PH, 8), 3);
-      k_gaborish_minmax<<<gr, b, 0, st>>>(f.idct, g.PW, g.PH, s.gaborish,
-                                          f.smoothed,
-                                          s.use_sharpened ? nullptr : mm); ++ctx->launches;
+      dim3 gr(Blocks(g.PW, kStripW), Blocks(g.PH, kStripH), 3);
+      k_gaborish_strips<<<gr, kStripThreads, 0, st>>>(
+          f.idct, g.PW, g.PH, s.gaborish, f.smoothed,
+          s.use_sharpened ? nullptr : mm); ++ctx->launches;
       if (!s.use_sharpened) guide_src = f.smoothed;
     }
     if (guide_src == f.idct) {
@@ -498,12 +501,13 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       ++ctx->launches;
     }
     if (n[kC4]) {
-      k_dct4_ar<<<Blocks(n[kC4], 16), 256, 0, st>>>(
+      k_dct4_ar<<<Blocks(n[kC4], kDct4Blocks), 256, 0, st>>>(
           g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
       ++ctx->launches;
     }
     if (n[kCSmall]) {
-      k_small_ar<<<Blocks(n[kCSmall], 64), 64, 0, st>>>(
+      k_small_ar<<<Blocks(n[kCSmall], kSmallArBlocks), 3 * kSmallArBlocks, 0,
+                   st>>>(
           g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
       ++ctx->launches;
     }
@@ -514,11 +518,13 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   }
   Mark(ctx, kTFinal);
   {
-    dim3 b(32, 8), gr(Blocks(g.W, 32), Blocks(g.H, 8));
-    k_final<<<gr, b, 0, st>>>(final_in, g.PW, g.PH, g.W, g.H, s.gaborish,
-                              ctx->keep_stages ? P<float>(ctx->dbg_pre)
-                                               : nullptr,
-                              lin, lin_stride, rgb8, rgb8_stride); ++ctx->launches;
+    const int vec_lin = lin && lin_stride % 4 == 0 && g.W % 4 == 0 &&
+                        reinterpret_cast<uintptr_t>(lin) % 16 == 0;
+    dim3 gr(Blocks(g.W, kStripW), Blocks(g.H, kStripH));
+    k_final_strips<<<gr, kStripThreads, 0, st>>>(
+        final_in, g.PW, g.PH, g.W, g.H, s.gaborish,
+        ctx->keep_stages ? P<float>(ctx->dbg_pre) : nullptr, lin, lin_stride,
+        vec_lin, rgb8, rgb8_stride); ++ctx->launches;
   }
   Mark(ctx, kNumTimed);
   CUDA_TRY(ctx, cudaGetLastError());

@@ -482,67 +482,10 @@ __global__ void k_export_guide(const float* src, int w, int h,
 }
 
 // ---------------------------------------------------------------------------
-// Gaborish / symmetric 3x3 convolution with mirrored borders
-// (ConvolveT<Symmetric3>, pik/convolve.h:500-629).
-__device__ __forceinline__ float Sym3(const float* p, int w, int h, int x,
-                                      int y, float w0, float w1, float w2) {
-  const float* t = p + size_t(MirrorIdx(y - 1, h)) * w;
-  const float* m = p + size_t(y) * w;
-  const float* b = p + size_t(MirrorIdx(y + 1, h)) * w;
-  const int xl = MirrorIdx(x - 1, w), xr = MirrorIdx(x + 1, w);
-  const float sum_tb = t[x] + b[x];
-  const float mul0 = m[x] * w0;
-  const float sum_lr = m[xl] + m[xr];
-  const float x1 = sum_tb + sum_lr;
-  const float mul1 = x1 * w1 + mul0;
-  const float sum_t2 = t[xl] + t[xr];
-  const float sum_b2 = b[xl] + b[xr];
-  const float x2 = sum_t2 + sum_b2;
-  return x2 * w2 + mul1;
-}
-
-// ConvolveGaborish (pik/gaborish.cc:137-159) plus min/max of the result,
-// reduced per CTA (256 threads) before one atomic per channel.
-__global__ void __launch_bounds__(256)
-    k_gaborish_minmax(const float* in, int w, int h, int strength, float* out,
-                      uint32_t* mm) {
-  __shared__ uint32_t s_lo[8], s_hi[8];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int c = blockIdx.z;
-  const size_t plane = size_t(w) * h;
-  const bool valid = x < w && y < h;
-  uint32_t lo = 0xFFFFFFFFu, hi = 0u;
-  if (valid) {
-    const float* wt = c_t.gaborish[strength];
-    const float v = Sym3(in + c * plane, w, h, x, y, wt[0], wt[1], wt[2]);
-    out[c * plane + size_t(y) * w + x] = v;
-    lo = hi = OrderedBits(v);
-  }
-  for (int off = 16; off; off >>= 1) {
-    lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, off));
-    hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, off));
-  }
-  const int t = threadIdx.y * blockDim.x + threadIdx.x;
-  if ((t & 31) == 0) {
-    s_lo[t >> 5] = lo;
-    s_hi[t >> 5] = hi;
-  }
-  __syncthreads();
-  if (t == 0 && mm) {
-    for (int i = 1; i < 8; ++i) {
-      lo = min(lo, s_lo[i]);
-      hi = max(hi, s_hi[i]);
-    }
-    atomicMin(&mm[c], lo);
-    atomicMax(&mm[3 + c], hi);
-  }
-}
-
-// Final stage: gaborish #2 (or copy), ShrinkTo(xsize, ysize), XybToRgb
-// (pik/opsin_inverse.cc:38-123), optional sRGB-8 (TF_SRGB +
-// ExternalImage::CopyTo rounding). Also writes the pre-opsin planes for the
-// stage export when `pre` != nullptr.
+// sRGB-8 of one linear value on the 0..255 scale: TF_SRGB's rational
+// polynomial (pik/color_management.cc:323-345) and the rounding of
+// ExternalImage::CopyTo (pik/external_image.cc:1205). The gaborish / opsin
+// stencil kernels are in stencil_kernels.cuh.
 __device__ __forceinline__ uint8_t Srgb8(float lin255) {
   const float x = lin255 * (1.0f / 255);
   const float a = fabsf(x);
@@ -562,49 +505,6 @@ __device__ __forceinline__ uint8_t Srgb8(float lin255) {
   const float cl = fminf(fmaxf(0.0f, e), 1.0f);
   const float sample = cl * 255.0f + 0.0f;
   return uint8_t(int(sample + 0.5f));
-}
-
-__global__ void k_final(const float* in, int pw, int ph, int w, int h,
-                        int strength, float* pre, float* lin, size_t lin_stride,
-                        uint8_t* rgb8, size_t rgb8_stride) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= w || y >= h) return;
-  const size_t plane = size_t(pw) * ph;
-  float v[3];
-  for (int c = 0; c < 3; ++c) {
-    if (strength) {
-      const float* wt = c_t.gaborish[strength];
-      v[c] = Sym3(in + c * plane, pw, ph, x, y, wt[0], wt[1], wt[2]);
-    } else {
-      v[c] = in[c * plane + size_t(y) * pw + x];
-    }
-    if (pre) pre[(size_t(c) * h + y) * w + x] = v[c];
-  }
-  const float* m = c_t.opsin_inv;
-  const float gr = 1.0f * (v[1] + v[0]);
-  const float gg = 1.0f * (v[1] - v[0]);
-  const float gb = v[2];
-  const float mr = gr * gr * gr + c_t.opsin_neg_bias[0];
-  const float mg = gg * gg * gg + c_t.opsin_neg_bias[1];
-  const float mb = gb * gb * gb + c_t.opsin_neg_bias[2];
-  float lr = m[0] * mr, lg = m[3] * mr, lb = m[6] * mr;
-  const float tr = m[1] * mg, tg = m[4] * mg, tb = m[7] * mg;
-  lr = m[2] * mb + lr;
-  lg = m[5] * mb + lg;
-  lb = m[8] * mb + lb;
-  const float r = lr + tr, g = lg + tg, b = lb + tb;
-  if (lin) {
-    lin[0 * lin_stride * h + size_t(y) * lin_stride + x] = r;
-    lin[1 * lin_stride * h + size_t(y) * lin_stride + x] = g;
-    lin[2 * lin_stride * h + size_t(y) * lin_stride + x] = b;
-  }
-  if (rgb8) {
-    uint8_t* o = rgb8 + size_t(y) * rgb8_stride + 3 * size_t(x);
-    o[0] = Srgb8(r);
-    o[1] = Srgb8(g);
-    o[2] = Srgb8(b);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -808,6 +708,8 @@ __global__ void k_lf_update(Geo g, DevFrame f, int predict_lf,
   }
 }
 
+constexpr int kDct4Blocks = 4;  // DCT4X4 blocks per CTA (x 64 coefficients)
+
 // ---------------------------------------------------------------------------
 // Cooperative batched transforms in shared memory. `nb` blocks of n x n,
 // contiguous in smem; T threads; every thread calls __syncthreads.
@@ -936,11 +838,12 @@ __global__ void __launch_bounds__(256)
 
 // DCT4X4 (and _NOHF): four 4x4 transforms with interleaved coefficients
 // (AcStrategy::TransformFromPixels/ToPixels, pik/ac_strategy.cc:604-629,
-// 762-790). 16 blocks per CTA (64 sub-blocks of 4x4).
+// 762-790). kDct4Blocks blocks per CTA, one thread per coefficient: few
+// blocks per CTA spread the (few) DCT4X4 blocks of a frame over many SMs.
 __global__ void __launch_bounds__(256)
     k_dct4_idct(Geo g, DevFrame f, const uint32_t* list, int count,
                 int predict_hf) {
-  constexpr int NB = 16;
+  constexpr int NB = kDct4Blocks;
   __shared__ float s_a[16], s_b[16];
   __shared__ float s_c[NB * 64], s_p[NB * 64], s_t[NB * 64], s_q[NB * 64];
   if (threadIdx.x < 16) {
@@ -1247,8 +1150,8 @@ __global__ void __launch_bounds__(256)
     k_dct4_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
               const int* count_ptr) {
   const int count = *count_ptr;
-  if (int(blockIdx.x) * 16 >= count) return;
-  constexpr int NB = 16;
+  constexpr int NB = kDct4Blocks;
+  if (int(blockIdx.x) * NB >= count) return;
   __shared__ float s_a[16], s_b[16];
   __shared__ float s_blk[3][NB * 64];
   __shared__ float s_r[NB * 64], s_t[NB * 64], s_p[NB * 64];
@@ -1448,51 +1351,68 @@ __device__ void SmallForward(int type, const float* px, int ps, float* co) {
   }
 }
 
-__global__ void k_small_ar(Geo g, DevFrame f, FrameScalars s,
-                           const uint32_t* list, const int* count_ptr) {
+// One thread per (block, channel): the warp of channel c of 32 blocks
+// computes its DCT and clamp ratios; the minimum over X, Y, B (in that order,
+// as the reference) is taken through shared memory.
+constexpr int kSmallArBlocks = 32;
+
+__global__ void __launch_bounds__(3 * kSmallArBlocks)
+    k_small_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
+               const int* count_ptr) {
+  __shared__ float s_ratio[3][kSmallArBlocks][65];
   const int count = *count_ptr;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const uint32_t pk = list[i];
-  const int bx = pk & 0xFFFF, by = pk >> 16;
-  const int type = f.acs[by * g.Bx + bx] >> 4;
-  const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
+  if (int(blockIdx.x) * kSmallArBlocks >= count) return;  // whole CTA
+  const int c = threadIdx.x / kSmallArBlocks;
+  const int lb = threadIdx.x % kSmallArBlocks;
+  const int i = blockIdx.x * kSmallArBlocks + lb;
+  const bool active = i < count;
   const size_t plane = size_t(g.PW) * g.PH;
-  const size_t o0 = size_t(by * 8) * g.PW + bx * 8;
-  float blk[3][64];
-  float mr[64];
-  for (int k = 0; k < 64; ++k) mr[k] = 1.0f;
-  for (int c = 0; c < 3; ++c) {
+  int type = 0;
+  size_t o0 = 0;
+  float blk[64];
+  if (active) {
+    const uint32_t pk = list[i];
+    const int bx = pk & 0xFFFF, by = pk >> 16;
+    type = f.acs[by * g.Bx + bx] >> 4;
+    const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
+    o0 = c * plane + size_t(by * 8) * g.PW + bx * 8;
     float diff[64];
     for (int y = 0; y < 8; ++y)
       for (int x = 0; x < 8; ++x) {
-        const size_t o = c * plane + o0 + size_t(y) * g.PW + x;
+        const size_t o = o0 + size_t(y) * g.PW + x;
         diff[y * 8 + x] = f.filt[o] - f.idct[o];
       }
-    SmallForward(type, diff, 8, blk[c]);
+    SmallForward(type, diff, 8, blk);
     for (int k = 0; k < 64; ++k) {
       const float interval = k == 0 ? 1.0f * s.mul_dc[c]
                                     : info.dm[c][k] * info.inv_quant_ac;
-      const float r = ClampRatio(blk[c][k], interval);
-      mr[k] = r < mr[k] ? r : mr[k];
+      s_ratio[c][lb][k] = ClampRatio(blk[k], interval);
     }
   }
-  for (int c = 0; c < 3; ++c) {
-    for (int k = 0; k < 64; ++k) blk[c][k] = blk[c][k] * mr[k];
-    float px[64];
-    SmallInverse(type, blk[c], px, 8);
-    for (int y = 0; y < 8; ++y)
-      for (int x = 0; x < 8; ++x) {
-        const size_t o = c * plane + o0 + size_t(y) * g.PW + x;
-        f.filt[o] = px[y * 8 + x] + f.idct[o];
-      }
+  __syncthreads();
+  if (!active) return;
+  for (int k = 0; k < 64; ++k) {
+    float mr = 1.0f;
+    for (int cc = 0; cc < 3; ++cc) {
+      const float r = s_ratio[cc][lb][k];
+      mr = r < mr ? r : mr;
+    }
+    blk[k] = blk[k] * mr;
   }
+  float px[64];
+  SmallInverse(type, blk, px, 8);
+  for (int y = 0; y < 8; ++y)
+    for (int x = 0; x < 8; ++x) {
+      const size_t o = o0 + size_t(y) * g.PW + x;
+      f.filt[o] = px[y * 8 + x] + f.idct[o];
+    }
 }
 
 }  // namespace pikgpu
 
 #include "square_kernels.cuh"
 #include "epf_kernel.cuh"
+#include "stencil_kernels.cuh"
 
 namespace pikgpu {
 
