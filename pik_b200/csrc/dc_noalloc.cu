@@ -166,8 +166,8 @@ int DcNoAlloc(pikgpu_ctx* ctx, const int16_t* quantized_dc, uint32_t bx,
   k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, nullptr, nullptr, nullptr,
                                                s.quant_dc / 2, mm, sig);
   k_epf_box<<<dim3(Blocks(dpw, kEpfW), Blocks(dph, kEpfH)), kEpfThreads,
-              kEpfSmemBytes, st>>>(dcpad, dcpad, nullptr, dpw, dph, mm, sig,
-                                   dcfilt);
+              kEpfSmemBytes, st>>>(dcpad, dcpad, nullptr, 0, dpw, dph, mm,
+                                   sig, dcfilt);
   dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
   k_dc_clamp<<<gr2, b, 0, st>>>(dc, dcfilt, g.Bx, g.By, dpw, dph,
                                 half_step[0], half_step[1], half_step[2]);

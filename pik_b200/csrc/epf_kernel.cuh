@@ -18,6 +18,12 @@
 // reference's neighbour order (cy = -3..3, cx = -3..4) with separately
 // rounded products and sums, so the output equals the per-pixel formulation
 // bit for bit.
+//
+// The guide is quantised from one of three sources: the verification
+// override (bytes), a plane (`guide_src`: the sharpened guide, a frame
+// without gaborish, the DC image), or -- the common case -- gaborish of
+// `in` computed here from the staged input tile (the smoothed plane is then
+// never written to memory; `gab` > 0 selects it and its strength).
 // Included by recon_kernels.cu.
 #pragma once
 
@@ -30,11 +36,16 @@ constexpr int kEpfGWords = 20;          // guide bytes x0 - 8 .. x0 + 71
 // Words per shifted copy; = 8 (mod 32), so that the 32 lanes' loads of 32
 // consecutive byte offsets fall in (at most one pair excepted) distinct banks.
 constexpr int kEpfCopyWords = kEpfGH * kEpfGWords + 8;
-constexpr int kEpfIW = kEpfW + 8;       // input cols: x0 - 3 .. x0 + 68
-constexpr int kEpfIH = kEpfH + 6;       // input rows: y0 - 3 .. y0 + 34
+// Input tile with a 5-pixel halo (enough for gaborish at the guide's
+// 4-pixel halo): rows y0 - 5 .. y0 + 36, cols x0 - 12 .. x0 + 75 (the
+// column range is widened to 16-byte boundaries for vector loads).
+constexpr int kEpfTH = kEpfH + 10;
+constexpr int kEpfTW = kEpfW + 24;
+constexpr int kEpfTS = kEpfTW;               // row stride in floats
+constexpr int kEpfTRow0 = 2, kEpfTCol0 = 9;  // tile index of (y0-3, x0-3)
 constexpr size_t kEpfGuideWords = size_t(3) * 4 * kEpfCopyWords;
 constexpr size_t kEpfSmemBytes =
-    kEpfGuideWords * 4 + size_t(3) * kEpfIH * kEpfIW * 4;
+    kEpfGuideWords * 4 + size_t(3) * kEpfTH * kEpfTS * 4;
 
 // WeightFast (pik/epf_target.cc:304-428) as 4 integer operations:
 // ((int16(min(sad, 507) << 6) * mul) >> 16 + (127 << 7)) in the high half of
@@ -47,12 +58,12 @@ __device__ __forceinline__ float EpfWeight(int mul64, int sad) {
 
 __global__ void __launch_bounds__(kEpfThreads, 2)
     k_epf_box(const float* in, const float* guide_src,
-              const uint8_t* guide_ovr, int w, int h, const uint32_t* mm,
-              const int32_t* sigma, float* out) {
+              const uint8_t* guide_ovr, int gab, int w, int h,
+              const uint32_t* mm, const int32_t* sigma, float* out) {
   extern __shared__ __align__(16) uint32_t epf_smem[];
   uint32_t* sg = epf_smem;  // [3][4][kEpfCopyWords]
-  float(*si)[kEpfIH][kEpfIW] =
-      reinterpret_cast<float(*)[kEpfIH][kEpfIW]>(epf_smem + kEpfGuideWords);
+  float(*tile)[kEpfTH][kEpfTS] =
+      reinterpret_cast<float(*)[kEpfTH][kEpfTS]>(epf_smem + kEpfGuideWords);
   const int x0 = blockIdx.x * kEpfW, y0 = blockIdx.y * kEpfH;
   const int tid = threadIdx.x;
   const int lane = tid & 31, wp = tid >> 5;
@@ -86,34 +97,104 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
 
   float amin, mul, stretch;
   GuideParams(mm, &amin, &mul, &stretch);
+  // Tiles whose halo lies inside the image take vector loads and no
+  // mirroring; border tiles mirror every coordinate.
+  const bool interior = x0 >= 12 && x0 + kEpfW + 12 <= w && y0 >= 5 &&
+                        y0 + kEpfH + 5 <= h;
+  if (interior) {
+    constexpr int Q = kEpfTW / 4;
+    for (int i = tid; i < 3 * kEpfTH * Q; i += kEpfThreads) {
+      const int c = i / (kEpfTH * Q);
+      const int r = (i / Q) % kEpfTH, q = i % Q;
+      *reinterpret_cast<float4*>(&tile[c][r][4 * q]) =
+          *reinterpret_cast<const float4*>(
+              in + c * plane + size_t(y0 - 5 + r) * w + x0 - 12 + 4 * q);
+    }
+  } else {
+    for (int i = tid; i < 3 * kEpfTH * kEpfTW; i += kEpfThreads) {
+      const int c = i / (kEpfTH * kEpfTW);
+      const int r = (i / kEpfTW) % kEpfTH, col = i % kEpfTW;
+      const int gx = x0 - 12 + col, gy = y0 - 5 + r;
+      tile[c][r][col] =
+          in[c * plane + size_t(MirrorIdx(gy, h)) * w + MirrorIdx(gx, w)];
+    }
+  }
+  if (gab) __syncthreads();  // the guide is computed from the tile
+  const float* gw = c_t.gaborish[gab];
+  auto quant = [&](float v) {
+    return uint32_t(uint8_t(uint32_t(__float2int_rz((v - amin) * mul))));
+  };
+  // Gaborish (Sym3 order) at tile position (ly, lx) from the tile.
+  auto smooth = [&](int c, int ly, int lx) {
+    const float* t = &tile[c][ly - 1][lx];
+    const float* m = &tile[c][ly][lx];
+    const float* bt = &tile[c][ly + 1][lx];
+    const float sum_tb = t[0] + bt[0];
+    const float mul0 = m[0] * gw[0];
+    const float sum_lr = m[-1] + m[1];
+    const float x1 = sum_tb + sum_lr;
+    const float mul1 = x1 * gw[1] + mul0;
+    const float sum_t2 = t[-1] + t[1];
+    const float sum_b2 = bt[-1] + bt[1];
+    const float x2 = sum_t2 + sum_b2;
+    return x2 * gw[2] + mul1;
+  };
   // u8 guide (MakeGuide, pik/epf_target.cc:1009-1070) into copy 0.
   for (int i = tid; i < 3 * kEpfGH * kEpfGWords; i += kEpfThreads) {
     const int c = i / (kEpfGH * kEpfGWords);
     const int r = (i / kEpfGWords) % kEpfGH, wd = i % kEpfGWords;
     const int gy = y0 - 4 + r;
     uint32_t word = 0;
-    for (int b = 0; b < 4; ++b) {
-      const int gx = x0 - 8 + 4 * wd + b;
-      uint32_t v;
-      if (guide_ovr) {
-        const bool ok = gx >= -6 && gx < w + 6 && gy >= -6 && gy < h + 6;
-        v = ok ? guide_ovr[(size_t(c) * (h + 12) + gy + 6) * (w + 12) + gx + 6]
-               : 0u;
+    if (interior && !guide_ovr) {
+      if (gab) {
+        // Four smoothed values from float4 row segments: tile row r + 1,
+        // cols 4 wd + 4 .. 4 wd + 7 (gx = x0 - 8 + 4 wd ..).
+        const int lx = 4 * wd + 4;
+        float v[3][6];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float* row = &tile[c][r + k][lx];
+          const float4 q = *reinterpret_cast<const float4*>(row);
+          v[k][0] = row[-1];
+          v[k][1] = q.x, v[k][2] = q.y, v[k][3] = q.z, v[k][4] = q.w;
+          v[k][5] = row[4];
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          word |= quant(Sym3Rows(v[0], v[1], v[2], b, gw[0], gw[1], gw[2]))
+                  << (8 * b);
+        }
       } else {
-        const float s = guide_src[c * plane + size_t(MirrorIdx(gy, h)) * w +
-                                  MirrorIdx(gx, w)];
-        v = uint8_t(uint32_t(__float2int_rz((s - amin) * mul)));
+        const float4 q = *reinterpret_cast<const float4*>(
+            guide_src + c * plane + size_t(gy) * w + x0 - 8 + 4 * wd);
+        word = quant(q.x) | quant(q.y) << 8 | quant(q.z) << 16 |
+               quant(q.w) << 24;
       }
-      word |= v << (8 * b);
+    } else {
+      for (int b = 0; b < 4; ++b) {
+        const int gx = x0 - 8 + 4 * wd + b;
+        uint32_t v = 0;
+        if (guide_ovr) {
+          const bool ok = gx >= -6 && gx < w + 6 && gy >= -6 && gy < h + 6;
+          v = ok ? guide_ovr[(size_t(c) * (h + 12) + gy + 6) * (w + 12) +
+                             gx + 6]
+                 : 0u;
+        } else if (gab) {
+          // Smoothed value at the mirrored position, from the tile;
+          // positions whose mirror leaves the tile are never read.
+          const int ly = MirrorIdx(gy, h) - (y0 - 5);
+          const int lx = MirrorIdx(gx, w) - (x0 - 12);
+          if (ly >= 1 && ly < kEpfTH - 1 && lx >= 1 && lx < kEpfTW - 1) {
+            v = quant(smooth(c, ly, lx));
+          }
+        } else {
+          v = quant(guide_src[c * plane + size_t(MirrorIdx(gy, h)) * w +
+                              MirrorIdx(gx, w)]);
+        }
+        word |= v << (8 * b);
+      }
     }
     sg[(c * 4) * kEpfCopyWords + r * kEpfGWords + wd] = word;
-  }
-  for (int i = tid; i < 3 * kEpfIH * kEpfIW; i += kEpfThreads) {
-    const int c = i / (kEpfIH * kEpfIW);
-    const int r = (i / kEpfIW) % kEpfIH, col = i % kEpfIW;
-    const int gx = x0 - 3 + col, gy = y0 - 3 + r;
-    si[c][r][col] =
-        in[c * plane + size_t(MirrorIdx(gy, h)) * w + MirrorIdx(gx, w)];
   }
   __syncthreads();
   // Copies 1..3: byte-shifted words of copy 0.
@@ -137,7 +218,7 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
       for (int c = 0; c < 3; ++c)
         for (int j = 0; j < 4; ++j)
           out[c * plane + size_t(py0 + j) * w + px] =
-              si[c][4 * wp + j + 3][lane + 32 * i + 3];
+              tile[c][4 * wp + j + 3 + kEpfTRow0][lane + 32 * i + 3 + kEpfTCol0];
     }
     return;
   }
@@ -200,16 +281,16 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const int ir = 4 * wp + j + 3 + cy;
+        const int ir = 4 * wp + j + 3 + cy + kEpfTRow0;
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
           const int p = j * 2 + i;
-          const int col = lane + 32 * i + 3 + cx;
+          const int col = lane + 32 * i + 3 + cx + kEpfTCol0;
           float wgt = EpfWeight(m64[i], sad[p]);
           if (!(wgt >= 0.05f)) wgt = 0.0f;
-          ws[0][p] += si[0][ir][col] * wgt;
-          ws[1][p] += si[1][ir][col] * wgt;
-          ws[2][p] += si[2][ir][col] * wgt;
+          ws[0][p] += tile[0][ir][col] * wgt;
+          ws[1][p] += tile[1][ir][col] * wgt;
+          ws[2][p] += tile[2][ir][col] * wgt;
           sw[p] += wgt;
         }
       }
@@ -226,7 +307,7 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
         const int p = j * 2 + i;
         out[c * plane + size_t(py0 + j) * w + px] =
             filtered[i] ? ws[c][p] / sw[p]
-                        : si[c][4 * wp + j + 3][lane + 32 * i + 3];
+                        : tile[c][4 * wp + j + 3 + kEpfTRow0][lane + 32 * i + 3 + kEpfTCol0];
       }
   }
 }

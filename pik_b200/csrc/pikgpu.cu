@@ -79,6 +79,8 @@ struct pikgpu_ctx {
   DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr;
   DevBuf sigma_ovr, counters, active[kNumClasses];
   bool use_guide_ovr = false, use_sigma_ovr = false;
+  // The smoothed frame (gaborish #1) is written only when an export asks.
+  bool smoothed_valid = false;
   cudaEvent_t ev[kNumTimed + 1] = {};
   float times[kNumTimed] = {};
   float dc_half_step[3] = {};
@@ -293,17 +295,36 @@ int UploadTables(pikgpu_ctx* ctx) {
 
 inline int Blocks(size_t n, int t) { return int((n + t - 1) / t); }
 
+// Writes the smoothed frame (gaborish #1 of the IDCT output) for the stage
+// and guide exports; the reconstruction itself never stores it.
+int EnsureSmoothed(pikgpu_ctx* ctx) {
+  if (ctx->smoothed_valid || !ctx->s.gaborish) return PIKGPU_OK;
+  const Geo& g = ctx->g;
+  const int rc = Ensure(ctx, &ctx->smoothed, 4 * 3 * size_t(g.PW) * g.PH);
+  if (rc != PIKGPU_OK) return rc;
+  dim3 gr(Blocks(g.PW, kStripW), Blocks(g.PH, kStripH), 3);
+  k_gaborish_strips<<<gr, kStripThreads, 0, ctx->stream>>>(
+      P<float>(ctx->idct), g.PW, g.PH, ctx->s.gaborish,
+      P<float>(ctx->smoothed), nullptr);
+  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->smoothed_valid = true;
+  return PIKGPU_OK;
+}
+
 void Mark(pikgpu_ctx* ctx, int i) {
   if (ctx->profile) cudaEventRecord(ctx->ev[i], ctx->stream);
 }
 
 // The frame EPF or the DC EPF: minmax of the guide source is expected in
-// ctx->mm already; sigma per block into `sig`.
-int RunEpf(pikgpu_ctx* ctx, const float* in, const float* guide_src, int w,
-           int h, const int32_t* sig, float* out, const uint8_t* guide_ovr) {
+// ctx->mm already; sigma per block in `sig`. `gab` > 0: the guide is
+// gaborish (that strength) of `in`, computed inside the kernel.
+int RunEpf(pikgpu_ctx* ctx, const float* in, const float* guide_src, int gab,
+           int w, int h, const int32_t* sig, float* out,
+           const uint8_t* guide_ovr) {
   dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
   k_epf_box<<<grid, kEpfThreads, kEpfSmemBytes, ctx->stream>>>(
-      in, guide_src, guide_ovr, w, h, P<uint32_t>(ctx->mm), sig, out);
+      in, guide_src, guide_ovr, gab, w, h, P<uint32_t>(ctx->mm), sig, out);
   ++ctx->launches;
   return PIKGPU_OK;
 }
@@ -337,6 +358,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   uint32_t* mm = P<uint32_t>(ctx->mm);
 
   ctx->launches = 0;
+  ctx->smoothed_valid = false;
   Mark(ctx, kTDc);
   // DC: dequant, EPF on the 8-padded DC image, clamp.
   k_dequant_dc<<<Blocks(size_t(g.Bx) * g.By, 256), 256, 0, st>>>(g, f, s); ++ctx->launches;
@@ -353,7 +375,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(
         nb, nullptr, nullptr, nullptr, s.quant_dc / 2, mm,
         P<int32_t>(ctx->dc_sigma)); ++ctx->launches;
-    RunEpf(ctx, dcpad, dcpad, dpw, dph, P<int32_t>(ctx->dc_sigma), dcfilt,
+    RunEpf(ctx, dcpad, dcpad, 0, dpw, dph, P<int32_t>(ctx->dc_sigma), dcfilt,
            nullptr);
     dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
     k_dc_clamp<<<gr2, b, 0, st>>>(f.dc, dcfilt, g.Bx, g.By, dpw, dph,
@@ -432,16 +454,16 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   Mark(ctx, kTGab1);
   if (s.have_ar) {
     const size_t npx = size_t(g.PW) * g.PH;
-    const float* guide_src = f.idct;
+    // Guide source: gaborish of the IDCT output (computed inside the EPF;
+    // here only its min/max), or the IDCT output itself (sharpened guide,
+    // or no gaborish).
+    const int gab = s.use_sharpened ? 0 : s.gaborish;
     k_minmax_init<<<1, 32, 0, st>>>(mm); ++ctx->launches;
-    if (s.gaborish) {
+    if (gab) {
       dim3 gr(Blocks(g.PW, kStripW), Blocks(g.PH, kStripH), 3);
       k_gaborish_strips<<<gr, kStripThreads, 0, st>>>(
-          f.idct, g.PW, g.PH, s.gaborish, f.smoothed,
-          s.use_sharpened ? nullptr : mm); ++ctx->launches;
-      if (!s.use_sharpened) guide_src = f.smoothed;
-    }
-    if (guide_src == f.idct) {
+          f.idct, g.PW, g.PH, gab, nullptr, mm); ++ctx->launches;
+    } else {
       k_minmax<<<dim3(Blocks(npx, 256 * 8), 3), 256, 0, st>>>(f.idct, npx,
                                                                mm); ++ctx->launches;
     }
@@ -455,7 +477,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, f.qf, f.acs, f.lut, 0,
                                                    mm, sig); ++ctx->launches;
     }
-    RunEpf(ctx, f.idct, guide_src, g.PW, g.PH, sig, f.filt,
+    RunEpf(ctx, f.idct, f.idct, gab, g.PW, g.PH, sig, f.filt,
            ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr);
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_epf.p, f.filt, sizeof(float) * 3 * npx,
@@ -675,7 +697,6 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
       {&ctx->pred2x2_g, 4 * kG2GroupFloats * ng},
       {&ctx->tmp2x2_g, 4 * kG2GroupFloats * ng},
       {&ctx->idct, 4 * 3 * npx},
-      {&ctx->smoothed, 4 * 3 * npx},
       {&ctx->filt, 4 * 3 * npx},
       {&ctx->mm, 64},
       {&ctx->sigma, 4 * nb},
@@ -905,12 +926,15 @@ int pikgpu_get_stage(pikgpu_ctx* ctx, int stage, float* const planes[3],
     case PIKGPU_STAGE_IDCT:
       src = P<float>(ctx->idct), w = g.PW, h = g.PH;
       break;
-    case PIKGPU_STAGE_SMOOTHED:
+    case PIKGPU_STAGE_SMOOTHED: {
       // Without gaborish the EPF guide source is the IDCT output itself
       // (DoAdaptiveReconstruction, pik/compressed_image.cc:1126-1132).
+      const int rc = EnsureSmoothed(ctx);
+      if (rc != PIKGPU_OK) return rc;
       src = P<float>(ctx->s.gaborish ? ctx->smoothed : ctx->idct);
       w = g.PW, h = g.PH;
       break;
+    }
     case PIKGPU_STAGE_EPF:
       src = P<float>(ctx->dbg_epf), w = g.PW, h = g.PH;
       break;
@@ -982,12 +1006,13 @@ int pikgpu_get_epf_decisions(pikgpu_ctx* ctx, uint8_t* guide,
   }
   if (guide) {
     const size_t n = 3 * size_t(g.PW + 12) * (g.PH + 12);
+    const bool smoothed = ctx->s.gaborish && !ctx->s.use_sharpened;
+    int rc;
+    if (smoothed && (rc = EnsureSmoothed(ctx)) != PIKGPU_OK) return rc;
     DevBuf tmp;
-    int rc = Ensure(ctx, &tmp, n);
-    if (rc) return rc;
-    const float* src = (ctx->s.gaborish && !ctx->s.use_sharpened)
-                           ? P<float>(ctx->smoothed)
-                           : P<float>(ctx->idct);
+    if ((rc = Ensure(ctx, &tmp, n))) return rc;
+    const float* src =
+        smoothed ? P<float>(ctx->smoothed) : P<float>(ctx->idct);
     dim3 b(32, 8), gr(Blocks(g.PW + 12, 32), Blocks(g.PH + 12, 8), 3);
     k_export_guide<<<gr, b, 0, ctx->stream>>>(src, g.PW, g.PH,
                                               P<uint32_t>(ctx->mm),

@@ -1411,8 +1411,8 @@ __global__ void __launch_bounds__(3 * kSmallArBlocks)
 }  // namespace pikgpu
 
 #include "square_kernels.cuh"
-#include "epf_kernel.cuh"
 #include "stencil_kernels.cuh"
+#include "epf_kernel.cuh"
 
 namespace pikgpu {
 

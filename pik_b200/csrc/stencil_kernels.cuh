@@ -1,7 +1,9 @@
 // Row-strip forms of the two full-frame 3x3 stencil passes:
 //  * k_gaborish_strips: ConvolveGaborish (pik/gaborish.cc:137-159) of one
-//    plane into `out`, plus the plane's min/max (MinMax,
-//    pik/epf_target.cc:980-1006) for the EPF guide;
+//    plane into `out` (skipped when `out` is null: the EPF recomputes the
+//    smoothed values it needs), plus the plane's min/max (MinMax,
+//    pik/epf_target.cc:980-1006) for the EPF guide (skipped when `mm` is
+//    null);
 //  * k_final_strips: gaborish #2 (or a copy), ShrinkTo(xsize, ysize), XybToRgb
 //    (pik/opsin_inverse.cc:38-123) and optional sRGB-8
 //    (pik/color_management.cc:323-345, pik/external_image.cc:1205).
@@ -67,7 +69,7 @@ __global__ void __launch_bounds__(kStripThreads)
   const int c = blockIdx.z;
   const size_t plane = size_t(w) * h;
   const float* p = in + c * plane;
-  float* o = out + c * plane;
+  float* o = out ? out + c * plane : nullptr;
   const int x0 = blockIdx.x * kStripW + 4 * lane;
   const int y0 = blockIdx.y * kStripH + warp * kStripRows;
   const float* wt = c_t.gaborish[strength];
@@ -89,8 +91,10 @@ __global__ void __launch_bounds__(kStripThreads)
           lo = min(lo, ob);
           hi = max(hi, ob);
         }
-        *reinterpret_cast<float4*>(o + size_t(y) * w + x0) =
-            make_float4(r[0], r[1], r[2], r[3]);
+        if (out) {
+          *reinterpret_cast<float4*>(o + size_t(y) * w + x0) =
+              make_float4(r[0], r[1], r[2], r[3]);
+        }
       }
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
