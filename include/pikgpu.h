@@ -187,9 +187,23 @@ int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
  *  KEEP_STAGES: keep the dequantised AC, EPF and pre-opsin planes for
  *               pikgpu_get_stage (costs extra device memory and copies);
  *  PROFILE:     time each kernel group with CUDA events
- *               (pikgpu_last_kernel_times). */
+ *               (pikgpu_last_kernel_times);
+ *  FORM:        PIKGPU_FORM_FP32 (default): every stage in FP32 on the CUDA
+ *               cores in the reference's operation order;
+ *               PIKGPU_FORM_SPLIT_BF16: the 16x16 transforms on the tensor
+ *               cores as split-BF16 GEMMs with FP32 accumulation, operands
+ *               split in two BF16 terms (hi + lo, three products; about
+ *               16 significant bits);
+ *               PIKGPU_FORM_SPLIT_BF16X3: the same with three terms
+ *               (hi + mid + lo, six products; FP32-level error).
+ *               The tensor-core forms are not bit-identical to the FP32
+ *               form. */
 #define PIKGPU_OPT_KEEP_STAGES 1
 #define PIKGPU_OPT_PROFILE 2
+#define PIKGPU_OPT_FORM 3
+#define PIKGPU_FORM_FP32 0
+#define PIKGPU_FORM_SPLIT_BF16 1
+#define PIKGPU_FORM_SPLIT_BF16X3 2
 int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value);
 
 /* Verification hooks for the EPF's discrete decisions, which make two

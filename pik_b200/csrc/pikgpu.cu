@@ -12,6 +12,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -68,6 +69,7 @@ struct pikgpu_ctx {
   std::string err;
   bool have_frame = false, have_ac = false, have_result = false;
   bool keep_stages = false, profile = false;
+  int form = PIKGPU_FORM_FP32;
   Geo g{};
   FrameScalars s{};
   // host copies needed after begin
@@ -77,11 +79,12 @@ struct pikgpu_ctx {
   DevBuf qdc, qac, dc, dcpad, dcfilt, ac, llf_g, lf2x2_g, pred2x2_g, tmp2x2_g;
   DevBuf idct, smoothed, filt, mm, sigma, dc_sigma, list[kNumClasses];
   DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr;
-  DevBuf sigma_ovr, counters, active[kNumClasses];
+  DevBuf sigma_ovr, counters, active[kNumClasses], tc_err;
   bool use_guide_ovr = false, use_sigma_ovr = false;
   // The smoothed frame (gaborish #1) is written only when an export asks.
   bool smoothed_valid = false;
   cudaEvent_t ev[kNumTimed + 1] = {};
+  int num_sms = 148;
   float times[kNumTimed] = {};
   float dc_half_step[3] = {};
   int launches = 0;
@@ -289,11 +292,18 @@ int UploadTables(pikgpu_ctx* ctx) {
   CUDA_TRY(ctx, cudaFuncSetAttribute(
                     k_epf_box, cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(kEpfSmemBytes)));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_final_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(kFinSmemBytes)));
   if (ctx->device < 64) g_tables_uploaded[ctx->device] = true;
   return PIKGPU_OK;
 }
 
 inline int Blocks(size_t n, int t) { return int((n + t - 1) / t); }
+
+// Persistent tensor-core transform CTAs per SM: 4 x 128 tensor-memory
+// columns fill the SM's 512.
+constexpr int kTcCtasPerSm = 4;
 
 // Writes the smoothed frame (gaborish #1 of the IDCT output) for the stage
 // and guide exports; the reconstruction itself never stores it.
@@ -302,8 +312,8 @@ int EnsureSmoothed(pikgpu_ctx* ctx) {
   const Geo& g = ctx->g;
   const int rc = Ensure(ctx, &ctx->smoothed, 4 * 3 * size_t(g.PW) * g.PH);
   if (rc != PIKGPU_OK) return rc;
-  dim3 gr(Blocks(g.PW, kStripW), Blocks(g.PH, kStripH), 3);
-  k_gaborish_strips<<<gr, kStripThreads, 0, ctx->stream>>>(
+  dim3 gr(Blocks(g.PW, kTileW), Blocks(g.PH, kGabTileH), 3);
+  k_gaborish_tile<<<gr, kTileThreads, 0, ctx->stream>>>(
       P<float>(ctx->idct), g.PW, g.PH, ctx->s.gaborish,
       P<float>(ctx->smoothed), nullptr);
   CUDA_TRY(ctx, cudaGetLastError());
@@ -401,8 +411,8 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   }
   Mark(ctx, kTDequant);
   {
-    dim3 b(64, 4), gr(Blocks(g.Bx, 4), g.By);
-    k_dequant_ac<<<gr, b, 0, st>>>(g, f, s); ++ctx->launches;
+    dim3 gr(Blocks(g.Bx, kDequantCells), g.By);
+    k_dequant_ac<<<gr, 256, 0, st>>>(g, f, s); ++ctx->launches;
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_dequant.p, f.ac,
                       sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
@@ -429,7 +439,18 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
                               st>>>(g, f, L[kC8], n[kC8], s.predict_hf);
       ++ctx->launches;
     }
-    if (n[kC16]) {
+    if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
+      const int items = (n[kC16] + 7) / 8;
+      const int grid = std::min(items, ctx->num_sms * kTcCtasPerSm);
+      if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
+        k_square_idct_tc<16, 2><<<grid, tc::kThreads, 0, st>>>(
+            g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
+      } else {
+        k_square_idct_tc<16, 3><<<grid, tc::kThreads, 0, st>>>(
+            g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
+      }
+      ++ctx->launches;
+    } else if (n[kC16]) {
       k_square_idct_rows<16><<<rows_grid(3 * n[kC16], 16), kSquareThreads, 0,
                                st>>>(g, f, L[kC16], n[kC16], s.predict_hf);
       ++ctx->launches;
@@ -460,8 +481,8 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     const int gab = s.use_sharpened ? 0 : s.gaborish;
     k_minmax_init<<<1, 32, 0, st>>>(mm); ++ctx->launches;
     if (gab) {
-      dim3 gr(Blocks(g.PW, kStripW), Blocks(g.PH, kStripH), 3);
-      k_gaborish_strips<<<gr, kStripThreads, 0, st>>>(
+      dim3 gr(Blocks(g.PW, kTileW), Blocks(g.PH, kGabTileH), 3);
+      k_gaborish_tile<<<gr, kTileThreads, 0, st>>>(
           f.idct, g.PW, g.PH, gab, nullptr, mm); ++ctx->launches;
     } else {
       k_minmax<<<dim3(Blocks(npx, 256 * 8), 3), 256, 0, st>>>(f.idct, npx,
@@ -542,8 +563,8 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   {
     const int vec_lin = lin && lin_stride % 4 == 0 && g.W % 4 == 0 &&
                         reinterpret_cast<uintptr_t>(lin) % 16 == 0;
-    dim3 gr(Blocks(g.W, kStripW), Blocks(g.H, kStripH));
-    k_final_strips<<<gr, kStripThreads, 0, st>>>(
+    dim3 gr(Blocks(g.W, kTileW), Blocks(g.H, kFinTileH));
+    k_final_tile<<<gr, kTileThreads, kFinSmemBytes, st>>>(
         final_in, g.PW, g.PH, g.W, g.H, s.gaborish,
         ctx->keep_stages ? P<float>(ctx->dbg_pre) : nullptr, lin, lin_stride,
         vec_lin, rgb8, rgb8_stride); ++ctx->launches;
@@ -584,6 +605,13 @@ int pikgpu_ctx_create(int device, pikgpu_ctx** out) {
   }
   ctx->stream = ctx->own_stream;
   for (auto& e : ctx->ev) cudaEventCreate(&e);
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount,
+                         device);
+  if (Ensure(ctx, &ctx->tc_err, sizeof(int)) != PIKGPU_OK ||
+      cudaMemset(ctx->tc_err.p, 0, sizeof(int)) != cudaSuccess) {
+    pikgpu_ctx_destroy(ctx);
+    return PIKGPU_ERR_NO_MEMORY;
+  }
   if (UploadTables(ctx) != PIKGPU_OK) {
     pikgpu_ctx_destroy(ctx);
     return PIKGPU_ERR_CUDA;
@@ -611,6 +639,7 @@ int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
   for (auto& b : ctx->list) FreeBuf(&b);
   for (auto& b : ctx->active) FreeBuf(&b);
   FreeBuf(&ctx->counters);
+  FreeBuf(&ctx->tc_err);
   for (auto& e : ctx->ev) {
     if (e) cudaEventDestroy(e);
   }
@@ -637,6 +666,13 @@ int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
       return PIKGPU_OK;
     case PIKGPU_OPT_PROFILE:
       ctx->profile = value != 0;
+      return PIKGPU_OK;
+    case PIKGPU_OPT_FORM:
+      if (value != PIKGPU_FORM_FP32 && value != PIKGPU_FORM_SPLIT_BF16 &&
+          value != PIKGPU_FORM_SPLIT_BF16X3) {
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "form %d", value);
+      }
+      ctx->form = value;
       return PIKGPU_OK;
   }
   return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "unknown option %d", option);
@@ -903,6 +939,16 @@ int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
     }
   }
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->form != PIKGPU_FORM_FP32) {
+    int tc_err = 0;
+    CUDA_TRY(ctx, cudaMemcpy(&tc_err, ctx->tc_err.p, sizeof(int),
+                             cudaMemcpyDeviceToHost));
+    if (tc_err) {
+      cudaMemset(ctx->tc_err.p, 0, sizeof(int));
+      return Fail(ctx, PIKGPU_ERR_CUDA,
+                  "tensor-core transform: MMA completion wait timed out");
+    }
+  }
   if (ctx->profile) {
     for (int i = 0; i < kNumTimed; ++i) {
       cudaEventElapsedTime(&ctx->times[i], ctx->ev[i], ctx->ev[i + 1]);

@@ -509,10 +509,22 @@ __device__ __forceinline__ uint8_t Srgb8(float lin255) {
 
 // ---------------------------------------------------------------------------
 // AC dequantisation + chroma from luma (Dequant<true>::DoAC,
-// pik/compressed_image.cc:586-707), one thread per (block, coefficient).
-__global__ void k_dequant_ac(Geo g, DevFrame f, FrameScalars s) {
-  const int k = threadIdx.x;  // 0..63
-  const int bx = blockIdx.x * (blockDim.y) + threadIdx.y;
+// pik/compressed_image.cc:586-707). A CTA covers 32 cells of one block row;
+// each thread dequantises 8 consecutive coefficients of one cell in all
+// three channels (128-bit loads of the int16 input, 128-bit stores).
+constexpr int kDequantCells = 32;
+
+__device__ __forceinline__ float AdjustQuantBias(float q, float one_bias) {
+  const float qa = fabsf(q);
+  if (qa >= 1.5f) return q - 0.145f / q;
+  if (qa >= 0.5f) return copysignf(1.0f - one_bias, q);
+  return q;
+}
+
+__global__ void __launch_bounds__(256) k_dequant_ac(Geo g, DevFrame f,
+                                                    FrameScalars s) {
+  const int part = threadIdx.x & 7;  // coefficients 8 part .. 8 part + 7
+  const int bx = blockIdx.x * kDequantCells + (threadIdx.x >> 3);
   const int by = blockIdx.y;
   if (bx >= g.Bx) return;
   const int cell = by * g.Bx + bx;
@@ -526,28 +538,49 @@ __global__ void k_dequant_ac(Geo g, DevFrame f, FrameScalars s) {
   const int blk = a & 0xF;
   const float x_cc = 1.0f * float(f.ytox[ty * g.Tx + tx] - 128) * (1.0f / 256);
   const float b_cc = 1.0f * float(f.ytob[ty * g.Tx + tx]) * (1.0f / 128);
-  const size_t pos = size_t(by) * g.ac_stride + size_t(bx) * 64 + k;
+  const size_t pos = size_t(by) * g.ac_stride + size_t(bx) * 64 + 8 * part;
   const size_t plane = size_t(g.ac_stride) * g.By;
-  float dq[3];
+  float dq[3][8];
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const float m = f.table[f.offsets[(table * 7 + kind) * 3 + c] + blk * 64 +
-                            k];
-    const float mulc = m * scaled;
-    const float q = float(f.qac[c * plane + pos]);
-    const float qa = fabsf(q);
-    float adj;
-    if (qa >= 1.5f) {
-      adj = q - 0.145f / q;
-    } else if (qa >= 0.5f) {
-      adj = copysignf(1.0f - c_t.one_bias[c], q);
+    const uint4 raw = *reinterpret_cast<const uint4*>(f.qac + c * plane + pos);
+    const float* m = f.table + f.offsets[(table * 7 + kind) * 3 + c] +
+                     blk * 64 + 8 * part;
+    float mv[8];
+    if ((reinterpret_cast<uintptr_t>(m) & 15) == 0) {
+      const float4 m0 = *reinterpret_cast<const float4*>(m);
+      const float4 m1 = *reinterpret_cast<const float4*>(m + 4);
+      mv[0] = m0.x, mv[1] = m0.y, mv[2] = m0.z, mv[3] = m0.w;
+      mv[4] = m1.x, mv[5] = m1.y, mv[6] = m1.z, mv[7] = m1.w;
     } else {
-      adj = q;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) mv[k] = m[k];
     }
-    dq[c] = adj * mulc;
+    const float ob = c_t.one_bias[c];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t word = k < 2 ? raw.x : k < 4 ? raw.y : k < 6 ? raw.z
+                                                                : raw.w;
+      const int16_t qi = int16_t(word >> (16 * (k & 1)));
+      const float mulc = mv[k] * scaled;
+      dq[c][k] = AdjustQuantBias(float(qi), ob) * mulc;
+    }
   }
-  f.ac[plane + pos] = dq[1];
-  f.ac[pos] = x_cc * dq[1] + dq[0];
-  f.ac[2 * plane + pos] = b_cc * dq[1] + dq[2];
+  float o0[8], o2[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    o0[k] = x_cc * dq[1][k] + dq[0][k];
+    o2[k] = b_cc * dq[1][k] + dq[2][k];
+  }
+  float4* d0 = reinterpret_cast<float4*>(f.ac + pos);
+  float4* d1 = reinterpret_cast<float4*>(f.ac + plane + pos);
+  float4* d2 = reinterpret_cast<float4*>(f.ac + 2 * plane + pos);
+  d1[0] = make_float4(dq[1][0], dq[1][1], dq[1][2], dq[1][3]);
+  d1[1] = make_float4(dq[1][4], dq[1][5], dq[1][6], dq[1][7]);
+  d0[0] = make_float4(o0[0], o0[1], o0[2], o0[3]);
+  d0[1] = make_float4(o0[4], o0[5], o0[6], o0[7]);
+  d2[0] = make_float4(o2[0], o2[1], o2[2], o2[3]);
+  d2[1] = make_float4(o2[4], o2[5], o2[6], o2[7]);
 }
 
 // ---------------------------------------------------------------------------
@@ -768,6 +801,35 @@ __device__ __forceinline__ float Upsample(const float* pred, int X, int Y) {
   }
   return bx[0] * c_t.ub4[0][iy] + bx[1] * c_t.ub4[1][iy] +
          bx[2] * c_t.ub4[2][iy];
+}
+
+// Upsample for the N pixels X0 .. X0 + N - 1 of row Y (X0 a multiple of 4):
+// the same arithmetic as Upsample, with the 3 x (N / 4 + 2) source values
+// loaded once.
+template <int N>
+__device__ __forceinline__ void UpsampleRow(const float* pred, int X0, int Y,
+                                            float* out) {
+  const int r = Y >> 2, q0 = X0 >> 2, iy = Y & 3;
+  constexpr int W = N / 4 + 2;
+  float src[3][W];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const float* row = pred + (r + j + 1) * kG2 + q0 + 1;
+#pragma unroll
+    for (int i = 0; i < W; ++i) src[j][i] = row[i];
+  }
+#pragma unroll
+  for (int x = 0; x < N; ++x) {
+    const int q = x >> 2, ix = x & 3;
+    float bx[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      bx[j] = src[j][q] * c_t.ub4[0][ix] + src[j][q + 1] * c_t.ub4[1][ix] +
+              src[j][q + 2] * c_t.ub4[2][ix];
+    }
+    out[x] = bx[0] * c_t.ub4[0][iy] + bx[1] * c_t.ub4[1][iy] +
+             bx[2] * c_t.ub4[2][iy];
+  }
 }
 
 // Square DCT blocks (DCT8, DCT_NOHF, DCT16, DCT32): HF prediction (if the
@@ -1411,6 +1473,7 @@ __global__ void __launch_bounds__(3 * kSmallArBlocks)
 }  // namespace pikgpu
 
 #include "square_kernels.cuh"
+#include "tc_kernels.cuh"
 #include "stencil_kernels.cuh"
 #include "epf_kernel.cuh"
 
@@ -1423,6 +1486,12 @@ template __global__ void k_square_idct_rows<16>(Geo, DevFrame,
                                                 const uint32_t*, int, int);
 template __global__ void k_square_idct_rows<32>(Geo, DevFrame,
                                                 const uint32_t*, int, int);
+template __global__ void k_square_idct_tc<16, 2>(Geo, DevFrame,
+                                                 const uint32_t*, int, int,
+                                                 int*);
+template __global__ void k_square_idct_tc<16, 3>(Geo, DevFrame,
+                                                 const uint32_t*, int, int,
+                                                 int*);
 template __global__ void k_square_ar_rows<8>(Geo, DevFrame, FrameScalars,
                                              const uint32_t*, const int*);
 template __global__ void k_square_ar_rows<16>(Geo, DevFrame, FrameScalars,

@@ -129,8 +129,7 @@ __global__ void __launch_bounds__(kSquareThreads)
     const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
     const int X0 = (bx & 63) * 8, Y = (by & 63) * 8 + r;
     float P[N], T[N];
-#pragma unroll
-    for (int x = 0; x < N; ++x) P[x] = Upsample(pred, X0 + x, Y);
+    UpsampleRow<N>(pred, X0, Y, P);
     DctRow<N>(P, T);
     PutCol<N>(tile, r, T);  // tmp[k][y = r]
     __syncwarp();

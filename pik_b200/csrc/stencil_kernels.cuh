@@ -1,52 +1,35 @@
-// Row-strip forms of the two full-frame 3x3 stencil passes:
-//  * k_gaborish_strips: ConvolveGaborish (pik/gaborish.cc:137-159) of one
+// Shared-memory tile forms of the two full-frame 3x3 stencil passes:
+//  * k_gaborish_tile: ConvolveGaborish (pik/gaborish.cc:137-159) of one
 //    plane into `out` (skipped when `out` is null: the EPF recomputes the
 //    smoothed values it needs), plus the plane's min/max (MinMax,
 //    pik/epf_target.cc:980-1006) for the EPF guide (skipped when `mm` is
 //    null);
-//  * k_final_strips: gaborish #2 (or a copy), ShrinkTo(xsize, ysize), XybToRgb
+//  * k_final_tile: gaborish #2 (or a copy), ShrinkTo(xsize, ysize), XybToRgb
 //    (pik/opsin_inverse.cc:38-123) and optional sRGB-8
 //    (pik/color_management.cc:323-345, pik/external_image.cc:1205).
 //
-// Each thread owns a 4-pixel-wide column strip of kStripRows rows: one
-// 128-bit load per input row, the left/right neighbours from the adjacent
-// lanes by shuffle (explicit loads only at warp and image edges) and a
-// 3-row sliding window in registers, so every input value is loaded once
-// per warp. A warp covers 128 pixels of a row band; the 8 warps of a CTA
-// stack vertically (128 x 64 pixels per CTA). The arithmetic of each output
-// is Sym3's, in the same order, so results are bit-identical to it.
-// Requires the padded plane width to be a multiple of 4 (it is 8 Bx).
+// A CTA stages a 128 x TH output tile with its 1-pixel halo (rows y0 - 1 ..
+// y0 + TH, columns x0 - 4 .. x0 + 131, widened to 16-byte boundaries) in
+// shared memory: interior tiles with independent 128-bit loads (many in
+// flight per thread), border tiles with mirrored scalar loads. Each thread
+// then computes 4 adjacent columns of TH / 8 rows, reading 128-bit row
+// segments and taking the left/right neighbours from the adjacent lanes.
+// The arithmetic of each output is Sym3's, in the same order, so results are
+// bit-identical to it. The padded plane width must be a multiple of 4 (it is
+// 8 Bx).
 // Included by recon_kernels.cu.
 #pragma once
 
 namespace pikgpu {
 
-constexpr int kStripRows = 8;
-constexpr int kStripThreads = 256;
-constexpr int kStripW = 128;                              // pixels per warp
-constexpr int kStripH = kStripRows * (kStripThreads / 32);  // rows per CTA
+constexpr int kTileW = 128, kTileThreads = 256;
+constexpr int kTileSW = kTileW + 8;  // staged columns x0 - 4 .. x0 + 131
+constexpr int kGabTileH = 64;        // rows per CTA, min/max pass
+constexpr int kFinTileH = 16;        // rows per CTA, final pass (3 planes)
+constexpr size_t kFinSmemBytes = size_t(3) * (kFinTileH + 2) * kTileSW * 4;
 
-// Row `y` (already mirrored) of a plane as 6 values: columns x0-1 .. x0+4.
-__device__ __forceinline__ void LoadRow6(const float* plane, int w, int y,
-                                         int x0, int lane, float v[6]) {
-  const float* row = plane + size_t(y) * w;
-  float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (x0 < w) q = *reinterpret_cast<const float4*>(row + x0);
-  float left = __shfl_up_sync(0xFFFFFFFFu, q.w, 1);
-  float right = __shfl_down_sync(0xFFFFFFFFu, q.x, 1);
-  if (x0 < w) {
-    if (lane == 0 || x0 == 0) left = row[MirrorIdx(x0 - 1, w)];
-    if (lane == 31 || x0 + 4 >= w) right = row[MirrorIdx(x0 + 4, w)];
-  }
-  v[0] = left;
-  v[1] = q.x;
-  v[2] = q.y;
-  v[3] = q.z;
-  v[4] = q.w;
-  v[5] = right;
-}
-
-// Sym3 of output column i (0..3) from the three rows, same order as Sym3.
+// Symmetric 3x3 stencil of output column i (0..3) from three 6-value rows
+// (columns x - 1 .. x + 4), in Sym3's operation order.
 __device__ __forceinline__ float Sym3Rows(const float* t, const float* m,
                                           const float* b, int i, float w0,
                                           float w1, float w2) {
@@ -61,48 +44,90 @@ __device__ __forceinline__ float Sym3Rows(const float* t, const float* m,
   return x2 * w2 + mul1;
 }
 
-__global__ void __launch_bounds__(kStripThreads)
-    k_gaborish_strips(const float* in, int w, int h, int strength, float* out,
-                      uint32_t* mm) {
-  __shared__ uint32_t s_lo[kStripThreads / 32], s_hi[kStripThreads / 32];
+// Stages plane `p` (w x h, row stride w) around (x0, y0) into `t`
+// (TH + 2 rows).
+template <int TH>
+__device__ __forceinline__ void StageTile(const float* p, int w, int h,
+                                          int x0, int y0,
+                                          float (*t)[kTileSW]) {
+  constexpr int kTileSH = TH + 2;
+  const bool interior =
+      x0 >= 4 && x0 + kTileW + 4 <= w && y0 >= 1 && y0 + TH + 1 <= h;
+  if (interior) {
+    constexpr int Q = kTileSW / 4;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < kTileSH * Q; i += kTileThreads) {
+      const int r = i / Q, q = i % Q;
+      *reinterpret_cast<float4*>(&t[r][4 * q]) =
+          *reinterpret_cast<const float4*>(p + size_t(y0 - 1 + r) * w + x0 -
+                                           4 + 4 * q);
+    }
+  } else {
+    for (int i = threadIdx.x; i < kTileSH * kTileSW; i += kTileThreads) {
+      const int r = i / kTileSW, col = i % kTileSW;
+      t[r][col] = p[size_t(MirrorIdx(y0 - 1 + r, h)) * w +
+                    MirrorIdx(x0 - 4 + col, w)];
+    }
+  }
+}
+
+// Staged row r as 6 values: columns 4 lane - 1 .. 4 lane + 4 of the tile.
+__device__ __forceinline__ void TileRow6(const float (*t)[kTileSW], int r,
+                                         int lane, float v[6]) {
+  const float4 q = *reinterpret_cast<const float4*>(&t[r][4 + 4 * lane]);
+  float left = __shfl_up_sync(0xFFFFFFFFu, q.w, 1);
+  float right = __shfl_down_sync(0xFFFFFFFFu, q.x, 1);
+  if (lane == 0) left = t[r][3];
+  if (lane == 31) right = t[r][4 + kTileW];
+  v[0] = left;
+  v[1] = q.x, v[2] = q.y, v[3] = q.z, v[4] = q.w;
+  v[5] = right;
+}
+
+__global__ void __launch_bounds__(kTileThreads)
+    k_gaborish_tile(const float* in, int w, int h, int strength, float* out,
+                    uint32_t* mm) {
+  constexpr int TH = kGabTileH, R = TH / 8;
+  __shared__ __align__(16) float t[TH + 2][kTileSW];
+  __shared__ uint32_t s_lo[kTileThreads / 32], s_hi[kTileThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int c = blockIdx.z;
   const size_t plane = size_t(w) * h;
-  const float* p = in + c * plane;
-  float* o = out ? out + c * plane : nullptr;
-  const int x0 = blockIdx.x * kStripW + 4 * lane;
-  const int y0 = blockIdx.y * kStripH + warp * kStripRows;
+  const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * TH;
+  StageTile<TH>(in + c * plane, w, h, x0, y0, t);
+  __syncthreads();
   const float* wt = c_t.gaborish[strength];
   const float w0 = wt[0], w1 = wt[1], w2 = wt[2];
+  const int x = x0 + 4 * lane;
   uint32_t lo = 0xFFFFFFFFu, hi = 0u;
-  if (y0 < h) {
-    float t[6], m[6], b[6];
-    LoadRow6(p, w, MirrorIdx(y0 - 1, h), x0, lane, t);
-    LoadRow6(p, w, y0, x0, lane, m);
-    const int y1 = min(y0 + kStripRows, h);
-    for (int y = y0; y < y1; ++y) {
-      LoadRow6(p, w, MirrorIdx(y + 1, h), x0, lane, b);
-      if (x0 < w) {
-        float r[4];
+  float a[6], m[6], b[6];
+  TileRow6(t, R * warp, lane, a);
+  TileRow6(t, R * warp + 1, lane, m);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          r[i] = Sym3Rows(t, m, b, i, w0, w1, w2);
-          const uint32_t ob = OrderedBits(r[i]);
-          lo = min(lo, ob);
-          hi = max(hi, ob);
-        }
-        if (out) {
-          *reinterpret_cast<float4*>(o + size_t(y) * w + x0) =
-              make_float4(r[0], r[1], r[2], r[3]);
-        }
+  for (int j = 0; j < R; ++j) {
+    TileRow6(t, R * warp + j + 2, lane, b);
+    const int y = y0 + R * warp + j;
+    if (x < w && y < h) {
+      float r[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        r[i] = Sym3Rows(a, m, b, i, w0, w1, w2);
+        const uint32_t ob = OrderedBits(r[i]);
+        lo = min(lo, ob);
+        hi = max(hi, ob);
       }
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        t[i] = m[i];
-        m[i] = b[i];
+      if (out) {
+        *reinterpret_cast<float4*>(out + c * plane + size_t(y) * w + x) =
+            make_float4(r[0], r[1], r[2], r[3]);
       }
     }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      a[i] = m[i];
+      m[i] = b[i];
+    }
   }
+  if (!mm) return;
   for (int off = 16; off; off >>= 1) {
     lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, off));
     hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, off));
@@ -112,8 +137,8 @@ __global__ void __launch_bounds__(kStripThreads)
     s_hi[warp] = hi;
   }
   __syncthreads();
-  if (threadIdx.x == 0 && mm) {
-    for (int i = 1; i < kStripThreads / 32; ++i) {
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < kTileThreads / 32; ++i) {
       lo = min(lo, s_lo[i]);
       hi = max(hi, s_hi[i]);
     }
@@ -146,58 +171,54 @@ __device__ __forceinline__ void XybToRgb(float x, float y, float b, float* r,
 
 // `vec_lin`: the linear outputs may be written as float4 (width, stride and
 // base all multiples of 4 floats / 16 bytes).
-__global__ void __launch_bounds__(kStripThreads)
-    k_final_strips(const float* in, int pw, int ph, int w, int h,
-                   int strength, float* pre, float* lin, size_t lin_stride,
-                   int vec_lin, uint8_t* rgb8, size_t rgb8_stride) {
+__global__ void __launch_bounds__(kTileThreads)
+    k_final_tile(const float* in, int pw, int ph, int w, int h, int strength,
+                 float* pre, float* lin, size_t lin_stride, int vec_lin,
+                 uint8_t* rgb8, size_t rgb8_stride) {
+  constexpr int TH = kFinTileH, R = TH / 8;
+  extern __shared__ __align__(16) float fin_smem[];
+  float(*t)[TH + 2][kTileSW] =
+      reinterpret_cast<float(*)[TH + 2][kTileSW]>(fin_smem);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const size_t plane = size_t(pw) * ph;
-  const int x0 = blockIdx.x * kStripW + 4 * lane;
-  const int y0 = blockIdx.y * kStripH + warp * kStripRows;
-  if (y0 >= h) return;  // whole warp: y0 is warp-uniform
+  const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * TH;
+  for (int c = 0; c < 3; ++c) {
+    StageTile<TH>(in + c * plane, pw, ph, x0, y0, t[c]);
+  }
+  __syncthreads();
   const float* wt = c_t.gaborish[strength];
   const float w0 = wt[0], w1 = wt[1], w2 = wt[2];
-  float t[3][6], m[3][6], b[3][6];
-  if (strength) {
+  const int x = x0 + 4 * lane;
+#pragma unroll 2
+  for (int j = 0; j < R; ++j) {
+    const int y = y0 + R * warp + j;
+    const int r0 = R * warp + j;  // staged row of y - 1
+    float v[3][4];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      LoadRow6(in + c * plane, pw, MirrorIdx(y0 - 1, ph), x0, lane, t[c]);
-      LoadRow6(in + c * plane, pw, y0, x0, lane, m[c]);
-    }
-  }
-  const int y1 = min(y0 + kStripRows, h);
-  for (int y = y0; y < y1; ++y) {
-    float v[3][4];
-    if (strength) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        LoadRow6(in + c * plane, pw, MirrorIdx(y + 1, ph), x0, lane, b[c]);
+      if (strength) {
+        float a[6], m[6], b[6];
+        TileRow6(t[c], r0, lane, a);
+        TileRow6(t[c], r0 + 1, lane, m);
+        TileRow6(t[c], r0 + 2, lane, b);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          v[c][i] = Sym3Rows(t[c], m[c], b[c], i, w0, w1, w2);
+          v[c][i] = Sym3Rows(a, m, b, i, w0, w1, w2);
         }
-#pragma unroll
-        for (int i = 0; i < 6; ++i) {
-          t[c][i] = m[c][i];
-          m[c][i] = b[c][i];
-        }
-      }
-    } else if (x0 < pw) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float4 q = *reinterpret_cast<const float4*>(
-            in + c * plane + size_t(y) * pw + x0);
+      } else {
+        const float4 q =
+            *reinterpret_cast<const float4*>(&t[c][r0 + 1][4 + 4 * lane]);
         v[c][0] = q.x, v[c][1] = q.y, v[c][2] = q.z, v[c][3] = q.w;
       }
     }
-    if (x0 >= w) continue;
-    const int n = min(4, w - x0);
+    if (x >= w || y >= h) continue;
+    const int n = min(4, w - x);
     if (pre) {
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          if (i < n) pre[(size_t(c) * h + y) * w + x0 + i] = v[c][i];
+          if (i < n) pre[(size_t(c) * h + y) * w + x + i] = v[c][i];
     }
     float r[4], g[4], bl[4];
 #pragma unroll
@@ -205,7 +226,7 @@ __global__ void __launch_bounds__(kStripThreads)
       XybToRgb(v[0][i], v[1][i], v[2][i], &r[i], &g[i], &bl[i]);
     }
     if (lin) {
-      float* o0 = lin + size_t(y) * lin_stride + x0;
+      float* o0 = lin + size_t(y) * lin_stride + x;
       float* o1 = o0 + lin_stride * h;
       float* o2 = o1 + lin_stride * h;
       if (vec_lin) {
@@ -225,7 +246,7 @@ __global__ void __launch_bounds__(kStripThreads)
       }
     }
     if (rgb8) {
-      uint8_t* o = rgb8 + size_t(y) * rgb8_stride + 3 * size_t(x0);
+      uint8_t* o = rgb8 + size_t(y) * rgb8_stride + 3 * size_t(x);
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         if (i < n) {

@@ -1,0 +1,416 @@
+// Split-BF16 tensor-core form of the square-block transforms (the
+// ComputeTransposedScaledIDCT / DCT passes of TransformToPixels and the HF
+// prediction's TransformFromPixels, pik/ac_strategy.cc:531-848,
+// pik/dct.h:362-507) on the 5th-generation tensor cores (tcgen05).
+//
+// Each separable pass over a batch of 128 / N blocks of N x N is one GEMM
+// D[128 x N] = A[128 x K] * B[N x K]^T with K = N: the rows of A are the
+// batch's block rows (row m = N * block + r), B is the transform matrix, D
+// accumulates in FP32 in tensor memory. The operands are split into BF16
+// terms. With S = 2, x = hi + lo (about 16 significant bits) and
+// D = A_hi B_hi + A_hi B_lo + A_lo B_hi (three MMAs): about 1e-5 relative
+// error per product. With S = 3, x = hi + mid + lo (the full 24 bits) and
+// six MMAs (hi hi, hi mid, mid hi, hi lo, lo hi, mid mid): FP32-level
+// error. The transpose
+// between the two passes of a 2-D transform costs nothing: each thread reads
+// its row of D from tensor memory and writes it back to shared memory as the
+// M-major A operand of the next pass.
+//
+// Operand layouts are the tcgen05 "no swizzle" canonical forms: 8 x 8 BF16
+// core matrices of 128 contiguous bytes (8 rows of 16 bytes), the K groups
+// of a row group 128 bytes apart and the row groups KC * 128 bytes apart
+// (KC = K / 8). One thread issues the MMAs and commits them to an mbarrier;
+// every wait on it is bounded and reports a timeout through `err` instead of
+// hanging.
+// Included by recon_kernels.cu.
+#pragma once
+
+#include <cuda_bf16.h>
+
+namespace pikgpu {
+namespace tc {
+
+constexpr int kThreads = 128;            // one row of D per thread
+constexpr int kTmemCols = 128;           // 3 channels x 2 accumulators
+constexpr uint32_t kMaxPolls = 1u << 22;  // bounded mbarrier wait
+
+__device__ __forceinline__ uint32_t SmemU32(const void* p) {
+  return uint32_t(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (no swizzle): start, leading (K-group)
+// and stride (row-group) byte offsets, descriptor version 1.
+__device__ __forceinline__ uint64_t Desc(const void* base, uint32_t lbo,
+                                         uint32_t sbo) {
+  const uint64_t a = SmemU32(base);
+  return ((a >> 4) & 0x3FFFull) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: BF16 x BF16 -> F32, M x N, B K-major,
+// A K-major (a_mn = 0) or M-major (a_mn = 1).
+__host__ __device__ constexpr uint32_t Idesc(int m, int n, int a_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(a_mn) << 15) |
+         (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void Mma(uint32_t d, uint64_t a, uint64_t b,
+                                    uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void FenceBefore() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void FenceAfter() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ bool TryWait(uint32_t mbar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+// 16 consecutive FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void Ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,"
+      "%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]),
+        "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
+        "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Splits 8 floats into S BF16 terms (each the rounded remainder of the
+// previous ones), stored as one 16-byte chunk in each term's array
+// (the arrays are `stride` bytes apart).
+template <int S>
+__device__ __forceinline__ void PutChunk(uint8_t* base, uint32_t stride,
+                                         uint32_t off, const float* v) {
+  float rest[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) rest[i] = v[i];
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      // One conversion for two values; element 2i in the low half.
+      const __nv_bfloat162 h =
+          __floats2bfloat162_rn(rest[2 * i], rest[2 * i + 1]);
+      w[i] = *reinterpret_cast<const uint32_t*>(&h);
+      if (t + 1 < S) {
+        const float2 b = __bfloat1622float2(h);
+        rest[2 * i] -= b.x;
+        rest[2 * i + 1] -= b.y;
+      }
+    }
+    *reinterpret_cast<uint4*>(base + t * stride + off) =
+        make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// Row m of a K-major operand (K = N): v[k], k = 0..N-1.
+template <int N, int S>
+__device__ __forceinline__ void PutRowK(uint8_t* base, int m, const float* v) {
+#pragma unroll
+  for (int kc = 0; kc < N / 8; ++kc) {
+    PutChunk<S>(base, 128 * N * 2,
+                (m >> 3) * (N / 8) * 128 + kc * 128 + (m & 7) * 16, v + 8 * kc);
+  }
+}
+
+// Column k of an M-major operand for rows m0 .. m0 + N - 1: v[i] is element
+// (m0 + i, k); m0 is a multiple of 8.
+template <int N, int S>
+__device__ __forceinline__ void PutColMN(uint8_t* base, int m0, int k,
+                                         const float* v) {
+#pragma unroll
+  for (int g = 0; g < N / 8; ++g) {
+    PutChunk<S>(base, 128 * N * 2,
+                ((m0 >> 3) + g) * (N / 8) * 128 + (k >> 3) * 128 + (k & 7) * 16,
+                v + 8 * g);
+  }
+}
+
+// Shared state of one CTA: the A operand of each channel (its S split
+// terms; K-major or M-major depending on the pass -- each pass's input is
+// consumed before the next is written) and the transform matrices.
+template <int N, int S>
+struct Smem {
+  static constexpr int kOpBytes = 128 * N * 2;  // 128 x N BF16
+  static constexpr int kMatBytes = N * N * 2;
+  alignas(128) uint8_t a[3][S * kOpBytes];
+  alignas(128) uint8_t idct[S * kMatBytes];
+  alignas(128) uint8_t dct[S * kMatBytes];
+  float corner[128][N / 4 + 1];  // HF prediction: 2 N/8 corner rows per row
+  alignas(8) uint64_t mbar;
+  uint32_t tmem;
+};
+
+// Tensor-memory column of channel c's accumulator j (0 or 1).
+template <int N>
+__device__ __forceinline__ uint32_t AccCol(int c, int j) {
+  return uint32_t(c * 2 * N + j * N);
+}
+
+// One split-BF16 GEMM pass for the three channels: D(c, j) = A(c) * B^T over
+// K = N, then waits for it. Called by all threads after writing their rows
+// of the A operands.
+template <int N, int S>
+__device__ __forceinline__ bool Pass(Smem<N, S>& s, int j, bool a_mn,
+                                     const uint8_t* b, uint32_t& phase) {
+  using Sm = Smem<N, S>;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  FenceBefore();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    FenceAfter();
+    const uint32_t idesc = Idesc(128, N, a_mn ? 1 : 0);
+    constexpr uint32_t sbo = (N / 8) * 128;
+    // Split-term pairs (i, k) with i + k <= S - 1 (S = 2: three products;
+    // S = 3: six), largest first.
+    constexpr int kPairs = S == 2 ? 3 : 6;
+    constexpr int pi[6] = {0, 0, 1, 0, 2, 1};
+    constexpr int pk[6] = {0, 1, 0, 2, 0, 1};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const uint32_t d = s.tmem + AccCol<N>(c, j);
+#pragma unroll
+      for (int kk = 0; kk < N / 16; ++kk) {
+#pragma unroll
+        for (int p = 0; p < kPairs; ++p) {
+          Mma(d, Desc(s.a[c] + pi[p] * Sm::kOpBytes + kk * 256, 128, sbo),
+              Desc(b + pk[p] * Sm::kMatBytes + kk * 256, 128, sbo), idesc,
+              (kk > 0 || p > 0) ? 1u : 0u);
+        }
+      }
+    }
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster."
+        "b64 [%0];" ::"r"(SmemU32(&s.mbar))
+        : "memory");
+  }
+  const uint32_t mb = SmemU32(&s.mbar);
+  bool ok = false;
+  for (uint32_t it = 0; it < kMaxPolls; ++it) {
+    if (TryWait(mb, phase)) {
+      ok = true;
+      break;
+    }
+  }
+  phase ^= 1u;
+  FenceAfter();
+  return ok;
+}
+
+// This thread's row of D (N FP32 columns from dcol).
+template <int N, int S>
+__device__ __forceinline__ void LoadRow(const Smem<N, S>& s, uint32_t dcol,
+                                        float* v) {
+  const uint32_t lane_base = (threadIdx.x & ~31u) << 16;
+#pragma unroll
+  for (int c = 0; c < N; c += 16) Ld16(s.tmem + lane_base + dcol + c, v + c);
+}
+
+// Transform matrix (row-major n x k in constant memory) as a K-major BF16
+// hi/lo B operand.
+template <int N, int S>
+__device__ __forceinline__ void PutMatrix(uint8_t* base, const float* m) {
+  for (int i = threadIdx.x; i < N * N / 8; i += kThreads) {
+    const int n = i / (N / 8), kc = i % (N / 8);
+    float v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = m[n * N + kc * 8 + e];
+    PutChunk<S>(base, N * N * 2,
+                (n >> 3) * (N / 8) * 128 + kc * 128 + (n & 7) * 16, v);
+  }
+}
+
+}  // namespace tc
+
+// UpsampleRow with fused multiply-adds (the tensor-core forms are not
+// bound to the reference's rounding of every product).
+template <int N>
+__device__ __forceinline__ void UpsampleRowFma(const float* pred, int X0,
+                                               int Y, float* out) {
+  const int r = Y >> 2, q0 = X0 >> 2, iy = Y & 3;
+  constexpr int W = N / 4 + 2;
+  float src[3][W];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const float* row = pred + (r + j + 1) * kG2 + q0 + 1;
+#pragma unroll
+    for (int i = 0; i < W; ++i) src[j][i] = row[i];
+  }
+  const float v0 = c_t.ub4[0][iy], v1 = c_t.ub4[1][iy], v2 = c_t.ub4[2][iy];
+#pragma unroll
+  for (int x = 0; x < N; ++x) {
+    const int q = x >> 2, ix = x & 3;
+    const float h0 = c_t.ub4[0][ix], h1 = c_t.ub4[1][ix], h2 = c_t.ub4[2][ix];
+    float bx[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      bx[j] = fmaf(src[j][q + 2], h2,
+                   fmaf(src[j][q + 1], h1, src[j][q] * h0));
+    }
+    out[x] = fmaf(bx[2], v2, fmaf(bx[1], v1, bx[0] * v0));
+  }
+}
+
+// HF prediction + AddBlockExceptLFAndLLFTo + IDCT for square DCT blocks on
+// the tensor cores (split-BF16 form of k_square_idct_rows). Persistent CTAs
+// of 128 threads; an item is a batch of 128 / N blocks in all three
+// channels (one MMA wait per pass for the three).
+template <int N, int S>
+__global__ void __launch_bounds__(tc::kThreads, 4)
+    k_square_idct_tc(Geo g, DevFrame f, const uint32_t* list, int count,
+                     int predict_hf, int* err) {
+  using namespace tc;
+  using square::CoefRowOffset;
+  constexpr int BPB = 128 / N;  // blocks per batch
+  constexpr int cov = N / 8;
+  __shared__ Smem<N, S> s;
+  const int t = threadIdx.x, bl = t / N, r = t % N;
+  if (t < 32) {
+    asm volatile(
+        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
+            "r"(SmemU32(&s.tmem)),
+        "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
+        SmemU32(&s.mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  PutMatrix<N, S>(s.idct, c_t.idct + MatOffset(N));
+  PutMatrix<N, S>(s.dct, c_t.dct + MatOffset(N));
+  FenceBefore();
+  __syncthreads();
+  FenceAfter();
+  uint32_t phase = 0;
+  const int nbat = (count + BPB - 1) / BPB;
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
+  const size_t plane_px = size_t(g.PW) * g.PH;
+  const float inv_nn = 1.0f / float(N * N);
+  bool ok = true;
+  for (int batch = blockIdx.x; batch < nbat && ok; batch += gridDim.x) {
+    const int idx = batch * BPB + bl;
+    const bool active = idx < count;
+    const uint32_t pkd = list[active ? idx : 0];
+    const int bx = pkd & 0xFFFF, by = pkd >> 16;
+    float X[3][N];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float* crow = f.ac + c * plane_ac + CoefRowOffset(g, bx, by, N, r);
+#pragma unroll
+      for (int i = 0; i < N; i += 4) {
+        const float4 v = active ? *reinterpret_cast<const float4*>(crow + i)
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+        X[c][i] = v.x, X[c][i + 1] = v.y, X[c][i + 2] = v.z,
+        X[c][i + 3] = v.w;
+      }
+    }
+    // HF prediction: adding the predicted coefficients outside the
+    // 2cov x 2cov corner and transforming back equals transforming the
+    // coefficients minus that corner of DCT(P) and adding P (IDCT(DCT(P))
+    // = P), so only the corner is computed: per channel, the corner rows of
+    // the row DCT of this pixel row, then the column sums over the block's
+    // N rows (lanes) by shuffles.
+    float P[3][N];
+    bool hf = false;
+    if (predict_hf) {
+      hf = active && PredictHFOf(f.acs[by * g.Bx + bx] >> 4);
+      const int gi = (by >> 6) * g.Gx + (bx >> 6);
+      const int X0 = (bx & 63) * 8, Y = (by & 63) * 8 + r;
+      constexpr int K = 2 * cov;
+      const float* B = c_t.dct + MatOffset(N);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+        if (hf) {
+          UpsampleRowFma<N>(pred, X0, Y, P[c]);
+        } else {
+#pragma unroll
+          for (int x = 0; x < N; ++x) P[c][x] = 0.f;
+        }
+        // Corner rows of the row DCT of this pixel row, shared with the
+        // block's other rows (the block's N rows are N lanes of one warp).
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          float a = 0.f;
+#pragma unroll
+          for (int x = 0; x < N; ++x) a = fmaf(B[k * N + x], P[c][x], a);
+          s.corner[t][k] = a;
+        }
+        __syncwarp();
+        if (hf && r < K) {
+#pragma unroll
+          for (int l = 0; l < K; ++l) {
+            float v = 0.f;
+#pragma unroll
+            for (int y = 0; y < N; ++y) {
+              v = fmaf(B[l * N + y], s.corner[N * bl + y][r], v);
+            }
+            X[c][l] -= v * inv_nn;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    float T[N];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) PutRowK<N, S>(s.a[c], t, X[c]);
+    ok = Pass<N, S>(s, 0, false, s.idct, phase) && ok;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      LoadRow<N, S>(s, AccCol<N>(c, 0), T);  // T[k = r][v]
+      PutColMN<N, S>(s.a[c], N * bl, r, T);
+    }
+    ok = Pass<N, S>(s, 1, true, s.idct, phase) && ok;
+    ok = __syncthreads_and(ok);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      LoadRow<N, S>(s, AccCol<N>(c, 1), T);  // pixel row v = r
+      if (hf) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) T[i] += P[c][i];
+      }
+      if (active && ok) {
+        float* out = f.idct + c * plane_px + size_t(by * 8 + r) * g.PW + bx * 8;
+#pragma unroll
+        for (int i = 0; i < N; i += 4) {
+          *reinterpret_cast<float4*>(out + i) =
+              make_float4(T[i], T[i + 1], T[i + 2], T[i + 3]);
+        }
+      }
+    }
+  }
+  if (!ok && t == 0) atomicExch(err, 1);
+  FenceBefore();
+  __syncthreads();
+  if (t < 32) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
+                     s.tmem),
+                 "r"(kTmemCols));
+  }
+}
+
+}  // namespace pikgpu

@@ -21,6 +21,8 @@ STAGES = {"dc": 0, "idct": 1, "smoothed": 2, "epf": 3, "ar": 4,
           "pre_opsin": 5, "dequant_ac": 6}
 OPT_KEEP_STAGES = 1
 OPT_PROFILE = 2
+OPT_FORM = 3
+FORMS = {"fp32": 0, "split_bf16": 1, "split_bf16x3": 2}
 
 _lib = None
 
@@ -104,7 +106,7 @@ class Context:
     """One pikgpu context (device memory + stream)."""
 
     def __init__(self, device: int = 0, *, keep_stages: bool = False,
-                 profile: bool = False):
+                 profile: bool = False, form: str = "fp32"):
         self.L = lib()
         h = ctypes.c_void_p()
         rc = self.L.pikgpu_ctx_create(device, ctypes.byref(h))
@@ -114,6 +116,7 @@ class Context:
         self._check(self.L.pikgpu_set_option(h, OPT_KEEP_STAGES,
                                              int(keep_stages)))
         self._check(self.L.pikgpu_set_option(h, OPT_PROFILE, int(profile)))
+        self._check(self.L.pikgpu_set_option(h, OPT_FORM, FORMS[form]))
         self.frame = None
         self._packed = None
 

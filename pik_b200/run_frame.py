@@ -1,7 +1,7 @@
 """Reconstructs a frozen frame file (layout.Frame .npz) on the GPU.
 
     python -m pik_b200.run_frame FRAME.npz [--crop W H] [--reps N]
-           [--out linear.npy]
+           [--form fp32|split_bf16|split_bf16x3] [--out linear.npy]
 
 `--crop` keeps the top-left W x H pixels (multiples of 64 keep the colour
 tiles and transform placement intact), which makes small cases of a large
@@ -51,11 +51,12 @@ def main(argv=None) -> int:
     ap.add_argument("--crop", nargs=2, type=int)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--out")
+    ap.add_argument("--form", default="fp32", choices=sorted(native.FORMS))
     args = ap.parse_args(argv)
     frame = layout.Frame.load(args.frame)
     if args.crop:
         frame = crop(frame, *args.crop)
-    ctx = native.Context(0)
+    ctx = native.Context(0, form=args.form)
     ctx.begin(frame)
     ctx.set_ac()
     t = time.perf_counter()
