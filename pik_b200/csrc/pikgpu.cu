@@ -531,7 +531,20 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
           g, f, s, P<uint32_t>(ctx->active[kC8]), counters + kC8);
       ++ctx->launches;
     }
-    if (n[kC16]) {
+    if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
+      const int grid =
+          std::min((n[kC16] + 7) / 8, ctx->num_sms * kTcCtasPerSm);
+      if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
+        k_square_ar_tc<16, 2><<<grid, tc::kThreads, 0, st>>>(
+            g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
+            P<int>(ctx->tc_err));
+      } else {
+        k_square_ar_tc<16, 3><<<grid, tc::kThreads, 0, st>>>(
+            g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
+            P<int>(ctx->tc_err));
+      }
+      ++ctx->launches;
+    } else if (n[kC16]) {
       k_square_ar_rows<16><<<rows_grid(n[kC16], 16), kSquareThreads, 0,
                              st>>>(g, f, s, P<uint32_t>(ctx->active[kC16]),
                                    counters + kC16);

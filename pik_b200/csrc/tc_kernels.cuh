@@ -413,4 +413,140 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
   }
 }
 
+// AdaptiveReconstruction clamp for square DCT blocks on the tensor cores
+// (split-BF16 form of k_square_ar_rows, pik/adaptive_reconstruction.cc:
+// 128-244, 334-471): DCT of (filtered - original) for the three channels,
+// the clamp ratio of each coefficient (minimum over X, Y, B) in registers,
+// then the IDCT of the scaled correction added to the original. `count` is
+// read from device memory (the compacted list of k_active_blocks).
+template <int N, int S>
+__global__ void __launch_bounds__(tc::kThreads, 4)
+    k_square_ar_tc(Geo g, DevFrame f, FrameScalars sc, const uint32_t* list,
+                   const int* count_ptr, int* err) {
+  using namespace tc;
+  constexpr int BPB = 128 / N;
+  constexpr int cov = N / 8;
+  __shared__ Smem<N, S> s;
+  const int t = threadIdx.x, bl = t / N, r = t % N;
+  if (t < 32) {
+    asm volatile(
+        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
+            "r"(SmemU32(&s.tmem)),
+        "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
+        SmemU32(&s.mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  PutMatrix<N, S>(s.idct, c_t.idct + MatOffset(N));
+  PutMatrix<N, S>(s.dct, c_t.dct + MatOffset(N));
+  FenceBefore();
+  __syncthreads();
+  FenceAfter();
+  uint32_t phase = 0;
+  const int count = *count_ptr;
+  const int nbat = (count + BPB - 1) / BPB;
+  const size_t plane = size_t(g.PW) * g.PH;
+  const float inv_nn = 1.0f / float(N * N);
+  bool ok = true;
+  for (int batch = blockIdx.x; batch < nbat && ok; batch += gridDim.x) {
+    const int idx = batch * BPB + bl;
+    const bool active = idx < count;
+    const uint32_t pkd = list[active ? idx : 0];
+    const int bx = pkd & 0xFFFF, by = pkd >> 16;
+    const size_t row0 = size_t(by * 8 + r) * g.PW + bx * 8;
+    float T[N];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int x = 0; x < N; x += 4) {
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), o = a;
+        if (active) {
+          a = *reinterpret_cast<const float4*>(f.filt + c * plane + row0 + x);
+          o = *reinterpret_cast<const float4*>(f.idct + c * plane + row0 + x);
+        }
+        T[x] = a.x - o.x, T[x + 1] = a.y - o.y;
+        T[x + 2] = a.z - o.z, T[x + 3] = a.w - o.w;
+      }
+      PutRowK<N, S>(s.a[c], t, T);  // pixel row y = r of the correction
+    }
+    ok = Pass<N, S>(s, 0, false, s.dct, phase);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      LoadRow<N, S>(s, AccCol<N>(c, 0), T);  // t_y[k]
+      PutColMN<N, S>(s.a[c], N * bl, r, T);
+    }
+    ok = Pass<N, S>(s, 1, true, s.dct, phase) && ok;
+    float Y[3][N];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      LoadRow<N, S>(s, AccCol<N>(c, 1), Y[c]);  // coefficient row k = r
+#pragma unroll
+      for (int l = 0; l < N; ++l) Y[c][l] *= inv_nn;
+    }
+    // Clamp ratios of coefficient row k = r, minimum over the channels.
+    {
+      const int type = f.acs[by * g.Bx + bx] >> 4;
+      const int qac = f.qf[by * g.Bx + bx];
+      const float inv_quant_ac = sc.inv_global_scale / float(qac);
+      const int cf = f.dq_cf[(by >> 3) * g.Tx + (bx >> 3)];
+      const int table = f.dq_map[cf * 256 + (qac - 1)];
+      const int kind = QuantKindOf(type);
+      const float* dm[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dm[c] = f.table + f.offsets[(table * 7 + kind) * 3 + c] + r * N;
+      }
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        const bool llf = r < cov && l < cov;
+        const float ls = llf ? LlfScale(type, l, r) : 0.f;
+        float mr = 1.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float rt = ClampRatio(
+              Y[c][l], llf ? ls * sc.mul_dc[c] : dm[c][l] * inv_quant_ac);
+          mr = rt < mr ? rt : mr;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Y[c][l] = Y[c][l] * mr;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) PutRowK<N, S>(s.a[c], t, Y[c]);
+    ok = Pass<N, S>(s, 0, false, s.idct, phase) && ok;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      LoadRow<N, S>(s, AccCol<N>(c, 0), T);
+      PutColMN<N, S>(s.a[c], N * bl, r, T);
+    }
+    ok = Pass<N, S>(s, 1, true, s.idct, phase) && ok;
+    ok = __syncthreads_and(ok);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      LoadRow<N, S>(s, AccCol<N>(c, 1), T);  // pixel row v = r
+      if (active && ok) {
+#pragma unroll
+        for (int x = 0; x < N; x += 4) {
+          const float4 o =
+              *reinterpret_cast<const float4*>(f.idct + c * plane + row0 + x);
+          *reinterpret_cast<float4*>(f.filt + c * plane + row0 + x) =
+              make_float4(T[x] + o.x, T[x + 1] + o.y, T[x + 2] + o.z,
+                          T[x + 3] + o.w);
+        }
+      }
+    }
+  }
+  if (!ok && t == 0) atomicExch(err, 1);
+  FenceBefore();
+  __syncthreads();
+  if (t < 32) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
+                     s.tmem),
+                 "r"(kTmemCols));
+  }
+}
+
 }  // namespace pikgpu
