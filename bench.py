@@ -10,7 +10,9 @@ One step = one full reconstruction of that frame (integer coefficients ->
 FP32 linear RGB), the reference's Dequant::DoAC + ReconOpsinImage over all
 groups + FinalizeFrameDecoding.
 
-  value  decoded MP/s with the inputs resident in device memory
+  value  decoded MP/s with the inputs resident in device memory, in the
+         form chosen by --form (default: split-BF16 tensor-core transforms);
+         "forms" gives every form's throughput on the same frame
   e2e    the same through the C ABI with host buffers: each step uploads the
          frame's side information and int16 coefficients from pinned host
          memory and reads the FP32 linear planes back.
@@ -43,6 +45,16 @@ METRIC = ("decoded MP/s at 4K, split-BF16 vs FP32 form @<=2e-5 err; "
 # Algorithmic bytes per pixel of the path: int16 AC in (6), DC (0.1875),
 # side info (0.094), CfL maps (~0.002), FP32 linear RGB out (12).
 PATH_BYTES_PER_PX = 18.28
+# Arithmetic forms of the reconstruction (PIKGPU_OPT_FORM). The headline is
+# the split-BF16 form; every form is timed on the same frame. Their errors
+# against the FP64 oracle are checked by tests/test_split_bf16.py.
+FORM_NAMES = {
+    "fp32": "plain FP32 on CUDA cores (bit-exact to the FP32 oracle)",
+    "split_bf16": "16x16 transforms on tcgen05 tensor cores, split-BF16 "
+                  "(hi+lo, 3 products, FP32 accumulate)",
+    "split_bf16x3": "16x16 transforms on tcgen05 tensor cores, split-BF16 "
+                    "(hi+mid+lo, 6 products, FP32 accumulate)",
+}
 
 
 def load_peaks():
@@ -196,6 +208,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours")
+    ap.add_argument("--form", default="split_bf16",
+                    choices=sorted(FORM_NAMES))
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -213,45 +227,61 @@ def main():
     by, bx = frame.blocks
     dev = torch.device("cuda", local)
 
-    # Device-resident run: AC already in HBM, outputs into device buffers.
-    ctx = native.Context(local)
-    ctx.begin(frame)
+    # Device-resident runs: AC already in HBM, outputs into device buffers.
     ac_dev = torch.from_numpy(frame.quantized_ac).to(dev)
     lin_dev = torch.empty((3, frame.ysize, frame.xsize), dtype=torch.float32,
                           device=dev)
     stream = torch.cuda.Stream(device=dev)
-    ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
     import ctypes
     planes = (ctypes.c_void_p * 3)(*[ac_dev[c].data_ptr() for c in range(3)])
 
-    def step():
-        ctx._check(ctx.L.pikgpu_frame_set_ac_device(ctx.h, planes, bx * 64))
-        ctx.reconstruct_device(lin_dev.data_ptr(), frame.xsize)
+    def time_device(form, sample_clocks=False):
+        ctx = native.Context(local, form=form)
+        ctx.begin(frame)
+        ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
 
-    for _ in range(max(3, args.warmup)):
-        step()
-    launches = ctx.L.pikgpu_last_launch_count(ctx.h)
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+        def step():
+            ctx._check(ctx.L.pikgpu_frame_set_ac_device(ctx.h, planes,
+                                                        bx * 64))
+            ctx.reconstruct_device(lin_dev.data_ptr(), frame.xsize)
+
+        for _ in range(max(3, args.warmup)):
+            step()
+        n_launch = ctx.L.pikgpu_last_launch_count(ctx.h)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        clk = ClockSampler(local) if sample_clocks else None
+        if clk:
+            clk.__enter__()
         torch.cuda.synchronize()
         start.record(stream)
         for _ in range(args.steps):
             step()
         end.record(stream)
         torch.cuda.synchronize()
-    ms = start.elapsed_time(end) / args.steps
-    if ws > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        if clk:
+            clk.__exit__()
+        t = start.elapsed_time(end) / args.steps
+        if ws > 1:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        ctx.close()
+        return t, n_launch, clk
+
+    ms, launches, clk = time_device(args.form, sample_clocks=True)
     value = ws * px / (ms * 1e-3) / 1e6
+    # The other forms on the same frame, for the form comparison.
+    forms = {args.form: ms}
+    for form in native.FORMS:
+        if form not in forms:
+            forms[form] = time_device(form)[0]
 
     # Per-kernel-group device times (CUDA events on the launching stream).
-    pctx = native.Context(local, profile=True)
+    pctx = native.Context(local, profile=True, form=args.form)
     pctx.begin(frame)
     pctx.L.pikgpu_set_stream(pctx.h, stream.cuda_stream)
     pctx._check(pctx.L.pikgpu_frame_set_ac_device(pctx.h, planes, bx * 64))
@@ -264,6 +294,8 @@ def main():
     pctx.close()
 
     # End to end through the C ABI with pinned host buffers.
+    ctx = native.Context(local, form=args.form)
+    ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
     pin = {
         "ac": torch.from_numpy(frame.quantized_ac).pin_memory(),
         "lin": torch.empty((3, frame.ysize, frame.xsize),
@@ -290,13 +322,10 @@ def main():
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    # Host wall clock: the region includes host-side validation and uploads.
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     if ws > 1:
@@ -340,7 +369,7 @@ def main():
                 "workload": "c2: 3840x2160 generator image, reference-encoded"
                             " at distance 1.0 (mixed blocks, adaptive qf, CfL,"
                             " gaborish + EPF on)",
-                "form": "plain FP32 (CUDA cores)",
+                "form": FORM_NAMES[args.form],
                 "l2": "working set > L2 (inputs 50 MB, planes 100 MB each)",
                 "parallelism": f"replicas x{ws}"},
             "roofline": {"bound": "hbm", "kernel": top,
@@ -352,6 +381,10 @@ def main():
                          "path_frac": round(PATH_BYTES_PER_PX * px /
                                             (ms * 1e-3) / 1e9 / peak, 4)},
             "kernel_ms": {k: round(v, 4) for k, v in acc.items()},
+            "forms": {f: {"value": round(ws * px / (t * 1e-3) / 1e6, 2),
+                          "ms_per_step": round(t, 4)}
+                      for f, t in forms.items()},
+            "speedup_vs_fp32": round(forms["fp32"] / ms, 3),
             "e2e": {"value": round(e2e, 2), "unit": "MP/s",
                     "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
