@@ -6,11 +6,12 @@
 // 32 apart (so the 32 lanes of a warp read 32 consecutive values of every
 // shared-memory row), four rows inside one 8x8 block row.
 //
-// The u8 guide is staged in shared memory as four copies, copy s holding at
-// word k the bytes 4k + s .. 4k + s + 3 of the row. The 4 guide bytes of a
-// patch row at any byte offset are then one 32-bit load, and the sum of
-// absolute differences against the centre pixel's patch row is one
-// __vsadu4. For every displacement (cy, cx) of the 7 x 8 neighbourhood and
+// The u8 guide is staged in shared memory as one 32-bit word per byte
+// offset: word o of a row holds the guide bytes o .. o + 3. The 4 guide bytes
+// of a patch row at any offset are then one 32-bit load (and the 32 lanes'
+// loads of 32 consecutive offsets hit 32 consecutive words, free of bank
+// conflicts), and the sum of absolute differences against the centre
+// pixel's patch row is one __vsadu4. For every displacement (cy, cx) of the 7 x 8 neighbourhood and
 // every channel, a lane forms the 6 patch-row SADs of each of its columns and
 // sums them vertically into the 3 x 4 patch SADs of its 4 rows; the SAD is
 // the maximum over the channels. The SADs are exact integers; the weights
@@ -32,10 +33,9 @@ namespace pikgpu {
 constexpr int kEpfW = 64, kEpfH = 32;   // output tile
 constexpr int kEpfThreads = 256;
 constexpr int kEpfGH = kEpfH + 8;       // guide rows: y0 - 4 .. y0 + 35
-constexpr int kEpfGWords = 20;          // guide bytes x0 - 8 .. x0 + 71
-// Words per shifted copy; = 8 (mod 32), so that the 32 lanes' loads of 32
-// consecutive byte offsets fall in (at most one pair excepted) distinct banks.
-constexpr int kEpfCopyWords = kEpfGH * kEpfGWords + 8;
+constexpr int kEpfGBytes = 80;          // guide bytes x0 - 8 .. x0 + 71
+constexpr int kEpfGRow = kEpfGBytes;    // words per guide row (one per byte)
+constexpr int kEpfGPlane = kEpfGH * kEpfGRow;
 // Input tile with a 5-pixel halo (enough for gaborish at the guide's
 // 4-pixel halo): rows y0 - 5 .. y0 + 36, cols x0 - 12 .. x0 + 75 (the
 // column range is widened to 16-byte boundaries for vector loads).
@@ -43,7 +43,7 @@ constexpr int kEpfTH = kEpfH + 10;
 constexpr int kEpfTW = kEpfW + 24;
 constexpr int kEpfTS = kEpfTW;               // row stride in floats
 constexpr int kEpfTRow0 = 2, kEpfTCol0 = 9;  // tile index of (y0-3, x0-3)
-constexpr size_t kEpfGuideWords = size_t(3) * 4 * kEpfCopyWords;
+constexpr size_t kEpfGuideWords = size_t(3) * kEpfGPlane;
 constexpr size_t kEpfSmemBytes =
     kEpfGuideWords * 4 + size_t(3) * kEpfTH * kEpfTS * 4;
 
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
               const uint8_t* guide_ovr, int gab, int w, int h,
               const uint32_t* mm, const int32_t* sigma, float* out) {
   extern __shared__ __align__(16) uint32_t epf_smem[];
-  uint32_t* sg = epf_smem;  // [3][4][kEpfCopyWords]
+  uint32_t* sg = epf_smem;  // [3][kEpfGH][kEpfGRow]
   float(*tile)[kEpfTH][kEpfTS] =
       reinterpret_cast<float(*)[kEpfTH][kEpfTS]>(epf_smem + kEpfGuideWords);
   const int x0 = blockIdx.x * kEpfW, y0 = blockIdx.y * kEpfH;
@@ -139,10 +139,12 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
     const float x2 = sum_t2 + sum_b2;
     return x2 * gw[2] + mul1;
   };
-  // u8 guide (MakeGuide, pik/epf_target.cc:1009-1070) into copy 0.
-  for (int i = tid; i < 3 * kEpfGH * kEpfGWords; i += kEpfThreads) {
-    const int c = i / (kEpfGH * kEpfGWords);
-    const int r = (i / kEpfGWords) % kEpfGH, wd = i % kEpfGWords;
+  // u8 guide (MakeGuide, pik/epf_target.cc:1009-1070): the aligned words
+  // (offsets 4 wd) first.
+  constexpr int kAligned = kEpfGBytes / 4;
+  for (int i = tid; i < 3 * kEpfGH * kAligned; i += kEpfThreads) {
+    const int c = i / (kEpfGH * kAligned);
+    const int r = (i / kAligned) % kEpfGH, wd = i % kAligned;
     const int gy = y0 - 4 + r;
     uint32_t word = 0;
     if (interior && !guide_ovr) {
@@ -194,18 +196,21 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
         word |= v << (8 * b);
       }
     }
-    sg[(c * 4) * kEpfCopyWords + r * kEpfGWords + wd] = word;
+    sg[c * kEpfGPlane + r * kEpfGRow + 4 * wd] = word;
   }
   __syncthreads();
-  // Copies 1..3: byte-shifted words of copy 0.
-  for (int i = tid; i < 3 * 3 * kEpfGH * kEpfGWords; i += kEpfThreads) {
-    const int c = i / (3 * kEpfGH * kEpfGWords);
-    const int s = 1 + (i / (kEpfGH * kEpfGWords)) % 3;
-    const int rk = i % (kEpfGH * kEpfGWords), k = rk % kEpfGWords;
-    const uint32_t* c0 = sg + (c * 4) * kEpfCopyWords;
-    const uint32_t lo = c0[rk];
-    const uint32_t hi = k + 1 < kEpfGWords ? c0[rk + 1] : 0u;
-    sg[(c * 4 + s) * kEpfCopyWords + rk] = __funnelshift_r(lo, hi, 8 * s);
+  // The other offsets 4 wd + s, s = 1..3, from the two aligned neighbours
+  // (bytes past the row end read as 0).
+  for (int i = tid; i < 3 * kEpfGH * kAligned * 3; i += kEpfThreads) {
+    const int s = 1 + i % 3;
+    const int j = i / 3;
+    const int c = j / (kEpfGH * kAligned);
+    const int r = (j / kAligned) % kEpfGH, wd = j % kAligned;
+    const uint32_t* row = sg + c * kEpfGPlane + r * kEpfGRow;
+    const uint32_t lo = row[4 * wd];
+    const uint32_t hi = wd + 1 < kAligned ? row[4 * wd + 4] : 0u;
+    sg[c * kEpfGPlane + r * kEpfGRow + 4 * wd + s] =
+        __funnelshift_r(lo, hi, 8 * s);
   }
   __syncthreads();
 
@@ -232,17 +237,15 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
   const int gr0 = 4 * wp + 3;  // guide smem row of py0 - 1
   uint32_t ref[3][6][2];
   {
-    const int off = lane + 7;  // byte offset of px - 1 from x0 - 8 (i = 0)
-    const uint32_t* g = sg + (off & 3) * kEpfCopyWords + gr0 * kEpfGWords +
-                        (off >> 2);
+    // Byte offset of px - 1 from x0 - 8 (i = 0; i = 1 is 32 further).
+    const uint32_t* g = sg + gr0 * kEpfGRow + lane + 7;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int r = 0; r < 6; ++r)
 #pragma unroll
         for (int i = 0; i < 2; ++i)
-          ref[c][r][i] =
-              g[c * 4 * kEpfCopyWords + r * kEpfGWords + 8 * i];
+          ref[c][r][i] = g[c * kEpfGPlane + r * kEpfGRow + 32 * i];
   }
 
   float ws[3][8], sw[8];
@@ -255,9 +258,8 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
   for (int cy = -3; cy <= 3; ++cy) {
 #pragma unroll 1
     for (int cx = -3; cx <= 4; ++cx) {
-      const int off = lane + 7 + cx;  // window byte offset (i = 0)
-      const uint32_t* g = sg + (off & 3) * kEpfCopyWords +
-                          (gr0 + cy) * kEpfGWords + (off >> 2);
+      // Window byte offset (i = 0): the patch start moved by cx.
+      const uint32_t* g = sg + (gr0 + cy) * kEpfGRow + lane + 7 + cx;
       int sad[8];  // [j * 2 + i]
 #pragma unroll
       for (int p = 0; p < 8; ++p) sad[p] = 0;
@@ -269,8 +271,7 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
 #pragma unroll
           for (int r = 0; r < 6; ++r) {
             hs[r] = int(__vsadu4(
-                ref[c][r][i],
-                g[c * 4 * kEpfCopyWords + r * kEpfGWords + 8 * i]));
+                ref[c][r][i], g[c * kEpfGPlane + r * kEpfGRow + 32 * i]));
           }
           const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
           sad[0 + i] = max(sad[0 + i], hs[0] + p12);
