@@ -221,6 +221,30 @@ int pikgpu_get_epf_decisions(pikgpu_ctx* ctx, uint8_t* guide, int32_t* sigma);
  * on; NULL restores the context's own stream. */
 int pikgpu_set_stream(pikgpu_ctx* ctx, void* stream);
 
+/* Batched reconstruction of many frames of uneven sizes. No counterpart in
+ * the reference, which reconstructs one frame per FinalizeFrameDecoding
+ * call. A batch owns one context per frame: fill each with
+ * pikgpu_frame_begin / pikgpu_frame_set_ac(_device) / pikgpu_set_option on
+ * the context that pikgpu_batch_frame returns. pikgpu_batch_reconstruct
+ * then runs all frames at once: on its first call (and after any frame's
+ * frame_begin, set_option or set_epf_decisions, or a change of outputs) it
+ * captures every frame's launch sequence into one CUDA graph, one branch
+ * per frame, and it replays that graph. Outputs are device pointers: frame
+ * i writes 3 consecutive planes of linear_strides[i] x ysize floats at
+ * out_linear[i]. `stream` (a cudaStream_t, NULL = the batch's own stream)
+ * is where the graph runs; the call blocks until it is done. Profiling
+ * (PIKGPU_OPT_PROFILE) is UNSUPPORTED in a batch. */
+typedef struct pikgpu_batch pikgpu_batch;
+int pikgpu_batch_create(int device, int num_frames, pikgpu_batch** out);
+int pikgpu_batch_destroy(pikgpu_batch* batch);
+pikgpu_ctx* pikgpu_batch_frame(pikgpu_batch* batch, int index);
+int pikgpu_batch_reconstruct(pikgpu_batch* batch, float* const* out_linear,
+                             const size_t* linear_strides, void* stream);
+const char* pikgpu_batch_last_error(const pikgpu_batch* batch);
+/* Kernels launched per replay, and graphs captured so far. */
+int pikgpu_batch_launch_count(const pikgpu_batch* batch);
+int pikgpu_batch_capture_count(const pikgpu_batch* batch);
+
 /* Allocation-free DC reconstruction. No counterpart in the reference: its
  * DequantDC + AdaptiveDCReconstruction (pik/compressed_dc.cc:181-231,
  * pik/adaptive_reconstruction.cc:300-332) allocate their images as they go.

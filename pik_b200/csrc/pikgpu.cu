@@ -88,6 +88,9 @@ struct pikgpu_ctx {
   float times[kNumTimed] = {};
   float dc_half_step[3] = {};
   int launches = 0;
+  // Bumped by every call that changes what the launch sequence does or
+  // which buffers it uses (a captured batch graph is then stale).
+  uint64_t generation = 0;
 };
 
 namespace {
@@ -673,6 +676,7 @@ int pikgpu_set_stream(pikgpu_ctx* ctx, void* stream) {
 
 int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  ++ctx->generation;
   switch (option) {
     case PIKGPU_OPT_KEEP_STAGES:
       ctx->keep_stages = value != 0;
@@ -693,6 +697,7 @@ int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
 
 int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  ++ctx->generation;
   ctx->have_frame = ctx->have_ac = ctx->have_result = false;
   ctx->use_guide_ovr = ctx->use_sigma_ovr = false;
   int rc = Validate(ctx, p);
@@ -1033,6 +1038,7 @@ int pikgpu_set_epf_decisions(pikgpu_ctx* ctx, const uint8_t* guide,
                              const int32_t* sigma) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
+  ++ctx->generation;
   const Geo& g = ctx->g;
   int rc;
   ctx->use_guide_ovr = guide != nullptr;
@@ -1106,3 +1112,4 @@ const char* pikgpu_kernel_name(int index) {
 }  // extern "C"
 
 #include "dc_noalloc.cu"
+#include "batch.cu"

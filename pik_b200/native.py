@@ -69,6 +69,17 @@ def lib() -> ctypes.CDLL:
     L.pikgpu_dc_reconstruct_noalloc.argtypes = [
         P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
         P, ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_char_p, S]
+    L.pikgpu_batch_create.argtypes = [ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(P)]
+    L.pikgpu_batch_destroy.argtypes = [P]
+    L.pikgpu_batch_frame.restype = P
+    L.pikgpu_batch_frame.argtypes = [P, ctypes.c_int]
+    L.pikgpu_batch_reconstruct.argtypes = [P, ctypes.POINTER(P),
+                                           ctypes.POINTER(S), P]
+    L.pikgpu_batch_last_error.restype = ctypes.c_char_p
+    L.pikgpu_batch_last_error.argtypes = [P]
+    L.pikgpu_batch_launch_count.argtypes = [P]
+    L.pikgpu_batch_capture_count.argtypes = [P]
     _lib = L
     return L
 
@@ -120,9 +131,21 @@ class Context:
         self.frame = None
         self._packed = None
 
+    @classmethod
+    def borrowed(cls, handle: int) -> "Context":
+        """A view of a context owned by something else (a batch frame)."""
+        self = cls.__new__(cls)
+        self.L = lib()
+        self.h = ctypes.c_void_p(handle)
+        self._owned = False
+        self.frame = None
+        self._packed = None
+        return self
+
     def close(self) -> None:
         if getattr(self, "h", None):
-            self.L.pikgpu_ctx_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.L.pikgpu_ctx_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -208,3 +231,49 @@ class Context:
         self._check(n)
         return {self.L.pikgpu_kernel_name(i).decode(): float(ms[i])
                 for i in range(n)}
+
+
+class Batch:
+    """pikgpu_batch: frames of uneven sizes reconstructed together by one
+    captured CUDA graph (one branch per frame). Frame i is configured through
+    `self.frames[i]` (a Context view: begin, set_ac, set_decisions)."""
+
+    def __init__(self, num_frames: int, device: int = 0, *,
+                 form: str = "fp32"):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        rc = self.L.pikgpu_batch_create(device, num_frames, ctypes.byref(h))
+        if rc != OK:
+            raise PikGpuError(rc, "pikgpu_batch_create failed")
+        self.h = h
+        self.frames = [Context.borrowed(self.L.pikgpu_batch_frame(h, i))
+                       for i in range(num_frames)]
+        for c in self.frames:
+            c._check(self.L.pikgpu_set_option(c.h, OPT_FORM, FORMS[form]))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            for c in self.frames:
+                c.h = None
+            self.L.pikgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def reconstruct_device(self, out_ptrs, strides, stream: int = 0) -> None:
+        """Frame i writes 3 consecutive planes (strides[i] x ysize floats)
+        at device address out_ptrs[i]."""
+        n = len(self.frames)
+        outs = (ctypes.c_void_p * n)(*out_ptrs)
+        st = (ctypes.c_size_t * n)(*strides)
+        rc = self.L.pikgpu_batch_reconstruct(self.h, outs, st, stream or None)
+        if rc != OK:
+            raise PikGpuError(rc,
+                              self.L.pikgpu_batch_last_error(self.h).decode())
+
+    def launch_count(self) -> int:
+        return self.L.pikgpu_batch_launch_count(self.h)
+
+    def capture_count(self) -> int:
+        return self.L.pikgpu_batch_capture_count(self.h)
