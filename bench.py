@@ -261,6 +261,8 @@ def batch_main(args):
         for c, o, f in zip(b.frames, outs, frames):
             c.reconstruct_device(o.data_ptr(), f.xsize)
 
+    ms_untuned = timed(graph_step)
+    shape = b.autotune(ptrs, strides, stream.cuda_stream)
     with ClockSampler(local) as clk:
         ms_graph = timed(graph_step)
     ms_single = timed(per_image_step)
@@ -278,6 +280,10 @@ def batch_main(args):
         "per_image": {"value": round(px / (ms_single * 1e-3) / 1e6, 2),
                       "ms_per_step": round(ms_single, 4)},
         "speedup_vs_per_image": round(ms_single / ms_graph, 3),
+        "untuned_graph": {"value": round(px / (ms_untuned * 1e-3) / 1e6, 2),
+                          "ms_per_step": round(ms_untuned, 4),
+                          "chains": len(frames), "tc_ctas_per_sm": 4},
+        "autotuned": shape,
         "gpu_launches": b.launch_count() * args.steps,
         "graph_captures": b.capture_count(),
         "clocks": clk.summary(),

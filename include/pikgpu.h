@@ -244,6 +244,16 @@ const char* pikgpu_batch_last_error(const pikgpu_batch* batch);
 /* Kernels launched per replay, and graphs captured so far. */
 int pikgpu_batch_launch_count(const pikgpu_batch* batch);
 int pikgpu_batch_capture_count(const pikgpu_batch* batch);
+/* Autotuner of the batch's launch shape: captures and times (median of 3
+ * replays) every combination of the number of concurrent graph branches
+ * (1, 2, 4, ... up to one per frame; frame i runs in branch i % chains) and,
+ * when a tensor-core form is in use, of the persistent 16x16 transform
+ * kernels' CTAs per SM (1, 2, 4), and keeps the fastest for later calls.
+ * The chosen values are written to `chains` and `tc_ctas_per_sm` (either
+ * may be NULL). Same outputs as pikgpu_batch_reconstruct. */
+int pikgpu_batch_autotune(pikgpu_batch* batch, float* const* out_linear,
+                          const size_t* linear_strides, void* stream,
+                          int* chains, int* tc_ctas_per_sm);
 
 /* Allocation-free DC reconstruction. No counterpart in the reference: its
  * DequantDC + AdaptiveDCReconstruction (pik/compressed_dc.cc:181-231,

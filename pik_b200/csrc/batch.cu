@@ -22,6 +22,12 @@ struct pikgpu_batch {
   std::vector<float*> outs;
   std::vector<size_t> strides;
   int captures = 0;
+  // Launch shape: frames run in `chains` concurrent branches (frame i in
+  // branch i % chains, in order within a branch), and the persistent
+  // tensor-core kernels use `tc_ctas` CTAs per SM.
+  int chains = 0;  // 0: one branch per frame
+  int tc_ctas = kTcCtasPerSm;
+  bool exec_valid_for_shape = false;  // the graph was captured with these
   std::string err;
 };
 
@@ -65,20 +71,23 @@ int Capture(pikgpu_batch* b, float* const* out, const size_t* strides) {
   int rc = PIKGPU_OK;
   e = cudaEventRecord(b->fork, b->stream);
   const size_t n = b->frames.size();
+  const size_t k = b->chains > 0 ? std::min<size_t>(b->chains, n) : n;
+  // Branch j runs on the stream of frame j, frames j, j + k, ... in order.
+  for (size_t j = 0; j < k && e == cudaSuccess; ++j) {
+    e = cudaStreamWaitEvent(b->frames[j]->own_stream, b->fork, 0);
+  }
   for (size_t i = 0; i < n && e == cudaSuccess && rc == PIKGPU_OK; ++i) {
     pikgpu_ctx* ctx = b->frames[i];
     cudaStream_t user = ctx->stream;
-    ctx->stream = ctx->own_stream;  // this frame's branch of the graph
-    e = cudaStreamWaitEvent(ctx->stream, b->fork, 0);
-    if (e == cudaSuccess) {
-      rc = LaunchAll(ctx, out[i], strides[i], nullptr, 0);
-      if (rc != PIKGPU_OK) {
-        BatchFail(b, rc, "frame %zu: %s", i, ctx->err.c_str());
-      }
-    }
-    if (e == cudaSuccess) e = cudaEventRecord(b->joins[i], ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->joins[i], 0);
+    ctx->stream = b->frames[i % k]->own_stream;
+    ctx->tc_ctas_per_sm = b->tc_ctas;
+    rc = LaunchAll(ctx, out[i], strides[i], nullptr, 0);
+    if (rc != PIKGPU_OK) BatchFail(b, rc, "frame %zu: %s", i, ctx->err.c_str());
     ctx->stream = user;
+  }
+  for (size_t j = 0; j < k && e == cudaSuccess; ++j) {
+    e = cudaEventRecord(b->joins[j], b->frames[j]->own_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->joins[j], 0);
   }
   cudaGraph_t graph = nullptr;
   const cudaError_t end = cudaStreamEndCapture(b->stream, &graph);
@@ -100,6 +109,7 @@ int Capture(pikgpu_batch* b, float* const* out, const size_t* strides) {
   b->outs.assign(out, out + n);
   b->strides.assign(strides, strides + n);
   for (size_t i = 0; i < n; ++i) b->gens[i] = b->frames[i]->generation;
+  b->exec_valid_for_shape = true;
   ++b->captures;
   return PIKGPU_OK;
 }
@@ -189,7 +199,7 @@ int pikgpu_batch_reconstruct(pikgpu_batch* b, float* const* out_linear,
     }
   }
   CUDA_TRY_B(b, cudaSetDevice(b->device));
-  bool stale = !b->exec;
+  bool stale = !b->exec || !b->exec_valid_for_shape;
   for (size_t i = 0; i < n && !stale; ++i) {
     stale = b->gens[i] != b->frames[i]->generation ||
             b->outs[i] != out_linear[i] ||
@@ -232,6 +242,67 @@ int pikgpu_batch_launch_count(const pikgpu_batch* b) {
 
 int pikgpu_batch_capture_count(const pikgpu_batch* b) {
   return b ? b->captures : PIKGPU_ERR_INVALID_ARG;
+}
+
+int pikgpu_batch_autotune(pikgpu_batch* b, float* const* out_linear,
+                          const size_t* linear_strides, void* stream,
+                          int* chains, int* tc_ctas_per_sm) {
+  if (!b) return PIKGPU_ERR_INVALID_ARG;
+  const int n = int(b->frames.size());
+  bool tensor = false;
+  for (auto* ctx : b->frames) tensor |= ctx->form != PIKGPU_FORM_FP32;
+  std::vector<int> chain_opts;
+  for (int k : {1, 2, 4, 8, 16, 32, n}) {
+    if (k <= n && (chain_opts.empty() || chain_opts.back() < k)) {
+      chain_opts.push_back(k);
+    }
+  }
+  std::vector<int> tc_opts = tensor ? std::vector<int>{1, 2, 4}
+                                    : std::vector<int>{kTcCtasPerSm};
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CUDA_TRY_B(b, cudaEventCreate(&e0));
+  CUDA_TRY_B(b, cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_k = n, best_tc = kTcCtasPerSm, rc = PIKGPU_OK;
+  for (int tc : tc_opts) {
+    for (int k : chain_opts) {
+      b->chains = k;
+      b->tc_ctas = tc;
+      b->exec_valid_for_shape = false;
+      // Capture and one warm-up replay, then the median of 3 timed ones.
+      rc = pikgpu_batch_reconstruct(b, out_linear, linear_strides, stream);
+      if (rc != PIKGPU_OK) break;
+      float t[3];
+      for (float& ti : t) {
+        cudaEventRecord(e0, st);
+        cudaGraphLaunch(b->exec, st);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+          rc = BatchFail(b, PIKGPU_ERR_CUDA, "autotune replay failed");
+          break;
+        }
+        cudaEventElapsedTime(&ti, e0, e1);
+      }
+      if (rc != PIKGPU_OK) break;
+      std::sort(t, t + 3);
+      if (t[1] < best) {
+        best = t[1];
+        best_k = k;
+        best_tc = tc;
+      }
+    }
+    if (rc != PIKGPU_OK) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->chains = best_k;
+  b->tc_ctas = best_tc;
+  b->exec_valid_for_shape = false;
+  if (rc != PIKGPU_OK) return rc;
+  if (chains) *chains = best_k;
+  if (tc_ctas_per_sm) *tc_ctas_per_sm = best_tc;
+  return PIKGPU_OK;
 }
 
 }  // extern "C"

@@ -60,6 +60,11 @@ struct DevBuf {
 std::mutex g_table_mutex;
 bool g_tables_uploaded[64] = {};
 
+// Persistent tensor-core transform CTAs per SM (default): 4 x 128
+// tensor-memory columns fill the SM's 512. A batch's autotuner may lower it
+// (pikgpu_batch_autotune).
+constexpr int kTcCtasPerSm = 4;
+
 }  // namespace
 
 struct pikgpu_ctx {
@@ -85,6 +90,7 @@ struct pikgpu_ctx {
   bool smoothed_valid = false;
   cudaEvent_t ev[kNumTimed + 1] = {};
   int num_sms = 148;
+  int tc_ctas_per_sm = kTcCtasPerSm;
   float times[kNumTimed] = {};
   float dc_half_step[3] = {};
   int launches = 0;
@@ -304,9 +310,6 @@ int UploadTables(pikgpu_ctx* ctx) {
 
 inline int Blocks(size_t n, int t) { return int((n + t - 1) / t); }
 
-// Persistent tensor-core transform CTAs per SM: 4 x 128 tensor-memory
-// columns fill the SM's 512.
-constexpr int kTcCtasPerSm = 4;
 
 // Writes the smoothed frame (gaborish #1 of the IDCT output) for the stage
 // and guide exports; the reconstruction itself never stores it.
@@ -444,7 +447,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     }
     if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
       const int items = (n[kC16] + 7) / 8;
-      const int grid = std::min(items, ctx->num_sms * kTcCtasPerSm);
+      const int grid = std::min(items, ctx->num_sms * ctx->tc_ctas_per_sm);
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
         k_square_idct_tc<16, 2><<<grid, tc::kThreads, 0, st>>>(
             g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
@@ -536,7 +539,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     }
     if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
       const int grid =
-          std::min((n[kC16] + 7) / 8, ctx->num_sms * kTcCtasPerSm);
+          std::min((n[kC16] + 7) / 8, ctx->num_sms * ctx->tc_ctas_per_sm);
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
         k_square_ar_tc<16, 2><<<grid, tc::kThreads, 0, st>>>(
             g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,

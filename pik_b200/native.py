@@ -80,6 +80,10 @@ def lib() -> ctypes.CDLL:
     L.pikgpu_batch_last_error.argtypes = [P]
     L.pikgpu_batch_launch_count.argtypes = [P]
     L.pikgpu_batch_capture_count.argtypes = [P]
+    L.pikgpu_batch_autotune.argtypes = [P, ctypes.POINTER(P),
+                                        ctypes.POINTER(S), P,
+                                        ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
 
@@ -271,6 +275,20 @@ class Batch:
         if rc != OK:
             raise PikGpuError(rc,
                               self.L.pikgpu_batch_last_error(self.h).decode())
+
+    def autotune(self, out_ptrs, strides, stream: int = 0) -> dict:
+        """Times the batch's launch shapes and keeps the fastest."""
+        n = len(self.frames)
+        outs = (ctypes.c_void_p * n)(*out_ptrs)
+        st = (ctypes.c_size_t * n)(*strides)
+        chains, tc = ctypes.c_int(), ctypes.c_int()
+        rc = self.L.pikgpu_batch_autotune(self.h, outs, st, stream or None,
+                                          ctypes.byref(chains),
+                                          ctypes.byref(tc))
+        if rc != OK:
+            raise PikGpuError(rc,
+                              self.L.pikgpu_batch_last_error(self.h).decode())
+        return {"chains": chains.value, "tc_ctas_per_sm": tc.value}
 
     def launch_count(self) -> int:
         return self.L.pikgpu_batch_launch_count(self.h)

@@ -67,6 +67,30 @@ def test_batch_equals_single_frames(form):
         b.close()
 
 
+def test_autotuned_batch_equals_single_frames():
+    frames = [synthetic.make_frame(w, h, seed=60 + i, qf_median=12.0)
+              for i, (w, h) in enumerate(SIZES)]
+    want = [single(f, "split_bf16") for f in frames]
+    b = native.Batch(len(frames), form="split_bf16")
+    try:
+        for c, f in zip(b.frames, frames):
+            c.begin(f)
+            c.set_ac()
+        outs = gpu_outputs(frames)
+        ptrs = [o.data_ptr() for o in outs]
+        strides = [f.xsize for f in frames]
+        shape = b.autotune(ptrs, strides)
+        assert 1 <= shape["chains"] <= len(frames)
+        assert shape["tc_ctas_per_sm"] in (1, 2, 4)
+        for o in outs:
+            o.fill_(float("nan"))
+        b.reconstruct_device(ptrs, strides)
+        for o, w in zip(outs, want):
+            np.testing.assert_array_equal(o.cpu().numpy(), w)
+    finally:
+        b.close()
+
+
 def test_batch_errors():
     b = native.Batch(2)
     try:
