@@ -51,6 +51,7 @@ def lib() -> ctypes.CDLL:
         L.pikoracle_epf_weight.argtypes = [ctypes.c_int, ctypes.c_int]
         L.pikoracle_opsin_inverse_matrix.argtypes = [P]
         L.pikoracle_dct_table.argtypes = [ctypes.c_int, ctypes.c_int, P]
+        L.pikoracle_adjoint_f64.argtypes = [P, P, P, P, P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -105,3 +106,44 @@ def run(frame: layout.Frame, *, precision: int = 32, want=STAGES,
     if export_decisions:
         out["guide"], out["sigma"] = gout, sout
     return out
+
+
+def adjoint(frame: layout.Frame, target: np.ndarray, *, guide=None,
+            sigma=None, dc_guide=None, dc_sigma=None, ac_dequant=None,
+            ar_scale=None, grads: bool = True):
+    """FP64 adjoint (pik_adjoint.inc): returns (loss, grad_ac, grad_qf);
+    grad_ac is (3, By, Bx*64) (dequantised AC, frame layout), grad_qf
+    (By, Bx). `target` is (3, ysize, xsize) XYB. EPF decisions should be
+    the base point's; `ac_dequant` / `ar_scale` move the forward off the
+    integer lattice for finite differences."""
+    L = lib()
+    packed = abi.PackedFrame(frame)
+    by, bx = frame.blocks
+    dec = Decisions()
+    keep = []
+    for field, arr, dt in (("guide", guide, np.uint8),
+                           ("sigma", sigma, np.int32),
+                           ("dc_guide", dc_guide, np.uint8),
+                           ("dc_sigma", dc_sigma, np.int32)):
+        if arr is not None:
+            a = np.ascontiguousarray(arr, dt)
+            keep.append(a)
+            setattr(dec, field, a.ctypes.data)
+    t = np.ascontiguousarray(target, np.float64)
+    assert t.shape == (3, frame.ysize, frame.xsize)
+    acd = None if ac_dequant is None else np.ascontiguousarray(ac_dequant,
+                                                               np.float64)
+    ars = None if ar_scale is None else np.ascontiguousarray(ar_scale,
+                                                             np.float64)
+    loss = np.zeros(1, np.float64)
+    g_ac = np.zeros((3, by, bx * 64), np.float64) if grads else None
+    g_qf = np.zeros((by, bx), np.float64) if grads else None
+    rc = L.pikoracle_adjoint_f64(
+        packed.ref, packed.ac.ctypes.data, ctypes.byref(dec),
+        acd.ctypes.data if acd is not None else None,
+        ars.ctypes.data if ars is not None else None, t.ctypes.data,
+        loss.ctypes.data, g_ac.ctypes.data if grads else None,
+        g_qf.ctypes.data if grads else None)
+    if rc != 0:
+        raise RuntimeError(f"oracle adjoint failed: {rc}")
+    return float(loss[0]), g_ac, g_qf

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <vector>
 
 namespace {
@@ -1008,6 +1009,9 @@ struct Frame {
 template <typename F>
 struct Recon {
   const Frame& f;
+  // Adjoint checks only: per-cell factors on 1 / qf in the clamp intervals
+  // (a quant field perturbed away from its integer values); NULL = 1.
+  const double* ar_scale = nullptr;
   explicit Recon(const Frame& fr) : f(fr) {}
 
   // DequantDC (pik/compressed_dc.cc:181-231) with mul_dc from
@@ -1357,7 +1361,10 @@ struct Recon {
         if (a & 0xF) continue;
         const int type = a >> 4, cov = Covered(type), n = 8 * cov;
         const int qac = f.Qf(bx, by);
-        const float inv_quant_ac = f.inv_global_scale / qac;
+        const float inv_quant_ac_f = f.inv_global_scale / qac;
+        const F inv_quant_ac =
+            ar_scale ? F(inv_quant_ac_f) * F(ar_scale[size_t(by) * f.bx + bx])
+                     : F(inv_quant_ac_f);
         const int tx = bx / kTileDimInBlocks, ty = by / kTileDimInBlocks;
         const int cf = f.p->dequant_control_field[size_t(ty) * f.tx + tx];
         const int table = f.p->dequant_map[cf * 256 + (qac - 1)];
@@ -1400,13 +1407,13 @@ struct Recon {
                   interval = F(1.0f) * dc_mul[c];
                 }
               } else {
-                interval = F(dm[ofs]) * F(inv_quant_ac);
+                interval = F(dm[ofs]) * inv_quant_ac;
               }
               clamp(ofs, interval);
             }
           }
           for (int k = cov * 8 * cov; k < n * n; ++k) {
-            clamp(k, F(dm[k]) * F(inv_quant_ac));
+            clamp(k, F(dm[k]) * inv_quant_ac);
           }
         }
         for (int c = 0; c < 3; ++c) {
@@ -1618,6 +1625,8 @@ int Run(const pikgpu_frame_params* p, const int16_t* ac, void* const* stages,
   return 0;
 }
 
+#include "pik_adjoint.inc"
+
 }  // namespace
 
 extern "C" {
@@ -1626,6 +1635,16 @@ int pikoracle_run_f32(const pikgpu_frame_params* p, const int16_t* ac,
                       void* const* stages, const pikoracle_decisions* dec,
                       uint8_t* guide_out, int32_t* sigma_out) {
   return Run<float>(p, ac, stages, dec, guide_out, sigma_out);
+}
+
+int pikoracle_adjoint_f64(const pikgpu_frame_params* p, const int16_t* ac,
+                          const pikoracle_decisions* decisions_in,
+                          const double* ac_dequant, const double* ar_scale,
+                          const double* target, double* loss,
+                          double* grad_ac, double* grad_qf) {
+  if (!target) return -1;
+  return Adjoint(p, ac, decisions_in, ac_dequant, ar_scale, target, loss,
+                 grad_ac, grad_qf);
 }
 
 int pikoracle_run_f64(const pikgpu_frame_params* p, const int16_t* ac,

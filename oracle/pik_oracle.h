@@ -62,6 +62,22 @@ int pikoracle_run_f64(const pikgpu_frame_params* p, const int16_t* ac,
                       const pikoracle_decisions* decisions_in,
                       uint8_t* guide_out, int32_t* sigma_out);
 
+/* FP64 adjoint: loss L = sum over xsize x ysize x 3 of (XYB
+ * reconstruction before OpsinToLinear - target)^2 and its gradient with
+ * respect to the dequantised AC coefficients (`grad_ac`, 3 planes of
+ * By x Bx*64, frame layout) and the per-cell quant field as a real number
+ * (`grad_qf`, By x Bx). EPF decisions are held fixed (pass the base point's
+ * in `decisions_in`). For finite differences the forward can be evaluated
+ * off the integer lattice: `ac_dequant` (may be NULL) replaces DoAC's
+ * output, `ar_scale` (may be NULL) multiplies 1/qf of each cell in the
+ * clamp intervals. `target`: 3 x ysize x xsize doubles. Gradient outputs
+ * may be NULL (loss only). */
+int pikoracle_adjoint_f64(const pikgpu_frame_params* p, const int16_t* ac,
+                          const pikoracle_decisions* decisions_in,
+                          const double* ac_dequant, const double* ar_scale,
+                          const double* target, double* loss,
+                          double* grad_ac, double* grad_qf);
+
 /* Single-function probes (FP64 unless noted), for unit tests:
  * transform one block of AcStrategy `type` (frame coefficient layout with
  * row stride `cstride`; pixels row stride `pstride`). */
