@@ -283,6 +283,61 @@ int pikgpu_dc_reconstruct_noalloc(const int16_t* quantized_dc,
                                   int32_t ytob_dc, float* dc, void* stream,
                                   char* msg, size_t msg_size);
 
+/* Adjoint of the reconstruction. No counterpart in the reference (a
+ * decoder). The variables are the dequantised AC coefficients -- the output
+ * of Dequant::DoAC (pik/compressed_image.cc:586-707), 3 planes of
+ * ysize_blocks x (64 xsize_blocks) floats in the frame layout of
+ * pikgpu_frame_set_ac -- and the per-cell quant field taken as a real
+ * number (ysize_blocks x xsize_blocks). The loss is
+ *   L = sum over the xsize x ysize pixels and X, Y, B of
+ *       (pre_opsin - target)^2,
+ * pre_opsin being the frame after gaborish #2 and before OpsinToLinear
+ * (PIKGPU_STAGE_PRE_OPSIN). The EPF's discrete decisions (u8 guide,
+ * per-block sigma) are held at their values in the forward pass, which this
+ * call runs first in the context's form.
+ *  target:  3 planes of ysize x xsize floats (XYB), contiguous;
+ *  loss:    1 double (may be NULL);
+ *  grad_ac: 3 planes of ysize_blocks x 64 xsize_blocks floats (may be NULL;
+ *           LLF entries, overwritten from DC, get 0);
+ *  grad_qf: ysize_blocks x xsize_blocks floats (may be NULL).
+ * All four in device memory if buffers_on_device, else host memory. */
+int pikgpu_adjoint(pikgpu_ctx* ctx, const float* target, double* loss,
+                   float* grad_ac, float* grad_qf, int buffers_on_device);
+
+/* Move the forward pass off the integer lattice (finite differences of
+ * pikgpu_adjoint, or a caller optimising coefficients). For the current
+ * frame only (pikgpu_frame_begin clears both); NULL clears.
+ * set_dequantized_ac: the dequantised AC coefficients used instead of
+ *   Dequant::DoAC's (layout of pikgpu_adjoint's grad_ac); the int16 AC is
+ *   then not needed.
+ * set_clamp_scale: a per-cell multiplier (ysize_blocks x xsize_blocks
+ *   floats) of the clamp's non-LLF intervals, which are half a quantisation
+ *   step (pik/adaptive_reconstruction.cc:160-171). A quant field qf' of
+ *   cell i in place of qf is modelled by scaling that cell's dequantised AC
+ *   and its clamp scale by qf / qf'; pikgpu_adjoint's grad_qf is then taken
+ *   at qf' = qf / scale. */
+/* Verification hooks for the clamp's discrete decisions, the counterpart of
+ * pikgpu_set_epf_decisions for AdaptiveReconstruction's clamp
+ * (pik/adaptive_reconstruction.cc:128-244). Per coefficient, the minimum of
+ * the three channels' ratios is taken by one of five branches, recorded as
+ * a code: 0 no ratio below 1 (correction kept), 1..3 the ratio of channel
+ * code - 1 (clamped), 4 a +0.0 correction (SymmetricClamp's ratio 0). Where
+ * a correction cancels to zero, rounding decides between code 4 and a
+ * neighbouring branch, so two precisions can take different branches on
+ * identical inputs; sharing the codes makes their gradients comparable.
+ * Layout: By x 64 Bx bytes (frame coefficient layout, first blocks'
+ * entries). `get` exports the codes of the last forward pass that recorded
+ * them (pikgpu_adjoint, or a reconstruction with PIKGPU_OPT_KEEP_STAGES set
+ * before frame_begin; frames with the EPF only); `set` makes later passes
+ * follow the given codes (NULL: computed). Host memory. */
+int pikgpu_set_clamp_decisions(pikgpu_ctx* ctx, const uint8_t* tape);
+int pikgpu_get_clamp_decisions(pikgpu_ctx* ctx, uint8_t* tape);
+
+int pikgpu_frame_set_dequantized_ac(pikgpu_ctx* ctx, const float* ac,
+                                    int on_device);
+int pikgpu_frame_set_clamp_scale(pikgpu_ctx* ctx, const float* scale,
+                                 int on_device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,7 +24,8 @@ STAGES = ("dc", "dequant_ac", "idct", "smoothed", "epf", "ar", "pre_opsin",
 
 class Decisions(ctypes.Structure):
     _fields_ = [("guide", ctypes.c_void_p), ("sigma", ctypes.c_void_p),
-                ("dc_guide", ctypes.c_void_p), ("dc_sigma", ctypes.c_void_p)]
+                ("dc_guide", ctypes.c_void_p), ("dc_sigma", ctypes.c_void_p),
+                ("clamp_tape", ctypes.c_void_p)]
 
 
 def available() -> bool:
@@ -68,7 +69,7 @@ def stage_shapes(frame: layout.Frame) -> dict:
 
 def run(frame: layout.Frame, *, precision: int = 32, want=STAGES,
         guide=None, sigma=None, dc_guide=None, dc_sigma=None,
-        export_decisions: bool = False):
+        clamp_tape=None, export_decisions: bool = False):
     """Runs the restatement. Returns {stage: array}; with export_decisions,
     also 'guide' (3, H+12, W+12) uint8 and 'sigma' (By, Bx) int32."""
     L = lib()
@@ -87,7 +88,8 @@ def run(frame: layout.Frame, *, precision: int = 32, want=STAGES,
     for field, arr, dt in (("guide", guide, np.uint8),
                            ("sigma", sigma, np.int32),
                            ("dc_guide", dc_guide, np.uint8),
-                           ("dc_sigma", dc_sigma, np.int32)):
+                           ("dc_sigma", dc_sigma, np.int32),
+                           ("clamp_tape", clamp_tape, np.uint8)):
         if arr is not None:
             a = np.ascontiguousarray(arr, dt)
             keep.append(a)
@@ -109,8 +111,8 @@ def run(frame: layout.Frame, *, precision: int = 32, want=STAGES,
 
 
 def adjoint(frame: layout.Frame, target: np.ndarray, *, guide=None,
-            sigma=None, dc_guide=None, dc_sigma=None, ac_dequant=None,
-            ar_scale=None, grads: bool = True):
+            sigma=None, dc_guide=None, dc_sigma=None, clamp_tape=None,
+            ac_dequant=None, ar_scale=None, grads: bool = True):
     """FP64 adjoint (pik_adjoint.inc): returns (loss, grad_ac, grad_qf);
     grad_ac is (3, By, Bx*64) (dequantised AC, frame layout), grad_qf
     (By, Bx). `target` is (3, ysize, xsize) XYB. EPF decisions should be
@@ -124,7 +126,8 @@ def adjoint(frame: layout.Frame, target: np.ndarray, *, guide=None,
     for field, arr, dt in (("guide", guide, np.uint8),
                            ("sigma", sigma, np.int32),
                            ("dc_guide", dc_guide, np.uint8),
-                           ("dc_sigma", dc_sigma, np.int32)):
+                           ("dc_sigma", dc_sigma, np.int32),
+                           ("clamp_tape", clamp_tape, np.uint8)):
         if arr is not None:
             a = np.ascontiguousarray(arr, dt)
             keep.append(a)

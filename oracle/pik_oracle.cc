@@ -1012,7 +1012,16 @@ struct Recon {
   // Adjoint checks only: per-cell factors on 1 / qf in the clamp intervals
   // (a quant field perturbed away from its integer values); NULL = 1.
   const double* ar_scale = nullptr;
+  // Verification: the clamp's branch per coefficient, from another
+  // implementation's forward pass (codes of pikgpu_get_clamp_decisions);
+  // NULL = computed here.
+  const uint8_t* clamp_tape = nullptr;
   explicit Recon(const Frame& fr) : f(fr) {}
+
+  // Minimum ratio of a coefficient on the branch a clamp tape code names.
+  static F TapeRatio(uint8_t code, const F ratio[3]) {
+    return code == 0 ? F(1.0f) : code <= 3 ? ratio[code - 1] : F(0.0f);
+  }
 
   // DequantDC (pik/compressed_dc.cc:181-231) with mul_dc from
   // DecodeDCGroups (pik/compressed_dc.cc:445-448).
@@ -1370,6 +1379,7 @@ struct Recon {
         const int table = f.p->dequant_map[cf * 256 + (qac - 1)];
         F blocks[3][32 * 32];
         F min_ratio[32 * 32];
+        F ratios[32 * 32][3];
         for (int k = 0; k < n * n; ++k) min_ratio[k] = F(1.0f);
         for (int c = 0; c < 3; ++c) {
           const float* dm = f.Matrix(table, QuantKind(type), c);
@@ -1391,6 +1401,7 @@ struct Recon {
             const bool is_zero = IsPositiveZero(corr);
             const F divisor = is_zero ? F(1E-7f) : corr;
             const F ratio = clamped / divisor;
+            ratios[k][c] = ratio;
             min_ratio[k] = ratio < min_ratio[k] ? ratio : min_ratio[k];
           };
           for (int y = 0; y < cov; ++y) {
@@ -1414,6 +1425,13 @@ struct Recon {
           }
           for (int k = cov * 8 * cov; k < n * n; ++k) {
             clamp(k, F(dm[k]) * inv_quant_ac);
+          }
+        }
+        if (clamp_tape) {
+          for (int k = 0; k < n * n; ++k) {
+            const size_t o = size_t(by + k / (64 * cov)) * (size_t(f.bx) * 64) +
+                             size_t(bx) * 64 + k % (64 * cov);
+            min_ratio[k] = TapeRatio(clamp_tape[o], ratios[k]);
           }
         }
         for (int c = 0; c < 3; ++c) {
@@ -1557,6 +1575,7 @@ int Run(const pikgpu_frame_params* p, const int16_t* ac, void* const* stages,
   fr.inv_global_scale = static_cast<float>(1.0 * 65536 / p->global_scale);
   fr.inv_quant_dc = fr.inv_global_scale / p->quant_dc;
   Recon<F> r(fr);
+  r.clamp_tape = dec ? dec->clamp_tape : nullptr;
 
   Img3<F> dc = r.DequantDC();
   r.DCRecon(&dc, dec);

@@ -47,6 +47,10 @@ typedef struct pikoracle_decisions {
   const int32_t* sigma;
   const uint8_t* dc_guide;
   const int32_t* dc_sigma;
+  /* The clamp's branch per coefficient (By x 64 Bx bytes, frame coefficient
+   * layout; the codes of pikgpu_get_clamp_decisions): 0 ratio 1, 1..3 the
+   * ratio of channel code - 1, 4 ratio 0. NULL: computed. */
+  const uint8_t* clamp_tape;
 } pikoracle_decisions;
 
 /* Runs the path in FP32. `ac` is 3 planes of By x Bx*64 int16. `stages`

@@ -185,7 +185,7 @@ int pikgpu_batch_reconstruct(pikgpu_batch* b, float* const* out_linear,
   const size_t n = b->frames.size();
   for (size_t i = 0; i < n; ++i) {
     const pikgpu_ctx* ctx = b->frames[i];
-    if (!ctx->have_frame || !ctx->have_ac) {
+    if (!ctx->have_frame || !(ctx->have_ac || ctx->use_dq_ovr)) {
       return BatchFail(b, PIKGPU_ERR_STATE, "frame %zu: frame or AC not "
                        "supplied", i);
     }

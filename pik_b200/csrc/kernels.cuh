@@ -98,6 +98,15 @@ struct DevFrame {
   float* idct;        // 3 x PH x PW
   float* smoothed;    // 3 x PH x PW
   float* filt;        // 3 x PH x PW
+  // Optional per-cell multiplier of the clamp's half-step interval (NULL:
+  // none), By x Bx.
+  const float* clamp_scale;
+  // Optional clamp tape (By x ac_stride bytes, frame coefficient layout;
+  // NULL: not written): the clamp's branch per coefficient, for the adjoint.
+  uint8_t* clamp_tape;
+  // Optional clamp tape to follow instead of the computed minimum (same
+  // layout; NULL: computed), pikgpu_set_clamp_decisions.
+  const uint8_t* clamp_tape_in;
 };
 
 }  // namespace pikgpu

@@ -86,6 +86,23 @@ struct pikgpu_ctx {
   DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr;
   DevBuf sigma_ovr, counters, active[kNumClasses], tc_err;
   bool use_guide_ovr = false, use_sigma_ovr = false;
+  // Dequantised AC supplied by the caller instead of Dequant::DoAC, and the
+  // per-cell clamp scale (pikgpu_frame_set_dequantized_ac / _clamp_scale).
+  DevBuf dq_ovr, clamp_scale;
+  bool use_dq_ovr = false, use_clamp_scale = false;
+  // Adjoint (adjoint.cu): gradient planes, coefficient gradient, group
+  // pred2x2 gradient, quant-field gradient, guide bytes, loss partials,
+  // per-type Jacobians, host target staging.
+  DevBuf adj_a, adj_b, adj_c, adj_coef, adj_pred, adj_qf, adj_guide;
+  DevBuf adj_partial, adj_jac, adj_target, adj_tape;
+  bool adj_jac_built = false;
+  // The clamp kernels record their branches (the clamp tape) in the
+  // adjoint's forward pass and with PIKGPU_OPT_KEEP_STAGES; tape_valid: the
+  // last forward pass wrote adj_tape. tape_in: branches to follow
+  // (pikgpu_set_clamp_decisions).
+  bool record_tape = false, tape_valid = false;
+  DevBuf tape_in;
+  bool use_tape_in = false;
   // The smoothed frame (gaborish #1) is written only when an export asks.
   bool smoothed_valid = false;
   cudaEvent_t ev[kNumTimed + 1] = {};
@@ -371,6 +388,13 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   f.idct = P<float>(ctx->idct);
   f.smoothed = P<float>(ctx->smoothed);
   f.filt = P<float>(ctx->filt);
+  f.clamp_scale = ctx->use_clamp_scale ? P<float>(ctx->clamp_scale) : nullptr;
+  const size_t nac = size_t(g.ac_stride) * g.By;
+  const bool rec = (ctx->record_tape || ctx->keep_stages) && s.have_ar &&
+                   ctx->adj_tape.cap >= nac;
+  f.clamp_tape = rec ? P<uint8_t>(ctx->adj_tape) : nullptr;
+  f.clamp_tape_in = ctx->use_tape_in ? P<uint8_t>(ctx->tape_in) : nullptr;
+  ctx->tape_valid = rec;
   uint32_t* mm = P<uint32_t>(ctx->mm);
 
   ctx->launches = 0;
@@ -418,7 +442,13 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   Mark(ctx, kTDequant);
   {
     dim3 gr(Blocks(g.Bx, kDequantCells), g.By);
-    k_dequant_ac<<<gr, 256, 0, st>>>(g, f, s); ++ctx->launches;
+    if (ctx->use_dq_ovr) {
+      cudaMemcpyAsync(f.ac, ctx->dq_ovr.p,
+                      sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
+                      cudaMemcpyDeviceToDevice, st);
+    } else {
+      k_dequant_ac<<<gr, 256, 0, st>>>(g, f, s); ++ctx->launches;
+    }
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_dequant.p, f.ac,
                       sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
@@ -518,6 +548,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       n[k] = int(ctx->lists[k].size());
     }
     // Only blocks the EPF filtered need the clamp (see k_active_blocks).
+    if (f.clamp_tape) cudaMemsetAsync(f.clamp_tape, 0, nac, st);
     int* counters = P<int>(ctx->counters);
     cudaMemsetAsync(counters, 0, sizeof(int) * kNumClasses, st);
     for (int k = 0; k < kNumClasses; ++k) {
@@ -653,7 +684,12 @@ int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
                     &ctx->filt,    &ctx->mm,        &ctx->sigma,
                     &ctx->dc_sigma, &ctx->out_lin,  &ctx->out_rgb8,
                     &ctx->dbg_dequant, &ctx->dbg_epf, &ctx->dbg_pre,
-                    &ctx->guide_ovr, &ctx->sigma_ovr};
+                    &ctx->guide_ovr, &ctx->sigma_ovr, &ctx->dq_ovr,
+                    &ctx->clamp_scale, &ctx->adj_a,  &ctx->adj_b,
+                    &ctx->adj_c,   &ctx->adj_coef,  &ctx->adj_pred,
+                    &ctx->adj_qf,  &ctx->adj_guide, &ctx->adj_partial,
+                    &ctx->adj_jac, &ctx->adj_target, &ctx->adj_tape,
+                    &ctx->tape_in};
   for (DevBuf* b : bufs) FreeBuf(b);
   for (auto& b : ctx->list) FreeBuf(&b);
   for (auto& b : ctx->active) FreeBuf(&b);
@@ -703,6 +739,8 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
   ++ctx->generation;
   ctx->have_frame = ctx->have_ac = ctx->have_result = false;
   ctx->use_guide_ovr = ctx->use_sigma_ovr = false;
+  ctx->use_dq_ovr = ctx->use_clamp_scale = false;
+  ctx->use_tape_in = ctx->tape_valid = false;
   int rc = Validate(ctx, p);
   if (rc != PIKGPU_OK) return rc;
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
@@ -766,7 +804,8 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
   if (ctx->keep_stages) {
     if ((rc = Ensure(ctx, &ctx->dbg_dequant, 4 * 3 * nac)) ||
         (rc = Ensure(ctx, &ctx->dbg_epf, 4 * 3 * npx)) ||
-        (rc = Ensure(ctx, &ctx->dbg_pre, 4 * 3 * size_t(g.W) * g.H))) {
+        (rc = Ensure(ctx, &ctx->dbg_pre, 4 * 3 * size_t(g.W) * g.H)) ||
+        (rc = Ensure(ctx, &ctx->adj_tape, nac))) {
       return rc;
     }
   }
@@ -888,7 +927,7 @@ int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
                        size_t linear_stride, uint8_t* out_srgb8,
                        size_t srgb8_stride, int outputs_on_device) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
-  if (!ctx->have_frame || !ctx->have_ac) {
+  if (!ctx->have_frame || !(ctx->have_ac || ctx->use_dq_ovr)) {
     return Fail(ctx, PIKGPU_ERR_STATE, "frame or AC not supplied");
   }
   const Geo& g = ctx->g;
@@ -1053,6 +1092,14 @@ int pikgpu_set_epf_decisions(pikgpu_ctx* ctx, const uint8_t* guide,
                              cudaMemcpyHostToDevice));
   }
   if (sigma) {
+    // The EPF indexes its weight table by sigma (pik/epf.h:70-76).
+    for (size_t i = 0; i < size_t(g.Bx) * g.By; ++i) {
+      if (sigma[i] > kMaxSigma) {
+        ctx->use_guide_ovr = ctx->use_sigma_ovr = false;
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "sigma %d > %d at block %zu",
+                    sigma[i], kMaxSigma, i);
+      }
+    }
     const size_t n = 4 * size_t(g.Bx) * g.By;
     if ((rc = Ensure(ctx, &ctx->sigma_ovr, n))) return rc;
     CUDA_TRY(ctx, cudaMemcpy(ctx->sigma_ovr.p, sigma, n,
@@ -1116,3 +1163,4 @@ const char* pikgpu_kernel_name(int index) {
 
 #include "dc_noalloc.cu"
 #include "batch.cu"
+#include "adjoint.cu"

@@ -1112,12 +1112,51 @@ struct ArBlockInfo {
   float inv_quant_ac;
 };
 
+// Clamp tape entry of one coefficient: 0 = no channel's ratio below 1 (the
+// correction is kept), 1..3 = channel code - 1 set the minimum ratio by
+// clamping, 4 = the minimum was the 0 of a +0.0 correction (SymmetricClamp
+// divides +0.0 by 1e-7). The adjoint follows these branches instead of
+// recomputing them, so rounding cannot send it down another one.
+__device__ __forceinline__ uint8_t ClampTapeCode(int arg, float co_arg) {
+  if (arg < 0) return 0;
+  return __float_as_uint(co_arg) == 0u ? 4 : uint8_t(arg + 1);
+}
+
+// Minimum ratio on the branch a clamp tape code names.
+__device__ __forceinline__ float TapeRatio(int code, float r0, float r1,
+                                           float r2) {
+  return code == 0   ? 1.0f
+         : code == 1 ? r0
+         : code == 2 ? r1
+         : code == 3 ? r2
+                     : 0.0f;
+}
+
+// Offset in the frame coefficient layout of element e (row-major in the
+// n x n block, n = 8 cov) of the block whose first cell is (bx, by).
+__device__ __forceinline__ size_t CoefOffset(const Geo& g, int bx, int by,
+                                             int cov, int e) {
+  const int chunk = 64 * cov;
+  return size_t(by + e / chunk) * g.ac_stride + size_t(bx) * 64 + e % chunk;
+}
+
+// inv_global_scale / qf of a block, times the optional per-cell clamp scale
+// (pikgpu_frame_set_clamp_scale): the factor of every non-LLF clamp
+// interval.
+__device__ __forceinline__ float ClampInvQuantAc(const Geo& g,
+                                                 const DevFrame& f,
+                                                 float inv_global_scale,
+                                                 int bx, int by, int qac) {
+  const float iq = inv_global_scale / float(qac);
+  return f.clamp_scale ? iq * f.clamp_scale[by * g.Bx + bx] : iq;
+}
+
 __device__ __forceinline__ ArBlockInfo ArInfo(const Geo& g, const DevFrame& f,
                                               const FrameScalars& s, int bx,
                                               int by, int type) {
   ArBlockInfo r;
   const int qac = f.qf[by * g.Bx + bx];
-  r.inv_quant_ac = s.inv_global_scale / float(qac);
+  r.inv_quant_ac = ClampInvQuantAc(g, f, s.inv_global_scale, bx, by, qac);
   const int cf = f.dq_cf[(by >> 3) * g.Tx + (bx >> 3)];
   const int table = f.dq_map[cf * 256 + (qac - 1)];
   const int kind = QuantKindOf(type);
@@ -1262,14 +1301,22 @@ __global__ void __launch_bounds__(256)
     const int bx = pk & 0xFFFF, by = pk >> 16;
     const int type = f.acs[by * g.Bx + bx] >> 4;
     const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
-    float mr = 1.0f;
+    float mr = 1.0f, rt[3];
+    int arg = -1;
     for (int c = 0; c < 3; ++c) {
       const float interval =
           e == 0 ? 1.0f * s.mul_dc[c] : info.dm[c][e] * info.inv_quant_ac;
-      const float r = ClampRatio(s_blk[c][i], interval);
-      mr = r < mr ? r : mr;
+      rt[c] = ClampRatio(s_blk[c][i], interval);
+      if (rt[c] < mr) mr = rt[c], arg = c;
+    }
+    const size_t to = CoefOffset(g, bx, by, 1, e);
+    uint8_t code = ClampTapeCode(arg, arg < 0 ? 0.f : s_blk[arg][i]);
+    if (f.clamp_tape_in) {
+      code = f.clamp_tape_in[to];
+      mr = TapeRatio(code, rt[0], rt[1], rt[2]);
     }
     s_r[i] = mr;
+    if (f.clamp_tape) f.clamp_tape[to] = code;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
@@ -1455,9 +1502,22 @@ __global__ void __launch_bounds__(3 * kSmallArBlocks)
   if (!active) return;
   for (int k = 0; k < 64; ++k) {
     float mr = 1.0f;
+    int arg = -1;
     for (int cc = 0; cc < 3; ++cc) {
       const float r = s_ratio[cc][lb][k];
-      mr = r < mr ? r : mr;
+      if (r < mr) mr = r, arg = cc;
+    }
+    if (f.clamp_tape || f.clamp_tape_in) {
+      const uint32_t pk = list[i];
+      const size_t to = CoefOffset(g, pk & 0xFFFF, pk >> 16, 1, k);
+      // The +0.0 case is the only one with a ratio of exactly 0.
+      uint8_t code = arg < 0 ? 0 : mr == 0.0f ? 4 : uint8_t(arg + 1);
+      if (f.clamp_tape_in) {
+        code = f.clamp_tape_in[to];
+        mr = TapeRatio(code, s_ratio[0][lb][k], s_ratio[1][lb][k],
+                       s_ratio[2][lb][k]);
+      }
+      if (f.clamp_tape && c == 0) f.clamp_tape[to] = code;
     }
     blk[k] = blk[k] * mr;
   }

@@ -222,24 +222,39 @@ __global__ void __launch_bounds__(kSquareThreads)
   }
   // Clamp ratios of coefficient row k = r, minimum over the channels.
   const int qac = f.qf[by * g.Bx + bx];
-  const float inv_quant_ac = s.inv_global_scale / float(qac);
+  const float inv_quant_ac =
+      ClampInvQuantAc(g, f, s.inv_global_scale, bx, by, qac);
   const int cf = f.dq_cf[(by >> 3) * g.Tx + (bx >> 3)];
   const int table = f.dq_map[cf * 256 + (qac - 1)];
   const int kind = QuantKindOf(type);
   const float* dm0 = f.table + f.offsets[(table * 7 + kind) * 3 + 0] + r * N;
   const float* dm1 = f.table + f.offsets[(table * 7 + kind) * 3 + 1] + r * N;
   const float* dm2 = f.table + f.offsets[(table * 7 + kind) * 3 + 2] + r * N;
+  const size_t tape_row = CoefOffset(g, bx, by, cov, r * N);
+  uint8_t* tape = f.clamp_tape && active ? f.clamp_tape + tape_row : nullptr;
+  const uint8_t* tin =
+      f.clamp_tape_in && active ? f.clamp_tape_in + tape_row : nullptr;
 #pragma unroll
   for (int l = 0; l < N; ++l) {
     const bool llf = r < cov && l < cov;
     const float ls = llf ? LlfScale(type, l, r) : 0.f;
     float mr = 1.0f;
-    float rt = ClampRatio(Y[0][l], llf ? ls * s.mul_dc[0] : dm0[l] * inv_quant_ac);
-    mr = rt < mr ? rt : mr;
-    rt = ClampRatio(Y[1][l], llf ? ls * s.mul_dc[1] : dm1[l] * inv_quant_ac);
-    mr = rt < mr ? rt : mr;
-    rt = ClampRatio(Y[2][l], llf ? ls * s.mul_dc[2] : dm2[l] * inv_quant_ac);
-    mr = rt < mr ? rt : mr;
+    int arg = -1;
+    const float rt0 =
+        ClampRatio(Y[0][l], llf ? ls * s.mul_dc[0] : dm0[l] * inv_quant_ac);
+    if (rt0 < mr) mr = rt0, arg = 0;
+    const float rt1 =
+        ClampRatio(Y[1][l], llf ? ls * s.mul_dc[1] : dm1[l] * inv_quant_ac);
+    if (rt1 < mr) mr = rt1, arg = 1;
+    const float rt2 =
+        ClampRatio(Y[2][l], llf ? ls * s.mul_dc[2] : dm2[l] * inv_quant_ac);
+    if (rt2 < mr) mr = rt2, arg = 2;
+    uint8_t code = arg < 0 ? 0 : mr == 0.0f ? 4 : uint8_t(arg + 1);
+    if (tin) {
+      code = tin[l];
+      mr = TapeRatio(code, rt0, rt1, rt2);
+    }
+    if (tape) tape[l] = code;
     Y[0][l] = Y[0][l] * mr;
     Y[1][l] = Y[1][l] * mr;
     Y[2][l] = Y[2][l] * mr;

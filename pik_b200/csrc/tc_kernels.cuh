@@ -490,7 +490,8 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
     {
       const int type = f.acs[by * g.Bx + bx] >> 4;
       const int qac = f.qf[by * g.Bx + bx];
-      const float inv_quant_ac = sc.inv_global_scale / float(qac);
+      const float inv_quant_ac =
+          ClampInvQuantAc(g, f, sc.inv_global_scale, bx, by, qac);
       const int cf = f.dq_cf[(by >> 3) * g.Tx + (bx >> 3)];
       const int table = f.dq_map[cf * 256 + (qac - 1)];
       const int kind = QuantKindOf(type);
@@ -499,17 +500,29 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
       for (int c = 0; c < 3; ++c) {
         dm[c] = f.table + f.offsets[(table * 7 + kind) * 3 + c] + r * N;
       }
+      const size_t tape_row = CoefOffset(g, bx, by, cov, r * N);
+      uint8_t* tape =
+          f.clamp_tape && active ? f.clamp_tape + tape_row : nullptr;
+      const uint8_t* tin =
+          f.clamp_tape_in && active ? f.clamp_tape_in + tape_row : nullptr;
 #pragma unroll
       for (int l = 0; l < N; ++l) {
         const bool llf = r < cov && l < cov;
         const float ls = llf ? LlfScale(type, l, r) : 0.f;
-        float mr = 1.0f;
+        float mr = 1.0f, rt[3];
+        int arg = -1;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const float rt = ClampRatio(
+          rt[c] = ClampRatio(
               Y[c][l], llf ? ls * sc.mul_dc[c] : dm[c][l] * inv_quant_ac);
-          mr = rt < mr ? rt : mr;
+          if (rt[c] < mr) mr = rt[c], arg = c;
         }
+        uint8_t code = arg < 0 ? 0 : mr == 0.0f ? 4 : uint8_t(arg + 1);
+        if (tin) {
+          code = tin[l];
+          mr = TapeRatio(code, rt[0], rt[1], rt[2]);
+        }
+        if (tape) tape[l] = code;
 #pragma unroll
         for (int c = 0; c < 3; ++c) Y[c][l] = Y[c][l] * mr;
       }

@@ -69,6 +69,11 @@ def lib() -> ctypes.CDLL:
     L.pikgpu_dc_reconstruct_noalloc.argtypes = [
         P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
         P, ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_char_p, S]
+    L.pikgpu_adjoint.argtypes = [P, P, P, P, P, ctypes.c_int]
+    L.pikgpu_frame_set_dequantized_ac.argtypes = [P, P, ctypes.c_int]
+    L.pikgpu_frame_set_clamp_scale.argtypes = [P, P, ctypes.c_int]
+    L.pikgpu_set_clamp_decisions.argtypes = [P, P]
+    L.pikgpu_get_clamp_decisions.argtypes = [P, P]
     L.pikgpu_batch_create.argtypes = [ctypes.c_int, ctypes.c_int,
                                       ctypes.POINTER(P)]
     L.pikgpu_batch_destroy.argtypes = [P]
@@ -228,6 +233,55 @@ class Context:
         self._check(self.L.pikgpu_get_epf_decisions(self.h, g.ctypes.data,
                                                     s.ctypes.data))
         return g, s
+
+    def adjoint(self, target: np.ndarray, *, grads: bool = True):
+        """pikgpu_adjoint with host buffers: (loss, grad_ac (3, By, Bx*64),
+        grad_qf (By, Bx)) of sum((pre_opsin - target)^2), `target` being
+        (3, ysize, xsize) XYB."""
+        f = self.frame
+        if f is None:
+            self._check(self.L.pikgpu_adjoint(self.h, None, None, None, None,
+                                              0))
+        by, bx = f.blocks
+        t = np.ascontiguousarray(target, np.float32)
+        if t.shape != (3, f.ysize, f.xsize):
+            raise ValueError(f"target shape {t.shape}")
+        loss = np.zeros(1, np.float64)
+        g_ac = np.zeros((3, by, bx * 64), np.float32) if grads else None
+        g_qf = np.zeros((by, bx), np.float32) if grads else None
+        self._check(self.L.pikgpu_adjoint(
+            self.h, t.ctypes.data, loss.ctypes.data,
+            g_ac.ctypes.data if grads else None,
+            g_qf.ctypes.data if grads else None, 0))
+        return float(loss[0]), g_ac, g_qf
+
+    def clamp_decisions(self) -> np.ndarray:
+        """The clamp tape of the last recording forward pass, (By, Bx*64)
+        uint8."""
+        by, bx = self.frame.blocks
+        t = np.zeros((by, bx * 64), np.uint8)
+        self._check(self.L.pikgpu_get_clamp_decisions(self.h, t.ctypes.data))
+        return t
+
+    def set_clamp_decisions(self, tape: np.ndarray | None) -> None:
+        t = None if tape is None else np.ascontiguousarray(tape, np.uint8)
+        self._keep_tape = t
+        self._check(self.L.pikgpu_set_clamp_decisions(
+            self.h, t.ctypes.data if t is not None else None))
+
+    def set_dequantized_ac(self, ac: np.ndarray | None) -> None:
+        """Dequantised AC (3, By, Bx*64) used instead of Dequant::DoAC's;
+        None restores dequantising the int16 AC."""
+        a = None if ac is None else np.ascontiguousarray(ac, np.float32)
+        self._check(self.L.pikgpu_frame_set_dequantized_ac(
+            self.h, a.ctypes.data if a is not None else None, 0))
+
+    def set_clamp_scale(self, scale: np.ndarray | None) -> None:
+        """Per-cell multiplier (By, Bx) of the clamp's non-LLF intervals."""
+        a = None if scale is None else np.ascontiguousarray(scale,
+                                                            np.float32)
+        self._check(self.L.pikgpu_frame_set_clamp_scale(
+            self.h, a.ctypes.data if a is not None else None, 0))
 
     def kernel_times(self) -> dict:
         ms = np.zeros(16, np.float32)

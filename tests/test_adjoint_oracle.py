@@ -7,7 +7,7 @@ absolute (gradients up to ~3) and the quant field within 1e-3 relative."""
 import numpy as np
 import pytest
 
-from oracle import decisions, oraclepy
+from oracle import decisions, finite_diff, oraclepy
 from pik_b200 import synthetic
 
 SHARES = {"DCT": 0.3, "DCT16X16": 0.3, "DCT32X32": 0.2, "DCT4X4": 0.05,
@@ -67,3 +67,27 @@ def test_oracle_adjoint_matches_finite_differences(variant):
     if variant == "epf_off":
         frame.have_ar = 0
     fd_check(frame)
+
+
+def test_finite_diff_module_matches_the_adjoint():
+    """oracle/finite_diff.py (the pool-based differences the CUDA adjoint is
+    checked with) against the FP64 adjoint, decisions held at the base
+    point's."""
+    frame = synthetic.make_frame(72, 64, seed=3, qf_median=10.0,
+                                 shares=SHARES)
+    base = oraclepy.run(frame, precision=64, want=("pre_opsin",),
+                        export_decisions=True)
+    dg, ds = decisions.dc_decisions(frame)
+    kw = dict(guide=base["guide"], sigma=base["sigma"], dc_guide=dg,
+              dc_sigma=ds)
+    rng = np.random.default_rng(2)
+    target = base["pre_opsin"] + rng.normal(0, 0.01, base["pre_opsin"].shape)
+    _, g_ac, g_qf = oraclepy.adjoint(frame, target, **kw)
+    idx = rng.choice(g_ac.size, 16, replace=False)
+    cells = [(1, 2), (5, 7)]
+    fd_ac, fd_qf = finite_diff.gradients(frame, target, kw, idx, cells,
+                                         workers=2)
+    np.testing.assert_allclose(fd_ac, g_ac.ravel()[idx], rtol=1e-3,
+                               atol=1e-7)
+    np.testing.assert_allclose(fd_qf, [g_qf[y, x] for y, x in cells],
+                               rtol=1e-3, atol=1e-9)
