@@ -291,6 +291,135 @@ def batch_main(args):
     b.close()
 
 
+ADJ_SHARES = {"DCT": 0.3, "DCT16X16": 0.3, "DCT32X32": 0.2, "DCT4X4": 0.05,
+              "DCT2X2": 0.05, "IDENTITY": 0.04, "LINES": 0.03,
+              "DCT_NOHF": 0.02, "DCT4X4_NOHF": 0.01}
+
+
+def adjoint_main(args):
+    """Gradient evaluations of sum((pre_opsin - target)^2) with respect to
+    the dequantised AC and the quant field (pikgpu_adjoint: forward pass
+    with the clamp tape, then the backward kernels) on a 1024x1024 frame at
+    distance 1.5 with every block size and the EPF on. Synthetic frame; the
+    target is its own reconstruction plus N(0, 0.01) noise."""
+    import ctypes
+    import torch
+    from pik_b200 import native, synthetic
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    frame = synthetic.make_frame(1024, 1024, seed=4, qf_median=12.0,
+                                 shares=ADJ_SHARES)
+    px = frame.xsize * frame.ysize
+    by, bx = frame.blocks
+    probe = native.Context(local, keep_stages=True, form=args.form)
+    probe.begin(frame)
+    probe.set_ac()
+    probe.reconstruct()
+    pre = probe.stage("pre_opsin")
+    probe.close()
+    rng = np.random.default_rng(0)
+    target = (pre + rng.normal(0, 0.01, pre.shape)).astype(np.float32)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = native.Context(local, form=args.form)
+    ctx.begin(frame)
+    ctx.set_ac()
+    ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
+    t_dev = torch.from_numpy(target).to(dev)
+    g_ac = torch.empty((3, by, bx * 64), dtype=torch.float32, device=dev)
+    g_qf = torch.empty((by, bx), dtype=torch.float32, device=dev)
+    loss = torch.empty(1, dtype=torch.float64, device=dev)
+    lin = torch.empty((3, frame.ysize, frame.xsize), device=dev)
+
+    def adj_step():
+        ctx._check(ctx.L.pikgpu_adjoint(ctx.h, t_dev.data_ptr(),
+                                        loss.data_ptr(), g_ac.data_ptr(),
+                                        g_qf.data_ptr(), 1))
+
+    def fwd_step():
+        ctx.reconstruct_device(lin.data_ptr(), frame.xsize)
+
+    def timed(fn, clk=None):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        if clk:
+            clk.__enter__()
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if clk:
+            clk.__exit__()
+        return e0.elapsed_time(e1) / args.steps
+
+    clk = ClockSampler(local)
+    ms_adj = timed(adj_step, clk)
+    launches = ctx.L.pikgpu_last_launch_count(ctx.h)
+    ms_fwd = timed(fwd_step)
+    # End to end with host buffers: target up, gradients and loss down.
+    pin_t = torch.from_numpy(target).pin_memory()
+    pin_ac = torch.empty(g_ac.shape, dtype=torch.float32).pin_memory()
+    pin_qf = torch.empty(g_qf.shape, dtype=torch.float32).pin_memory()
+    pin_l = torch.empty(1, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        ctx._check(ctx.L.pikgpu_adjoint(ctx.h, pin_t.data_ptr(),
+                                        pin_l.data_ptr(), pin_ac.data_ptr(),
+                                        pin_qf.data_ptr(), 0))
+
+    for _ in range(max(3, args.warmup)):
+        e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    ctx.close()
+    # FP64 oracle adjoint on the host (one thread), a bounded sample: one
+    # gradient evaluation of the same frame.
+    cpu = None
+    try:
+        from oracle import decisions as odec, oraclepy
+        dg, ds = odec.dc_decisions(frame)
+        t0 = time.perf_counter()
+        oraclepy.adjoint(frame, target.astype(np.float64), dc_guide=dg,
+                         dc_sigma=ds)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": round(px / cpu_s / 1e6, 4), "unit": "MP/s",
+               "cores": 1, "kind": "port",
+               "sample": "one FP64 oracle gradient evaluation of the same "
+                         "1024x1024 frame"}
+    except Exception as e:  # oracle library not built on this host
+        cpu = {"unavailable": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "adjoint gradient evaluations of a 1024x1024 frame "
+                      "(forward + backward), MP/s",
+            "value": round(px / (ms_adj * 1e-3) / 1e6, 2), "unit": "MP/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_adj, 4), "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "adjoint1k: 1024x1024 synthetic frame, "
+                       "distance 1.5 (quant field ~12), every block size, "
+                       "gaborish + EPF on",
+                       "form": FORM_NAMES[args.form]},
+            "forward_only": {"value": round(px / (ms_fwd * 1e-3) / 1e6, 2),
+                             "ms_per_step": round(ms_fwd, 4)},
+            "backward_over_forward": round((ms_adj - ms_fwd) / ms_fwd, 3),
+            "e2e": {"value": round(px / (e2e_ms * 1e-3) / 1e6, 2),
+                    "unit": "MP/s",
+                    "h2d_bytes_per_step": int(target.nbytes),
+                    "d2h_bytes_per_step": int(pin_ac.numel() * 4 +
+                                              pin_qf.numel() * 4 + 8)},
+            "gpu_launches": launches * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -300,12 +429,14 @@ def main():
     ap.add_argument("--form", default="split_bf16",
                     choices=sorted(FORM_NAMES))
     ap.add_argument("--workload", default="c2_4k",
-                    choices=["c2_4k", "batch64"])
+                    choices=["c2_4k", "batch64", "adjoint1k"])
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
     if args.workload == "batch64":
         return batch_main(args)
+    if args.workload == "adjoint1k":
+        return adjoint_main(args)
 
     import torch
     import torch.distributed as dist
