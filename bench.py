@@ -459,8 +459,8 @@ def main():
     import ctypes
     planes = (ctypes.c_void_p * 3)(*[ac_dev[c].data_ptr() for c in range(3)])
 
-    def time_device(form, sample_clocks=False):
-        ctx = native.Context(local, form=form)
+    def time_device(form, sample_clocks=False, graphs=True):
+        ctx = native.Context(local, form=form, graphs=graphs)
         ctx.begin(frame)
         ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
 
@@ -498,6 +498,8 @@ def main():
 
     ms, launches, clk = time_device(args.form, sample_clocks=True)
     value = ws * px / (ms * 1e-3) / 1e6
+    # The same without graph replay: every step launches its ~30 kernels.
+    ms_direct = time_device(args.form, graphs=False)[0]
     # The other forms on the same frame, for the form comparison.
     forms = {args.form: ms}
     for form in native.FORMS:
@@ -609,6 +611,12 @@ def main():
                           "ms_per_step": round(t, 4)}
                       for f, t in forms.items()},
             "speedup_vs_fp32": round(forms["fp32"] / ms, 3),
+            "launch_mode": "CUDA graph replay of the frame's launch "
+                           "sequence (PIKGPU_OPT_GRAPHS), one graph launch "
+                           "per step",
+            "direct_launches": {
+                "value": round(ws * px / (ms_direct * 1e-3) / 1e6, 2),
+                "ms_per_step": round(ms_direct, 4)},
             "e2e": {"value": round(e2e, 2), "unit": "MP/s",
                     "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},

@@ -197,14 +197,26 @@ int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
  *               PIKGPU_FORM_SPLIT_BF16X3: the same with three terms
  *               (hi + mid + lo, six products; FP32-level error).
  *               The tensor-core forms are not bit-identical to the FP32
- *               form. */
+ *               form;
+ *  GRAPHS:      1 (default): when pikgpu_reconstruct is called again with
+ *               the launch state of the previous call (frame geometry,
+ *               header scalars, blocks per transform class, options,
+ *               device buffers, outputs and stream all unchanged -- the
+ *               coefficients and side information may differ), the launch
+ *               sequence is captured once into a CUDA graph and replayed
+ *               as one launch; 0: every call launches its ~30 kernels. */
 #define PIKGPU_OPT_KEEP_STAGES 1
 #define PIKGPU_OPT_PROFILE 2
 #define PIKGPU_OPT_FORM 3
+#define PIKGPU_OPT_GRAPHS 4
 #define PIKGPU_FORM_FP32 0
 #define PIKGPU_FORM_SPLIT_BF16 1
 #define PIKGPU_FORM_SPLIT_BF16X3 2
 int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value);
+/* Graphs captured by this context so far (PIKGPU_OPT_GRAPHS), and whether
+ * the last pikgpu_reconstruct ran as a graph replay (either may be NULL). */
+int pikgpu_graph_stats(const pikgpu_ctx* ctx, int* captures,
+                       int* last_replayed);
 
 /* Verification hooks for the EPF's discrete decisions, which make two
  * implementations comparable on arithmetic alone: the u8 guide (3 planes of

@@ -112,8 +112,34 @@ struct pikgpu_ctx {
   float dc_half_step[3] = {};
   int launches = 0;
   // Bumped by every call that changes what the launch sequence does or
-  // which buffers it uses (a captured batch graph is then stale).
+  // which buffers it uses, and by every device (re)allocation: a captured
+  // graph (single frame or batch) is then stale.
   uint64_t generation = 0;
+  // Single-frame graph replay (PIKGPU_OPT_GRAPHS): the launch state of the
+  // last pikgpu_reconstruct call, and its graph once a call repeated it.
+  struct GraphKey {
+    uint64_t generation;
+    float* lin;
+    size_t lin_stride;
+    uint8_t* rgb8;
+    size_t rgb8_stride;
+    cudaStream_t stream;
+    int tc_ctas;
+    bool operator==(const GraphKey& o) const {
+      return generation == o.generation && lin == o.lin &&
+             lin_stride == o.lin_stride && rgb8 == o.rgb8 &&
+             rgb8_stride == o.rgb8_stride && stream == o.stream &&
+             tc_ctas == o.tc_ctas;
+    }
+  };
+  bool use_graphs = true, have_key = false;
+  GraphKey key{};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_launches = 0, graph_captures = 0;
+  bool graph_tape_valid = false, last_replayed = false;
+  // Pinned host word the tensor-core error flag is read back into.
+  int* tc_err_host = nullptr;
 };
 
 namespace {
@@ -143,6 +169,7 @@ int Ensure(pikgpu_ctx* ctx, DevBuf* b, size_t bytes) {
   if (b->p) cudaFree(b->p);
   b->p = nullptr;
   b->cap = 0;
+  if (ctx) ++ctx->generation;
   const cudaError_t e = cudaMalloc(&b->p, bytes);
   if (e != cudaSuccess) {
     return Fail(ctx, PIKGPU_ERR_NO_MEMORY, "cudaMalloc(%zu): %s", bytes,
@@ -624,6 +651,78 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   return PIKGPU_OK;
 }
 
+void DropFrameGraph(pikgpu_ctx* ctx) {
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  ctx->graph_exec = nullptr;
+  ctx->graph = nullptr;
+}
+
+// The launch sequence of one pikgpu_reconstruct. A call that repeats the
+// previous call's launch state (GraphKey: generation, outputs, stream,
+// tensor-core CTAs per SM) replays the sequence from a CUDA graph, captured
+// on the first repeat; any other call launches kernel by kernel and
+// remembers its state.
+int RunFrame(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
+             size_t rgb8_stride) {
+  ctx->last_replayed = false;
+  if (!ctx->use_graphs || ctx->profile) {
+    DropFrameGraph(ctx);
+    ctx->have_key = false;
+    return LaunchAll(ctx, lin, lin_stride, rgb8, rgb8_stride);
+  }
+  const pikgpu_ctx::GraphKey key{ctx->generation, lin,        lin_stride,
+                                 rgb8,            rgb8_stride, ctx->stream,
+                                 ctx->tc_ctas_per_sm};
+  const bool repeat = ctx->have_key && key == ctx->key;
+  if (repeat && ctx->graph_exec) {
+    CUDA_TRY(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+    ctx->launches = ctx->graph_launches;
+    ctx->smoothed_valid = false;
+    ctx->tape_valid = ctx->graph_tape_valid;
+    ctx->last_replayed = true;
+    return PIKGPU_OK;
+  }
+  DropFrameGraph(ctx);
+  if (!repeat) {
+    ctx->key = key;
+    ctx->have_key = true;
+    return LaunchAll(ctx, lin, lin_stride, rgb8, rgb8_stride);
+  }
+  // First repeat: capture, instantiate and launch. If capturing is not
+  // possible (the stream is being captured by the caller, say), launch
+  // directly.
+  if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    ctx->have_key = false;
+    return LaunchAll(ctx, lin, lin_stride, rgb8, rgb8_stride);
+  }
+  const int rc = LaunchAll(ctx, lin, lin_stride, rgb8, rgb8_stride);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(ctx->stream, &graph);
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t inst =
+      rc == PIKGPU_OK && end == cudaSuccess
+          ? cudaGraphInstantiate(&exec, graph, 0)
+          : cudaErrorUnknown;
+  if (inst != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    ctx->have_key = false;
+    if (rc != PIKGPU_OK) return rc;
+    return LaunchAll(ctx, lin, lin_stride, rgb8, rgb8_stride);
+  }
+  ctx->graph = graph;
+  ctx->graph_exec = exec;
+  ctx->graph_launches = ctx->launches;
+  ctx->graph_tape_valid = ctx->tape_valid;
+  ++ctx->graph_captures;
+  CUDA_TRY(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+  ctx->last_replayed = true;
+  return PIKGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -658,7 +757,8 @@ int pikgpu_ctx_create(int device, pikgpu_ctx** out) {
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount,
                          device);
   if (Ensure(ctx, &ctx->tc_err, sizeof(int)) != PIKGPU_OK ||
-      cudaMemset(ctx->tc_err.p, 0, sizeof(int)) != cudaSuccess) {
+      cudaMemset(ctx->tc_err.p, 0, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&ctx->tc_err_host, sizeof(int)) != cudaSuccess) {
     pikgpu_ctx_destroy(ctx);
     return PIKGPU_ERR_NO_MEMORY;
   }
@@ -695,6 +795,8 @@ int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
   for (auto& b : ctx->active) FreeBuf(&b);
   FreeBuf(&ctx->counters);
   FreeBuf(&ctx->tc_err);
+  DropFrameGraph(ctx);
+  if (ctx->tc_err_host) cudaFreeHost(ctx->tc_err_host);
   for (auto& e : ctx->ev) {
     if (e) cudaEventDestroy(e);
   }
@@ -723,6 +825,9 @@ int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
     case PIKGPU_OPT_PROFILE:
       ctx->profile = value != 0;
       return PIKGPU_OK;
+    case PIKGPU_OPT_GRAPHS:
+      ctx->use_graphs = value != 0;
+      return PIKGPU_OK;
     case PIKGPU_OPT_FORM:
       if (value != PIKGPU_FORM_FP32 && value != PIKGPU_FORM_SPLIT_BF16 &&
           value != PIKGPU_FORM_SPLIT_BF16X3) {
@@ -736,7 +841,21 @@ int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
 
 int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
-  ++ctx->generation;
+  // The launch state before this frame: a frame that leaves it unchanged
+  // (and reallocates nothing, which Ensure would record) keeps the
+  // generation, so a captured graph stays valid for it.
+  const bool had_frame = ctx->have_frame;
+  const bool had_overrides = ctx->use_guide_ovr || ctx->use_sigma_ovr ||
+                             ctx->use_dq_ovr || ctx->use_clamp_scale ||
+                             ctx->use_tape_in;
+  const Geo old_g = ctx->g;
+  const FrameScalars old_s = ctx->s;
+  float old_half[3];
+  memcpy(old_half, ctx->dc_half_step, sizeof(old_half));
+  size_t old_n[kNumClasses];
+  for (int k = 0; k < kNumClasses; ++k) old_n[k] = ctx->lists[k].size();
+  ++ctx->generation;  // until the frame is known to keep the state
+  const uint64_t gen0 = ctx->generation;
   ctx->have_frame = ctx->have_ac = ctx->have_result = false;
   ctx->use_guide_ovr = ctx->use_sigma_ovr = false;
   ctx->use_dq_ovr = ctx->use_clamp_scale = false;
@@ -856,6 +975,14 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
   CUDA_TRY(ctx, cudaMemcpyAsync(ctx->qdc.p, p->quantized_dc, 2 * 3 * nb,
                                 cudaMemcpyHostToDevice, st));
   ctx->have_frame = true;
+  bool same = had_frame && !had_overrides && ctx->generation == gen0 &&
+              memcmp(&old_g, &ctx->g, sizeof(Geo)) == 0 &&
+              memcmp(&old_s, &ctx->s, sizeof(FrameScalars)) == 0 &&
+              memcmp(old_half, ctx->dc_half_step, sizeof(old_half)) == 0;
+  for (int k = 0; k < kNumClasses; ++k) {
+    same = same && old_n[k] == ctx->lists[k].size();
+  }
+  if (same) ctx->generation = gen0 - 1;
   return PIKGPU_OK;
 }
 
@@ -980,7 +1107,7 @@ int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
       rgb8 = P<uint8_t>(ctx->out_rgb8);
     }
   }
-  rc = LaunchAll(ctx, lin, lin_stride, rgb8, rgb8_stride);
+  rc = RunFrame(ctx, lin, lin_stride, rgb8, rgb8_stride);
   if (rc != PIKGPU_OK) return rc;
   if (!outputs_on_device) {
     if (out_linear) {
@@ -998,16 +1125,19 @@ int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
                                       cudaMemcpyDeviceToHost, ctx->stream));
     }
   }
+  // The tensor-core error flag comes back with the same synchronisation.
+  const bool tc = ctx->form != PIKGPU_FORM_FP32;
+  if (tc) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->tc_err_host, ctx->tc_err.p,
+                                  sizeof(int), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+  }
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  if (ctx->form != PIKGPU_FORM_FP32) {
-    int tc_err = 0;
-    CUDA_TRY(ctx, cudaMemcpy(&tc_err, ctx->tc_err.p, sizeof(int),
-                             cudaMemcpyDeviceToHost));
-    if (tc_err) {
-      cudaMemset(ctx->tc_err.p, 0, sizeof(int));
-      return Fail(ctx, PIKGPU_ERR_CUDA,
-                  "tensor-core transform: MMA completion wait timed out");
-    }
+  if (tc && *ctx->tc_err_host) {
+    *ctx->tc_err_host = 0;
+    cudaMemset(ctx->tc_err.p, 0, sizeof(int));
+    return Fail(ctx, PIKGPU_ERR_CUDA,
+                "tensor-core transform: MMA completion wait timed out");
   }
   if (ctx->profile) {
     for (int i = 0; i < kNumTimed; ++i) {
@@ -1153,6 +1283,14 @@ int pikgpu_last_kernel_times(pikgpu_ctx* ctx, float* ms, int n) {
 
 int pikgpu_last_launch_count(const pikgpu_ctx* ctx) {
   return ctx ? ctx->launches : PIKGPU_ERR_INVALID_ARG;
+}
+
+int pikgpu_graph_stats(const pikgpu_ctx* ctx, int* captures,
+                       int* last_replayed) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (captures) *captures = ctx->graph_captures;
+  if (last_replayed) *last_replayed = ctx->last_replayed ? 1 : 0;
+  return PIKGPU_OK;
 }
 
 const char* pikgpu_kernel_name(int index) {

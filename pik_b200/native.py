@@ -22,6 +22,7 @@ STAGES = {"dc": 0, "idct": 1, "smoothed": 2, "epf": 3, "ar": 4,
 OPT_KEEP_STAGES = 1
 OPT_PROFILE = 2
 OPT_FORM = 3
+OPT_GRAPHS = 4
 FORMS = {"fp32": 0, "split_bf16": 1, "split_bf16x3": 2}
 
 _lib = None
@@ -70,6 +71,7 @@ def lib() -> ctypes.CDLL:
         P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
         P, ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_char_p, S]
     L.pikgpu_adjoint.argtypes = [P, P, P, P, P, ctypes.c_int]
+    L.pikgpu_graph_stats.argtypes = [P, P, P]
     L.pikgpu_frame_set_dequantized_ac.argtypes = [P, P, ctypes.c_int]
     L.pikgpu_frame_set_clamp_scale.argtypes = [P, P, ctypes.c_int]
     L.pikgpu_set_clamp_decisions.argtypes = [P, P]
@@ -126,7 +128,8 @@ class Context:
     """One pikgpu context (device memory + stream)."""
 
     def __init__(self, device: int = 0, *, keep_stages: bool = False,
-                 profile: bool = False, form: str = "fp32"):
+                 profile: bool = False, form: str = "fp32",
+                 graphs: bool = True):
         self.L = lib()
         h = ctypes.c_void_p()
         rc = self.L.pikgpu_ctx_create(device, ctypes.byref(h))
@@ -137,6 +140,7 @@ class Context:
                                              int(keep_stages)))
         self._check(self.L.pikgpu_set_option(h, OPT_PROFILE, int(profile)))
         self._check(self.L.pikgpu_set_option(h, OPT_FORM, FORMS[form]))
+        self._check(self.L.pikgpu_set_option(h, OPT_GRAPHS, int(graphs)))
         self.frame = None
         self._packed = None
 
@@ -282,6 +286,12 @@ class Context:
                                                             np.float32)
         self._check(self.L.pikgpu_frame_set_clamp_scale(
             self.h, a.ctypes.data if a is not None else None, 0))
+
+    def graph_stats(self) -> dict:
+        cap, rep = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.pikgpu_graph_stats(self.h, ctypes.byref(cap),
+                                              ctypes.byref(rep)))
+        return {"captures": cap.value, "last_replayed": bool(rep.value)}
 
     def kernel_times(self) -> dict:
         ms = np.zeros(16, np.float32)
