@@ -106,6 +106,11 @@ struct pikgpu_ctx {
   // The smoothed frame (gaborish #1) is written only when an export asks.
   bool smoothed_valid = false;
   cudaEvent_t ev[kNumTimed + 1] = {};
+  // Side streams and fork/join events of the launch sequence's concurrent
+  // branches (LaunchAll).
+  static constexpr int kSide = 4;
+  cudaStream_t side[kSide] = {};
+  cudaEvent_t fork_ev[3] = {}, join_ev[3][kSide] = {};
   int num_sms = 148;
   int tc_ctas_per_sm = kTcCtasPerSm;
   float times[kNumTimed] = {};
@@ -379,21 +384,58 @@ void Mark(pikgpu_ctx* ctx, int i) {
 // The frame EPF or the DC EPF: minmax of the guide source is expected in
 // ctx->mm already; sigma per block in `sig`. `gab` > 0: the guide is
 // gaborish (that strength) of `in`, computed inside the kernel.
-int RunEpf(pikgpu_ctx* ctx, const float* in, const float* guide_src, int gab,
-           int w, int h, const int32_t* sig, float* out,
-           const uint8_t* guide_ovr) {
+int RunEpf(pikgpu_ctx* ctx, cudaStream_t st, const float* in,
+           const float* guide_src, int gab, int w, int h, const int32_t* sig,
+           float* out, const uint8_t* guide_ovr) {
   dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
-  k_epf_box<<<grid, kEpfThreads, kEpfSmemBytes, ctx->stream>>>(
+  k_epf_box<<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
       in, guide_src, guide_ovr, gab, w, h, P<uint32_t>(ctx->mm), sig, out);
   ++ctx->launches;
   return PIKGPU_OK;
 }
 
+// Concurrent branches of the launch sequence. Fork(i, n) makes side streams
+// 0..n-1 wait for the main stream's work so far; Join(i, n) makes the main
+// stream wait for theirs. Without branches (profiling, whose per-group
+// event times need one stream) every branch is the main stream and both
+// are no-ops. Events are recorded and waited in stream order, so this also
+// holds inside a stream capture (the branches become graph dependencies).
+struct Branches {
+  pikgpu_ctx* ctx;
+  bool on;
+  cudaStream_t main;
+  cudaStream_t operator[](int i) const {
+    return on ? ctx->side[i] : main;
+  }
+  void Fork(int i, int n) const {
+    if (!on) return;
+    cudaEventRecord(ctx->fork_ev[i], main);
+    for (int k = 0; k < n; ++k) cudaStreamWaitEvent(ctx->side[k], ctx->fork_ev[i], 0);
+  }
+  void Join(int i, int n) const {
+    if (!on) return;
+    for (int k = 0; k < n; ++k) {
+      cudaEventRecord(ctx->join_ev[i][k], ctx->side[k]);
+      cudaStreamWaitEvent(main, ctx->join_ev[i][k], 0);
+    }
+  }
+};
+
+// The launch sequence of one frame. Its DAG:
+//   side 0: DC dequant, DC EPF and clamp, then the per-group LF prediction
+//   main:   AC dequantisation            (both from the inputs only)
+//   main:   LLF / LF update, pred2x2      (joins the two)
+//   main + sides: the inverse transforms, one transform class each (their
+//           blocks are disjoint)
+//   main:   gaborish minmax, sigma, EPF
+//   main + sides: the clamp, one transform class each
+//   main:   gaborish #2, opsin, outputs
 int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
               size_t rgb8_stride) {
   const Geo& g = ctx->g;
   const FrameScalars& s = ctx->s;
   cudaStream_t st = ctx->stream;
+  const Branches br{ctx, !ctx->profile, st};
   DevFrame f;
   f.acs = P<uint8_t>(ctx->acs);
   f.qf = P<int32_t>(ctx->qf);
@@ -423,51 +465,63 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   f.clamp_tape_in = ctx->use_tape_in ? P<uint8_t>(ctx->tape_in) : nullptr;
   ctx->tape_valid = rec;
   uint32_t* mm = P<uint32_t>(ctx->mm);
+  const uint32_t* L[kNumClasses];
+  int n[kNumClasses];
+  for (int k = 0; k < kNumClasses; ++k) {
+    L[k] = P<uint32_t>(ctx->list[k]);
+    n[k] = int(ctx->lists[k].size());
+  }
+  // Side stream of each transform class's branch (the main stream takes
+  // DCT8, usually the most blocks).
+  auto cls = [&](int k) { return k == kC8 ? st : br[k - 1]; };
 
   ctx->launches = 0;
   ctx->smoothed_valid = false;
+  br.Fork(0, 1);
   Mark(ctx, kTDc);
-  // DC: dequant, EPF on the 8-padded DC image, clamp.
-  k_dequant_dc<<<Blocks(size_t(g.Bx) * g.By, 256), 256, 0, st>>>(g, f, s); ++ctx->launches;
+  // DC: dequant, EPF on the 8-padded DC image, clamp (side stream 0).
+  cudaStream_t sd = br[0];
+  k_dequant_dc<<<Blocks(size_t(g.Bx) * g.By, 256), 256, 0, sd>>>(g, f, s); ++ctx->launches;
   const int dpw = (g.Bx + 7) / 8 * 8, dph = (g.By + 7) / 8 * 8;
   float* dcpad = P<float>(ctx->dcpad);
   float* dcfilt = P<float>(ctx->dcfilt);
   {
     dim3 b(32, 8), gr(Blocks(dpw, 32), Blocks(dph, 8), 3);
-    k_pad_replicate<<<gr, b, 0, st>>>(f.dc, g.Bx, g.By, dcpad, dpw, dph); ++ctx->launches;
-    k_minmax_init<<<1, 32, 0, st>>>(mm); ++ctx->launches;
-    k_minmax<<<dim3(Blocks(size_t(dpw) * dph, 256 * 8), 3), 256, 0, st>>>(
+    k_pad_replicate<<<gr, b, 0, sd>>>(f.dc, g.Bx, g.By, dcpad, dpw, dph); ++ctx->launches;
+    k_minmax_init<<<1, 32, 0, sd>>>(mm); ++ctx->launches;
+    k_minmax<<<dim3(Blocks(size_t(dpw) * dph, 256 * 8), 3), 256, 0, sd>>>(
         dcpad, size_t(dpw) * dph, mm); ++ctx->launches;
     const int nb = (dpw / 8) * (dph / 8);
-    k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(
+    k_epf_sigma<<<Blocks(nb, 256), 256, 0, sd>>>(
         nb, nullptr, nullptr, nullptr, s.quant_dc / 2, mm,
         P<int32_t>(ctx->dc_sigma)); ++ctx->launches;
-    RunEpf(ctx, dcpad, dcpad, 0, dpw, dph, P<int32_t>(ctx->dc_sigma), dcfilt,
-           nullptr);
+    RunEpf(ctx, sd, dcpad, dcpad, 0, dpw, dph, P<int32_t>(ctx->dc_sigma),
+           dcfilt, nullptr);
     dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
-    k_dc_clamp<<<gr2, b, 0, st>>>(f.dc, dcfilt, g.Bx, g.By, dpw, dph,
+    k_dc_clamp<<<gr2, b, 0, sd>>>(f.dc, dcfilt, g.Bx, g.By, dpw, dph,
                                   ctx->dc_half_step[0], ctx->dc_half_step[1],
                                   ctx->dc_half_step[2]); ++ctx->launches;
   }
   Mark(ctx, kTLf);
-  // Per-group LF prediction.
+  // Per-group LF prediction (side stream 0, after DC).
   const int ng = g.Gx * g.Gy;
   {
     dim3 b(16, 16), gr(Blocks(kGB, 16), Blocks(kGB, 16), 3 * ng);
-    k_llf<<<gr, b, 0, st>>>(g, f); ++ctx->launches;
+    k_llf<<<gr, b, 0, sd>>>(g, f); ++ctx->launches;
     if (s.predict_lf) {
-      k_tmp2x2<<<gr, b, 0, st>>>(g, f); ++ctx->launches;
+      k_tmp2x2<<<gr, b, 0, sd>>>(g, f); ++ctx->launches;
       dim3 gr2(Blocks(kG2, 16), Blocks(kG2, 16), 3 * ng);
-      k_lf_blur<<<gr2, b, 0, st>>>(g, f); ++ctx->launches;
-      k_lf_from_2x2<<<gr, b, 0, st>>>(g, f); ++ctx->launches;
+      k_lf_blur<<<gr2, b, 0, sd>>>(g, f); ++ctx->launches;
+      k_lf_from_2x2<<<gr, b, 0, sd>>>(g, f); ++ctx->launches;
     }
     if (s.predict_hf) {
       k_pred_border<<<dim3(Blocks(4 * (kGB + 2), 128), 1, 3 * ng), 128, 0,
-                      st>>>(g, f, s.predict_lf); ++ctx->launches;
+                      sd>>>(g, f, s.predict_lf); ++ctx->launches;
     }
   }
   Mark(ctx, kTDequant);
   {
+    // AC dequantisation (main stream, concurrent with DC and LF).
     dim3 gr(Blocks(g.Bx, kDequantCells), g.By);
     if (ctx->use_dq_ovr) {
       cudaMemcpyAsync(f.ac, ctx->dq_ovr.p,
@@ -481,17 +535,13 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
                       sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
                       cudaMemcpyDeviceToDevice, st);
     }
+    br.Join(0, 1);
     dim3 b2(32, 8), gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
     k_lf_update<<<gr2, b2, 0, st>>>(g, f, s.predict_lf, s.predict_hf); ++ctx->launches;
   }
   Mark(ctx, kTIdct);
+  br.Fork(1, ctx->kSide);
   {
-    const uint32_t* L[kNumClasses];
-    int n[kNumClasses];
-    for (int k = 0; k < kNumClasses; ++k) {
-      L[k] = P<uint32_t>(ctx->list[k]);
-      n[k] = int(ctx->lists[k].size());
-    }
     auto rows_grid = [](int items, int n) {
       const int upw = 32 / n;
       const int warps = (items + upw - 1) / upw;
@@ -499,41 +549,44 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     };
     if (n[kC8]) {
       k_square_idct_rows<8><<<rows_grid(3 * n[kC8], 8), kSquareThreads, 0,
-                              st>>>(g, f, L[kC8], n[kC8], s.predict_hf);
+                              cls(kC8)>>>(g, f, L[kC8], n[kC8], s.predict_hf);
       ++ctx->launches;
     }
     if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
       const int items = (n[kC16] + 7) / 8;
       const int grid = std::min(items, ctx->num_sms * ctx->tc_ctas_per_sm);
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
-        k_square_idct_tc<16, 2><<<grid, tc::kThreads, 0, st>>>(
+        k_square_idct_tc<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
       } else {
-        k_square_idct_tc<16, 3><<<grid, tc::kThreads, 0, st>>>(
+        k_square_idct_tc<16, 3><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
       }
       ++ctx->launches;
     } else if (n[kC16]) {
       k_square_idct_rows<16><<<rows_grid(3 * n[kC16], 16), kSquareThreads, 0,
-                               st>>>(g, f, L[kC16], n[kC16], s.predict_hf);
+                               cls(kC16)>>>(g, f, L[kC16], n[kC16],
+                                            s.predict_hf);
       ++ctx->launches;
     }
     if (n[kC32]) {
       k_square_idct_rows<32><<<rows_grid(3 * n[kC32], 32), kSquareThreads, 0,
-                               st>>>(g, f, L[kC32], n[kC32], s.predict_hf);
+                               cls(kC32)>>>(g, f, L[kC32], n[kC32],
+                                            s.predict_hf);
       ++ctx->launches;
     }
     if (n[kC4]) {
-      k_dct4_idct<<<Blocks(n[kC4], kDct4Blocks), 256, 0, st>>>(g, f, L[kC4], n[kC4],
-                                                      s.predict_hf);
+      k_dct4_idct<<<Blocks(n[kC4], kDct4Blocks), 256, 0, cls(kC4)>>>(
+          g, f, L[kC4], n[kC4], s.predict_hf);
       ++ctx->launches;
     }
     if (n[kCSmall]) {
-      k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, st>>>(
+      k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, cls(kCSmall)>>>(
           g, f, L[kCSmall], n[kCSmall]);
       ++ctx->launches;
     }
   }
+  br.Join(1, ctx->kSide);
   const float* final_in = f.idct;
   Mark(ctx, kTGab1);
   if (s.have_ar) {
@@ -561,26 +614,21 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, f.qf, f.acs, f.lut, 0,
                                                    mm, sig); ++ctx->launches;
     }
-    RunEpf(ctx, f.idct, f.idct, gab, g.PW, g.PH, sig, f.filt,
+    RunEpf(ctx, st, f.idct, f.idct, gab, g.PW, g.PH, sig, f.filt,
            ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr);
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_epf.p, f.filt, sizeof(float) * 3 * npx,
                       cudaMemcpyDeviceToDevice, st);
     }
     Mark(ctx, kTAr);
-    const uint32_t* L[kNumClasses];
-    int n[kNumClasses];
-    for (int k = 0; k < kNumClasses; ++k) {
-      L[k] = P<uint32_t>(ctx->list[k]);
-      n[k] = int(ctx->lists[k].size());
-    }
     // Only blocks the EPF filtered need the clamp (see k_active_blocks).
     if (f.clamp_tape) cudaMemsetAsync(f.clamp_tape, 0, nac, st);
     int* counters = P<int>(ctx->counters);
     cudaMemsetAsync(counters, 0, sizeof(int) * kNumClasses, st);
+    br.Fork(2, ctx->kSide);
     for (int k = 0; k < kNumClasses; ++k) {
       if (!n[k]) continue;
-      k_active_blocks<<<Blocks(n[k], 256), 256, 0, st>>>(
+      k_active_blocks<<<Blocks(n[k], 256), 256, 0, cls(k)>>>(
           g, sig, f.acs, L[k], n[k], P<uint32_t>(ctx->active[k]),
           counters + k);
       ++ctx->launches;
@@ -591,46 +639,50 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       return (warps * 32 + kSquareThreads - 1) / kSquareThreads;
     };
     if (n[kC8]) {
-      k_square_ar_rows<8><<<rows_grid(n[kC8], 8), kSquareThreads, 0, st>>>(
-          g, f, s, P<uint32_t>(ctx->active[kC8]), counters + kC8);
+      k_square_ar_rows<8><<<rows_grid(n[kC8], 8), kSquareThreads, 0,
+                            cls(kC8)>>>(g, f, s, P<uint32_t>(ctx->active[kC8]),
+                                        counters + kC8);
       ++ctx->launches;
     }
     if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
       const int grid =
           std::min((n[kC16] + 7) / 8, ctx->num_sms * ctx->tc_ctas_per_sm);
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
-        k_square_ar_tc<16, 2><<<grid, tc::kThreads, 0, st>>>(
+        k_square_ar_tc<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
             P<int>(ctx->tc_err));
       } else {
-        k_square_ar_tc<16, 3><<<grid, tc::kThreads, 0, st>>>(
+        k_square_ar_tc<16, 3><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
             P<int>(ctx->tc_err));
       }
       ++ctx->launches;
     } else if (n[kC16]) {
       k_square_ar_rows<16><<<rows_grid(n[kC16], 16), kSquareThreads, 0,
-                             st>>>(g, f, s, P<uint32_t>(ctx->active[kC16]),
-                                   counters + kC16);
+                             cls(kC16)>>>(g, f, s,
+                                          P<uint32_t>(ctx->active[kC16]),
+                                          counters + kC16);
       ++ctx->launches;
     }
     if (n[kC32]) {
       k_square_ar_rows<32><<<rows_grid(n[kC32], 32), kSquareThreads, 0,
-                             st>>>(g, f, s, P<uint32_t>(ctx->active[kC32]),
-                                   counters + kC32);
+                             cls(kC32)>>>(g, f, s,
+                                          P<uint32_t>(ctx->active[kC32]),
+                                          counters + kC32);
       ++ctx->launches;
     }
     if (n[kC4]) {
-      k_dct4_ar<<<Blocks(n[kC4], kDct4Blocks), 256, 0, st>>>(
+      k_dct4_ar<<<Blocks(n[kC4], kDct4Blocks), 256, 0, cls(kC4)>>>(
           g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
       ++ctx->launches;
     }
     if (n[kCSmall]) {
       k_small_ar<<<Blocks(n[kCSmall], kSmallArBlocks), 3 * kSmallArBlocks, 0,
-                   st>>>(
+                   cls(kCSmall)>>>(
           g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
       ++ctx->launches;
     }
+    br.Join(2, ctx->kSide);
     final_in = f.filt;
   } else {
     Mark(ctx, kTEpf);
@@ -754,6 +806,18 @@ int pikgpu_ctx_create(int device, pikgpu_ctx** out) {
   }
   ctx->stream = ctx->own_stream;
   for (auto& e : ctx->ev) cudaEventCreate(&e);
+  for (auto& s : ctx->side) {
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      pikgpu_ctx_destroy(ctx);
+      return PIKGPU_ERR_CUDA;
+    }
+  }
+  for (auto& e : ctx->fork_ev) {
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  }
+  for (auto& row : ctx->join_ev) {
+    for (auto& e : row) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  }
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount,
                          device);
   if (Ensure(ctx, &ctx->tc_err, sizeof(int)) != PIKGPU_OK ||
@@ -799,6 +863,17 @@ int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
   if (ctx->tc_err_host) cudaFreeHost(ctx->tc_err_host);
   for (auto& e : ctx->ev) {
     if (e) cudaEventDestroy(e);
+  }
+  for (auto& e : ctx->fork_ev) {
+    if (e) cudaEventDestroy(e);
+  }
+  for (auto& row : ctx->join_ev) {
+    for (auto& e : row) {
+      if (e) cudaEventDestroy(e);
+    }
+  }
+  for (auto& s : ctx->side) {
+    if (s) cudaStreamDestroy(s);
   }
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
