@@ -1,9 +1,9 @@
 // Edge-preserving filter (AdaptiveFilter + WeightedSum,
 // pik/epf_target.cc:526-801, 1113-1278) on packed guide bytes.
 //
-// One CTA filters a 64 x 32 pixel tile with 8 warps. Lane l of warp w owns
-// the pixels (x0 + l + 32 i, y0 + 4 w + j), i = 0..1, j = 0..3: two columns
-// 32 apart (so the 32 lanes of a warp read 32 consecutive values of every
+// One CTA filters a 64 x 32 pixel tile with 16 warps. Lane l of warp w owns
+// the pixels (x0 + 32 (w mod 2) + l, y0 + 4 (w / 2) + j), j = 0..3: one
+// column (the 32 lanes of a warp read 32 consecutive values of every
 // shared-memory row), four rows inside one 8x8 block row.
 //
 // The u8 guide is staged in shared memory as one 32-bit word per byte
@@ -31,7 +31,11 @@
 namespace pikgpu {
 
 constexpr int kEpfW = 64, kEpfH = 32;   // output tile
-constexpr int kEpfThreads = 256;
+// Columns per lane: 1 (512 threads, each lane 4 pixels of one column, two
+// warps per 4-row band) keeps a thread at <= 64 registers, so two CTAs of
+// 16 warps share an SM; 2 (256 threads, 8 pixels per lane) needs ~123.
+constexpr int kEpfLaneCols = 1;
+constexpr int kEpfThreads = 256 * 2 / kEpfLaneCols;
 constexpr int kEpfGH = kEpfH + 8;       // guide rows: y0 - 4 .. y0 + 35
 constexpr int kEpfGBytes = 80;          // guide bytes x0 - 8 .. x0 + 71
 constexpr int kEpfGRow = kEpfGBytes;    // words per guide row (one per byte)
@@ -66,26 +70,30 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
       reinterpret_cast<float(*)[kEpfTH][kEpfTS]>(epf_smem + kEpfGuideWords);
   const int x0 = blockIdx.x * kEpfW, y0 = blockIdx.y * kEpfH;
   const int tid = threadIdx.x;
+  constexpr int LC = kEpfLaneCols;
   const int lane = tid & 31, wp = tid >> 5;
+  // 4-row band of the warp and its first column (tile-local).
+  const int band = wp / (2 / LC), col0 = 32 * (wp % (2 / LC));
   const size_t plane = size_t(w) * h;
   const int bw = w / 8;
-  const int py0 = y0 + 4 * wp;  // first row; w and h are multiples of 8
-  bool inside[2], filtered[2];
-  int sig[2];
+  const int py0 = y0 + 4 * band;  // first row; w and h are multiples of 8
+  bool inside[LC], filtered[LC], any_filtered = false;
+  int sig[LC];
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int px = x0 + lane + 32 * i;
+  for (int i = 0; i < LC; ++i) {
+    const int px = x0 + lane + col0 + 32 * i;
     inside[i] = px < w && py0 < h;
     sig[i] = inside[i] ? sigma[(py0 >> 3) * bw + (px >> 3)] : 0;
     filtered[i] = sig[i] >= kMinSigma;
+    any_filtered |= filtered[i];
   }
 
   // Tiles without filtered blocks are copies (CopyOriginalBlock).
-  if (!__syncthreads_or(filtered[0] || filtered[1])) {
+  if (!__syncthreads_or(any_filtered)) {
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < LC; ++i) {
       if (!inside[i]) continue;
-      const int px = x0 + lane + 32 * i;
+      const int px = x0 + lane + col0 + 32 * i;
       for (int c = 0; c < 3; ++c)
         for (int j = 0; j < 4; ++j) {
           const size_t o = c * plane + size_t(py0 + j) * w + px;
@@ -215,42 +223,43 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
   __syncthreads();
 
   // Warps (half a block row of 8 blocks) without filtered blocks copy.
-  if (!__any_sync(0xFFFFFFFFu, filtered[0] || filtered[1])) {
+  if (!__any_sync(0xFFFFFFFFu, any_filtered)) {
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < LC; ++i) {
       if (!inside[i]) continue;
-      const int px = x0 + lane + 32 * i;
+      const int px = x0 + lane + col0 + 32 * i;
       for (int c = 0; c < 3; ++c)
         for (int j = 0; j < 4; ++j)
           out[c * plane + size_t(py0 + j) * w + px] =
-              tile[c][4 * wp + j + 3 + kEpfTRow0][lane + 32 * i + 3 + kEpfTCol0];
+              tile[c][4 * band + j + 3 + kEpfTRow0]
+                  [lane + col0 + 32 * i + 3 + kEpfTCol0];
     }
     return;
   }
-  int m64[2];
+  int m64[LC];
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < LC; ++i) {
     m64[i] = c_t.mul_table[filtered[i] ? sig[i] : kMinSigma] * 64;
   }
 
   // Centre patch rows: guide rows py0 - 1 .. py0 + 4, bytes px - 1 .. px + 2.
-  const int gr0 = 4 * wp + 3;  // guide smem row of py0 - 1
-  uint32_t ref[3][6][2];
+  const int gr0 = 4 * band + 3;  // guide smem row of py0 - 1
+  uint32_t ref[3][6][LC];
   {
-    // Byte offset of px - 1 from x0 - 8 (i = 0; i = 1 is 32 further).
-    const uint32_t* g = sg + gr0 * kEpfGRow + lane + 7;
+    // Byte offset of px - 1 from x0 - 8 (column i is 32 further).
+    const uint32_t* g = sg + gr0 * kEpfGRow + lane + col0 + 7;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int r = 0; r < 6; ++r)
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < LC; ++i)
           ref[c][r][i] = g[c * kEpfGPlane + r * kEpfGRow + 32 * i];
   }
 
-  float ws[3][8], sw[8];
+  float ws[3][4 * LC], sw[4 * LC];
 #pragma unroll
-  for (int p = 0; p < 8; ++p) {
+  for (int p = 0; p < 4 * LC; ++p) {
     ws[0][p] = ws[1][p] = ws[2][p] = 0.f;
     sw[p] = 0.f;
   }
@@ -258,15 +267,15 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
   for (int cy = -3; cy <= 3; ++cy) {
 #pragma unroll 1
     for (int cx = -3; cx <= 4; ++cx) {
-      // Window byte offset (i = 0): the patch start moved by cx.
-      const uint32_t* g = sg + (gr0 + cy) * kEpfGRow + lane + 7 + cx;
-      int sad[8];  // [j * 2 + i]
+      // Window byte offset (column 0): the patch start moved by cx.
+      const uint32_t* g = sg + (gr0 + cy) * kEpfGRow + lane + col0 + 7 + cx;
+      int sad[4 * LC];  // [j * LC + i]
 #pragma unroll
-      for (int p = 0; p < 8; ++p) sad[p] = 0;
+      for (int p = 0; p < 4 * LC; ++p) sad[p] = 0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < LC; ++i) {
           int hs[6];
 #pragma unroll
           for (int r = 0; r < 6; ++r) {
@@ -274,19 +283,19 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
                 ref[c][r][i], g[c * kEpfGPlane + r * kEpfGRow + 32 * i]));
           }
           const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
-          sad[0 + i] = max(sad[0 + i], hs[0] + p12);
-          sad[2 + i] = max(sad[2 + i], p12 + hs[3]);
-          sad[4 + i] = max(sad[4 + i], hs[2] + p34);
-          sad[6 + i] = max(sad[6 + i], p34 + hs[5]);
+          sad[0 * LC + i] = max(sad[0 * LC + i], hs[0] + p12);
+          sad[1 * LC + i] = max(sad[1 * LC + i], p12 + hs[3]);
+          sad[2 * LC + i] = max(sad[2 * LC + i], hs[2] + p34);
+          sad[3 * LC + i] = max(sad[3 * LC + i], p34 + hs[5]);
         }
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const int ir = 4 * wp + j + 3 + cy + kEpfTRow0;
+        const int ir = 4 * band + j + 3 + cy + kEpfTRow0;
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const int p = j * 2 + i;
-          const int col = lane + 32 * i + 3 + cx + kEpfTCol0;
+        for (int i = 0; i < LC; ++i) {
+          const int p = j * LC + i;
+          const int col = lane + col0 + 32 * i + 3 + cx + kEpfTCol0;
           float wgt = EpfWeight(m64[i], sad[p]);
           if (!(wgt >= 0.05f)) wgt = 0.0f;
           ws[0][p] += tile[0][ir][col] * wgt;
@@ -298,17 +307,18 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
     }
   }
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < LC; ++i) {
     if (!inside[i]) continue;
-    const int px = x0 + lane + 32 * i;
+    const int px = x0 + lane + col0 + 32 * i;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const int p = j * 2 + i;
+        const int p = j * LC + i;
         out[c * plane + size_t(py0 + j) * w + px] =
             filtered[i] ? ws[c][p] / sw[p]
-                        : tile[c][4 * wp + j + 3 + kEpfTRow0][lane + 32 * i + 3 + kEpfTCol0];
+                        : tile[c][4 * band + j + 3 + kEpfTRow0]
+                              [lane + col0 + 32 * i + 3 + kEpfTCol0];
       }
   }
 }
