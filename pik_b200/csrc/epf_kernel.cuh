@@ -114,10 +114,10 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
     for (int i = tid; i < 3 * kEpfTH * Q; i += kEpfThreads) {
       const int c = i / (kEpfTH * Q);
       const int r = (i / Q) % kEpfTH, q = i % Q;
-      *reinterpret_cast<float4*>(&tile[c][r][4 * q]) =
-          *reinterpret_cast<const float4*>(
-              in + c * plane + size_t(y0 - 5 + r) * w + x0 - 12 + 4 * q);
+      CpAsync16(&tile[c][r][4 * q],
+                in + c * plane + size_t(y0 - 5 + r) * w + x0 - 12 + 4 * q);
     }
+    CpAsyncWaitAll();
   } else {
     for (int i = tid; i < 3 * kEpfTH * kEpfTW; i += kEpfThreads) {
       const int c = i / (kEpfTH * kEpfTW);

@@ -44,8 +44,24 @@ __device__ __forceinline__ float Sym3Rows(const float* t, const float* m,
   return x2 * w2 + mul1;
 }
 
+// Asynchronous 16-byte global -> shared copies: interior tiles are staged
+// without passing through registers, every copy of a tile (all planes) in
+// flight at once, and one wait before the CTA's barrier. The hardware
+// tracks completion per thread, so the wait is no spin loop.
+__device__ __forceinline__ void CpAsync16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   uint32_t(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void CpAsyncWaitAll() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" :::
+                   "memory");
+}
+
 // Stages plane `p` (w x h, row stride w) around (x0, y0) into `t`
-// (TH + 2 rows).
+// (TH + 2 rows). Interior tiles are copied asynchronously: the caller
+// calls CpAsyncWaitAll before its barrier.
 template <int TH>
 __device__ __forceinline__ void StageTile(const float* p, int w, int h,
                                           int x0, int y0,
@@ -55,12 +71,9 @@ __device__ __forceinline__ void StageTile(const float* p, int w, int h,
       x0 >= 4 && x0 + kTileW + 4 <= w && y0 >= 1 && y0 + TH + 1 <= h;
   if (interior) {
     constexpr int Q = kTileSW / 4;
-#pragma unroll 4
     for (int i = threadIdx.x; i < kTileSH * Q; i += kTileThreads) {
       const int r = i / Q, q = i % Q;
-      *reinterpret_cast<float4*>(&t[r][4 * q]) =
-          *reinterpret_cast<const float4*>(p + size_t(y0 - 1 + r) * w + x0 -
-                                           4 + 4 * q);
+      CpAsync16(&t[r][4 * q], p + size_t(y0 - 1 + r) * w + x0 - 4 + 4 * q);
     }
   } else {
     for (int i = threadIdx.x; i < kTileSH * kTileSW; i += kTileThreads) {
@@ -95,6 +108,7 @@ __global__ void __launch_bounds__(kTileThreads)
   const size_t plane = size_t(w) * h;
   const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * TH;
   StageTile<TH>(in + c * plane, w, h, x0, y0, t);
+  CpAsyncWaitAll();
   __syncthreads();
   const float* wt = c_t.gaborish[strength];
   const float w0 = wt[0], w1 = wt[1], w2 = wt[2];
@@ -185,6 +199,7 @@ __global__ void __launch_bounds__(kTileThreads)
   for (int c = 0; c < 3; ++c) {
     StageTile<TH>(in + c * plane, pw, ph, x0, y0, t[c]);
   }
+  CpAsyncWaitAll();
   __syncthreads();
   const float* wt = c_t.gaborish[strength];
   const float w0 = wt[0], w1 = wt[1], w2 = wt[2];
