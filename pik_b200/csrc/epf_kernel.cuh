@@ -60,6 +60,10 @@ __device__ __forceinline__ float EpfWeight(int mul64, int sad) {
   return __uint_as_float((uint32_t(t) & 0xFFFF0000u) + 0x3F800000u);
 }
 
+// kFma: the weighted sums with fused multiply-adds (the tensor-core forms,
+// which are not bound to the reference's rounding); otherwise every product
+// and sum is rounded separately, as the reference does.
+template <bool kFma>
 __global__ void __launch_bounds__(kEpfThreads, 2)
     k_epf_box(const float* in, const float* guide_src,
               const uint8_t* guide_ovr, int gab, int w, int h,
@@ -298,9 +302,15 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
           const int col = lane + col0 + 32 * i + 3 + cx + kEpfTCol0;
           float wgt = EpfWeight(m64[i], sad[p]);
           if (!(wgt >= 0.05f)) wgt = 0.0f;
-          ws[0][p] += tile[0][ir][col] * wgt;
-          ws[1][p] += tile[1][ir][col] * wgt;
-          ws[2][p] += tile[2][ir][col] * wgt;
+          if (kFma) {
+            ws[0][p] = fmaf(tile[0][ir][col], wgt, ws[0][p]);
+            ws[1][p] = fmaf(tile[1][ir][col], wgt, ws[1][p]);
+            ws[2][p] = fmaf(tile[2][ir][col], wgt, ws[2][p]);
+          } else {
+            ws[0][p] += tile[0][ir][col] * wgt;
+            ws[1][p] += tile[1][ir][col] * wgt;
+            ws[2][p] += tile[2][ir][col] * wgt;
+          }
           sw[p] += wgt;
         }
       }

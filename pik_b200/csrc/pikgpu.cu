@@ -348,7 +348,12 @@ int UploadTables(pikgpu_ctx* ctx) {
   BuildTables(&t);
   CUDA_TRY(ctx, cudaMemcpyToSymbol(c_t, &t, sizeof(t)));
   CUDA_TRY(ctx, cudaFuncSetAttribute(
-                    k_epf_box, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    k_epf_box<false>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(kEpfSmemBytes)));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_epf_box<true>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(kEpfSmemBytes)));
   CUDA_TRY(ctx, cudaFuncSetAttribute(
                     k_final_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -388,8 +393,13 @@ int RunEpf(pikgpu_ctx* ctx, cudaStream_t st, const float* in,
            const float* guide_src, int gab, int w, int h, const int32_t* sig,
            float* out, const uint8_t* guide_ovr) {
   dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
-  k_epf_box<<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
-      in, guide_src, guide_ovr, gab, w, h, P<uint32_t>(ctx->mm), sig, out);
+  if (ctx->form == PIKGPU_FORM_FP32) {
+    k_epf_box<false><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
+        in, guide_src, guide_ovr, gab, w, h, P<uint32_t>(ctx->mm), sig, out);
+  } else {
+    k_epf_box<true><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
+        in, guide_src, guide_ovr, gab, w, h, P<uint32_t>(ctx->mm), sig, out);
+  }
   ++ctx->launches;
   return PIKGPU_OK;
 }
