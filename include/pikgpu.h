@@ -158,6 +158,23 @@ int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
                        size_t linear_stride, uint8_t* out_srgb8,
                        size_t srgb8_stride, int outputs_on_device);
 
+/* Non-blocking form of pikgpu_reconstruct, for streaming decoders: enqueues
+ * the reconstruction and the copies into the outputs on the context's
+ * stream and returns. The outputs are complete, and errors of the GPU work
+ * are reported, when pikgpu_wait returns. Host inputs given to
+ * pikgpu_frame_set_ac and host outputs should be page-locked (pinned) for
+ * the copies to run asynchronously, and must stay valid and unchanged until
+ * pikgpu_wait. Until then every other call on the context fails with
+ * PIKGPU_ERR_STATE: to overlap one frame's copies with another frame's
+ * computation, alternate two or more contexts (each has its own stream).
+ * No counterpart in the reference, which reconstructs synchronously. */
+int pikgpu_reconstruct_async(pikgpu_ctx* ctx, float* const out_linear[3],
+                             size_t linear_stride, uint8_t* out_srgb8,
+                             size_t srgb8_stride, int outputs_on_device);
+/* Waits for the context's pikgpu_reconstruct_async (returns at once if
+ * there is none) and returns its status. */
+int pikgpu_wait(pikgpu_ctx* ctx);
+
 /* Intermediate planes for stage-by-stage parity checks, valid after
  * pikgpu_reconstruct. Each is 3 planes in host memory. */
 #define PIKGPU_STAGE_DC 0          /* Bx x By: DC after AdaptiveDCRecon. */

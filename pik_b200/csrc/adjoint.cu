@@ -853,6 +853,7 @@ extern "C" {
 int pikgpu_frame_set_dequantized_ac(pikgpu_ctx* ctx, const float* ac,
                                     int on_device) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
   ++ctx->generation;
   ctx->use_dq_ovr = ac != nullptr;
@@ -873,6 +874,7 @@ int pikgpu_frame_set_dequantized_ac(pikgpu_ctx* ctx, const float* ac,
 int pikgpu_frame_set_clamp_scale(pikgpu_ctx* ctx, const float* scale,
                                  int on_device) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
   ++ctx->generation;
   ctx->use_clamp_scale = scale != nullptr;
@@ -891,6 +893,7 @@ int pikgpu_frame_set_clamp_scale(pikgpu_ctx* ctx, const float* scale,
 
 int pikgpu_set_clamp_decisions(pikgpu_ctx* ctx, const uint8_t* tape) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
   ++ctx->generation;
   ctx->use_tape_in = false;
@@ -912,6 +915,7 @@ int pikgpu_set_clamp_decisions(pikgpu_ctx* ctx, const uint8_t* tape) {
 
 int pikgpu_get_clamp_decisions(pikgpu_ctx* ctx, uint8_t* tape) {
   if (!ctx || !tape) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_result || !ctx->tape_valid) {
     return Fail(ctx, PIKGPU_ERR_STATE,
                 "no clamp tape: needs a frame with the EPF and a forward pass "
@@ -928,6 +932,7 @@ int pikgpu_get_clamp_decisions(pikgpu_ctx* ctx, uint8_t* tape) {
 int pikgpu_adjoint(pikgpu_ctx* ctx, const float* target, double* loss,
                    float* grad_ac, float* grad_qf, int buffers_on_device) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame || !(ctx->have_ac || ctx->use_dq_ovr)) {
     return Fail(ctx, PIKGPU_ERR_STATE, "frame or AC not supplied");
   }

@@ -145,6 +145,9 @@ struct pikgpu_ctx {
   bool graph_tape_valid = false, last_replayed = false;
   // Pinned host word the tensor-core error flag is read back into.
   int* tc_err_host = nullptr;
+  // pikgpu_reconstruct_async enqueued work that pikgpu_wait has not yet
+  // finished (with the tensor-core flag to check).
+  bool pending = false, pending_tc = false;
 };
 
 namespace {
@@ -158,6 +161,16 @@ int Fail(pikgpu_ctx* ctx, int code, const char* fmt, ...) {
   if (ctx) ctx->err = buf;
   return code;
 }
+
+// Every call but pikgpu_wait refuses a context whose asynchronous
+// reconstruction has not been waited for.
+#define PIKGPU_NOT_PENDING(ctx)                                             \
+  do {                                                                      \
+    if ((ctx)->pending) {                                                   \
+      return Fail(ctx, PIKGPU_ERR_STATE,                                    \
+                  "reconstruction in flight: call pikgpu_wait first");      \
+    }                                                                       \
+  } while (0)
 
 #define CUDA_TRY(ctx, call)                                                 \
   do {                                                                      \
@@ -896,12 +909,14 @@ const char* pikgpu_last_error(const pikgpu_ctx* ctx) {
 
 int pikgpu_set_stream(pikgpu_ctx* ctx, void* stream) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
   return PIKGPU_OK;
 }
 
 int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   ++ctx->generation;
   switch (option) {
     case PIKGPU_OPT_KEEP_STAGES:
@@ -926,6 +941,7 @@ int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
 
 int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   // The launch state before this frame: a frame that leaves it unchanged
   // (and reallocates nothing, which Ensure would record) keeps the
   // generation, so a captured graph stays valid for it.
@@ -1074,6 +1090,7 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
 int pikgpu_frame_set_ac(pikgpu_ctx* ctx, const int16_t* const planes[3],
                         size_t stride) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
   if (!planes || stride < size_t(ctx->g.ac_stride)) {
     return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "bad AC planes/stride");
@@ -1093,6 +1110,7 @@ int pikgpu_frame_set_ac(pikgpu_ctx* ctx, const int16_t* const planes[3],
 int pikgpu_frame_set_group_ac(pikgpu_ctx* ctx, uint32_t group_index,
                               const int16_t* const planes[3], size_t stride) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
   const Geo& g = ctx->g;
   if (group_index >= uint32_t(g.Gx * g.Gy)) {
@@ -1119,6 +1137,7 @@ int pikgpu_frame_set_group_ac(pikgpu_ctx* ctx, uint32_t group_index,
 int pikgpu_frame_set_ac_device(pikgpu_ctx* ctx, const int16_t* const planes[3],
                                size_t stride) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
   if (!planes || stride < size_t(ctx->g.ac_stride)) {
     return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "bad AC planes/stride");
@@ -1135,10 +1154,16 @@ int pikgpu_frame_set_ac_device(pikgpu_ctx* ctx, const int16_t* const planes[3],
   return PIKGPU_OK;
 }
 
-int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
+}  // extern "C"
+
+namespace {
+
+// Enqueues one reconstruction and its output copies on the context's
+// stream (pikgpu_reconstruct without the final synchronisation).
+int EnqueueReconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
                        size_t linear_stride, uint8_t* out_srgb8,
                        size_t srgb8_stride, int outputs_on_device) {
-  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  ctx->have_result = false;
   if (!ctx->have_frame || !(ctx->have_ac || ctx->use_dq_ovr)) {
     return Fail(ctx, PIKGPU_ERR_STATE, "frame or AC not supplied");
   }
@@ -1217,6 +1242,15 @@ int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
                                   sizeof(int), cudaMemcpyDeviceToHost,
                                   ctx->stream));
   }
+  ctx->pending = true;
+  ctx->pending_tc = tc;
+  return PIKGPU_OK;
+}
+
+// Waits for the enqueued reconstruction and checks it.
+int FinishReconstruct(pikgpu_ctx* ctx) {
+  ctx->pending = false;
+  const bool tc = ctx->pending_tc;
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (tc && *ctx->tc_err_host) {
     *ctx->tc_err_host = 0;
@@ -1233,9 +1267,42 @@ int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
   return PIKGPU_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int pikgpu_reconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
+                       size_t linear_stride, uint8_t* out_srgb8,
+                       size_t srgb8_stride, int outputs_on_device) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
+  const int rc = EnqueueReconstruct(ctx, out_linear, linear_stride,
+                                    out_srgb8, srgb8_stride,
+                                    outputs_on_device);
+  if (rc != PIKGPU_OK) return rc;
+  return FinishReconstruct(ctx);
+}
+
+int pikgpu_reconstruct_async(pikgpu_ctx* ctx, float* const out_linear[3],
+                             size_t linear_stride, uint8_t* out_srgb8,
+                             size_t srgb8_stride, int outputs_on_device) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
+  return EnqueueReconstruct(ctx, out_linear, linear_stride, out_srgb8,
+                            srgb8_stride, outputs_on_device);
+}
+
+int pikgpu_wait(pikgpu_ctx* ctx) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  if (!ctx->pending) return PIKGPU_OK;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  return FinishReconstruct(ctx);
+}
+
 int pikgpu_get_stage(pikgpu_ctx* ctx, int stage, float* const planes[3],
                      size_t stride, size_t xsize, size_t ysize) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_result) return Fail(ctx, PIKGPU_ERR_STATE, "no result");
   const Geo& g = ctx->g;
   const float* src = nullptr;
@@ -1294,6 +1361,7 @@ int pikgpu_get_stage(pikgpu_ctx* ctx, int stage, float* const planes[3],
 int pikgpu_set_epf_decisions(pikgpu_ctx* ctx, const uint8_t* guide,
                              const int32_t* sigma) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
   ++ctx->generation;
   const Geo& g = ctx->g;
@@ -1326,6 +1394,7 @@ int pikgpu_set_epf_decisions(pikgpu_ctx* ctx, const uint8_t* guide,
 int pikgpu_get_epf_decisions(pikgpu_ctx* ctx, uint8_t* guide,
                              int32_t* sigma) {
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_result || !ctx->s.have_ar) {
     return Fail(ctx, PIKGPU_ERR_STATE, "no EPF result");
   }

@@ -72,6 +72,9 @@ def lib() -> ctypes.CDLL:
         P, ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_char_p, S]
     L.pikgpu_adjoint.argtypes = [P, P, P, P, P, ctypes.c_int]
     L.pikgpu_graph_stats.argtypes = [P, P, P]
+    L.pikgpu_reconstruct_async.argtypes = [P, ctypes.POINTER(P), S, P, S,
+                                           ctypes.c_int]
+    L.pikgpu_wait.argtypes = [P]
     L.pikgpu_frame_set_dequantized_ac.argtypes = [P, P, ctypes.c_int]
     L.pikgpu_frame_set_clamp_scale.argtypes = [P, P, ctypes.c_int]
     L.pikgpu_set_clamp_decisions.argtypes = [P, P]
@@ -208,6 +211,21 @@ class Context:
                                            lin_ptr + 2 * plane)
         self._check(self.L.pikgpu_reconstruct(self.h, planes, lin_stride,
                                               rgb_ptr or None, rgb_stride, 1))
+
+    def reconstruct_async(self, lin_planes, lin_stride: int,
+                          rgb_ptr: int = 0, rgb_stride: int = 0,
+                          on_device: bool = False) -> None:
+        """pikgpu_reconstruct_async: `lin_planes` are 3 pointers (host
+        pinned memory, or device); complete after wait()."""
+        planes = None
+        if lin_planes is not None:
+            planes = (ctypes.c_void_p * 3)(*lin_planes)
+        self._check(self.L.pikgpu_reconstruct_async(
+            self.h, planes, lin_stride, rgb_ptr or None, rgb_stride,
+            int(on_device)))
+
+    def wait(self) -> None:
+        self._check(self.L.pikgpu_wait(self.h))
 
     def stage(self, name: str) -> np.ndarray:
         f = self.frame
