@@ -15,7 +15,7 @@ groups + FinalizeFrameDecoding.
          "forms" gives every form's throughput on the same frame
   e2e    the same through the C ABI with host buffers: each step uploads the
          frame's side information and int16 coefficients from pinned host
-         memory and reads the FP32 linear planes back; two contexts take
+         memory and reads the FP32 linear planes back; three contexts take
          the frames in turn with the non-blocking call, so one frame's
          copies overlap the other's kernels (the blocking one-context figure
          is "e2e_blocking").
@@ -294,6 +294,11 @@ def batch_main(args):
     b.close()
 
 
+# Contexts that take the frames of the streaming end-to-end run in turn:
+# with three, the read-back of one frame (the bound: 100 MB at ~57 GB/s)
+# overlaps the upload and kernels of the next two.
+STREAM_CONTEXTS = 3
+
 ADJ_SHARES = {"DCT": 0.3, "DCT16X16": 0.3, "DCT32X32": 0.2, "DCT4X4": 0.05,
               "DCT2X2": 0.05, "IDENTITY": 0.04, "LINES": 0.03,
               "DCT_NOHF": 0.02, "DCT4X4_NOHF": 0.01}
@@ -564,21 +569,23 @@ def main():
     e2e_blocking = ws * px / (e2e_ms * 1e-3) / 1e6
     ctx.close()
 
-    # Streaming end to end: two contexts in turn with the non-blocking call,
+    # Streaming end to end: three contexts in turn with the non-blocking call,
     # so one frame's uploads, kernels and read-back overlap the other's.
     # Every step still uploads its side information and int16 AC from
     # pinned host memory and reads its linear planes back into pinned host
     # memory; the region ends when the last frame is read back.
-    ctxs = [native.Context(local, form=args.form) for _ in range(2)]
-    pin_lins = [pin["lin"], torch.empty_like(pin["lin"]).pin_memory()]
+    ctxs = [native.Context(local, form=args.form)
+            for _ in range(STREAM_CONTEXTS)]
+    pin_lins = [pin["lin"]] + [torch.empty_like(pin["lin"]).pin_memory()
+                               for _ in range(STREAM_CONTEXTS - 1)]
     lin_ptrs = [[p[c].data_ptr() for c in range(3)] for p in pin_lins]
 
     def stream_step(i):
-        c = ctxs[i % 2]
+        c = ctxs[i % STREAM_CONTEXTS]
         c.wait()
         c._check(c.L.pikgpu_frame_begin(c.h, packed.ref))
         c._check(c.L.pikgpu_frame_set_ac(c.h, ac_planes, bx * 64))
-        c.reconstruct_async(lin_ptrs[i % 2], frame.xsize)
+        c.reconstruct_async(lin_ptrs[i % STREAM_CONTEXTS], frame.xsize)
 
     for i in range(max(3, args.warmup)):
         stream_step(i)
@@ -659,9 +666,9 @@ def main():
             "e2e": {"value": round(e2e, 2), "unit": "MP/s",
                     "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
-                    "mode": "two contexts in turn, pikgpu_reconstruct_async "
-                            "+ pikgpu_wait (copies of one frame overlap the "
-                            "other's kernels)"},
+                    "mode": f"{STREAM_CONTEXTS} contexts in turn, "
+                            "pikgpu_reconstruct_async + pikgpu_wait (copies "
+                            "of one frame overlap another's kernels)"},
             "e2e_blocking": {"value": round(e2e_blocking, 2), "unit": "MP/s",
                              "mode": "one context, blocking "
                                      "pikgpu_reconstruct per frame"},
