@@ -526,22 +526,11 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
                                   ctx->dc_half_step[2]); ++ctx->launches;
   }
   Mark(ctx, kTLf);
-  // Per-group LF prediction (side stream 0, after DC).
+  // Per-group LF prediction (side stream 0, after DC): one CTA per group
+  // and channel.
   const int ng = g.Gx * g.Gy;
-  {
-    dim3 b(16, 16), gr(Blocks(kGB, 16), Blocks(kGB, 16), 3 * ng);
-    k_llf<<<gr, b, 0, sd>>>(g, f); ++ctx->launches;
-    if (s.predict_lf) {
-      k_tmp2x2<<<gr, b, 0, sd>>>(g, f); ++ctx->launches;
-      dim3 gr2(Blocks(kG2, 16), Blocks(kG2, 16), 3 * ng);
-      k_lf_blur<<<gr2, b, 0, sd>>>(g, f); ++ctx->launches;
-      k_lf_from_2x2<<<gr, b, 0, sd>>>(g, f); ++ctx->launches;
-    }
-    if (s.predict_hf) {
-      k_pred_border<<<dim3(Blocks(4 * (kGB + 2), 128), 1, 3 * ng), 128, 0,
-                      sd>>>(g, f, s.predict_lf); ++ctx->launches;
-    }
-  }
+  k_lf_chain<<<3 * ng, kLfThreads, 0, sd>>>(g, f, s.predict_lf,
+                                           s.predict_hf); ++ctx->launches;
   Mark(ctx, kTDequant);
   {
     // AC dequantisation (main stream, concurrent with DC and LF).

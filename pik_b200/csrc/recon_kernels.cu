@@ -585,57 +585,51 @@ __global__ void __launch_bounds__(256) k_dequant_ac(Geo g, DevFrame f,
 
 // ---------------------------------------------------------------------------
 // Per-group LF prediction (ComputeLlf, PredictLf, pik/ac_predictions.cc:
-// 380-470), one thread per bordered cell. Group-local cell (bx, by) in
-// [0, gxs+2) x [0, gys+2); border ring acts as DCT8; DC from the frame with
-// mirroring (InitializeDecCache, pik/compressed_dc.cc:530-556).
-__global__ void k_llf(Geo g, DevFrame f) {
-  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
-  int x0, y0, gxs, gys;
-  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
-  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int by = blockIdx.y * blockDim.y + threadIdx.y;
-  if (bx >= gxs + 2 || by >= gys + 2) return;
-  const bool border = bx == 0 || by == 0 || bx == gxs + 1 || by == gys + 1;
-  const int a = border ? 0 : f.acs[(y0 + by - 1) * g.Bx + x0 + bx - 1];
+// 380-470). Group-local cell (bx, by) in [0, gxs+2) x [0, gys+2); the border
+// ring acts as DCT8; DC from the frame with mirroring (InitializeDecCache,
+// pik/compressed_dc.cc:530-556). One CTA runs all phases of one group and
+// channel (k_lf_chain), with a barrier between phases: the phases are small
+// and were launch- and latency-bound as separate kernels.
+struct LfGroup {
+  int gi, c, x0, y0, gxs, gys;
+  __device__ int Acs(const Geo& g, const DevFrame& f, int bx, int by) const {
+    const bool border = bx == 0 || by == 0 || bx == gxs + 1 || by == gys + 1;
+    return border ? 0 : f.acs[(y0 + by - 1) * g.Bx + x0 + bx - 1];
+  }
+};
+
+__device__ void LlfCell(const Geo& g, const DevFrame& f, const LfGroup& q,
+                        int bx, int by) {
+  const int a = q.Acs(g, f, bx, by);
   if (a & 0xF) return;
   const int type = a >> 4, cov = Covered(type);
   float dc[16];
   for (int iy = 0; iy < cov; ++iy)
     for (int ix = 0; ix < cov; ++ix)
       dc[iy * 4 + ix] =
-          f.dc[(size_t(c) * g.By + MirrorIdx(y0 + by - 1 + iy, g.By)) * g.Bx +
-               MirrorIdx(x0 + bx - 1 + ix, g.Bx)];
-  float* llf = f.llf_g + gi * kLlfGroupFloats + c * kGB * kGB;
+          f.dc[(size_t(q.c) * g.By + MirrorIdx(q.y0 + by - 1 + iy, g.By)) *
+                   g.Bx +
+               MirrorIdx(q.x0 + bx - 1 + ix, g.Bx)];
+  float* llf = f.llf_g + q.gi * kLlfGroupFloats + q.c * kGB * kGB;
   LowestFreqFromDC(type, dc, 4, llf + by * kGB + bx, kGB);
 }
 
-__global__ void k_tmp2x2(Geo g, DevFrame f) {
-  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
-  int x0, y0, gxs, gys;
-  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
-  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int by = blockIdx.y * blockDim.y + threadIdx.y;
-  if (bx >= gxs + 2 || by >= gys + 2) return;
-  const bool border = bx == 0 || by == 0 || bx == gxs + 1 || by == gys + 1;
-  const int a = border ? 0 : f.acs[(y0 + by - 1) * g.Bx + x0 + bx - 1];
+__device__ void Tmp2x2Cell(const Geo& g, const DevFrame& f, const LfGroup& q,
+                           int bx, int by) {
+  const int a = q.Acs(g, f, bx, by);
   if (a & 0xF) return;
-  const float* llf = f.llf_g + gi * kLlfGroupFloats + c * kGB * kGB;
-  float* tmp = f.tmp2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  const float* llf = f.llf_g + q.gi * kLlfGroupFloats + q.c * kGB * kGB;
+  float* tmp = f.tmp2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   DC2x2FromLowestFreq(a >> 4, llf + by * kGB + bx, kGB,
                       tmp + 2 * by * kG2 + 2 * bx, kG2);
 }
 
 // LFPredictionBlur over the group's 2x2 image (ConvolveT<Symmetric3>).
-__global__ void k_lf_blur(Geo g, DevFrame f) {
-  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
-  int x0, y0, gxs, gys;
-  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
-  const int w2 = 2 * (gxs + 2), h2 = 2 * (gys + 2);
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= w2 || y >= h2) return;
-  const float* tmp = f.tmp2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
-  float* lf = f.lf2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+__device__ void LfBlurPixel(const DevFrame& f, const LfGroup& q, int x,
+                            int y) {
+  const int w2 = 2 * (q.gxs + 2), h2 = 2 * (q.gys + 2);
+  const float* tmp = f.tmp2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
+  float* lf = f.lf2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   const float* t = tmp + MirrorIdx(y - 1, h2) * kG2;
   const float* m = tmp + y * kG2;
   const float* b = tmp + MirrorIdx(y + 1, h2) * kG2;
@@ -652,41 +646,30 @@ __global__ void k_lf_blur(Geo g, DevFrame f) {
   lf[y * kG2 + x] = x2 * w2_ + mul1;
 }
 
-__global__ void k_lf_from_2x2(Geo g, DevFrame f) {
-  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
-  int x0, y0, gxs, gys;
-  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
-  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int by = blockIdx.y * blockDim.y + threadIdx.y;
-  if (bx >= gxs + 2 || by >= gys + 2) return;
-  const bool border = bx == 0 || by == 0 || bx == gxs + 1 || by == gys + 1;
-  const int a = border ? 0 : f.acs[(y0 + by - 1) * g.Bx + x0 + bx - 1];
+__device__ void LfFrom2x2Cell(const Geo& g, const DevFrame& f,
+                              const LfGroup& q, int bx, int by) {
+  const int a = q.Acs(g, f, bx, by);
   if (a & 0xF) return;
-  float* lf = f.lf2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  float* lf = f.lf2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   LowFreqFromDC2x2(a >> 4, lf + 2 * by * kG2 + 2 * bx, kG2);
 }
 
-// Border ring of pred2x2 (pik/compressed_image.cc:978-1039).
-__global__ void k_pred_border(Geo g, DevFrame f, int predict_lf) {
-  const int gi = blockIdx.z / 3, c = blockIdx.z % 3;
-  int x0, y0, gxs, gys;
-  GroupDims(g, gi, &x0, &y0, &gxs, &gys);
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  // Ring cells: 2 columns of (gys + 2) then 2 rows of (gxs + 2).
+// Border ring of pred2x2 (pik/compressed_image.cc:978-1039); ring cell i:
+// 2 columns of (gys + 2), then 2 rows of (gxs + 2).
+__device__ void PredBorderCell(const DevFrame& f, const LfGroup& q, int i,
+                               int predict_lf) {
   int x, y;
-  if (i < 2 * (gys + 2)) {
-    x = (i & 1) ? gxs + 1 : 0;
+  if (i < 2 * (q.gys + 2)) {
+    x = (i & 1) ? q.gxs + 1 : 0;
     y = i >> 1;
-  } else if (i < 2 * (gys + 2) + 2 * (gxs + 2)) {
-    const int j = i - 2 * (gys + 2);
-    y = (j & 1) ? gys + 1 : 0;
-    x = j >> 1;
   } else {
-    return;
+    const int j = i - 2 * (q.gys + 2);
+    y = (j & 1) ? q.gys + 1 : 0;
+    x = j >> 1;
   }
-  const float* llf = f.llf_g + gi * kLlfGroupFloats + c * kGB * kGB;
-  const float* lf = f.lf2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
-  float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+  const float* llf = f.llf_g + q.gi * kLlfGroupFloats + q.c * kGB * kGB;
+  const float* lf = f.lf2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
+  float* pred = f.pred2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   if (predict_lf) {
     float blk[10];
     blk[0] = llf[y * kGB + x];
@@ -698,6 +681,45 @@ __global__ void k_pred_border(Geo g, DevFrame f, int predict_lf) {
   } else {
     DC2x2FromLowestFreq(kDCT, llf + y * kGB + x, kGB,
                         pred + 2 * y * kG2 + 2 * x, kG2);
+  }
+}
+
+constexpr int kLfThreads = 512;
+
+// All LF prediction phases of one group and channel (blockIdx.x = 3 gi + c):
+// LLF from DC; then, with LF prediction, the 2x2 image, its blur and the LF
+// coefficients from it; then, with HF prediction, the pred2x2 border ring.
+__global__ void __launch_bounds__(kLfThreads)
+    k_lf_chain(Geo g, DevFrame f, int predict_lf, int predict_hf) {
+  LfGroup q;
+  q.gi = blockIdx.x / 3;
+  q.c = blockIdx.x % 3;
+  GroupDims(g, q.gi, &q.x0, &q.y0, &q.gxs, &q.gys);
+  const int cw = q.gxs + 2, ncell = cw * (q.gys + 2);
+  for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
+    LlfCell(g, f, q, i % cw, i / cw);
+  }
+  __syncthreads();
+  if (predict_lf) {
+    for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
+      Tmp2x2Cell(g, f, q, i % cw, i / cw);
+    }
+    __syncthreads();
+    const int w2 = 2 * cw, n2 = w2 * 2 * (q.gys + 2);
+    for (int i = threadIdx.x; i < n2; i += kLfThreads) {
+      LfBlurPixel(f, q, i % w2, i / w2);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
+      LfFrom2x2Cell(g, f, q, i % cw, i / cw);
+    }
+    __syncthreads();
+  }
+  if (predict_hf) {
+    const int nring = 2 * (q.gys + 2) + 2 * (q.gxs + 2);
+    for (int i = threadIdx.x; i < nring; i += kLfThreads) {
+      PredBorderCell(f, q, i, predict_lf);
+    }
   }
 }
 
