@@ -440,101 +440,213 @@ __global__ void __launch_bounds__(kAdjThreads)
   }
 }
 
-// EPF with frozen weights, transposed. A CTA takes a 32 x 16 pixel tile;
-// every filtered pixel recomputes its 56 weights from the guide exactly as
-// the forward (patch SADs, maximum over the channels, WeightFast, the 0.05
-// cut, the sum in neighbour order) and scatters g / sum(w) * w to its
-// neighbours in a shared-memory accumulator with a 3 / 4 pixel halo; pixels
-// the EPF copied pass their gradient through. The accumulator is then added
-// to the IDCT-output gradient at the mirrored coordinates.
-constexpr int kAdjEpfW = 32, kAdjEpfH = 16;
-constexpr int kAdjEpfGW = kAdjEpfW + 12, kAdjEpfGH = kAdjEpfH + 8;
-constexpr int kAdjEpfAW = kAdjEpfW + 8, kAdjEpfAH = kAdjEpfH + 6;
+// EPF with frozen weights, transposed. The forward pass computes, for a
+// filtered pixel p, out(p) = sum_d w(p, d) in(p + d) / sum_d w(p, d) over
+// the 7 x 8 window d = (cx, cy), cx in [-3, 4], cy in [-3, 3], where
+// w(p, d) = W(mul(p), SAD(p, p + d)) and in() is mirrored at the frame
+// border. Its transpose sends g(p) w(p, d) / sum_w(p) to p + d. The patch
+// SAD is symmetric, SAD(p, p + d) = SAD(q, q - d) for q = p + d, so the
+// transpose is a gather at q over the mirrored window e = -d
+// (cx in [-4, 3]) with the weight of the sending pixel p = q + e:
+//   pass 1 (k_adj_epf_pass<false>): gv(p) = g(p) / sum_w(p) for filtered
+//          pixels, 0 for copied ones;
+//   pass 2 (k_adj_epf_pass<true>):  g_idct(q) += sum_e gv(q + e)
+//          W(mul(q + e), SAD(q, q + e)) (+ g(q) itself where q was copied),
+//          for q + e inside the frame;
+//   pass 3 (k_adj_epf_border): the terms whose target p + d lies outside
+//          the frame (p within 4 pixels of the border), scattered to the
+//          mirrored position.
+// Passes 1 and 2 follow the forward kernel's design (k_epf_box): 64 x 32
+// tiles, one column of four rows per lane, the u8 guide staged as one
+// 32-bit word per byte offset and patch SADs by __vsadu4, summed vertically
+// across the lane's rows.
+constexpr int kAdjEpfTH = kEpfH + 6;   // gather tile rows y0 - 3 .. y0 + 34
+constexpr int kAdjEpfTW = kEpfW + 8;   // gather tile cols x0 - 4 .. x0 + 67
+constexpr size_t kAdjEpfSmemBytes =
+    kEpfGuideWords * 4 + size_t(3) * kAdjEpfTH * kAdjEpfTW * 4;
 
-__global__ void __launch_bounds__(kAdjThreads)
-    k_adj_epf(int w, int h, const uint8_t* guide, const int32_t* sigma,
-              const float* g_filt, float* g_idct) {
-  __shared__ uint8_t s_gd[3][kAdjEpfGH][kAdjEpfGW];  // rows y0-4, cols x0-4
-  __shared__ float s_acc[3][kAdjEpfAH][kAdjEpfAW];   // rows y0-3, cols x0-3
-  const int x0 = blockIdx.x * kAdjEpfW, y0 = blockIdx.y * kAdjEpfH;
-  const int tid = threadIdx.x;
-  const int gw = w + 12, gh = h + 12, bw = w / 8;
+template <bool kGather>
+__global__ void __launch_bounds__(kEpfThreads, 2)
+    k_adj_epf_pass(int w, int h, const uint8_t* guide, const int32_t* sigma,
+                   const float* g_filt, const float* gv_in, float* out) {
+  extern __shared__ __align__(16) uint32_t adj_epf_smem[];
+  uint32_t* sg = adj_epf_smem;  // [3][kEpfGH][kEpfGRow]
+  float(*tile)[kAdjEpfTH][kAdjEpfTW] =
+      reinterpret_cast<float(*)[kAdjEpfTH][kAdjEpfTW]>(adj_epf_smem +
+                                                       kEpfGuideWords);
+  __shared__ int s_m64[6][10];  // mul * 64 of blocks y0/8-1.., x0/8-1..
+  const int x0 = blockIdx.x * kEpfW, y0 = blockIdx.y * kEpfH;
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const int band = wp >> 1, col0 = 32 * (wp & 1);
   const size_t plane = size_t(w) * h;
-  for (int i = tid; i < 3 * kAdjEpfGH * kAdjEpfGW; i += kAdjThreads) {
-    const int c = i / (kAdjEpfGH * kAdjEpfGW);
-    const int r = (i / kAdjEpfGW) % kAdjEpfGH, col = i % kAdjEpfGW;
-    const int gy = y0 - 4 + r, gx = x0 - 4 + col;
-    uint8_t v = 0;
-    if (gy >= -6 && gy < h + 6 && gx >= -6 && gx < w + 6) {
-      v = guide[(size_t(c) * gh + gy + 6) * gw + gx + 6];
+  const int bw = w / 8, bh = h / 8;
+  const int px = x0 + lane + col0, py0 = y0 + 4 * band;
+  const bool inside = px < w && py0 < h;
+  const int sig = inside ? sigma[(py0 >> 3) * bw + (px >> 3)] : 0;
+  const bool filtered = sig >= kMinSigma;
+  // The u8 guide (6-pixel mirrored border) as words: bytes x0 - 8 ..
+  // x0 + 71 of rows y0 - 4 .. y0 + 35; bytes outside the buffer read 0.
+  const int gwid = w + 12, ght = h + 12;
+  constexpr int kAligned = kEpfGBytes / 4;
+  for (int i = tid; i < 3 * kEpfGH * kAligned; i += kEpfThreads) {
+    const int c = i / (kEpfGH * kAligned);
+    const int r = (i / kAligned) % kEpfGH, wd = i % kAligned;
+    const int gy = y0 - 4 + r;
+    uint32_t word = 0;
+    for (int b = 0; b < 4; ++b) {
+      const int gx = x0 - 8 + 4 * wd + b;
+      const bool ok = gx >= -6 && gx < w + 6 && gy >= -6 && gy < h + 6;
+      const uint32_t v =
+          ok ? guide[(size_t(c) * ght + gy + 6) * gwid + gx + 6] : 0u;
+      word |= v << (8 * b);
     }
-    s_gd[c][r][col] = v;
+    sg[c * kEpfGPlane + r * kEpfGRow + 4 * wd] = word;
   }
-  for (int i = tid; i < 3 * kAdjEpfAH * kAdjEpfAW; i += kAdjThreads) {
-    (&s_acc[0][0][0])[i] = 0.0f;
+  if (kGather) {
+    // gv around the tile, 0 outside the frame (those terms are pass 3's).
+    for (int i = tid; i < 3 * kAdjEpfTH * kAdjEpfTW; i += kEpfThreads) {
+      const int c = i / (kAdjEpfTH * kAdjEpfTW);
+      const int r = (i / kAdjEpfTW) % kAdjEpfTH, col = i % kAdjEpfTW;
+      const int gx = x0 - 4 + col, gy = y0 - 3 + r;
+      tile[c][r][col] = (gx >= 0 && gx < w && gy >= 0 && gy < h)
+                            ? gv_in[c * plane + size_t(gy) * w + gx]
+                            : 0.0f;
+    }
+    for (int i = tid; i < 60; i += kEpfThreads) {
+      const int by = y0 / 8 - 1 + i / 10, bx = x0 / 8 - 1 + i % 10;
+      int m = 0;
+      if (by >= 0 && by < bh && bx >= 0 && bx < bw) {
+        const int sg_ = sigma[by * bw + bx];
+        m = sg_ >= kMinSigma ? c_t.mul_table[sg_] * 64 : 0;
+      }
+      s_m64[i / 10][i % 10] = m;
+    }
   }
   __syncthreads();
-  const int lx = tid & 31;
-  for (int jj = 0; jj < 2; ++jj) {
-    const int ly = (tid >> 5) + 8 * jj;
-    const int x = x0 + lx, y = y0 + ly;
-    if (x >= w || y >= h) continue;
-    const int sg = sigma[(y >> 3) * bw + (x >> 3)];
-    float gf[3];
-    for (int c = 0; c < 3; ++c) gf[c] = g_filt[c * plane + size_t(y) * w + x];
-    if (sg < kMinSigma) {
-      for (int c = 0; c < 3; ++c) atomicAdd(&s_acc[c][ly + 3][lx + 3], gf[c]);
-      continue;
+  for (int i = tid; i < 3 * kEpfGH * kAligned * 3; i += kEpfThreads) {
+    const int sft = 1 + i % 3;
+    const int j = i / 3;
+    const int c = j / (kEpfGH * kAligned);
+    const int r = (j / kAligned) % kEpfGH, wd = j % kAligned;
+    const uint32_t* row = sg + c * kEpfGPlane + r * kEpfGRow;
+    const uint32_t lo = row[4 * wd];
+    const uint32_t hi = wd + 1 < kAligned ? row[4 * wd + 4] : 0u;
+    sg[c * kEpfGPlane + r * kEpfGRow + 4 * wd + sft] =
+        __funnelshift_r(lo, hi, 8 * sft);
+  }
+  __syncthreads();
+  if (!inside) return;  // no barrier follows
+  if (!kGather && !filtered) {
+    for (int c = 0; c < 3; ++c)
+      for (int j = 0; j < 4; ++j)
+        out[c * plane + size_t(py0 + j) * w + px] = 0.0f;
+    return;
+  }
+  const int gr0 = 4 * band + 3;  // guide smem row of py0 - 1
+  uint32_t ref[3][6];
+  {
+    const uint32_t* g = sg + gr0 * kEpfGRow + lane + col0 + 7;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) ref[c][r] = g[c * kEpfGPlane + r * kEpfGRow];
+  }
+  const int m64c = filtered ? c_t.mul_table[sig] * 64 : 0;
+  float acc[3][4], sw[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    acc[0][j] = acc[1][j] = acc[2][j] = 0.f;
+    sw[j] = 0.f;
+  }
+  constexpr int kCx0 = kGather ? -4 : -3;
+#pragma unroll 1
+  for (int cy = -3; cy <= 3; ++cy) {
+#pragma unroll 1
+    for (int cx = kCx0; cx <= kCx0 + 7; ++cx) {
+      const uint32_t* g = sg + (gr0 + cy) * kEpfGRow + lane + col0 + 7 + cx;
+      int sad[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        int hs[6];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+          hs[r] = int(__vsadu4(ref[c][r], g[c * kEpfGPlane + r * kEpfGRow]));
+        }
+        const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
+        sad[0] = max(sad[0], hs[0] + p12);
+        sad[1] = max(sad[1], p12 + hs[3]);
+        sad[2] = max(sad[2], hs[2] + p34);
+        sad[3] = max(sad[3], p34 + hs[5]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (kGather) {
+          // The sending pixel q + e and its block's weight multiplier.
+          const int sy = py0 + j + cy, sx = px + cx;
+          const int m = s_m64[(sy >> 3) - y0 / 8 + 1][(sx >> 3) - x0 / 8 + 1];
+          float wgt = EpfWeight(m, sad[j]);
+          if (!(wgt >= 0.05f) || m == 0) wgt = 0.0f;
+          const int tr = 4 * band + j + 3 + cy, tc = lane + col0 + 4 + cx;
+          acc[0][j] = fmaf(tile[0][tr][tc], wgt, acc[0][j]);
+          acc[1][j] = fmaf(tile[1][tr][tc], wgt, acc[1][j]);
+          acc[2][j] = fmaf(tile[2][tr][tc], wgt, acc[2][j]);
+        } else {
+          float wgt = EpfWeight(m64c, sad[j]);
+          if (!(wgt >= 0.05f)) wgt = 0.0f;
+          sw[j] += wgt;
+        }
+      }
     }
-    const int m64 = c_t.mul_table[sg] * 64;
-    // Weight of neighbour (cy, cx), as in the forward.
-    auto weight = [&](int cy, int cx) {
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const size_t o = c * plane + size_t(py0 + j) * w + px;
+      if (kGather) {
+        out[o] += acc[c][j] + (filtered ? 0.0f : g_filt[o]);
+      } else {
+        out[o] = g_filt[o] / sw[j];
+      }
+    }
+}
+
+// Pass 3: the EPF terms that the forward mirrored back into the frame
+// (p + d outside it), scattered from the 4-pixel border band.
+__global__ void k_adj_epf_border(int w, int h, const uint8_t* guide,
+                                 const int32_t* sigma, const float* gv,
+                                 float* g_idct) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  if (x >= 3 && x < w - 4 && y >= 3 && y < h - 3) return;  // interior
+  const int sg = sigma[(y >> 3) * (w / 8) + (x >> 3)];
+  if (sg < kMinSigma) return;
+  const size_t plane = size_t(w) * h;
+  const int gwid = w + 12, ght = h + 12;
+  const int m64 = c_t.mul_table[sg] * 64;
+  auto gb = [&](int c, int yy, int xx) {
+    return int(guide[(size_t(c) * ght + yy + 6) * gwid + xx + 6]);
+  };
+  float gvp[3];
+  for (int c = 0; c < 3; ++c) gvp[c] = gv[c * plane + size_t(y) * w + x];
+  for (int cy = -3; cy <= 3; ++cy) {
+    for (int cx = -3; cx <= 4; ++cx) {
+      const int tx = x + cx, ty = y + cy;
+      if (tx >= 0 && tx < w && ty >= 0 && ty < h) continue;  // gathered
       int sad_max = 0;
       for (int c = 0; c < 3; ++c) {
         int sad = 0;
-#pragma unroll
-        for (int py = -1; py <= 1; ++py) {
-#pragma unroll
-          for (int px = -1; px <= 2; ++px) {
-            sad += abs(int(s_gd[c][ly + 4 + py][lx + 4 + px]) -
-                       int(s_gd[c][ly + 4 + cy + py][lx + 4 + cx + px]));
-          }
-        }
+        for (int py = -1; py <= 1; ++py)
+          for (int q = -1; q <= 2; ++q)
+            sad += abs(gb(c, y + py, x + q) - gb(c, ty + py, tx + q));
         sad_max = max(sad_max, sad);
       }
-      const float wv = EpfWeight(m64, sad_max);
-      return wv >= 0.05f ? wv : 0.0f;
-    };
-    // Pass 1: the weight sum in the forward's neighbour order; pass 2:
-    // the weights again, scattered.
-    float sw = 0.0f;
-#pragma unroll 1
-    for (int cy = -3; cy <= 3; ++cy) {
-#pragma unroll
-      for (int cx = -3; cx <= 4; ++cx) sw += weight(cy, cx);
+      float wgt = EpfWeight(m64, sad_max);
+      if (!(wgt >= 0.05f)) continue;
+      const size_t o = size_t(MirrorIdx(ty, h)) * w + MirrorIdx(tx, w);
+      for (int c = 0; c < 3; ++c) atomicAdd(&g_idct[c * plane + o], gvp[c] * wgt);
     }
-    float gv[3];
-    for (int c = 0; c < 3; ++c) gv[c] = gf[c] / sw;
-#pragma unroll 1
-    for (int cy = -3; cy <= 3; ++cy) {
-#pragma unroll
-      for (int cx = -3; cx <= 4; ++cx) {
-        const float wv = weight(cy, cx);
-        if (wv == 0.0f) continue;
-        for (int c = 0; c < 3; ++c) {
-          atomicAdd(&s_acc[c][ly + 3 + cy][lx + 3 + cx], gv[c] * wv);
-        }
-      }
-    }
-  }
-  __syncthreads();
-  for (int i = tid; i < 3 * kAdjEpfAH * kAdjEpfAW; i += kAdjThreads) {
-    const float v = (&s_acc[0][0][0])[i];
-    if (v == 0.0f) continue;
-    const int c = i / (kAdjEpfAH * kAdjEpfAW);
-    const int r = (i / kAdjEpfAW) % kAdjEpfAH, col = i % kAdjEpfAW;
-    const int X = MirrorIdx(x0 - 3 + col, w), Y = MirrorIdx(y0 - 3 + r, h);
-    atomicAdd(&g_idct[c * plane + size_t(Y) * w + X], v);
   }
 }
 
@@ -797,9 +909,16 @@ int LaunchAdjoint(pikgpu_ctx* ctx, const float* target) {
           g_qf);
       ++ctx->launches;
     }
-    dim3 gr(Blocks(g.PW, kAdjEpfW), Blocks(g.PH, kAdjEpfH));
-    k_adj_epf<<<gr, kAdjThreads, 0, st>>>(g.PW, g.PH, guide, sig, g_filt, gc);
-    ++ctx->launches;
+    // gv = g_filt / sum_w in the plane g_cur no longer needs.
+    float* gv = g_filt == ga ? gb : ga;
+    dim3 gr(Blocks(g.PW, kEpfW), Blocks(g.PH, kEpfH));
+    k_adj_epf_pass<false><<<gr, kEpfThreads, kAdjEpfSmemBytes, st>>>(
+        g.PW, g.PH, guide, sig, g_filt, nullptr, gv);
+    k_adj_epf_pass<true><<<gr, kEpfThreads, kAdjEpfSmemBytes, st>>>(
+        g.PW, g.PH, guide, sig, g_filt, gv, gc);
+    dim3 b3(32, 8), g3(Blocks(g.PW, 32), Blocks(g.PH, 8));
+    k_adj_epf_border<<<g3, b3, 0, st>>>(g.PW, g.PH, guide, sig, gv, gc);
+    ctx->launches += 3;
     g_idct = gc;
   }
   // g_up: the upsampled-prediction gradient (zero outside HF blocks), in
@@ -964,6 +1083,14 @@ int pikgpu_adjoint(pikgpu_ctx* ctx, const float* target, double* loss,
   }
   cudaStream_t st = ctx->stream;
   if (!ctx->adj_jac_built) {
+    CUDA_TRY(ctx, cudaFuncSetAttribute(
+                      k_adj_epf_pass<false>,
+                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                      int(kAdjEpfSmemBytes)));
+    CUDA_TRY(ctx, cudaFuncSetAttribute(
+                      k_adj_epf_pass<true>,
+                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                      int(kAdjEpfSmemBytes)));
     k_adj_build_jac<<<2 * kJTypes + 9, 64, 0, st>>>(P<AdjJac>(ctx->adj_jac));
     CUDA_TRY(ctx, cudaGetLastError());
     ctx->adj_jac_built = true;
