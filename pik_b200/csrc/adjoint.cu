@@ -346,15 +346,17 @@ __global__ void __launch_bounds__(kAdjThreads)
   }
 }
 
-// Transposed square-DCT matrices staged in shared memory.
+// Square-DCT matrices staged in shared memory for the transposed-matrix
+// transforms (CoopTsIdctT / CoopTsDctT, which take M^T to apply M): `a` =
+// A (applies A^T, the transpose of the IDCT), `b` = B (applies B^T, the
+// transpose of the scaled DCT), `bt` = B^T (applies B, the DCT).
 template <int N>
-__device__ __forceinline__ void StageTransposed(float* at, float* bt,
-                                                float* b) {
+__device__ __forceinline__ void StageMatrices(float* a, float* b, float* bt) {
   for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
     const int r = i / N, c = i % N;
-    at[i] = IdctMat(N)[c * N + r];
-    bt[i] = DctMat(N)[c * N + r];
-    if (b) b[i] = DctMat(N)[i];
+    a[i] = IdctMat(N)[i];
+    b[i] = DctMat(N)[i];
+    if (bt) bt[i] = DctMat(N)[c * N + r];
   }
 }
 
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(kAdjThreads)
                 const float* epf, const float* g_cur, float* g_filt,
                 float* g_idct, float* g_qf) {
   constexpr int NN = N * N, cov = N / 8;
-  __shared__ float s_b[NN], s_at[NN], s_bt[NN];
+  __shared__ float s_b[NN], s_a[NN], s_bt[NN];
   __shared__ float s_co[3][NN], s_g[3][NN], s_t[NN];
   __shared__ float s_q[kAdjThreads / 32];
   const int item = blockIdx.x;
@@ -392,7 +394,7 @@ __global__ void __launch_bounds__(kAdjThreads)
     }
     return;
   }
-  StageTransposed<N>(s_at, s_bt, s_b);
+  StageMatrices<N>(s_a, s_b, s_bt);
   for (int i = threadIdx.x; i < 3 * NN; i += blockDim.x) {
     const int c = i / NN, e = i % NN;
     const size_t o = pix(c, e);
@@ -401,8 +403,8 @@ __global__ void __launch_bounds__(kAdjThreads)
   }
   __syncthreads();
   for (int c = 0; c < 3; ++c) {
-    CoopTsDct(N, 1, s_b, s_co[c], s_t, s_co[c]);
-    CoopTsIdct(N, 1, s_at, s_g[c], s_t, s_g[c]);
+    CoopTsDctT(N, 1, s_bt, s_co[c], s_t, s_co[c]);   // B
+    CoopTsIdctT(N, 1, s_a, s_g[c], s_t, s_g[c]);    // A^T
   }
   const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
   const float qf_eff = QfEff(g, f, bx, by);
@@ -422,7 +424,9 @@ __global__ void __launch_bounds__(kAdjThreads)
     for (int c = 0; c < 3; ++c) s_g[c][e] = gc[c];
   }
   __syncthreads();
-  for (int c = 0; c < 3; ++c) CoopTsDct(N, 1, s_bt, s_g[c], s_t, s_g[c]);
+  for (int c = 0; c < 3; ++c) {
+    CoopTsDctT(N, 1, s_b, s_g[c], s_t, s_g[c]);  // B^T
+  }
   for (int i = threadIdx.x; i < 3 * NN; i += blockDim.x) {
     const int c = i / NN, e = i % NN;
     const size_t o = pix(c, e);
@@ -700,21 +704,21 @@ __global__ void __launch_bounds__(kAdjThreads)
                    int predict_hf, const float* g_idct, float* g_coef,
                    float* g_up) {
   constexpr int NN = N * N, cov = N / 8, chunk = 64 * cov;
-  __shared__ float s_at[NN], s_bt[NN], s_x[NN], s_t[NN];
+  __shared__ float s_a[NN], s_b[NN], s_x[NN], s_t[NN];
   const int item = blockIdx.x;
   if (item >= count) return;
   const uint32_t pk = list[item];
   const int bx = pk & 0xFFFF, by = pk >> 16;
   const size_t plane = size_t(g.PW) * g.PH;
   const size_t plane_ac = size_t(g.ac_stride) * g.By;
-  StageTransposed<N>(s_at, s_bt, nullptr);
+  StageMatrices<N>(s_a, s_b, nullptr);
   for (int c = 0; c < 3; ++c) {
     for (int e = threadIdx.x; e < NN; e += blockDim.x) {
       s_x[e] = g_idct[c * plane + size_t(by * 8 + e / N) * g.PW + bx * 8 +
                       e % N];
     }
     __syncthreads();
-    CoopTsIdct(N, 1, s_at, s_x, s_t, s_x);
+    CoopTsIdctT(N, 1, s_a, s_x, s_t, s_x);  // A^T
     float* base = g_coef + c * plane_ac + size_t(by) * g.ac_stride +
                   size_t(bx) * 64;
     for (int e = threadIdx.x; e < NN; e += blockDim.x) {
@@ -723,7 +727,7 @@ __global__ void __launch_bounds__(kAdjThreads)
     }
     __syncthreads();
     if (!predict_hf) continue;  // CTA-uniform
-    CoopTsDct(N, 1, s_bt, s_x, s_t, s_x);
+    CoopTsDctT(N, 1, s_b, s_x, s_t, s_x);  // B^T
     for (int e = threadIdx.x; e < NN; e += blockDim.x) {
       g_up[c * plane + size_t(by * 8 + e / N) * g.PW + bx * 8 + e % N] =
           s_x[e];

@@ -582,9 +582,9 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       ++ctx->launches;
     }
     if (n[kC32]) {
-      k_square_idct_rows<32><<<rows_grid(3 * n[kC32], 32), kSquareThreads, 0,
-                               cls(kC32)>>>(g, f, L[kC32], n[kC32],
-                                            s.predict_hf);
+      // One 256-thread CTA per block.
+      k_square_idct<32><<<n[kC32], 256, 0, cls(kC32)>>>(g, f, L[kC32], n[kC32],
+                                                       s.predict_hf);
       ++ctx->launches;
     }
     if (n[kC4]) {
@@ -677,10 +677,8 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       ++ctx->launches;
     }
     if (n[kC32]) {
-      k_square_ar_rows<32><<<rows_grid(n[kC32], 32), kSquareThreads, 0,
-                             cls(kC32)>>>(g, f, s,
-                                          P<uint32_t>(ctx->active[kC32]),
-                                          counters + kC32);
+      k_square_ar<32><<<n[kC32], 256, 0, cls(kC32)>>>(
+          g, f, s, P<uint32_t>(ctx->active[kC32]), counters + kC32);
       ++ctx->launches;
     }
     if (n[kC4]) {

@@ -811,6 +811,55 @@ __device__ void CoopTsDct(int n, int nb, const float* bm, const float* in,
   __syncthreads();
 }
 
+// The same two transforms with the matrix given transposed (aT[l n + v] =
+// A[v][l], bT[x n + k] = B[k][x]) and the first DCT pass mapped with k
+// fastest: consecutive threads then read consecutive shared-memory words of
+// the matrix (the plain forms read it with a stride of n words, an n-way
+// bank conflict at n = 32). Every output is the same sum of the same
+// products in the same order, so the results are bit-identical.
+__device__ void CoopTsIdctT(int n, int nb, const float* aT, const float* in,
+                            float* tmp, float* out) {
+  const int nn = n * n;
+  for (int i = threadIdx.x; i < nb * nn; i += blockDim.x) {
+    const int b = i / nn, r = i % nn, k = r / n, v = r % n;
+    const float* src = in + b * nn + k * n;
+    float s = 0.f;
+    for (int l = 0; l < n; ++l) s += src[l] * aT[l * n + v];
+    tmp[b * nn + k * n + v] = s;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb * nn; i += blockDim.x) {
+    const int b = i / nn, r = i % nn, v = r / n, u = r % n;
+    const float* t = tmp + b * nn;
+    float s = 0.f;
+    for (int k = 0; k < n; ++k) s += aT[k * n + u] * t[k * n + v];
+    out[b * nn + v * n + u] = s;
+  }
+  __syncthreads();
+}
+
+__device__ void CoopTsDctT(int n, int nb, const float* bT, const float* in,
+                           float* tmp, float* out) {
+  const int nn = n * n;
+  for (int i = threadIdx.x; i < nb * nn; i += blockDim.x) {
+    const int b = i / nn, r = i % nn, y = r / n, k = r % n;
+    const float* src = in + b * nn + y * n;
+    float s = 0.f;
+    for (int x = 0; x < n; ++x) s += bT[x * n + k] * src[x];
+    tmp[b * nn + k * n + y] = s;
+  }
+  __syncthreads();
+  const float scale = 1.0f / float(nn);
+  for (int i = threadIdx.x; i < nb * nn; i += blockDim.x) {
+    const int b = i / nn, r = i % nn, k = r / n, l = r % n;
+    const float* t = tmp + b * nn + k * n;
+    float s = 0.f;
+    for (int y = 0; y < n; ++y) s += t[y] * bT[y * n + l];
+    out[b * nn + k * n + l] = s * scale;
+  }
+  __syncthreads();
+}
+
 // Upsampled-blurred HF prediction pixel (UpSample4x4BlurDCT,
 // pik/ac_predictions.cc:263-374) at group-local pixel (X, Y).
 __device__ __forceinline__ float Upsample(const float* pred, int X, int Y) {
@@ -865,9 +914,9 @@ __global__ void __launch_bounds__(256)
   constexpr int NB = NN >= 256 ? 1 : 256 / NN;
   __shared__ float s_a[NN], s_b[NN];
   __shared__ float s_c[NB * NN], s_t[NB * NN], s_p[NB * NN];
-  for (int i = threadIdx.x; i < NN; i += blockDim.x) {
-    s_a[i] = c_t.idct[MatOffset(N) + i];
-    s_b[i] = c_t.dct[MatOffset(N) + i];
+  for (int i = threadIdx.x; i < NN; i += blockDim.x) {  // transposed
+    s_a[i] = c_t.idct[MatOffset(N) + (i % N) * N + i / N];
+    s_b[i] = c_t.dct[MatOffset(N) + (i % N) * N + i / N];
   }
   const int first = blockIdx.x * NB;
   const int nb = min(NB, count - first);
@@ -896,7 +945,7 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
     if (predict_hf) {
-      CoopTsDct(N, nb, s_b, s_p, s_t, s_p);
+      CoopTsDctT(N, nb, s_b, s_p, s_t, s_p);
       for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
         const int e = i % NN, y = e / N, x = e % N;
         if (y < 2 * cov && x < 2 * cov) continue;
@@ -908,7 +957,7 @@ __global__ void __launch_bounds__(256)
       }
       __syncthreads();
     }
-    CoopTsIdct(N, nb, s_a, s_c, s_t, s_p);
+    CoopTsIdctT(N, nb, s_a, s_c, s_t, s_p);
     for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
       const int b = i / NN, e = i % NN;
       const uint32_t pk = list[first + b];
@@ -1204,19 +1253,25 @@ __device__ __forceinline__ float LlfScale(int type, int x, int y) {
   return 1.0f;
 }
 
+// One CTA of 256 threads per DCT32 block (the rows form's one warp per
+// block leaves most SMs idle at a few hundred blocks). `count` is read from
+// device memory (the compacted list of k_active_blocks); the grid covers the
+// class's whole list.
 template <int N>
 __global__ void __launch_bounds__(256)
     k_square_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
-                int count) {
+                const int* count_ptr) {
   constexpr int NN = N * N;
   constexpr int NB = NN >= 256 ? 1 : 256 / NN;
   constexpr int cov = N / 8;
+  const int count = *count_ptr;
+  if (int(blockIdx.x) * NB >= count) return;  // whole CTA
   __shared__ float s_a[NN], s_b[NN];
   __shared__ float s_blk[3][NB * NN];
   __shared__ float s_r[NB * NN], s_t[NB * NN], s_p[NB * NN];
-  for (int i = threadIdx.x; i < NN; i += blockDim.x) {
-    s_a[i] = c_t.idct[MatOffset(N) + i];
-    s_b[i] = c_t.dct[MatOffset(N) + i];
+  for (int i = threadIdx.x; i < NN; i += blockDim.x) {  // transposed
+    s_a[i] = c_t.idct[MatOffset(N) + (i % N) * N + i / N];
+    s_b[i] = c_t.dct[MatOffset(N) + (i % N) * N + i / N];
   }
   const int first = blockIdx.x * NB;
   const int nb = min(NB, count - first);
@@ -1231,7 +1286,7 @@ __global__ void __launch_bounds__(256)
       s_p[i] = f.filt[o] - f.idct[o];
     }
     __syncthreads();
-    CoopTsDct(N, nb, s_b, s_p, s_t, s_blk[c]);
+    CoopTsDctT(N, nb, s_b, s_p, s_t, s_blk[c]);
   }
   for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
     const int b = i / NN, e = i % NN, y = e / N, x = e % N;
@@ -1239,14 +1294,24 @@ __global__ void __launch_bounds__(256)
     const int bx = pk & 0xFFFF, by = pk >> 16;
     const int type = f.acs[by * g.Bx + bx] >> 4;
     const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
-    float mr = 1.0f;
+    float mr = 1.0f, rt[3];
+    int arg = -1;
     for (int c = 0; c < 3; ++c) {
       const float interval =
           (y < cov && x < cov)
               ? LlfScale(type, x, y) * s.mul_dc[c]
               : info.dm[c][e] * info.inv_quant_ac;
-      const float r = ClampRatio(s_blk[c][i], interval);
-      mr = r < mr ? r : mr;
+      rt[c] = ClampRatio(s_blk[c][i], interval);
+      if (rt[c] < mr) mr = rt[c], arg = c;
+    }
+    if (f.clamp_tape || f.clamp_tape_in) {
+      const size_t to = CoefOffset(g, bx, by, cov, e);
+      uint8_t code = arg < 0 ? 0 : mr == 0.0f ? 4 : uint8_t(arg + 1);
+      if (f.clamp_tape_in) {
+        code = f.clamp_tape_in[to];
+        mr = TapeRatio(code, rt[0], rt[1], rt[2]);
+      }
+      if (f.clamp_tape) f.clamp_tape[to] = code;
     }
     s_r[i] = mr;
   }
@@ -1256,7 +1321,7 @@ __global__ void __launch_bounds__(256)
       s_blk[c][i] = s_blk[c][i] * s_r[i];
     }
     __syncthreads();
-    CoopTsIdct(N, nb, s_a, s_blk[c], s_t, s_p);
+    CoopTsIdctT(N, nb, s_a, s_blk[c], s_t, s_p);
     for (int i = threadIdx.x; i < nb * NN; i += blockDim.x) {
       const int b = i / NN, e = i % NN;
       const uint32_t pk = list[first + b];
