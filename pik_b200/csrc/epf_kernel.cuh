@@ -50,6 +50,10 @@ constexpr int kEpfTRow0 = 2, kEpfTCol0 = 9;  // tile index of (y0-3, x0-3)
 constexpr size_t kEpfGuideWords = size_t(3) * kEpfGPlane;
 constexpr size_t kEpfSmemBytes =
     kEpfGuideWords * 4 + size_t(3) * kEpfTH * kEpfTS * 4;
+// Shared memory of k_epf_box with a tile of `th` rows.
+constexpr size_t EpfSmemBytes(int th) {
+  return size_t(3) * (th + 8) * kEpfGRow * 4 + size_t(3) * (th + 10) * kEpfTS * 4;
+}
 
 // WeightFast (pik/epf_target.cc:304-428) as 4 integer operations:
 // ((int16(min(sad, 507) << 6) * mul) >> 16 + (127 << 7)) in the high half of
@@ -63,16 +67,21 @@ __device__ __forceinline__ float EpfWeight(int mul64, int sad) {
 // kFma: the weighted sums with fused multiply-adds (the tensor-core forms,
 // which are not bound to the reference's rounding); otherwise every product
 // and sum is rounded separately, as the reference does.
-template <bool kFma>
-__global__ void __launch_bounds__(kEpfThreads, 2)
+// TH: tile rows (32 for frames; 8 for small images such as the DC image,
+// which would otherwise be a few CTAs of a full tile's latency each).
+template <bool kFma, int TH>
+__global__ void __launch_bounds__(16 * TH, 2)
     k_epf_box(const float* in, const float* guide_src,
               const uint8_t* guide_ovr, int gab, int w, int h,
               const uint32_t* mm, const int32_t* sigma, float* out) {
+  constexpr int kH = TH, kGH = TH + 8, kTH = TH + 10;
+  constexpr int kGPlane = kGH * kEpfGRow, kThreads = 16 * TH;
+  constexpr size_t kGuideWords = size_t(3) * kGPlane;
   extern __shared__ __align__(16) uint32_t epf_smem[];
-  uint32_t* sg = epf_smem;  // [3][kEpfGH][kEpfGRow]
-  float(*tile)[kEpfTH][kEpfTS] =
-      reinterpret_cast<float(*)[kEpfTH][kEpfTS]>(epf_smem + kEpfGuideWords);
-  const int x0 = blockIdx.x * kEpfW, y0 = blockIdx.y * kEpfH;
+  uint32_t* sg = epf_smem;  // [3][kGH][kEpfGRow]
+  float(*tile)[kTH][kEpfTS] =
+      reinterpret_cast<float(*)[kTH][kEpfTS]>(epf_smem + kGuideWords);
+  const int x0 = blockIdx.x * kEpfW, y0 = blockIdx.y * kH;
   const int tid = threadIdx.x;
   constexpr int LC = kEpfLaneCols;
   const int lane = tid & 31, wp = tid >> 5;
@@ -112,20 +121,20 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
   // Tiles whose halo lies inside the image take vector loads and no
   // mirroring; border tiles mirror every coordinate.
   const bool interior = x0 >= 12 && x0 + kEpfW + 12 <= w && y0 >= 5 &&
-                        y0 + kEpfH + 5 <= h;
+                        y0 + kH + 5 <= h;
   if (interior) {
     constexpr int Q = kEpfTW / 4;
-    for (int i = tid; i < 3 * kEpfTH * Q; i += kEpfThreads) {
-      const int c = i / (kEpfTH * Q);
-      const int r = (i / Q) % kEpfTH, q = i % Q;
+    for (int i = tid; i < 3 * kTH * Q; i += kThreads) {
+      const int c = i / (kTH * Q);
+      const int r = (i / Q) % kTH, q = i % Q;
       CpAsync16(&tile[c][r][4 * q],
                 in + c * plane + size_t(y0 - 5 + r) * w + x0 - 12 + 4 * q);
     }
     CpAsyncWaitAll();
   } else {
-    for (int i = tid; i < 3 * kEpfTH * kEpfTW; i += kEpfThreads) {
-      const int c = i / (kEpfTH * kEpfTW);
-      const int r = (i / kEpfTW) % kEpfTH, col = i % kEpfTW;
+    for (int i = tid; i < 3 * kTH * kEpfTW; i += kThreads) {
+      const int c = i / (kTH * kEpfTW);
+      const int r = (i / kEpfTW) % kTH, col = i % kEpfTW;
       const int gx = x0 - 12 + col, gy = y0 - 5 + r;
       tile[c][r][col] =
           in[c * plane + size_t(MirrorIdx(gy, h)) * w + MirrorIdx(gx, w)];
@@ -154,9 +163,9 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
   // u8 guide (MakeGuide, pik/epf_target.cc:1009-1070): the aligned words
   // (offsets 4 wd) first.
   constexpr int kAligned = kEpfGBytes / 4;
-  for (int i = tid; i < 3 * kEpfGH * kAligned; i += kEpfThreads) {
-    const int c = i / (kEpfGH * kAligned);
-    const int r = (i / kAligned) % kEpfGH, wd = i % kAligned;
+  for (int i = tid; i < 3 * kGH * kAligned; i += kThreads) {
+    const int c = i / (kGH * kAligned);
+    const int r = (i / kAligned) % kGH, wd = i % kAligned;
     const int gy = y0 - 4 + r;
     uint32_t word = 0;
     if (interior && !guide_ovr) {
@@ -198,7 +207,7 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
           // positions whose mirror leaves the tile are never read.
           const int ly = MirrorIdx(gy, h) - (y0 - 5);
           const int lx = MirrorIdx(gx, w) - (x0 - 12);
-          if (ly >= 1 && ly < kEpfTH - 1 && lx >= 1 && lx < kEpfTW - 1) {
+          if (ly >= 1 && ly < kTH - 1 && lx >= 1 && lx < kEpfTW - 1) {
             v = quant(smooth(c, ly, lx));
           }
         } else {
@@ -208,20 +217,20 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
         word |= v << (8 * b);
       }
     }
-    sg[c * kEpfGPlane + r * kEpfGRow + 4 * wd] = word;
+    sg[c * kGPlane + r * kEpfGRow + 4 * wd] = word;
   }
   __syncthreads();
   // The other offsets 4 wd + s, s = 1..3, from the two aligned neighbours
   // (bytes past the row end read as 0).
-  for (int i = tid; i < 3 * kEpfGH * kAligned * 3; i += kEpfThreads) {
+  for (int i = tid; i < 3 * kGH * kAligned * 3; i += kThreads) {
     const int s = 1 + i % 3;
     const int j = i / 3;
-    const int c = j / (kEpfGH * kAligned);
-    const int r = (j / kAligned) % kEpfGH, wd = j % kAligned;
-    const uint32_t* row = sg + c * kEpfGPlane + r * kEpfGRow;
+    const int c = j / (kGH * kAligned);
+    const int r = (j / kAligned) % kGH, wd = j % kAligned;
+    const uint32_t* row = sg + c * kGPlane + r * kEpfGRow;
     const uint32_t lo = row[4 * wd];
     const uint32_t hi = wd + 1 < kAligned ? row[4 * wd + 4] : 0u;
-    sg[c * kEpfGPlane + r * kEpfGRow + 4 * wd + s] =
+    sg[c * kGPlane + r * kEpfGRow + 4 * wd + s] =
         __funnelshift_r(lo, hi, 8 * s);
   }
   __syncthreads();
@@ -258,7 +267,7 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
       for (int r = 0; r < 6; ++r)
 #pragma unroll
         for (int i = 0; i < LC; ++i)
-          ref[c][r][i] = g[c * kEpfGPlane + r * kEpfGRow + 32 * i];
+          ref[c][r][i] = g[c * kGPlane + r * kEpfGRow + 32 * i];
   }
 
   float ws[3][4 * LC], sw[4 * LC];
@@ -284,7 +293,7 @@ __global__ void __launch_bounds__(kEpfThreads, 2)
 #pragma unroll
           for (int r = 0; r < 6; ++r) {
             hs[r] = int(__vsadu4(
-                ref[c][r][i], g[c * kEpfGPlane + r * kEpfGRow + 32 * i]));
+                ref[c][r][i], g[c * kGPlane + r * kEpfGRow + 32 * i]));
           }
           const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
           sad[0 * LC + i] = max(sad[0 * LC + i], hs[0] + p12);

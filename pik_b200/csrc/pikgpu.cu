@@ -361,13 +361,21 @@ int UploadTables(pikgpu_ctx* ctx) {
   BuildTables(&t);
   CUDA_TRY(ctx, cudaMemcpyToSymbol(c_t, &t, sizeof(t)));
   CUDA_TRY(ctx, cudaFuncSetAttribute(
-                    k_epf_box<false>,
+                    k_epf_box<false, 32>,
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                    int(kEpfSmemBytes)));
+                    int(EpfSmemBytes(32))));
   CUDA_TRY(ctx, cudaFuncSetAttribute(
-                    k_epf_box<true>,
+                    k_epf_box<false, 8>,
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                    int(kEpfSmemBytes)));
+                    int(EpfSmemBytes(8))));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_epf_box<true, 32>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(EpfSmemBytes(32))));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_epf_box<true, 8>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(EpfSmemBytes(8))));
   CUDA_TRY(ctx, cudaFuncSetAttribute(
                     k_final_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(kFinSmemBytes)));
@@ -405,13 +413,30 @@ void Mark(pikgpu_ctx* ctx, int i) {
 int RunEpf(pikgpu_ctx* ctx, cudaStream_t st, const float* in,
            const float* guide_src, int gab, int w, int h, const int32_t* sig,
            float* out, const uint8_t* guide_ovr) {
-  dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
-  if (ctx->form == PIKGPU_FORM_FP32) {
-    k_epf_box<false><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
-        in, guide_src, guide_ovr, gab, w, h, P<uint32_t>(ctx->mm), sig, out);
+  // Images that fill fewer than two CTAs per SM with 32-row tiles (the DC
+  // image) take 8-row tiles: four times the CTAs, a quarter of the latency.
+  const bool small =
+      Blocks(w, kEpfW) * Blocks(h, kEpfH) < 2 * ctx->num_sms;
+  const bool fma = ctx->form != PIKGPU_FORM_FP32;
+  const uint32_t* mm = P<uint32_t>(ctx->mm);
+  if (small) {
+    dim3 grid(Blocks(w, kEpfW), Blocks(h, 8));
+    if (fma) {
+      k_epf_box<true, 8><<<grid, 16 * 8, EpfSmemBytes(8), st>>>(
+          in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
+    } else {
+      k_epf_box<false, 8><<<grid, 16 * 8, EpfSmemBytes(8), st>>>(
+          in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
+    }
   } else {
-    k_epf_box<true><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
-        in, guide_src, guide_ovr, gab, w, h, P<uint32_t>(ctx->mm), sig, out);
+    dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
+    if (fma) {
+      k_epf_box<true, kEpfH><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
+          in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
+    } else {
+      k_epf_box<false, kEpfH><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
+          in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
+    }
   }
   ++ctx->launches;
   return PIKGPU_OK;
