@@ -70,7 +70,7 @@ __device__ __forceinline__ float EpfWeight(int mul64, int sad) {
 // TH: tile rows (32 for frames; 8 for small images such as the DC image,
 // which would otherwise be a few CTAs of a full tile's latency each).
 template <bool kFma, int TH>
-__global__ void __launch_bounds__(16 * TH, 2)
+__global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
     k_epf_box(const float* in, const float* guide_src,
               const uint8_t* guide_ovr, int gab, int w, int h,
               const uint32_t* mm, const int32_t* sigma, float* out) {
@@ -276,51 +276,119 @@ __global__ void __launch_bounds__(16 * TH, 2)
     ws[0][p] = ws[1][p] = ws[2][p] = 0.f;
     sw[p] = 0.f;
   }
-#pragma unroll 1
-  for (int cy = -3; cy <= 3; ++cy) {
+  if constexpr (kFma && LC == 1) {
+    // Tensor-core forms: cx outermost. For one cx the 7 vertical offsets
+    // read 12 distinct guide rows per channel (one load each), and each
+    // staged input row serves every pixel of the lane it reaches: about
+    // 84 shared-memory loads per cx and lane instead of 210. Each pixel's
+    // sums run cx-major, not in the reference's cy-major order (these
+    // forms are not bound to its rounding).
 #pragma unroll 1
     for (int cx = -3; cx <= 4; ++cx) {
-      // Window byte offset (column 0): the patch start moved by cx.
-      const uint32_t* g = sg + (gr0 + cy) * kEpfGRow + lane + col0 + 7 + cx;
-      int sad[4 * LC];  // [j * LC + i]
+      const uint32_t* g = sg + (gr0 - 3) * kEpfGRow + lane + col0 + 7 + cx;
+      int sad[4][7];
 #pragma unroll
-      for (int p = 0; p < 4 * LC; ++p) sad[p] = 0;
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int k = 0; k < 7; ++k) sad[j][k] = 0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
+        uint32_t wd[12];  // guide rows gr0 - 3 .. gr0 + 8 at this cx
 #pragma unroll
-        for (int i = 0; i < LC; ++i) {
+        for (int t = 0; t < 12; ++t) wd[t] = g[c * kGPlane + t * kEpfGRow];
+        // The centre patch words again from shared memory (registers are
+        // the limit at two 512-thread CTAs per SM).
+        uint32_t rf[6];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+          rf[r] = sg[c * kGPlane + (gr0 + r) * kEpfGRow + lane + col0 + 7];
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {  // cy = k - 3: rows k .. k + 5
           int hs[6];
 #pragma unroll
-          for (int r = 0; r < 6; ++r) {
-            hs[r] = int(__vsadu4(
-                ref[c][r][i], g[c * kGPlane + r * kEpfGRow + 32 * i]));
-          }
+          for (int r = 0; r < 6; ++r) hs[r] = int(__vsadu4(rf[r], wd[k + r]));
           const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
-          sad[0 * LC + i] = max(sad[0 * LC + i], hs[0] + p12);
-          sad[1 * LC + i] = max(sad[1 * LC + i], p12 + hs[3]);
-          sad[2 * LC + i] = max(sad[2 * LC + i], hs[2] + p34);
-          sad[3 * LC + i] = max(sad[3 * LC + i], p34 + hs[5]);
+          sad[0][k] = max(sad[0][k], hs[0] + p12);
+          sad[1][k] = max(sad[1][k], p12 + hs[3]);
+          sad[2][k] = max(sad[2][k], hs[2] + p34);
+          sad[3][k] = max(sad[3][k], p34 + hs[5]);
         }
       }
+      float wt[4][7];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int ir = 4 * band + j + 3 + cy + kEpfTRow0;
+      for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int i = 0; i < LC; ++i) {
-          const int p = j * LC + i;
-          const int col = lane + col0 + 32 * i + 3 + cx + kEpfTCol0;
-          float wgt = EpfWeight(m64[i], sad[p]);
+        for (int k = 0; k < 7; ++k) {
+          float wgt = EpfWeight(m64[0], sad[j][k]);
           if (!(wgt >= 0.05f)) wgt = 0.0f;
-          if (kFma) {
-            ws[0][p] = fmaf(tile[0][ir][col], wgt, ws[0][p]);
-            ws[1][p] = fmaf(tile[1][ir][col], wgt, ws[1][p]);
-            ws[2][p] = fmaf(tile[2][ir][col], wgt, ws[2][p]);
-          } else {
-            ws[0][p] += tile[0][ir][col] * wgt;
-            ws[1][p] += tile[1][ir][col] * wgt;
-            ws[2][p] += tile[2][ir][col] * wgt;
+          wt[j][k] = wgt;
+          sw[j] += wgt;
+        }
+      // Input rows band + R - 3 (R = j + cy + 3 = 0..9) at column px + cx.
+      const int col = lane + col0 + 3 + cx + kEpfTCol0;
+#pragma unroll
+      for (int R = 0; R < 10; ++R) {
+        const int ir = 4 * band + R + kEpfTRow0;
+        const float v0 = tile[0][ir][col], v1 = tile[1][ir][col],
+                    v2 = tile[2][ir][col];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int k = R - j;  // cy + 3
+          if (k < 0 || k > 6) continue;
+          ws[0][j] = fmaf(v0, wt[j][k], ws[0][j]);
+          ws[1][j] = fmaf(v1, wt[j][k], ws[1][j]);
+          ws[2][j] = fmaf(v2, wt[j][k], ws[2][j]);
+        }
+      }
+    }
+  } else {
+  #pragma unroll 1
+    for (int cy = -3; cy <= 3; ++cy) {
+  #pragma unroll 1
+      for (int cx = -3; cx <= 4; ++cx) {
+        // Window byte offset (column 0): the patch start moved by cx.
+        const uint32_t* g = sg + (gr0 + cy) * kEpfGRow + lane + col0 + 7 + cx;
+        int sad[4 * LC];  // [j * LC + i]
+  #pragma unroll
+        for (int p = 0; p < 4 * LC; ++p) sad[p] = 0;
+  #pragma unroll
+        for (int c = 0; c < 3; ++c) {
+  #pragma unroll
+          for (int i = 0; i < LC; ++i) {
+            int hs[6];
+  #pragma unroll
+            for (int r = 0; r < 6; ++r) {
+              hs[r] = int(__vsadu4(
+                  ref[c][r][i], g[c * kGPlane + r * kEpfGRow + 32 * i]));
+            }
+            const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
+            sad[0 * LC + i] = max(sad[0 * LC + i], hs[0] + p12);
+            sad[1 * LC + i] = max(sad[1 * LC + i], p12 + hs[3]);
+            sad[2 * LC + i] = max(sad[2 * LC + i], hs[2] + p34);
+            sad[3 * LC + i] = max(sad[3 * LC + i], p34 + hs[5]);
           }
-          sw[p] += wgt;
+        }
+  #pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int ir = 4 * band + j + 3 + cy + kEpfTRow0;
+  #pragma unroll
+          for (int i = 0; i < LC; ++i) {
+            const int p = j * LC + i;
+            const int col = lane + col0 + 32 * i + 3 + cx + kEpfTCol0;
+            float wgt = EpfWeight(m64[i], sad[p]);
+            if (!(wgt >= 0.05f)) wgt = 0.0f;
+            if (kFma) {
+              ws[0][p] = fmaf(tile[0][ir][col], wgt, ws[0][p]);
+              ws[1][p] = fmaf(tile[1][ir][col], wgt, ws[1][p]);
+              ws[2][p] = fmaf(tile[2][ir][col], wgt, ws[2][p]);
+            } else {
+              ws[0][p] += tile[0][ir][col] * wgt;
+              ws[1][p] += tile[1][ir][col] * wgt;
+              ws[2][p] += tile[2][ir][col] * wgt;
+            }
+            sw[p] += wgt;
+          }
         }
       }
     }

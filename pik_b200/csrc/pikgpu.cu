@@ -373,6 +373,10 @@ int UploadTables(pikgpu_ctx* ctx) {
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(EpfSmemBytes(32))));
   CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_epf_box<true, 16>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(EpfSmemBytes(16))));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
                     k_epf_box<true, 8>,
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(EpfSmemBytes(8))));
@@ -429,11 +433,14 @@ int RunEpf(pikgpu_ctx* ctx, cudaStream_t st, const float* in,
           in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
     }
   } else {
-    dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
     if (fma) {
-      k_epf_box<true, kEpfH><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
+      // 16-row tiles of 256 threads, three CTAs per SM: the cx-major loop
+      // of these forms needs ~85 registers.
+      dim3 grid(Blocks(w, kEpfW), Blocks(h, 16));
+      k_epf_box<true, 16><<<grid, 16 * 16, EpfSmemBytes(16), st>>>(
           in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
     } else {
+      dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
       k_epf_box<false, kEpfH><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
           in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
     }
