@@ -165,9 +165,9 @@ int DcNoAlloc(pikgpu_ctx* ctx, const int16_t* quantized_dc, uint32_t bx,
       dcpad, size_t(dpw) * dph, mm);
   k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, nullptr, nullptr, nullptr,
                                                s.quant_dc / 2, mm, sig);
-  k_epf_box<false, kEpfH><<<dim3(Blocks(dpw, kEpfW), Blocks(dph, kEpfH)), kEpfThreads,
-              kEpfSmemBytes, st>>>(dcpad, dcpad, nullptr, 0, dpw, dph, mm,
-                                   sig, dcfilt);
+  k_epf_box<false, kEpfH><<<Blocks(dpw, kEpfW) * Blocks(dph, kEpfH),
+                            kEpfThreads, kEpfSmemBytes, st>>>(
+      dcpad, dcpad, nullptr, 0, dpw, dph, mm, sig, dcfilt);
   dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
   k_dc_clamp<<<gr2, b, 0, st>>>(dc, dcfilt, g.Bx, g.By, dpw, dph,
                                 half_step[0], half_step[1], half_step[2]);

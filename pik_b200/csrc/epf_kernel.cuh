@@ -1,8 +1,8 @@
 // Edge-preserving filter (AdaptiveFilter + WeightedSum,
 // pik/epf_target.cc:526-801, 1113-1278) on packed guide bytes.
 //
-// One CTA filters a 64 x 32 pixel tile with 16 warps. Lane l of warp w owns
-// the pixels (x0 + 32 (w mod 2) + l, y0 + 4 (w / 2) + j), j = 0..3: one
+// A CTA filters 64 x TH pixel tiles with 2 TH / 4 warps. Lane l of warp w
+// owns the pixels (x0 + 32 (w mod 2) + l, y0 + 4 (w / 2) + j), j = 0..3: one
 // column (the 32 lanes of a warp read 32 consecutive values of every
 // shared-memory row), four rows inside one 8x8 block row.
 //
@@ -30,12 +30,8 @@
 
 namespace pikgpu {
 
-constexpr int kEpfW = 64, kEpfH = 32;   // output tile
-// Columns per lane: 1 (512 threads, each lane 4 pixels of one column, two
-// warps per 4-row band) keeps a thread at <= 64 registers, so two CTAs of
-// 16 warps share an SM; 2 (256 threads, 8 pixels per lane) needs ~123.
-constexpr int kEpfLaneCols = 1;
-constexpr int kEpfThreads = 256 * 2 / kEpfLaneCols;
+constexpr int kEpfW = 64, kEpfH = 32;   // output tile (TH = kEpfH)
+constexpr int kEpfThreads = 16 * kEpfH;  // two warps per 4-row band
 constexpr int kEpfGH = kEpfH + 8;       // guide rows: y0 - 4 .. y0 + 35
 constexpr int kEpfGBytes = 80;          // guide bytes x0 - 8 .. x0 + 71
 constexpr int kEpfGRow = kEpfGBytes;    // words per guide row (one per byte)
@@ -48,12 +44,15 @@ constexpr int kEpfTW = kEpfW + 24;
 constexpr int kEpfTS = kEpfTW;               // row stride in floats
 constexpr int kEpfTRow0 = 2, kEpfTCol0 = 9;  // tile index of (y0-3, x0-3)
 constexpr size_t kEpfGuideWords = size_t(3) * kEpfGPlane;
-constexpr size_t kEpfSmemBytes =
-    kEpfGuideWords * 4 + size_t(3) * kEpfTH * kEpfTS * 4;
-// Shared memory of k_epf_box with a tile of `th` rows.
+constexpr int kEpfAligned = kEpfGBytes / 4;  // aligned guide words per row
+// Shared memory of k_epf_box with a tile of `th` rows: the guide words (one
+// per byte offset), the input tile and the aligned guide words.
 constexpr size_t EpfSmemBytes(int th) {
-  return size_t(3) * (th + 8) * kEpfGRow * 4 + size_t(3) * (th + 10) * kEpfTS * 4;
+  return size_t(3) * (th + 8) * kEpfGRow * 4 +
+         size_t(3) * (th + 10) * kEpfTS * 4 +
+         size_t(3) * (th + 8) * kEpfAligned * 4;
 }
+constexpr size_t kEpfSmemBytes = EpfSmemBytes(kEpfH);
 
 // WeightFast (pik/epf_target.cc:304-428) as 4 integer operations:
 // ((int16(min(sad, 507) << 6) * mul) >> 16 + (127 << 7)) in the high half of
@@ -64,65 +63,88 @@ __device__ __forceinline__ float EpfWeight(int mul64, int sad) {
   return __uint_as_float((uint32_t(t) & 0xFFFF0000u) + 0x3F800000u);
 }
 
-// kFma: the weighted sums with fused multiply-adds (the tensor-core forms,
-// which are not bound to the reference's rounding); otherwise every product
-// and sum is rounded separately, as the reference does.
-// TH: tile rows (32 for frames; 8 for small images such as the DC image,
-// which would otherwise be a few CTAs of a full tile's latency each).
-template <bool kFma, int TH>
-__global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
-    k_epf_box(const float* in, const float* guide_src,
-              const uint8_t* guide_ovr, int gab, int w, int h,
-              const uint32_t* mm, const int32_t* sigma, float* out) {
-  constexpr int kH = TH, kGH = TH + 8, kTH = TH + 10;
-  constexpr int kGPlane = kGH * kEpfGRow, kThreads = 16 * TH;
-  constexpr size_t kGuideWords = size_t(3) * kGPlane;
-  extern __shared__ __align__(16) uint32_t epf_smem[];
-  uint32_t* sg = epf_smem;  // [3][kGH][kEpfGRow]
-  float(*tile)[kTH][kEpfTS] =
-      reinterpret_cast<float(*)[kTH][kEpfTS]>(epf_smem + kGuideWords);
-  const int x0 = blockIdx.x * kEpfW, y0 = blockIdx.y * kH;
-  const int tid = threadIdx.x;
-  constexpr int LC = kEpfLaneCols;
-  const int lane = tid & 31, wp = tid >> 5;
-  // 4-row band of the warp and its first column (tile-local).
-  const int band = wp / (2 / LC), col0 = 32 * (wp % (2 / LC));
+// The weight with the reference's cut-off (weights below 0.05 are 0) in
+// four integer operations. EpfWeight falls as the SAD grows (mul < 0), so
+// the cut-off is a SAD threshold `thr` per sigma (c_t.epf_thr); above it
+// the weight is `cap`: 0, or EpfWeight(507) when even the largest clamped
+// SAD keeps its weight (then thr = 507). For sad <= thr <= 507 the product
+// has no wrap and the clamp is the identity; larger SADs only select `cap`.
+struct EpfCut {
+  uint32_t thr;
+  float cap;
+};
+__device__ __forceinline__ EpfCut EpfCutOf(int sigma, int mul64) {
+  EpfCut k;
+  k.thr = uint32_t(c_t.epf_thr[sigma]);
+  k.cap = k.thr == 507u ? EpfWeight(mul64, 507) : 0.0f;
+  return k;
+}
+__device__ __forceinline__ float EpfCutWeight(int mul64, EpfCut k,
+                                              uint32_t sad) {
+  const uint32_t u = sad * uint32_t(mul64) + 0x3F800000u;
+  return sad <= k.thr ? __uint_as_float(u & 0xFFFF0000u) : k.cap;
+}
+
+// Sum of the absolute differences of the four bytes of a and b, plus c
+// (the accumulating form of __vsadu4).
+__device__ __forceinline__ uint32_t Sad4(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %3;"
+      : "=r"(d)
+      : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
+// The 3-row patch SADs of 4 pixel rows from 6 patch-row pairs (centre row
+// r against window row r): six byte-SADs (rows 1 + 2 and 3 + 4 accumulated
+// onto rows 2 and 3, rows 0 and 5 onto those pairs) and two adds, which
+// need not run on the integer ALU. c0: the first channel (no maximum).
+template <bool c0>
+__device__ __forceinline__ void PatchSads4(const uint32_t* rf,
+                                           const uint32_t* wd, uint32_t* sad) {
+  const uint32_t h2 = Sad4(rf[2], wd[2], 0u);
+  const uint32_t h3 = Sad4(rf[3], wd[3], 0u);
+  const uint32_t p12 = Sad4(rf[1], wd[1], h2);
+  const uint32_t p34 = Sad4(rf[4], wd[4], h3);
+  const uint32_t s0 = Sad4(rf[0], wd[0], p12);
+  const uint32_t s1 = p12 + h3;
+  const uint32_t s2 = p34 + h2;
+  const uint32_t s3 = Sad4(rf[5], wd[5], p34);
+  if (c0) {
+    sad[0] = s0, sad[1] = s1, sad[2] = s2, sad[3] = s3;
+  } else {
+    sad[0] = max(sad[0], s0), sad[1] = max(sad[1], s1);
+    sad[2] = max(sad[2], s2), sad[3] = max(sad[3], s3);
+  }
+}
+
+// Sigma of this thread's block in the tile at (x0, y0); 0 outside the image.
+__device__ __forceinline__ int EpfLaneSigma(const int32_t* sigma, int w, int h,
+                                            int x0, int y0) {
+  const int t = threadIdx.x;
+  const int px = x0 + (t & 31) + 32 * ((t >> 5) & 1), py0 = y0 + 4 * (t >> 6);
+  return px < w && py0 < h ? sigma[(py0 >> 3) * (w / 8) + (px >> 3)] : 0;
+}
+
+// Tiles whose halo lies inside the image take vector copies and no
+// mirroring; border tiles mirror every coordinate.
+template <int TH>
+__device__ __forceinline__ bool EpfInterior(int w, int h, int x0, int y0) {
+  return x0 >= 12 && x0 + kEpfW + 12 <= w && y0 >= 5 && y0 + TH + 5 <= h;
+}
+
+// Stages input rows y0 - 5 .. y0 + TH + 4, columns x0 - 12 .. x0 + 75 of
+// the three planes into `tile` by asynchronous copies: 16 bytes each for
+// interior tiles, 4 bytes per mirrored coordinate at the image border. The
+// caller commits them and waits.
+template <int TH>
+__device__ __forceinline__ void EpfStage(const float* in, int w, int h, int x0,
+                                         int y0,
+                                         float (*tile)[TH + 10][kEpfTS]) {
+  constexpr int kTH = TH + 10, kThreads = 16 * TH;
   const size_t plane = size_t(w) * h;
-  const int bw = w / 8;
-  const int py0 = y0 + 4 * band;  // first row; w and h are multiples of 8
-  bool inside[LC], filtered[LC], any_filtered = false;
-  int sig[LC];
-#pragma unroll
-  for (int i = 0; i < LC; ++i) {
-    const int px = x0 + lane + col0 + 32 * i;
-    inside[i] = px < w && py0 < h;
-    sig[i] = inside[i] ? sigma[(py0 >> 3) * bw + (px >> 3)] : 0;
-    filtered[i] = sig[i] >= kMinSigma;
-    any_filtered |= filtered[i];
-  }
-
-  // Tiles without filtered blocks are copies (CopyOriginalBlock).
-  if (!__syncthreads_or(any_filtered)) {
-#pragma unroll
-    for (int i = 0; i < LC; ++i) {
-      if (!inside[i]) continue;
-      const int px = x0 + lane + col0 + 32 * i;
-      for (int c = 0; c < 3; ++c)
-        for (int j = 0; j < 4; ++j) {
-          const size_t o = c * plane + size_t(py0 + j) * w + px;
-          out[o] = in[o];
-        }
-    }
-    return;
-  }
-
-  float amin, mul, stretch;
-  GuideParams(mm, &amin, &mul, &stretch);
-  // Tiles whose halo lies inside the image take vector loads and no
-  // mirroring; border tiles mirror every coordinate.
-  const bool interior = x0 >= 12 && x0 + kEpfW + 12 <= w && y0 >= 5 &&
-                        y0 + kH + 5 <= h;
-  if (interior) {
+  const int tid = threadIdx.x;
+  if (EpfInterior<TH>(w, h, x0, y0)) {
     constexpr int Q = kEpfTW / 4;
     for (int i = tid; i < 3 * kTH * Q; i += kThreads) {
       const int c = i / (kTH * Q);
@@ -130,17 +152,55 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
       CpAsync16(&tile[c][r][4 * q],
                 in + c * plane + size_t(y0 - 5 + r) * w + x0 - 12 + 4 * q);
     }
-    CpAsyncWaitAll();
   } else {
     for (int i = tid; i < 3 * kTH * kEpfTW; i += kThreads) {
       const int c = i / (kTH * kEpfTW);
       const int r = (i / kEpfTW) % kTH, col = i % kEpfTW;
       const int gx = x0 - 12 + col, gy = y0 - 5 + r;
-      tile[c][r][col] =
-          in[c * plane + size_t(MirrorIdx(gy, h)) * w + MirrorIdx(gx, w)];
+      CpAsync4(&tile[c][r][col],
+               in + c * plane + size_t(MirrorIdx(gy, h)) * w + MirrorIdx(gx, w));
     }
   }
-  if (gab) __syncthreads();  // the guide is computed from the tile
+}
+
+// Filters the staged tile at (x0, y0) into `out`. The tile's copies are
+// complete in every thread (the first barrier below publishes them); `sig`
+// is EpfLaneSigma of this thread; (amin, mul) quantise the guide
+// (GuideParams). `sa` holds the aligned guide words while the guide is
+// built. Returns after the tile's last barrier.
+//
+// kFma: the weighted sums with fused multiply-adds (the tensor-core forms,
+// which are not bound to the reference's rounding); otherwise every product
+// and sum is rounded separately, as the reference does.
+template <bool kFma, int TH>
+__device__ __forceinline__ void EpfFilterTile(
+    const float* guide_src, const uint8_t* guide_ovr, int gab, int w, int h,
+    float amin, float mul, int sig, float* out, uint32_t* sg, uint32_t* sa,
+    float (*tile)[TH + 10][kEpfTS], int x0, int y0) {
+  constexpr int kGH = TH + 8, kTH = TH + 10;
+  constexpr int kGPlane = kGH * kEpfGRow, kThreads = 16 * TH;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, wp = tid >> 5;
+  // 4-row band of the warp and its first column (tile-local).
+  const int band = wp >> 1, col0 = 32 * (wp & 1);
+  const size_t plane = size_t(w) * h;
+  const int px = x0 + lane + col0, py0 = y0 + 4 * band;
+  const bool inside = px < w && py0 < h;  // w and h are multiples of 8
+  const bool filtered = sig >= kMinSigma;
+  // Tile position of the pixel (px, py0).
+  const int tr0 = 4 * band + 3 + kEpfTRow0, tc0 = lane + col0 + 3 + kEpfTCol0;
+
+  // Tiles without filtered blocks are copies (CopyOriginalBlock).
+  if (!__syncthreads_or(filtered)) {
+    if (inside) {
+      for (int c = 0; c < 3; ++c)
+        for (int j = 0; j < 4; ++j)
+          out[c * plane + size_t(py0 + j) * w + px] = tile[c][tr0 + j][tc0];
+    }
+    return;
+  }
+
+  const bool interior = EpfInterior<TH>(w, h, x0, y0);
   const float* gw = c_t.gaborish[gab];
   auto quant = [&](float v) {
     return uint32_t(uint8_t(uint32_t(__float2int_rz((v - amin) * mul))));
@@ -161,11 +221,12 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
     return x2 * gw[2] + mul1;
   };
   // u8 guide (MakeGuide, pik/epf_target.cc:1009-1070): the aligned words
-  // (offsets 4 wd) first.
-  constexpr int kAligned = kEpfGBytes / 4;
+  // (bytes 4 wd .. 4 wd + 3 of a row) first, into `sa` (row-major, one
+  // row of kEpfAligned words per channel and guide row).
+  constexpr int kAligned = kEpfAligned;
   for (int i = tid; i < 3 * kGH * kAligned; i += kThreads) {
-    const int c = i / (kGH * kAligned);
-    const int r = (i / kAligned) % kGH, wd = i % kAligned;
+    const int cr = i / kAligned, wd = i - cr * kAligned;
+    const int c = cr / kGH, r = cr - c * kGH;
     const int gy = y0 - 4 + r;
     uint32_t word = 0;
     if (interior && !guide_ovr) {
@@ -217,66 +278,44 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
         word |= v << (8 * b);
       }
     }
-    sg[c * kGPlane + r * kEpfGRow + 4 * wd] = word;
+    sa[i] = word;
   }
   __syncthreads();
-  // The other offsets 4 wd + s, s = 1..3, from the two aligned neighbours
-  // (bytes past the row end read as 0).
-  for (int i = tid; i < 3 * kGH * kAligned * 3; i += kThreads) {
-    const int s = 1 + i % 3;
-    const int j = i / 3;
-    const int c = j / (kGH * kAligned);
-    const int r = (j / kAligned) % kGH, wd = j % kAligned;
-    const uint32_t* row = sg + c * kGPlane + r * kEpfGRow;
-    const uint32_t lo = row[4 * wd];
-    const uint32_t hi = wd + 1 < kAligned ? row[4 * wd + 4] : 0u;
-    sg[c * kGPlane + r * kEpfGRow + 4 * wd + s] =
-        __funnelshift_r(lo, hi, 8 * s);
+  // The words of offsets 4 wd .. 4 wd + 3 from the two aligned neighbours
+  // (bytes past the row end read as 0), one 16-byte store each.
+  for (int i = tid; i < 3 * kGH * kAligned; i += kThreads) {
+    const int cr = i / kAligned, wd = i - cr * kAligned;
+    const uint32_t lo = sa[i];
+    const uint32_t hi = wd + 1 < kAligned ? sa[i + 1] : 0u;
+    *reinterpret_cast<uint4*>(sg + cr * kEpfGRow + 4 * wd) =
+        make_uint4(lo, __funnelshift_r(lo, hi, 8), __funnelshift_r(lo, hi, 16),
+                   __funnelshift_r(lo, hi, 24));
   }
   __syncthreads();
 
   // Warps (half a block row of 8 blocks) without filtered blocks copy.
-  if (!__any_sync(0xFFFFFFFFu, any_filtered)) {
-#pragma unroll
-    for (int i = 0; i < LC; ++i) {
-      if (!inside[i]) continue;
-      const int px = x0 + lane + col0 + 32 * i;
+  if (!__any_sync(0xFFFFFFFFu, filtered)) {
+    if (inside) {
       for (int c = 0; c < 3; ++c)
         for (int j = 0; j < 4; ++j)
-          out[c * plane + size_t(py0 + j) * w + px] =
-              tile[c][4 * band + j + 3 + kEpfTRow0]
-                  [lane + col0 + 32 * i + 3 + kEpfTCol0];
+          out[c * plane + size_t(py0 + j) * w + px] = tile[c][tr0 + j][tc0];
     }
     return;
   }
-  int m64[LC];
-#pragma unroll
-  for (int i = 0; i < LC; ++i) {
-    m64[i] = c_t.mul_table[filtered[i] ? sig[i] : kMinSigma] * 64;
-  }
+  const int m64 = c_t.mul_table[filtered ? sig : kMinSigma] * 64;
+  const EpfCut cut = EpfCutOf(filtered ? sig : kMinSigma, m64);
 
-  // Centre patch rows: guide rows py0 - 1 .. py0 + 4, bytes px - 1 .. px + 2.
+  // Centre patch rows: guide rows py0 - 1 .. py0 + 4, bytes px - 1 .. px + 2
+  // (byte offset of px - 1 from x0 - 8).
   const int gr0 = 4 * band + 3;  // guide smem row of py0 - 1
-  uint32_t ref[3][6][LC];
-  {
-    // Byte offset of px - 1 from x0 - 8 (column i is 32 further).
-    const uint32_t* g = sg + gr0 * kEpfGRow + lane + col0 + 7;
+  const int gc0 = lane + col0 + 7;
+  float ws[3][4], sw[4];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int r = 0; r < 6; ++r)
-#pragma unroll
-        for (int i = 0; i < LC; ++i)
-          ref[c][r][i] = g[c * kGPlane + r * kEpfGRow + 32 * i];
+  for (int j = 0; j < 4; ++j) {
+    ws[0][j] = ws[1][j] = ws[2][j] = 0.f;
+    sw[j] = 0.f;
   }
-
-  float ws[3][4 * LC], sw[4 * LC];
-#pragma unroll
-  for (int p = 0; p < 4 * LC; ++p) {
-    ws[0][p] = ws[1][p] = ws[2][p] = 0.f;
-    sw[p] = 0.f;
-  }
-  if constexpr (kFma && LC == 1) {
+  if constexpr (kFma) {
     // Tensor-core forms: cx outermost. For one cx the 7 vertical offsets
     // read 12 distinct guide rows per channel (one load each), and each
     // staged input row serves every pixel of the lane it reaches: about
@@ -285,34 +324,27 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
     // forms are not bound to its rounding).
 #pragma unroll 1
     for (int cx = -3; cx <= 4; ++cx) {
-      const uint32_t* g = sg + (gr0 - 3) * kEpfGRow + lane + col0 + 7 + cx;
-      int sad[4][7];
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int k = 0; k < 7; ++k) sad[j][k] = 0;
+      const uint32_t* g = sg + (gr0 - 3) * kEpfGRow + gc0 + cx;
+      uint32_t sad[7][4];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         uint32_t wd[12];  // guide rows gr0 - 3 .. gr0 + 8 at this cx
 #pragma unroll
         for (int t = 0; t < 12; ++t) wd[t] = g[c * kGPlane + t * kEpfGRow];
         // The centre patch words again from shared memory (registers are
-        // the limit at two 512-thread CTAs per SM).
+        // the limit).
         uint32_t rf[6];
 #pragma unroll
         for (int r = 0; r < 6; ++r) {
-          rf[r] = sg[c * kGPlane + (gr0 + r) * kEpfGRow + lane + col0 + 7];
+          rf[r] = sg[c * kGPlane + (gr0 + r) * kEpfGRow + gc0];
         }
 #pragma unroll
         for (int k = 0; k < 7; ++k) {  // cy = k - 3: rows k .. k + 5
-          int hs[6];
-#pragma unroll
-          for (int r = 0; r < 6; ++r) hs[r] = int(__vsadu4(rf[r], wd[k + r]));
-          const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
-          sad[0][k] = max(sad[0][k], hs[0] + p12);
-          sad[1][k] = max(sad[1][k], p12 + hs[3]);
-          sad[2][k] = max(sad[2][k], hs[2] + p34);
-          sad[3][k] = max(sad[3][k], p34 + hs[5]);
+          if (c == 0) {
+            PatchSads4<true>(rf, wd + k, sad[k]);
+          } else {
+            PatchSads4<false>(rf, wd + k, sad[k]);
+          }
         }
       }
       float wt[4][7];
@@ -320,16 +352,15 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
       for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-          float wgt = EpfWeight(m64[0], sad[j][k]);
-          if (!(wgt >= 0.05f)) wgt = 0.0f;
+          const float wgt = EpfCutWeight(m64, cut, sad[k][j]);
           wt[j][k] = wgt;
           sw[j] += wgt;
         }
       // Input rows band + R - 3 (R = j + cy + 3 = 0..9) at column px + cx.
-      const int col = lane + col0 + 3 + cx + kEpfTCol0;
+      const int col = tc0 + cx;
 #pragma unroll
       for (int R = 0; R < 10; ++R) {
-        const int ir = 4 * band + R + kEpfTRow0;
+        const int ir = tr0 - 3 + R;
         const float v0 = tile[0][ir][col], v1 = tile[1][ir][col],
                     v2 = tile[2][ir][col];
 #pragma unroll
@@ -343,71 +374,77 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
       }
     }
   } else {
-  #pragma unroll 1
+    // The reference's order: cy-major, products and sums rounded separately.
+    uint32_t ref[3][6];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 6; ++r)
+        ref[c][r] = sg[c * kGPlane + (gr0 + r) * kEpfGRow + gc0];
+#pragma unroll 1
     for (int cy = -3; cy <= 3; ++cy) {
-  #pragma unroll 1
+#pragma unroll 1
       for (int cx = -3; cx <= 4; ++cx) {
-        // Window byte offset (column 0): the patch start moved by cx.
-        const uint32_t* g = sg + (gr0 + cy) * kEpfGRow + lane + col0 + 7 + cx;
-        int sad[4 * LC];  // [j * LC + i]
-  #pragma unroll
-        for (int p = 0; p < 4 * LC; ++p) sad[p] = 0;
-  #pragma unroll
+        // Window byte offset: the patch start moved by cx.
+        const uint32_t* g = sg + (gr0 + cy) * kEpfGRow + gc0 + cx;
+        uint32_t sad[4];
+#pragma unroll
         for (int c = 0; c < 3; ++c) {
-  #pragma unroll
-          for (int i = 0; i < LC; ++i) {
-            int hs[6];
-  #pragma unroll
-            for (int r = 0; r < 6; ++r) {
-              hs[r] = int(__vsadu4(
-                  ref[c][r][i], g[c * kGPlane + r * kEpfGRow + 32 * i]));
-            }
-            const int p12 = hs[1] + hs[2], p34 = hs[3] + hs[4];
-            sad[0 * LC + i] = max(sad[0 * LC + i], hs[0] + p12);
-            sad[1 * LC + i] = max(sad[1 * LC + i], p12 + hs[3]);
-            sad[2 * LC + i] = max(sad[2 * LC + i], hs[2] + p34);
-            sad[3 * LC + i] = max(sad[3 * LC + i], p34 + hs[5]);
+          uint32_t wd[6];
+#pragma unroll
+          for (int r = 0; r < 6; ++r) wd[r] = g[c * kGPlane + r * kEpfGRow];
+          if (c == 0) {
+            PatchSads4<true>(ref[c], wd, sad);
+          } else {
+            PatchSads4<false>(ref[c], wd, sad);
           }
         }
-  #pragma unroll
+        const int col = tc0 + cx;
+#pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const int ir = 4 * band + j + 3 + cy + kEpfTRow0;
-  #pragma unroll
-          for (int i = 0; i < LC; ++i) {
-            const int p = j * LC + i;
-            const int col = lane + col0 + 32 * i + 3 + cx + kEpfTCol0;
-            float wgt = EpfWeight(m64[i], sad[p]);
-            if (!(wgt >= 0.05f)) wgt = 0.0f;
-            if (kFma) {
-              ws[0][p] = fmaf(tile[0][ir][col], wgt, ws[0][p]);
-              ws[1][p] = fmaf(tile[1][ir][col], wgt, ws[1][p]);
-              ws[2][p] = fmaf(tile[2][ir][col], wgt, ws[2][p]);
-            } else {
-              ws[0][p] += tile[0][ir][col] * wgt;
-              ws[1][p] += tile[1][ir][col] * wgt;
-              ws[2][p] += tile[2][ir][col] * wgt;
-            }
-            sw[p] += wgt;
-          }
+          const int ir = tr0 + j + cy;
+          const float wgt = EpfCutWeight(m64, cut, sad[j]);
+          ws[0][j] += tile[0][ir][col] * wgt;
+          ws[1][j] += tile[1][ir][col] * wgt;
+          ws[2][j] += tile[2][ir][col] * wgt;
+          sw[j] += wgt;
         }
       }
     }
   }
+  if (!inside) return;
 #pragma unroll
-  for (int i = 0; i < LC; ++i) {
-    if (!inside[i]) continue;
-    const int px = x0 + lane + col0 + 32 * i;
+  for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int p = j * LC + i;
-        out[c * plane + size_t(py0 + j) * w + px] =
-            filtered[i] ? ws[c][p] / sw[p]
-                        : tile[c][4 * band + j + 3 + kEpfTRow0]
-                              [lane + col0 + 32 * i + 3 + kEpfTCol0];
-      }
-  }
+    for (int j = 0; j < 4; ++j) {
+      out[c * plane + size_t(py0 + j) * w + px] =
+          filtered ? ws[c][j] / sw[j] : tile[c][tr0 + j][tc0];
+    }
+}
+
+// One CTA per 64 x TH tile (1-D grid, row-major tile order). More CTAs
+// than resident slots balance the uneven tiles (copies, border tiles)
+// better than CTAs that loop over tiles.
+template <bool kFma, int TH>
+__global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
+    k_epf_box(const float* in, const float* guide_src,
+              const uint8_t* guide_ovr, int gab, int w, int h,
+              const uint32_t* mm, const int32_t* sigma, float* out) {
+  extern __shared__ __align__(16) uint32_t epf_smem[];
+  uint32_t* sg = epf_smem;  // [3][TH + 8][kEpfGRow]
+  auto* tile = reinterpret_cast<float(*)[TH + 10][kEpfTS]>(
+      epf_smem + 3 * (TH + 8) * kEpfGRow);
+  uint32_t* sa = epf_smem + 3 * (TH + 8) * kEpfGRow + 3 * (TH + 10) * kEpfTS;
+  const int tiles_x = (w + kEpfW - 1) / kEpfW;
+  const int x0 = (blockIdx.x % tiles_x) * kEpfW;
+  const int y0 = (blockIdx.x / tiles_x) * TH;
+  float amin, mul, stretch;
+  GuideParams(mm, &amin, &mul, &stretch);
+  const int sig = EpfLaneSigma(sigma, w, h, x0, y0);
+  EpfStage<TH>(in, w, h, x0, y0, tile);
+  CpAsyncWaitAll();
+  EpfFilterTile<kFma, TH>(guide_src, guide_ovr, gab, w, h, amin, mul, sig,
+                          out, sg, sa, tile, x0, y0);
 }
 
 }  // namespace pikgpu

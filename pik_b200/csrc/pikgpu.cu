@@ -369,10 +369,6 @@ int UploadTables(pikgpu_ctx* ctx) {
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(EpfSmemBytes(8))));
   CUDA_TRY(ctx, cudaFuncSetAttribute(
-                    k_epf_box<true, 32>,
-                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                    int(EpfSmemBytes(32))));
-  CUDA_TRY(ctx, cudaFuncSetAttribute(
                     k_epf_box<true, 16>,
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(EpfSmemBytes(16))));
@@ -423,26 +419,26 @@ int RunEpf(pikgpu_ctx* ctx, cudaStream_t st, const float* in,
       Blocks(w, kEpfW) * Blocks(h, kEpfH) < 2 * ctx->num_sms;
   const bool fma = ctx->form != PIKGPU_FORM_FP32;
   const uint32_t* mm = P<uint32_t>(ctx->mm);
+  // One CTA per 64 x th tile.
+  auto grid = [&](int th, int) { return Blocks(w, kEpfW) * Blocks(h, th); };
   if (small) {
-    dim3 grid(Blocks(w, kEpfW), Blocks(h, 8));
     if (fma) {
-      k_epf_box<true, 8><<<grid, 16 * 8, EpfSmemBytes(8), st>>>(
+      k_epf_box<true, 8><<<grid(8, 2), 16 * 8, EpfSmemBytes(8), st>>>(
           in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
     } else {
-      k_epf_box<false, 8><<<grid, 16 * 8, EpfSmemBytes(8), st>>>(
+      k_epf_box<false, 8><<<grid(8, 2), 16 * 8, EpfSmemBytes(8), st>>>(
           in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
     }
   } else {
     if (fma) {
       // 16-row tiles of 256 threads, three CTAs per SM: the cx-major loop
       // of these forms needs ~85 registers.
-      dim3 grid(Blocks(w, kEpfW), Blocks(h, 16));
-      k_epf_box<true, 16><<<grid, 16 * 16, EpfSmemBytes(16), st>>>(
+      k_epf_box<true, 16><<<grid(16, 3), 16 * 16, EpfSmemBytes(16), st>>>(
           in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
     } else {
-      dim3 grid(Blocks(w, kEpfW), Blocks(h, kEpfH));
-      k_epf_box<false, kEpfH><<<grid, kEpfThreads, kEpfSmemBytes, st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
+      k_epf_box<false, kEpfH><<<grid(kEpfH, 2), kEpfThreads, kEpfSmemBytes,
+                                st>>>(in, guide_src, guide_ovr, gab, w, h, mm,
+                                      sig, out);
     }
   }
   ++ctx->launches;

@@ -54,6 +54,12 @@ __device__ __forceinline__ void CpAsync16(void* smem, const void* gmem) {
                "l"(gmem)
                : "memory");
 }
+__device__ __forceinline__ void CpAsync4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                   uint32_t(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
 __device__ __forceinline__ void CpAsyncWaitAll() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" :::
                    "memory");

@@ -4,6 +4,7 @@
 
 #include <string.h>
 
+#include <algorithm>
 #include <cmath>
 
 namespace pikgpu {
@@ -204,6 +205,21 @@ void BuildTables(DevTables* t) {
       for (int i = 1; i < gap; ++i) {
         t->mul_table[sigma + i] = t->mul_table[sigma] + i * step;
       }
+    }
+    // The weight falls as the SAD grows: scan down from the clamp.
+    for (int sigma = 0; sigma < kMinSigma; ++sigma) t->epf_thr[sigma] = 507;
+    for (int sigma = kMinSigma; sigma <= kMaxSigma; ++sigma) {
+      const int m64 = t->mul_table[sigma] * 64;
+      auto w = [&](int sad) {
+        const uint32_t u =
+            (uint32_t(std::min(sad, 507) * m64) & 0xFFFF0000u) + 0x3F800000u;
+        float f;
+        memcpy(&f, &u, 4);
+        return f;
+      };
+      int thr = 507;
+      while (thr > 0 && !(w(thr) >= 0.05f)) --thr;
+      t->epf_thr[sigma] = thr;
     }
   }
   {

@@ -54,6 +54,9 @@ struct DevTables {
   // EPF: MulTable (pik/epf_target.cc:371-413), SigmaFromQuant LUTs
   // (pik/epf_target.cc:1160-1195).
   int mul_table[kMaxSigma + 1];
+  // Largest SAD whose weight (the device's EpfWeight of mul_table * 64) is
+  // at least 0.05, per sigma; 507 when every clamped SAD keeps its weight.
+  int epf_thr[kMaxSigma + 1];
   float sigma_lut[2][16];
   // sRGB TF_SRGB::EncodedFromDisplay polynomial (pik/color_management.cc:
   // 323-349): p[5], q[5].
