@@ -376,9 +376,6 @@ int UploadTables(pikgpu_ctx* ctx) {
                     k_epf_box<true, 8>,
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(EpfSmemBytes(8))));
-  CUDA_TRY(ctx, cudaFuncSetAttribute(
-                    k_final_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                    int(kFinSmemBytes)));
   if (ctx->device < 64) g_tables_uploaded[ctx->device] = true;
   return PIKGPU_OK;
 }
@@ -637,9 +634,9 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     const int gab = s.use_sharpened ? 0 : s.gaborish;
     k_minmax_init<<<1, 32, 0, st>>>(mm); ++ctx->launches;
     if (gab) {
-      dim3 gr(Blocks(g.PW, kTileW), Blocks(g.PH, kGabTileH), 3);
-      k_gaborish_tile<<<gr, kTileThreads, 0, st>>>(
-          f.idct, g.PW, g.PH, gab, nullptr, mm); ++ctx->launches;
+      const int warps = Blocks(g.PW, 128) * Blocks(g.PH, kGmmRows);
+      k_gaborish_minmax<<<dim3(Blocks(warps, 8), 3), 256, 0, st>>>(
+          f.idct, g.PW, g.PH, gab, mm); ++ctx->launches;
     } else {
       k_minmax<<<dim3(Blocks(npx, 256 * 8), 3), 256, 0, st>>>(f.idct, npx,
                                                                mm); ++ctx->launches;
@@ -730,11 +727,18 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   {
     const int vec_lin = lin && lin_stride % 4 == 0 && g.W % 4 == 0 &&
                         reinterpret_cast<uintptr_t>(lin) % 16 == 0;
-    dim3 gr(Blocks(g.W, kTileW), Blocks(g.H, kFinTileH));
-    k_final_tile<<<gr, kTileThreads, kFinSmemBytes, st>>>(
-        final_in, g.PW, g.PH, g.W, g.H, s.gaborish,
-        ctx->keep_stages ? P<float>(ctx->dbg_pre) : nullptr, lin, lin_stride,
-        vec_lin, rgb8, rgb8_stride); ++ctx->launches;
+    const int warps = Blocks(g.W, 128) * Blocks(g.H, kFinRows);
+    float* pre = ctx->keep_stages ? P<float>(ctx->dbg_pre) : nullptr;
+    if (s.gaborish) {
+      k_final_direct<true><<<Blocks(warps, 8), 256, 0, st>>>(
+          final_in, g.PW, g.PH, g.W, g.H, s.gaborish, pre, lin, lin_stride,
+          vec_lin, rgb8, rgb8_stride);
+    } else {
+      k_final_direct<false><<<Blocks(warps, 8), 256, 0, st>>>(
+          final_in, g.PW, g.PH, g.W, g.H, 0, pre, lin, lin_stride, vec_lin,
+          rgb8, rgb8_stride);
+    }
+    ++ctx->launches;
   }
   Mark(ctx, kNumTimed);
   CUDA_TRY(ctx, cudaGetLastError());

@@ -4,11 +4,12 @@
 //    smoothed values it needs), plus the plane's min/max (MinMax,
 //    pik/epf_target.cc:980-1006) for the EPF guide (skipped when `mm` is
 //    null);
-//  * k_final_tile: gaborish #2 (or a copy), ShrinkTo(xsize, ysize), XybToRgb
-//    (pik/opsin_inverse.cc:38-123) and optional sRGB-8
+//  * k_gaborish_minmax: the same min/max without staging (the frame path);
+//  * k_final_direct: gaborish #2 (or a copy), ShrinkTo(xsize, ysize),
+//    XybToRgb (pik/opsin_inverse.cc:38-123) and optional sRGB-8
 //    (pik/color_management.cc:323-345, pik/external_image.cc:1205).
 //
-// A CTA stages a 128 x TH output tile with its 1-pixel halo (rows y0 - 1 ..
+// k_gaborish_tile stages a 128 x TH output tile with its 1-pixel halo (rows y0 - 1 ..
 // y0 + TH, columns x0 - 4 .. x0 + 131, widened to 16-byte boundaries) in
 // shared memory: interior tiles with independent 128-bit loads (many in
 // flight per thread), border tiles with mirrored scalar loads. Each thread
@@ -25,8 +26,6 @@ namespace pikgpu {
 constexpr int kTileW = 128, kTileThreads = 256;
 constexpr int kTileSW = kTileW + 8;  // staged columns x0 - 4 .. x0 + 131
 constexpr int kGabTileH = 64;        // rows per CTA, min/max pass
-constexpr int kFinTileH = 16;        // rows per CTA, final pass (3 planes)
-constexpr size_t kFinSmemBytes = size_t(3) * (kFinTileH + 2) * kTileSW * 4;
 
 // Symmetric 3x3 stencil of output column i (0..3) from three 6-value rows
 // (columns x - 1 .. x + 4), in Sym3's operation order.
@@ -169,6 +168,93 @@ __global__ void __launch_bounds__(kTileThreads)
   }
 }
 
+// Min/max of gaborish #1 without staging or barriers: each warp owns 128
+// columns (4 per lane) of kGmmRows rows and loads its kGmmRows + 2 input
+// rows as independent 16-byte loads (all in flight at once); lanes take
+// their left/right neighbours from the adjacent lanes, lane 0 and the
+// warp's last lane by scalar loads. Coordinates mirror at the image border
+// and each output follows Sym3's operation order, so the min/max equal
+// those of k_gaborish_tile. Grid: (warps of a plane / 8, 3).
+constexpr int kGmmRows = 8;
+__global__ void __launch_bounds__(256)
+    k_gaborish_minmax(const float* in, int w, int h, int strength,
+                      uint32_t* mm) {
+  constexpr int R = kGmmRows;
+  __shared__ uint32_t s_lo[8], s_hi[8];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int c = blockIdx.y;
+  const int tiles_x = (w + 127) / 128;
+  const int wg = blockIdx.x * 8 + wib;
+  const int x0 = (wg % tiles_x) * 128, y0 = (wg / tiles_x) * R;
+  const int x = x0 + 4 * lane;
+  uint32_t lo = 0xFFFFFFFFu, hi = 0u;
+  if (y0 < h) {  // warp-uniform
+    const float* p = in + c * size_t(w) * h;
+    const bool xv = x < w;
+    // Lanes whose right neighbour is not in the next lane's registers.
+    const bool own_right = lane == 31 || x + 4 >= w;
+    const int xl = MirrorIdx(x0 - 1, w), xr = MirrorIdx(x + 4, w);
+    float4 q[R + 2];
+    float el[R + 2], er[R + 2];
+#pragma unroll
+    for (int r = 0; r < R + 2; ++r) {
+      const float* row = p + size_t(MirrorIdx(y0 - 1 + r, h)) * w;
+      q[r] = xv ? *reinterpret_cast<const float4*>(row + x)
+                : make_float4(0.f, 0.f, 0.f, 0.f);
+      el[r] = lane == 0 ? row[xl] : 0.f;
+      er[r] = own_right && xv ? row[xr] : 0.f;
+    }
+    const float* wt = c_t.gaborish[strength];
+    const float w0 = wt[0], w1 = wt[1], w2 = wt[2];
+    auto row6 = [&](int r, float v[6]) {
+      const float left = __shfl_up_sync(0xFFFFFFFFu, q[r].w, 1);
+      const float right = __shfl_down_sync(0xFFFFFFFFu, q[r].x, 1);
+      v[0] = lane == 0 ? el[r] : left;
+      v[1] = q[r].x, v[2] = q[r].y, v[3] = q[r].z, v[4] = q[r].w;
+      v[5] = own_right ? er[r] : right;
+    };
+    float a[6], m[6], b[6];
+    row6(0, a);
+    row6(1, m);
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      row6(j + 2, b);
+      if (xv) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const uint32_t ob = OrderedBits(Sym3Rows(a, m, b, i, w0, w1, w2));
+          lo = min(lo, ob);
+          hi = max(hi, ob);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        a[i] = m[i];
+        m[i] = b[i];
+      }
+    }
+  }
+  for (int off = 16; off; off >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, off));
+    hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, off));
+  }
+  if (lane == 0) {
+    s_lo[wib] = lo;
+    s_hi[wib] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < 8; ++i) {
+      lo = min(lo, s_lo[i]);
+      hi = max(hi, s_hi[i]);
+    }
+    if (lo <= hi) {
+      atomicMin(&mm[c], lo);
+      atomicMax(&mm[3 + c], hi);
+    }
+  }
+}
+
 // Opsin inverse of one pixel (XybToRgb), same operation order as before.
 __device__ __forceinline__ void XybToRgb(float x, float y, float b, float* r,
                                          float* g, float* bl) {
@@ -189,47 +275,74 @@ __device__ __forceinline__ void XybToRgb(float x, float y, float b, float* r,
   *bl = lb + tb;
 }
 
-// `vec_lin`: the linear outputs may be written as float4 (width, stride and
-// base all multiples of 4 floats / 16 bytes).
-__global__ void __launch_bounds__(kTileThreads)
-    k_final_tile(const float* in, int pw, int ph, int w, int h, int strength,
-                 float* pre, float* lin, size_t lin_stride, int vec_lin,
-                 uint8_t* rgb8, size_t rgb8_stride) {
-  constexpr int TH = kFinTileH, R = TH / 8;
-  extern __shared__ __align__(16) float fin_smem[];
-  float(*t)[TH + 2][kTileSW] =
-      reinterpret_cast<float(*)[TH + 2][kTileSW]>(fin_smem);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// The final pass without staging or barriers: each warp owns 128 columns x
+// kFinRows output rows of the three planes and loads its input rows
+// (kFinRows + 2 per plane with gaborish, kFinRows without) as independent
+// 16-byte loads up front;
+// horizontal neighbours come from the adjacent lanes, lane 0's and the
+// row's last lane's by scalar loads. Coordinates mirror at the padded
+// plane's border (pw x ph). `vec_lin`: the linear outputs may be written as
+// float4 (width, stride and base all multiples of 4 floats / 16 bytes).
+// Grid: warps / 8.
+constexpr int kFinRows = 2;
+template <bool kGab>
+__global__ void __launch_bounds__(256)
+    k_final_direct(const float* in, int pw, int ph, int w, int h,
+                   int strength, float* pre, float* lin, size_t lin_stride,
+                   int vec_lin, uint8_t* rgb8, size_t rgb8_stride) {
+  constexpr int R = kFinRows, NR = kGab ? R + 2 : R;
+  const int lane = threadIdx.x & 31;
+  const int wg = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int tiles_x = (w + 127) / 128;
+  const int x0 = (wg % tiles_x) * 128, y0 = (wg / tiles_x) * R;
+  if (y0 >= h) return;  // warp-uniform; no barriers below
   const size_t plane = size_t(pw) * ph;
-  const int x0 = blockIdx.x * kTileW, y0 = blockIdx.y * TH;
-  for (int c = 0; c < 3; ++c) {
-    StageTile<TH>(in + c * plane, pw, ph, x0, y0, t[c]);
-  }
-  CpAsyncWaitAll();
-  __syncthreads();
+  const int x = x0 + 4 * lane;
+  const bool xv = x < pw;
+  const bool own_right = lane == 31 || x + 4 >= pw;
+  const int xl = MirrorIdx(x0 - 1, pw), xr = MirrorIdx(x + 4, pw);
+  float4 q[3][NR];
+  float el[3][NR], er[3][NR];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      const int y = kGab ? y0 - 1 + r : y0 + r;
+      const float* row = in + c * plane + size_t(MirrorIdx(y, ph)) * pw;
+      q[c][r] = xv ? *reinterpret_cast<const float4*>(row + x)
+                   : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (kGab) {
+        el[c][r] = lane == 0 ? row[xl] : 0.f;
+        er[c][r] = own_right && xv ? row[xr] : 0.f;
+      }
+    }
   const float* wt = c_t.gaborish[strength];
   const float w0 = wt[0], w1 = wt[1], w2 = wt[2];
-  const int x = x0 + 4 * lane;
-#pragma unroll 2
+  auto row6 = [&](int c, int r, float v[6]) {
+    const float left = __shfl_up_sync(0xFFFFFFFFu, q[c][r].w, 1);
+    const float right = __shfl_down_sync(0xFFFFFFFFu, q[c][r].x, 1);
+    v[0] = lane == 0 ? el[c][r] : left;
+    v[1] = q[c][r].x, v[2] = q[c][r].y, v[3] = q[c][r].z, v[4] = q[c][r].w;
+    v[5] = own_right ? er[c][r] : right;
+  };
+#pragma unroll
   for (int j = 0; j < R; ++j) {
-    const int y = y0 + R * warp + j;
-    const int r0 = R * warp + j;  // staged row of y - 1
+    const int y = y0 + j;
     float v[3][4];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      if (strength) {
+      if (kGab) {
         float a[6], m[6], b[6];
-        TileRow6(t[c], r0, lane, a);
-        TileRow6(t[c], r0 + 1, lane, m);
-        TileRow6(t[c], r0 + 2, lane, b);
+        row6(c, j, a);
+        row6(c, j + 1, m);
+        row6(c, j + 2, b);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           v[c][i] = Sym3Rows(a, m, b, i, w0, w1, w2);
         }
       } else {
-        const float4 q =
-            *reinterpret_cast<const float4*>(&t[c][r0 + 1][4 + 4 * lane]);
-        v[c][0] = q.x, v[c][1] = q.y, v[c][2] = q.z, v[c][3] = q.w;
+        v[c][0] = q[c][j].x, v[c][1] = q[c][j].y;
+        v[c][2] = q[c][j].z, v[c][3] = q[c][j].w;
       }
     }
     if (x >= w || y >= h) continue;
