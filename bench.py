@@ -623,7 +623,7 @@ def main():
     # DRAM bytes per launch of the 4K workload measured with ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum, one cold launch each).
     ncu_traffic_4k = {
-        "epf": 155.10e6 + 68.46e6,
+        "epf": 100.09e6 + 65.80e6,
         "gaborish1_minmax": 99.54e6 + 64.64e6,
         "gaborish2_opsin_srgb": 99.55e6 + 63.85e6,
     }
