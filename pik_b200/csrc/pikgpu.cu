@@ -591,12 +591,14 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     }
     if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
       const int items = (n[kC16] + 7) / 8;
-      const int grid = std::min(items, ctx->num_sms * ctx->tc_ctas_per_sm);
+      // One channel per CTA: up to 2 tc_ctas_per_sm CTAs per SM.
+      const int grid =
+          std::min(3 * items, ctx->num_sms * 2 * ctx->tc_ctas_per_sm);
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
-        k_square_idct_tc<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
+        k_square_idct_tc1<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
       } else {
-        k_square_idct_tc<16, 3><<<grid, tc::kThreads, 0, cls(kC16)>>>(
+        k_square_idct_tc1<16, 3><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
       }
       ++ctx->launches;

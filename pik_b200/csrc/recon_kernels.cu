@@ -1633,12 +1633,12 @@ template __global__ void k_square_idct_rows<16>(Geo, DevFrame,
                                                 const uint32_t*, int, int);
 template __global__ void k_square_idct_rows<32>(Geo, DevFrame,
                                                 const uint32_t*, int, int);
-template __global__ void k_square_idct_tc<16, 2>(Geo, DevFrame,
-                                                 const uint32_t*, int, int,
-                                                 int*);
-template __global__ void k_square_idct_tc<16, 3>(Geo, DevFrame,
-                                                 const uint32_t*, int, int,
-                                                 int*);
+template __global__ void k_square_idct_tc1<16, 2>(Geo, DevFrame,
+                                                  const uint32_t*, int, int,
+                                                  int*);
+template __global__ void k_square_idct_tc1<16, 3>(Geo, DevFrame,
+                                                  const uint32_t*, int, int,
+                                                  int*);
 template __global__ void k_square_ar_tc<16, 2>(Geo, DevFrame, FrameScalars,
                                                const uint32_t*, const int*,
                                                int*);

@@ -116,6 +116,18 @@ void BuildTables(DevTables* t) {
       t->ub4[1][k] = o1;
       t->ub4[2][k] = o2;
     }
+    const float* b16 = t->dct + MatOffset(16);
+    for (int k = 0; k < 4; ++k)
+      for (int m = 0; m < 6; ++m) {
+        double acc = 0.0;
+        for (int x = 0; x < 16; ++x) {
+          const int i = m - x / 4;
+          if (i >= 0 && i <= 2) {
+            acc += double(b16[k * 16 + x]) * double(t->ub4[i][x % 4]);
+          }
+        }
+        t->hf_corner16[k][m] = float(acc);
+      }
   }
   t->lf_blur[0] = 0.41459272584128337f;
   t->lf_blur[1] = 0.25489157325704559f;

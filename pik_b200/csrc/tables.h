@@ -42,6 +42,11 @@ struct DevTables {
   float lines_inv[9][8][8];
   // UpSample4x4BlurDCT kernel (pik/ac_predictions.cc:234-254).
   float ub4[3][4];
+  // HF prediction corner of a 16x16 block: hf_corner16[k][m] = sum over x of
+  // dct16[k][x] * ub4[m - x / 4][x % 4] (taps 0..2), so that the 4x4 corner
+  // of the 2-D DCT of the upsampled prediction is C * Pred * C^T with Pred
+  // the block's 6x6 window of 2x2-cell values.
+  float hf_corner16[4][6];
   // LFPredictionBlur (pik/ac_predictions.cc:120-133) w0, w1, w2.
   float lf_blur[3];
   // Gaborish weights per strength 1..4 (pik/gaborish.cc:16-88): w0, w1, w2.

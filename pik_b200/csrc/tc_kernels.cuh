@@ -159,7 +159,6 @@ struct Smem {
   alignas(128) uint8_t a[3][S * kOpBytes];
   alignas(128) uint8_t idct[S * kMatBytes];
   alignas(128) uint8_t dct[S * kMatBytes];
-  float corner[128][N / 4 + 1];  // HF prediction: 2 N/8 corner rows per row
   alignas(8) uint64_t mbar;
   uint32_t tmem;
 };
@@ -243,175 +242,76 @@ __device__ __forceinline__ void PutMatrix(uint8_t* base, const float* m) {
   }
 }
 
-}  // namespace tc
-
-// UpsampleRow with fused multiply-adds (the tensor-core forms are not
-// bound to the reference's rounding of every product).
-template <int N>
-__device__ __forceinline__ void UpsampleRowFma(const float* pred, int X0,
-                                               int Y, float* out) {
-  const int r = Y >> 2, q0 = X0 >> 2, iy = Y & 3;
-  constexpr int W = N / 4 + 2;
-  float src[3][W];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const float* row = pred + (r + j + 1) * kG2 + q0 + 1;
-#pragma unroll
-    for (int i = 0; i < W; ++i) src[j][i] = row[i];
-  }
-  const float v0 = c_t.ub4[0][iy], v1 = c_t.ub4[1][iy], v2 = c_t.ub4[2][iy];
-#pragma unroll
-  for (int x = 0; x < N; ++x) {
-    const int q = x >> 2, ix = x & 3;
-    const float h0 = c_t.ub4[0][ix], h1 = c_t.ub4[1][ix], h2 = c_t.ub4[2][ix];
-    float bx[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      bx[j] = fmaf(src[j][q + 2], h2,
-                   fmaf(src[j][q + 1], h1, src[j][q] * h0));
-    }
-    out[x] = fmaf(bx[2], v2, fmaf(bx[1], v1, bx[0] * v0));
-  }
-}
-
-// HF prediction + AddBlockExceptLFAndLLFTo + IDCT for square DCT blocks on
-// the tensor cores (split-BF16 form of k_square_idct_rows). Persistent CTAs
-// of 128 threads; an item is a batch of 128 / N blocks in all three
-// channels (one MMA wait per pass for the three).
+// One-channel operands: a CTA transforms one channel of a batch (the
+// channels of a block are independent in the IDCT), so a thread holds a
+// third of the registers of the three-channel kernels and more CTAs share
+// an SM, each with its own MMA round trips.
 template <int N, int S>
-__global__ void __launch_bounds__(tc::kThreads, 4)
-    k_square_idct_tc(Geo g, DevFrame f, const uint32_t* list, int count,
-                     int predict_hf, int* err) {
-  using namespace tc;
-  using square::CoefRowOffset;
-  constexpr int BPB = 128 / N;  // blocks per batch
-  constexpr int cov = N / 8;
-  __shared__ Smem<N, S> s;
-  const int t = threadIdx.x, bl = t / N, r = t % N;
-  if (t < 32) {
-    asm volatile(
-        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
-            "r"(SmemU32(&s.tmem)),
-        "r"(kTmemCols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  if (t == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
-        SmemU32(&s.mbar)));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  PutMatrix<N, S>(s.idct, c_t.idct + MatOffset(N));
-  PutMatrix<N, S>(s.dct, c_t.dct + MatOffset(N));
-  FenceBefore();
-  __syncthreads();
-  FenceAfter();
-  uint32_t phase = 0;
-  const int nbat = (count + BPB - 1) / BPB;
-  const size_t plane_ac = size_t(g.ac_stride) * g.By;
-  const size_t plane_px = size_t(g.PW) * g.PH;
-  const float inv_nn = 1.0f / float(N * N);
-  bool ok = true;
-  for (int batch = blockIdx.x; batch < nbat && ok; batch += gridDim.x) {
-    const int idx = batch * BPB + bl;
-    const bool active = idx < count;
-    const uint32_t pkd = list[active ? idx : 0];
-    const int bx = pkd & 0xFFFF, by = pkd >> 16;
-    float X[3][N];
+struct Smem1 {
+  static constexpr int kOpBytes = 128 * N * 2;
+  static constexpr int kMatBytes = N * N * 2;
+  alignas(128) uint8_t a[S * kOpBytes];
+  alignas(128) uint8_t idct[S * kMatBytes];
+  float win[128 / N][36];  // HF prediction: each block's 6x6 cell window
+  alignas(8) uint64_t mbar;
+  uint32_t tmem;
+};
+constexpr int kTmemCols1 = 32;  // 2 accumulators x N = 16
+
+// This thread's row of D (N FP32 columns from dcol).
+template <int N, int S>
+__device__ __forceinline__ void LoadRow1(const Smem1<N, S>& s, uint32_t dcol,
+                                         float* v) {
+  const uint32_t lane_base = (threadIdx.x & ~31u) << 16;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float* crow = f.ac + c * plane_ac + CoefRowOffset(g, bx, by, N, r);
-#pragma unroll
-      for (int i = 0; i < N; i += 4) {
-        const float4 v = active ? *reinterpret_cast<const float4*>(crow + i)
-                                : make_float4(0.f, 0.f, 0.f, 0.f);
-        X[c][i] = v.x, X[c][i + 1] = v.y, X[c][i + 2] = v.z,
-        X[c][i + 3] = v.w;
-      }
-    }
-    // HF prediction: adding the predicted coefficients outside the
-    // 2cov x 2cov corner and transforming back equals transforming the
-    // coefficients minus that corner of DCT(P) and adding P (IDCT(DCT(P))
-    // = P), so only the corner is computed: per channel, the corner rows of
-    // the row DCT of this pixel row, then the column sums over the block's
-    // N rows (lanes) by shuffles.
-    float P[3][N];
-    bool hf = false;
-    if (predict_hf) {
-      hf = active && PredictHFOf(f.acs[by * g.Bx + bx] >> 4);
-      const int gi = (by >> 6) * g.Gx + (bx >> 6);
-      const int X0 = (bx & 63) * 8, Y = (by & 63) * 8 + r;
-      constexpr int K = 2 * cov;
-      const float* B = c_t.dct + MatOffset(N);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
-        if (hf) {
-          UpsampleRowFma<N>(pred, X0, Y, P[c]);
-        } else {
-#pragma unroll
-          for (int x = 0; x < N; ++x) P[c][x] = 0.f;
-        }
-        // Corner rows of the row DCT of this pixel row, shared with the
-        // block's other rows (the block's N rows are N lanes of one warp).
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          float a = 0.f;
-#pragma unroll
-          for (int x = 0; x < N; ++x) a = fmaf(B[k * N + x], P[c][x], a);
-          s.corner[t][k] = a;
-        }
-        __syncwarp();
-        if (hf && r < K) {
-#pragma unroll
-          for (int l = 0; l < K; ++l) {
-            float v = 0.f;
-#pragma unroll
-            for (int y = 0; y < N; ++y) {
-              v = fmaf(B[l * N + y], s.corner[N * bl + y][r], v);
-            }
-            X[c][l] -= v * inv_nn;
-          }
-        }
-        __syncwarp();
-      }
-    }
-    float T[N];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) PutRowK<N, S>(s.a[c], t, X[c]);
-    ok = Pass<N, S>(s, 0, false, s.idct, phase) && ok;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      LoadRow<N, S>(s, AccCol<N>(c, 0), T);  // T[k = r][v]
-      PutColMN<N, S>(s.a[c], N * bl, r, T);
-    }
-    ok = Pass<N, S>(s, 1, true, s.idct, phase) && ok;
-    ok = __syncthreads_and(ok);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      LoadRow<N, S>(s, AccCol<N>(c, 1), T);  // pixel row v = r
-      if (hf) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) T[i] += P[c][i];
-      }
-      if (active && ok) {
-        float* out = f.idct + c * plane_px + size_t(by * 8 + r) * g.PW + bx * 8;
-#pragma unroll
-        for (int i = 0; i < N; i += 4) {
-          *reinterpret_cast<float4*>(out + i) =
-              make_float4(T[i], T[i + 1], T[i + 2], T[i + 3]);
-        }
-      }
-    }
-  }
-  if (!ok && t == 0) atomicExch(err, 1);
-  FenceBefore();
-  __syncthreads();
-  if (t < 32) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
-                     s.tmem),
-                 "r"(kTmemCols));
-  }
+  for (int c = 0; c < N; c += 16) Ld16(s.tmem + lane_base + dcol + c, v + c);
 }
+
+// One split-BF16 GEMM pass of the CTA's channel: D(j) = A * B^T over K = N
+// (tensor-memory columns j N ..), then waits for it (bounded).
+template <int N, int S>
+__device__ __forceinline__ bool Pass1(Smem1<N, S>& s, int j, bool a_mn,
+                                      const uint8_t* b, uint32_t& phase) {
+  using Sm = Smem1<N, S>;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  FenceBefore();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    FenceAfter();
+    const uint32_t idesc = Idesc(128, N, a_mn ? 1 : 0);
+    constexpr uint32_t sbo = (N / 8) * 128;
+    constexpr int kPairs = S == 2 ? 3 : 6;
+    constexpr int pi[6] = {0, 0, 1, 0, 2, 1};
+    constexpr int pk[6] = {0, 1, 0, 2, 0, 1};
+    const uint32_t d = s.tmem + uint32_t(j * N);
+#pragma unroll
+    for (int kk = 0; kk < N / 16; ++kk) {
+#pragma unroll
+      for (int p = 0; p < kPairs; ++p) {
+        Mma(d, Desc(s.a + pi[p] * Sm::kOpBytes + kk * 256, 128, sbo),
+            Desc(b + pk[p] * Sm::kMatBytes + kk * 256, 128, sbo), idesc,
+            (kk > 0 || p > 0) ? 1u : 0u);
+      }
+    }
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster."
+        "b64 [%0];" ::"r"(SmemU32(&s.mbar))
+        : "memory");
+  }
+  const uint32_t mb = SmemU32(&s.mbar);
+  bool ok = false;
+  for (uint32_t it = 0; it < kMaxPolls; ++it) {
+    if (TryWait(mb, phase)) {
+      ok = true;
+      break;
+    }
+  }
+  phase ^= 1u;
+  FenceAfter();
+  return ok;
+}
+
+}  // namespace tc
 
 // AdaptiveReconstruction clamp for square DCT blocks on the tensor cores
 // (split-BF16 form of k_square_ar_rows, pik/adaptive_reconstruction.cc:
@@ -457,6 +357,21 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
     const uint32_t pkd = list[active ? idx : 0];
     const int bx = pkd & 0xFFFF, by = pkd >> 16;
     const size_t row0 = size_t(by * 8 + r) * g.PW + bx * 8;
+    // The block's clamp intervals (a chain of dependent table loads) are
+    // looked up first, so that the loads resolve during the DCT passes. The
+    // class holds only DCT16X16 blocks.
+    static_assert(N == 16, "the class of this kernel is DCT16X16");
+    constexpr int type = kDCT16X16;
+    const int qac = f.qf[by * g.Bx + bx];
+    const float inv_quant_ac =
+        ClampInvQuantAc(g, f, sc.inv_global_scale, bx, by, qac);
+    const int cf = f.dq_cf[(by >> 3) * g.Tx + (bx >> 3)];
+    const int table = f.dq_map[cf * 256 + (qac - 1)];
+    uint32_t dm_off[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      dm_off[c] = f.offsets[(table * 7 + QuantKindOf(type)) * 3 + c] + r * N;
+    }
     float T[N];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -488,25 +403,33 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
     }
     // Clamp ratios of coefficient row k = r, minimum over the channels.
     {
-      const int type = f.acs[by * g.Bx + bx] >> 4;
-      const int qac = f.qf[by * g.Bx + bx];
-      const float inv_quant_ac =
-          ClampInvQuantAc(g, f, sc.inv_global_scale, bx, by, qac);
-      const int cf = f.dq_cf[(by >> 3) * g.Tx + (bx >> 3)];
-      const int table = f.dq_map[cf * 256 + (qac - 1)];
-      const int kind = QuantKindOf(type);
       const float* dm[3];
+      bool dm_vec = true;  // rows 16-byte aligned: float4 loads
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        dm[c] = f.table + f.offsets[(table * 7 + kind) * 3 + c] + r * N;
+        dm[c] = f.table + dm_off[c];
+        dm_vec = dm_vec && (reinterpret_cast<uintptr_t>(dm[c]) & 15) == 0;
       }
       const size_t tape_row = CoefOffset(g, bx, by, cov, r * N);
       uint8_t* tape =
           f.clamp_tape && active ? f.clamp_tape + tape_row : nullptr;
       const uint8_t* tin =
           f.clamp_tape_in && active ? f.clamp_tape_in + tape_row : nullptr;
+      float dq[3][4];  // dm[c][l0 .. l0 + 3]
 #pragma unroll
       for (int l = 0; l < N; ++l) {
+        if ((l & 3) == 0) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            if (dm_vec) {
+              const float4 q = *reinterpret_cast<const float4*>(dm[c] + l);
+              dq[c][0] = q.x, dq[c][1] = q.y, dq[c][2] = q.z, dq[c][3] = q.w;
+            } else {
+#pragma unroll
+              for (int e = 0; e < 4; ++e) dq[c][e] = dm[c][l + e];
+            }
+          }
+        }
         const bool llf = r < cov && l < cov;
         const float ls = llf ? LlfScale(type, l, r) : 0.f;
         float mr = 1.0f, rt[3];
@@ -514,7 +437,7 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           rt[c] = ClampRatio(
-              Y[c][l], llf ? ls * sc.mul_dc[c] : dm[c][l] * inv_quant_ac);
+              Y[c][l], llf ? ls * sc.mul_dc[c] : dq[c][l & 3] * inv_quant_ac);
           if (rt[c] < mr) mr = rt[c], arg = c;
         }
         uint8_t code = arg < 0 ? 0 : mr == 0.0f ? 4 : uint8_t(arg + 1);
@@ -559,6 +482,164 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
                      s.tmem),
                  "r"(kTmemCols));
+  }
+}
+
+// HF prediction + AddBlockExceptLFAndLLFTo + IDCT for 16x16 DCT blocks on
+// the tensor cores (split-BF16 form of k_square_idct_rows). Persistent CTAs
+// of 128 threads; an item is one channel of a batch of 128 / N blocks
+// ((batch, channel) pairs, batch-major; the channels of a block are
+// independent here). A thread holds one row of one channel, so eight CTAs
+// share an SM, each with its own MMA round trips; the next item's
+// coefficient row is loaded while this item's passes run.
+template <int N, int S>
+__global__ void __launch_bounds__(tc::kThreads, 8)
+    k_square_idct_tc1(Geo g, DevFrame f, const uint32_t* list, int count,
+                      int predict_hf, int* err) {
+  using namespace tc;
+  using square::CoefRowOffset;
+  static_assert(N == 16, "the HF corner table is for 16x16 blocks");
+  constexpr int BPB = 128 / N;  // blocks per batch
+  constexpr int cov = N / 8;
+  __shared__ Smem1<N, S> s;
+  const int t = threadIdx.x, bl = t / N, r = t % N;
+  if (t < 32) {
+    asm volatile(
+        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
+            "r"(SmemU32(&s.tmem)),
+        "r"(kTmemCols1));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
+        SmemU32(&s.mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  PutMatrix<N, S>(s.idct, c_t.idct + MatOffset(N));
+  FenceBefore();
+  __syncthreads();
+  FenceAfter();
+  uint32_t phase = 0;
+  const int nbat = (count + BPB - 1) / BPB;
+  const int nitems = 3 * nbat;
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
+  const size_t plane_px = size_t(g.PW) * g.PH;
+  const float inv_nn = 1.0f / float(N * N);
+  float cr[6];  // this lane's row of the HF corner table (rows r < 4)
+#pragma unroll
+  for (int m = 0; m < 6; ++m) cr[m] = c_t.hf_corner16[r & 3][m];
+  bool ok = true;
+  // The next item's coefficient row is loaded while this item's passes
+  // run (the CTAs of an SM otherwise wait for their loads in step).
+  float X[N];
+  auto load_row = [&](int it) {
+    const int bt = it / 3, ch = it - 3 * bt;
+    const int i = bt * BPB + bl;
+    const uint32_t pk = list[i < count ? i : 0];
+    const float* crow = f.ac + ch * plane_ac +
+                        CoefRowOffset(g, pk & 0xFFFF, pk >> 16, N, r);
+#pragma unroll
+    for (int j = 0; j < N; j += 4) {
+      const float4 v = i < count ? *reinterpret_cast<const float4*>(crow + j)
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+      X[j] = v.x, X[j + 1] = v.y, X[j + 2] = v.z, X[j + 3] = v.w;
+    }
+    return pk;
+  };
+  uint32_t pkd_next = blockIdx.x < nitems ? load_row(blockIdx.x) : 0u;
+  for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+    const int batch = item / 3, c = item - 3 * batch;
+    const int idx = batch * BPB + bl;
+    const bool active = idx < count;
+    const uint32_t pkd = pkd_next;
+    const int bx = pkd & 0xFFFF, by = pkd >> 16;
+    // HF prediction: adding the predicted coefficients outside the
+    // 2cov x 2cov corner and transforming back equals transforming the
+    // coefficients minus that corner of DCT(P) and adding P (IDCT(DCT(P))
+    // = P). The upsampled prediction P of this pixel row is the 3-tap
+    // vertical blend of three rows of the 2x2-cell grid (6 columns), then
+    // the 3-tap horizontal blend; its DCT corner is C Pred C^T over the
+    // block's 6x6 cell window (C = hf_corner16), of which lanes r < 4
+    // subtract row r. The class holds only DCT16X16 blocks, which predict
+    // HF. The block's 16 lanes first stage its 6x6 cell window in shared
+    // memory (up to three loads per lane instead of 18 to 54 scalar loads
+    // of cells that the lanes share).
+    float P[N];
+    const bool hf = active && predict_hf;
+    if (predict_hf) {
+      const int gi = (by >> 6) * g.Gx + (bx >> 6);
+      const int rb = (by & 63) * 2, q0 = (bx & 63) * 2;
+      const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2 +
+                          (rb + 1) * kG2 + q0 + 1;
+      for (int e = r; e < 36; e += N) s.win[bl][e] = pred[(e / 6) * kG2 + e % 6];
+      __syncwarp();
+    }
+    if (hf) {
+      const float* w = s.win[bl];
+      const int iy = r & 3;
+      const float* w0 = w + (r >> 2) * 6;
+      const float v0 = c_t.ub4[0][iy], v1 = c_t.ub4[1][iy],
+                  v2 = c_t.ub4[2][iy];
+      float col[6];
+#pragma unroll
+      for (int m = 0; m < 6; ++m) {
+        col[m] = fmaf(w0[12 + m], v2, fmaf(w0[6 + m], v1, w0[m] * v0));
+      }
+#pragma unroll
+      for (int x = 0; x < N; ++x) {
+        const int q = x >> 2, ix = x & 3;
+        P[x] = fmaf(col[q + 2], c_t.ub4[2][ix],
+                    fmaf(col[q + 1], c_t.ub4[1][ix], col[q] * c_t.ub4[0][ix]));
+      }
+      if (r < 2 * cov) {
+        float u[6];
+#pragma unroll
+        for (int rho = 0; rho < 6; ++rho) {
+          float a = 0.f;
+#pragma unroll
+          for (int m = 0; m < 6; ++m) a = fmaf(w[rho * 6 + m], cr[m], a);
+          u[rho] = a;
+        }
+#pragma unroll
+        for (int l = 0; l < 2 * cov; ++l) {
+          float v = 0.f;
+#pragma unroll
+          for (int rho = 0; rho < 6; ++rho) {
+            v = fmaf(c_t.hf_corner16[l][rho], u[rho], v);
+          }
+          X[l] -= v * inv_nn;
+        }
+      }
+    }
+    float T[N];
+    PutRowK<N, S>(s.a, t, X);
+    if (item + int(gridDim.x) < nitems) pkd_next = load_row(item + gridDim.x);
+    ok = Pass1<N, S>(s, 0, false, s.idct, phase) && ok;
+    LoadRow1<N, S>(s, 0, T);  // T[k = r][v]
+    PutColMN<N, S>(s.a, N * bl, r, T);
+    ok = Pass1<N, S>(s, 1, true, s.idct, phase) && ok;
+    ok = __syncthreads_and(ok);
+    LoadRow1<N, S>(s, N, T);  // pixel row v = r
+    if (hf) {
+#pragma unroll
+      for (int i = 0; i < N; ++i) T[i] += P[i];
+    }
+    if (active && ok) {
+      float* out = f.idct + c * plane_px + size_t(by * 8 + r) * g.PW + bx * 8;
+#pragma unroll
+      for (int i = 0; i < N; i += 4) {
+        *reinterpret_cast<float4*>(out + i) =
+            make_float4(T[i], T[i + 1], T[i + 2], T[i + 3]);
+      }
+    }
+  }
+  if (!ok && t == 0) atomicExch(err, 1);
+  FenceBefore();
+  __syncthreads();
+  if (t < 32) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
+                     s.tmem),
+                 "r"(kTmemCols1));
   }
 }
 
