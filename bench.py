@@ -428,6 +428,220 @@ def adjoint_main(args):
         }))
 
 
+def c5_frame(xsize=8192, ysize=8192, seed=5):
+    """The memory-bound roofline case: an 8192x8192 frame at distance 0.5
+    with every block size, gaborish and EPF on, and 1% of the area in
+    highlights at 4x linear light (pik_b200.synthetic.make_highlight_frame).
+    A synthetic frame stands in for the reference encoder's output: encoding
+    67 MP with butteraugli iterations takes hours on the host."""
+    from pik_b200 import synthetic
+    return synthetic.make_highlight_frame(xsize, ysize, seed=seed)
+
+
+def c5_main(args):
+    """Achieved HBM GB/s of the 8192x8192 reconstruction (FP32 linear planes
+    out, 805 MB) in the split-BF16 and plain FP32 forms: 18.28 algorithmic
+    bytes per pixel x pixels / device time per frame, inputs resident."""
+    import torch
+    import torch.distributed as dist
+    from pik_b200 import native
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    frame = c5_frame()
+    px = frame.xsize * frame.ysize
+    by, bx = frame.blocks
+    import ctypes
+    ac_dev = torch.from_numpy(frame.quantized_ac).to(dev)
+    planes = (ctypes.c_void_p * 3)(*[ac_dev[c].data_ptr() for c in range(3)])
+    stream = torch.cuda.Stream(device=dev)
+    outs = {}
+
+    def time_form(form, sample_clocks=False):
+        ctx = native.Context(local, form=form)
+        ctx.begin(frame)
+        ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
+        lin = torch.empty((3, frame.ysize, frame.xsize), dtype=torch.float32,
+                          device=dev)
+
+        def step():
+            ctx._check(ctx.L.pikgpu_frame_set_ac_device(ctx.h, planes,
+                                                        bx * 64))
+            ctx.reconstruct_device(lin.data_ptr(), frame.xsize)
+
+        for _ in range(max(3, args.warmup)):
+            step()
+        n_launch = ctx.L.pikgpu_last_launch_count(ctx.h)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        clk = ClockSampler(local) if sample_clocks else None
+        if clk:
+            clk.__enter__()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if clk:
+            clk.__exit__()
+        t = e0.elapsed_time(e1) / args.steps
+        if ws > 1:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        ctx.close()
+        outs[form] = lin
+        return t, n_launch, clk
+
+    ms, launches, clk = time_form(args.form, sample_clocks=True)
+    forms = {args.form: ms}
+    for form in ("fp32", "split_bf16"):
+        if form not in forms:
+            forms[form] = time_form(form)[0]
+    # The forms against each other on the [0, 1] scale (value / 255).
+    diff = None
+    if "fp32" in outs and args.form != "fp32":
+        d = (outs[args.form] - outs["fp32"]).abs_() / 255.0
+        diff = {"max_abs": float(d.max().item()),
+                "frac_above_2e-5": float((d > 2e-5).float().mean().item())}
+        del d
+    outs.clear()
+
+    # Per-kernel-group device times of the headline form.
+    pctx = native.Context(local, profile=True, form=args.form)
+    pctx.begin(frame)
+    pctx.L.pikgpu_set_stream(pctx.h, stream.cuda_stream)
+    pctx._check(pctx.L.pikgpu_frame_set_ac_device(pctx.h, planes, bx * 64))
+    lin = torch.empty((3, frame.ysize, frame.xsize), dtype=torch.float32,
+                      device=dev)
+    acc = {}
+    for i in range(3 + args.steps):
+        pctx.reconstruct_device(lin.data_ptr(), frame.xsize)
+        if i >= 3:
+            for k, v in pctx.kernel_times().items():
+                acc[k] = acc.get(k, 0.0) + v / args.steps
+    pctx.close()
+    del lin
+
+    # End to end through the C ABI: one context, blocking calls, int16 AC
+    # and side information up from pinned host memory, FP32 planes back.
+    from pik_b200 import abi
+    ctx = native.Context(local, form=args.form)
+    ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
+    pin_ac = torch.from_numpy(frame.quantized_ac).pin_memory()
+    pin_lin = torch.empty((3, frame.ysize, frame.xsize),
+                          dtype=torch.float32).pin_memory()
+    ac_planes = (ctypes.c_void_p * 3)(*[pin_ac[c].data_ptr()
+                                        for c in range(3)])
+    lin_planes = (ctypes.c_void_p * 3)(*[pin_lin[c].data_ptr()
+                                         for c in range(3)])
+    packed = abi.PackedFrame(frame)
+    h2d = frame.quantized_ac.nbytes + sum(a.nbytes for a in
+                                          packed.arrays.values())
+    d2h = pin_lin.numel() * 4
+
+    def e2e_step():
+        ctx._check(ctx.L.pikgpu_frame_begin(ctx.h, packed.ref))
+        ctx._check(ctx.L.pikgpu_frame_set_ac(ctx.h, ac_planes, bx * 64))
+        ctx._check(ctx.L.pikgpu_reconstruct(ctx.h, lin_planes, frame.xsize,
+                                            None, 0, 0))
+
+    for _ in range(max(3, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    ctx.close()
+
+    # CPU: the FP32 oracle restatement (one host thread) on a bounded
+    # sample, a 4096x4096 frame from the same generator settings.
+    cpu = None
+    if rank == 0:
+        try:
+            from oracle import oraclepy
+            sample = c5_frame(4096, 4096)
+            t0 = time.perf_counter()
+            oraclepy.run(sample, want=("linear",))
+            cpu_s = time.perf_counter() - t0
+            cpu = {"value": round(sample.xsize * sample.ysize / cpu_s / 1e6,
+                                  3),
+                   "unit": "MP/s", "cores": 1, "kind": "port",
+                   "sample": "one FP32 oracle reconstruction of a 4096x4096 "
+                             "frame with the same generator settings"}
+        except Exception as e:  # oracle library not built on this host
+            cpu = {"unavailable": str(e)[:200]}
+
+    peak, peak_kind = load_peaks()
+    gbs = {f: PATH_BYTES_PER_PX * px / (t * 1e-3) / 1e9
+           for f, t in forms.items()}
+    top = max(acc, key=acc.get)
+    group_bytes = {"epf": 36, "ar_clamp": 36, "hf_idct": 24,
+                   "gaborish1_minmax": 24, "gaborish2_opsin_srgb": 24,
+                   "dequant_ac_lf_update": 18}
+    achieved = group_bytes.get(top, 12) * px / (acc[top] * 1e-3) / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": "achieved HBM GB/s of the 8192x8192 reconstruction "
+                      "(18.28 algorithmic B/px x px / frame time)",
+            "value": round(ws * gbs[args.form], 1), "unit": "GB/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "c5_8k: 8192x8192 synthetic frame, "
+                       "distance 0.5, 1% highlights at 4x, every block "
+                       "size, gaborish + EPF on, FP32 linear planes out "
+                       "(805 MB)",
+                       "form": FORM_NAMES[args.form],
+                       "l2": "working set > L2 (inputs 403 MB, planes "
+                             "805 MB each)",
+                       "parallelism": f"replicas x{ws}"},
+            "megapixels_per_s": round(ws * px / (ms * 1e-3) / 1e6, 1),
+            "roofline": {"bound": "hbm", "kernel": top,
+                         "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": None, "peak_kind": peak_kind,
+                         "path_achieved": round(gbs[args.form], 1),
+                         "path_frac": round(gbs[args.form] / peak, 4)},
+            "forms": {f: {"GB/s": round(gbs[f], 1),
+                          "MP/s": round(px / (t * 1e-3) / 1e6, 1),
+                          "ms_per_step": round(t, 4)}
+                      for f, t in forms.items()},
+            "speedup_vs_fp32": round(forms["fp32"] / ms, 3),
+            "form_vs_fp32": diff,
+            "kernel_ms": {k: round(v, 4) for k, v in acc.items()},
+            "e2e": {"value": round(ws * PATH_BYTES_PER_PX * px /
+                                   (e2e_ms * 1e-3) / 1e9, 1),
+                    "unit": "GB/s",
+                    "megapixels_per_s": round(ws * px / (e2e_ms * 1e-3)
+                                              / 1e6, 1),
+                    "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h),
+                    "mode": "one context, blocking pikgpu_reconstruct"},
+            "gpu_launches": launches * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -437,7 +651,7 @@ def main():
     ap.add_argument("--form", default="split_bf16",
                     choices=sorted(FORM_NAMES))
     ap.add_argument("--workload", default="c2_4k",
-                    choices=["c2_4k", "batch64", "adjoint1k"])
+                    choices=["c2_4k", "batch64", "adjoint1k", "c5_8k"])
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -445,6 +659,8 @@ def main():
         return batch_main(args)
     if args.workload == "adjoint1k":
         return adjoint_main(args)
+    if args.workload == "c5_8k":
+        return c5_main(args)
 
     import torch
     import torch.distributed as dist

@@ -1,6 +1,6 @@
 """Seeded synthetic workloads for the reconstruction path.
 
-Two generators:
+Three generators:
 
 * ``make_image`` -- the test-image generator the benchmark configurations are
   defined with: a sum of random 2-D sinusoids (period 4..64 px, random
@@ -16,6 +16,9 @@ Two generators:
   butteraugli distance ~1. It lets the benchmark build 4K/8K inputs on the
   GPU host without running an encoder; its statistics are documented in
   the design notes and compared against real encoder output in the tests.
+
+* ``make_highlight_frame`` -- ``make_frame`` at a lower distance (finer
+  quant field, larger AC) with a share of the area in highlights.
 """
 
 from __future__ import annotations
@@ -24,7 +27,8 @@ import numpy as np
 
 from . import layout
 
-__all__ = ["make_image", "make_frame", "srgb8_to_linear255"]
+__all__ = ["make_image", "make_frame", "make_highlight_frame",
+           "srgb8_to_linear255"]
 
 
 def make_image(xsize: int, ysize: int, *, seed: int = 0, sinusoids: int = 6,
@@ -76,7 +80,8 @@ def make_frame(xsize: int, ysize: int, *, seed: int = 0,
                shares: dict | None = None, have_ar: bool = True,
                gaborish: int = 2, global_scale: int = 3065,
                quant_dc: int = 16, qf_median: float = 18.0,
-               qf_spread: float = 0.3, ac_scale: float = 1.0) -> "layout.Frame":
+               qf_spread: float = 0.3, ac_scale: float = 1.0,
+               qf_max: int = 31) -> "layout.Frame":
     """Synthetic decoded frame of ``xsize`` x ``ysize`` pixels.
 
     Defaults follow the reference encoder on the generator images at
@@ -84,6 +89,7 @@ def make_frame(xsize: int, ysize: int, *, seed: int = 0,
     log-normal around 18 (5th-95th percentile ~11-25), quantized DC of
     X ~ -10 +- 20, Y ~ 240 +- 48, B ~ 0 +- 27, and sparse AC whose mean
     magnitude falls off with frequency (Y dominant, X and B ~10x smaller).
+    The raw quant field is clipped to [6, qf_max].
     """
     rng = np.random.default_rng(seed)
     shares = dict(_DEFAULT_SHARES if shares is None else shares)
@@ -129,7 +135,7 @@ def make_frame(xsize: int, ysize: int, *, seed: int = 0,
 
     qf = qf_median * np.exp(smooth((by, bx), 8, qf_spread) +
                             rng.normal(0.0, 0.08, size=(by, bx)))
-    raw_qf = np.clip(np.round(qf), 6, 31).astype(np.int32)
+    raw_qf = np.clip(np.round(qf), 6, qf_max).astype(np.int32)
     layout.broadcast_first_block(acs, raw_qf)
     lut = np.zeros((by, bx), dtype=np.uint8)
 
@@ -168,3 +174,36 @@ def make_frame(xsize: int, ysize: int, *, seed: int = 0,
         quant_dc=quant_dc, ytox_dc=130, ytob_dc=120, ytox_map=ytox,
         ytob_map=ytob, ac_strategy=acs, raw_quant_field=raw_qf,
         ar_sigma_lut_ids=lut, quantized_dc=dc, quantized_ac=ac)
+
+
+def make_highlight_frame(xsize: int, ysize: int, *, seed: int = 0,
+                         distance: float = 0.5, highlight_share: float = 0.01,
+                         highlight_gain: float = 4.0) -> "layout.Frame":
+    """Synthetic frame of a high-quality encode with highlights.
+
+    ``make_frame`` at ``distance``: the quant field scales with 1 / distance
+    (clipped to [6, 64]) and the AC magnitudes with 1 / distance. Random
+    axis-aligned rectangles cover ``highlight_share`` of the blocks; their
+    light is ``highlight_gain`` x the rest, which in the cube-root XYB domain
+    scales their quantized Y DC and their AC by highlight_gain^(1/3).
+    """
+    f = make_frame(xsize, ysize, seed=seed, qf_median=18.0 / distance,
+                   ac_scale=1.0 / distance, qf_max=64)
+    by, bx = f.blocks
+    rng = np.random.default_rng(seed)
+    mask = np.zeros((by, bx), bool)
+    target = max(1, int(highlight_share * by * bx))
+    while mask.sum() < target:
+        h = min(by, int(rng.integers(2, max(3, by // 32))))
+        w = min(bx, int(rng.integers(2, max(3, bx // 32))))
+        y0 = int(rng.integers(0, by - h + 1))
+        x0 = int(rng.integers(0, bx - w + 1))
+        mask[y0:y0 + h, x0:x0 + w] = True
+    gain = highlight_gain ** (1.0 / 3.0)
+    f.quantized_dc[1][mask] = np.clip(
+        np.round(f.quantized_dc[1][mask] * gain), -2000, 2000)
+    acm = np.repeat(mask, 64, axis=1)
+    for c in range(3):
+        f.quantized_ac[c][acm] = np.clip(
+            np.round(f.quantized_ac[c][acm] * gain), -2000, 2000)
+    return f

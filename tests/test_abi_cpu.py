@@ -112,3 +112,22 @@ def test_frame_save_load_roundtrip(tmp_path):
               "quantized_dc", "ytox_map"):
         np.testing.assert_array_equal(getattr(f, k), getattr(g, k))
     assert g.global_scale == f.global_scale and g.xsize == f.xsize
+
+
+@pytest.mark.parametrize("size", [(1, 1), (13, 7), (300, 200), (1030, 530)])
+def test_highlight_frame_generator(size):
+    """The high-quality highlight frames of the 8192x8192 workload: valid at
+    the ABI, quant field within [6, 64], the highlight share reached, and
+    deterministic for a seed."""
+    w, h = size
+    f = synthetic.make_highlight_frame(w, h, seed=5)
+    assert native.validate(f)[0] == 0
+    assert f.raw_quant_field.min() >= 6 and f.raw_quant_field.max() <= 64
+    base = synthetic.make_frame(w, h, seed=5, qf_median=36.0, ac_scale=2.0,
+                                qf_max=64)
+    changed = (f.quantized_dc[1] != base.quantized_dc[1]).mean()
+    if f.raw_quant_field.size >= 400:  # else one 2x2 rectangle is > 1%
+        assert changed <= 0.05
+    g = synthetic.make_highlight_frame(w, h, seed=5)
+    np.testing.assert_array_equal(f.quantized_ac, g.quantized_ac)
+    np.testing.assert_array_equal(f.quantized_dc, g.quantized_dc)
