@@ -1,0 +1,53 @@
+"""The oracle against the reference compiled from its own sources, run live
+on fresh bitstreams. CPU only.
+
+Generator images of ragged sizes are encoded by the reference encoder at
+distances 0.5 to 3, which gives mixed blocks, adaptive quant fields, CfL and
+the EPF. The reference's scalar build decodes each bitstream to the
+reconstruction boundary and runs its own stages on it. The FP32
+restatement must then give:
+- DC and the dequantised AC bit for bit;
+- IDCT and the gaborish guide source within 2e-6;
+- linear output within 2e-5 on the [0,1] scale (reference value / 255),
+  given the reference's EPF decisions (u8 guide, per-block sigma).
+
+With its own decisions, only rounding-boundary flips of the u8 guide are
+allowed (the guide sources agree to 2e-6). They are at most 2e-4 of the
+guide bytes, and no per-block sigma flips."""
+
+import numpy as np
+import pytest
+
+from oracle import decisions, oraclepy, refpy
+from pik_b200 import synthetic
+
+pytestmark = pytest.mark.skipif(
+    not (oraclepy.available() and refpy.available("scalar")
+         and refpy.available("avx2")),
+    reason="oracle or reference build (oracle/_ref) not built")
+
+CASES = [(200, 136, 0.5, 1), (333, 201, 2.0, 2), (129, 67, 3.0, 3),
+         (520, 72, 1.0, 4)]
+
+
+@pytest.mark.parametrize("w,h,distance,seed", CASES)
+def test_oracle_matches_live_reference(w, h, distance, seed):
+    img = synthetic.srgb8_to_linear255(synthetic.make_image(w, h, seed=seed))
+    bs = refpy.encode(img, distance, flavour="avx2")
+    fz = refpy.Frozen(bs, flavour="scalar")
+    stages = ("dc", "dequant_ac", "idct", "smoothed", "linear")
+    ref, _ = fz.run_stages(threads=1, want=stages)
+    frame = fz.frame()
+    assert frame.have_ar
+    o = oraclepy.run(frame, precision=32, want=stages, export_decisions=True)
+    np.testing.assert_array_equal(o["dc"], ref["dc"])
+    np.testing.assert_array_equal(o["dequant_ac"], ref["dequant_ac"])
+    assert np.abs(o["idct"] - ref["idct"]).max() <= 2e-6
+    assert np.abs(o["smoothed"] - ref["smoothed"]).max() <= 2e-6
+    g, s = decisions.frame_decisions(ref["smoothed"], frame.raw_quant_field,
+                                     frame.ac_strategy,
+                                     frame.ar_sigma_lut_ids)
+    np.testing.assert_array_equal(o["sigma"], s)
+    assert (o["guide"] != g).mean() <= 2e-4
+    o2 = oraclepy.run(frame, precision=32, want=("linear",), guide=g, sigma=s)
+    assert np.abs(o2["linear"] - ref["linear"]).max() / 255 <= 2e-5
