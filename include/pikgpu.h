@@ -134,8 +134,12 @@ int pikgpu_frame_set_ac(pikgpu_ctx* ctx, const int16_t* const planes[3],
 
 /* Same for one 512x512 group (group_index = gy * ceil(xsize/512) + gx),
  * i.e. what DecodeFromBitstream decodes for that group
- * (pik/compressed_image.cc:720-813). Groups may be supplied from different
- * host threads concurrently; each writes a disjoint staging region. */
+ * (pik/compressed_image.cc:720-813), as pik's group threads do
+ * (pik/pik_frame.cc:1108-1135). Groups may be supplied from different host
+ * threads concurrently: each call copies into its own region of the
+ * context's device AC buffer, on the context's stream, from the calling
+ * thread (with the context's device made current there). No other call on
+ * the context may run while such uploads are in progress. */
 int pikgpu_frame_set_group_ac(pikgpu_ctx* ctx, uint32_t group_index,
                               const int16_t* const planes[3], size_t stride);
 

@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -71,8 +72,13 @@ struct pikgpu_ctx {
   int device = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  // Last error message; Fail() may run on several host threads at once
+  // (concurrent pikgpu_frame_set_group_ac calls).
   std::string err;
-  bool have_frame = false, have_ac = false, have_result = false;
+  std::mutex err_mu;
+  bool have_frame = false, have_result = false;
+  // Set by every AC upload; group uploads may run on several host threads.
+  std::atomic<bool> have_ac{false};
   bool keep_stages = false, profile = false;
   int form = PIKGPU_FORM_FP32;
   Geo g{};
@@ -158,7 +164,10 @@ int Fail(pikgpu_ctx* ctx, int code, const char* fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
-  if (ctx) ctx->err = buf;
+  if (ctx) {
+    std::lock_guard<std::mutex> lock(ctx->err_mu);
+    ctx->err = buf;
+  }
   return code;
 }
 
@@ -1113,6 +1122,9 @@ int pikgpu_frame_set_ac(pikgpu_ctx* ctx, const int16_t* const planes[3],
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
   PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
+  // The copies go to the context's stream from the caller's thread, whose
+  // current device may be another one.
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   if (!planes || stride < size_t(ctx->g.ac_stride)) {
     return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "bad AC planes/stride");
   }
@@ -1133,6 +1145,9 @@ int pikgpu_frame_set_group_ac(pikgpu_ctx* ctx, uint32_t group_index,
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
   PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
+  // The copies go to the context's stream from the caller's thread, whose
+  // current device may be another one.
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   const Geo& g = ctx->g;
   if (group_index >= uint32_t(g.Gx * g.Gy)) {
     return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "group %u of %d", group_index,
@@ -1160,6 +1175,9 @@ int pikgpu_frame_set_ac_device(pikgpu_ctx* ctx, const int16_t* const planes[3],
   if (!ctx) return PIKGPU_ERR_INVALID_ARG;
   PIKGPU_NOT_PENDING(ctx);
   if (!ctx->have_frame) return Fail(ctx, PIKGPU_ERR_STATE, "no frame");
+  // The copies go to the context's stream from the caller's thread, whose
+  // current device may be another one.
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   if (!planes || stride < size_t(ctx->g.ac_stride)) {
     return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "bad AC planes/stride");
   }

@@ -143,6 +143,32 @@ def test_group_upload_matches_frame_upload():
     np.testing.assert_array_equal(lin, whole)
 
 
+def test_group_uploads_from_concurrent_threads():
+    """Groups uploaded from several host threads at once, as pik's group
+    threads decode them (pik/pik_frame.cc:1108-1135), give the same frame
+    as one whole-frame upload. ctypes releases the GIL during each call, so
+    the uploads overlap."""
+    from concurrent.futures import ThreadPoolExecutor
+    frame = synthetic.make_frame(2100, 1100, seed=6)
+    whole = run_gpu(frame, keep=False)["linear"]
+    gx = -(-frame.xsize // 512)
+    parts = []
+    for gi in range(frame.num_groups):
+        x0, y0 = (gi % gx) * 64, (gi // gx) * 64
+        parts.append(np.ascontiguousarray(
+            frame.quantized_ac[:, y0:y0 + 64, x0 * 64:(x0 + 64) * 64]))
+    ctx = native.Context(0)
+    try:
+        ctx.begin(frame)
+        with ThreadPoolExecutor(max_workers=8) as pool:
+            list(pool.map(lambda gi: ctx.set_group_ac(gi, parts[gi]),
+                          range(frame.num_groups)))
+        lin, _ = ctx.reconstruct(linear=True)
+    finally:
+        ctx.close()
+    np.testing.assert_array_equal(lin, whole)
+
+
 def test_errors_leave_context_usable():
     frame = synthetic.make_frame(64, 64, seed=1)
     ctx = native.Context(0)
