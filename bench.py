@@ -138,6 +138,21 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(value: float, device) -> float:
+    """The maximum of a per-rank time over all ranks of the process group
+    (the value itself with one rank or no group). Every rank must call it at
+    the same point."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return value
+    if dist.get_world_size() == 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def reference_arm(args):
     """The reference's CPU reconstruction on the same frame."""
     ws, rank, _ = dist_env()
@@ -491,10 +506,7 @@ def c5_main(args):
         if clk:
             clk.__exit__()
         t = e0.elapsed_time(e1) / args.steps
-        if ws > 1:
-            tt = torch.tensor([t], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(t, dev)
         ctx.close()
         outs[form] = lin
         return t, n_launch, clk
@@ -562,10 +574,7 @@ def c5_main(args):
         e2e_step()
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dev)
     ctx.close()
 
     # CPU: the FP32 oracle restatement (one host thread) on a bounded
@@ -713,10 +722,7 @@ def main():
         if clk:
             clk.__exit__()
         t = start.elapsed_time(end) / args.steps
-        if ws > 1:
-            tt = torch.tensor([t], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(t, dev)
         ctx.close()
         return t, n_launch, clk
 
@@ -778,10 +784,7 @@ def main():
         e2e_step()
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dev)
     e2e_blocking = ws * px / (e2e_ms * 1e-3) / 1e6
     ctx.close()
 
@@ -815,10 +818,7 @@ def main():
     for c in ctxs:
         c.wait()
     stream_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if ws > 1:
-        t = torch.tensor([stream_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        stream_ms = float(t.item())
+    stream_ms = max_over_ranks(stream_ms, dev)
     e2e = ws * px / (stream_ms * 1e-3) / 1e6
     for c in ctxs:
         c.close()
