@@ -223,9 +223,10 @@ def cpu_baseline(frame_px):
 def batch_frames(n=64):
     """The 64-image batch: image sides drawn uniformly from 256..2048 px
     (independently per axis) and distances from 0.5..3.0, seeds 0..63.
-    Synthetic frames of those sizes (pik_b200.synthetic, calibrated to the
-    reference encoder's frames at distance 1; the quant field scales with
-    1 / distance) stand in for reference-encoded images."""
+    Synthetic frames of those sizes (pik_b200.synthetic: scalars and quant
+    field set from the reference encoder's frames at distance 1, the quant
+    field scaled with 1 / distance, a broad transform mix) stand in for
+    reference-encoded images."""
     from pik_b200 import synthetic
     rng = np.random.default_rng(2024)
     frames = []

@@ -14,8 +14,12 @@ Three generators:
   ids, colour-correlation maps, quantized DC and AC), drawn from seeded
   distributions shaped like the reference encoder's output at
   butteraugli distance ~1. It lets the benchmark build 4K/8K inputs on the
-  GPU host without running an encoder; its statistics are documented in
-  the design notes and compared against real encoder output in the tests.
+  GPU host without running an encoder. Its global scale and quant_dc equal
+  the reference encoder's on the generator images at distance 1, and its
+  quant-field and DC distributions are close to them (quant field median
+  18 against 15, Y DC mean 240 against 253). Its AC is sparser (3.6% of
+  the Y coefficients non-zero against 11%), and its transform mix is
+  broader (see _DEFAULT_SHARES).
 
 * ``make_highlight_frame`` -- ``make_frame`` at a lower distance (finer
   quant field, larger AC) with a share of the area in highlights.
