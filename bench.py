@@ -444,14 +444,26 @@ def adjoint_main(args):
         }))
 
 
-def c5_frame(xsize=8192, ysize=8192, seed=5):
+C5_MIXES = {
+    "broad": "every transform type (36% DCT8, 22% DCT16X16, 18% DCT32X32, "
+             "the rest small types)",
+    "encoder": "the reference encoder's mix at distance 0.5 (72% DCT16X16, "
+               "22% DCT32X32, 5% DCT8)",
+}
+
+
+def c5_frame(xsize=8192, ysize=8192, seed=5, mix="broad"):
     """The memory-bound roofline case: an 8192x8192 frame at distance 0.5
-    with every block size, gaborish and EPF on, and 1% of the area in
-    highlights at 4x linear light (pik_b200.synthetic.make_highlight_frame).
-    A synthetic frame stands in for the reference encoder's output: encoding
-    67 MP with butteraugli iterations takes hours on the host."""
+    with gaborish and EPF on, and 1% of the area in highlights at 4x linear
+    light (pik_b200.synthetic.make_highlight_frame). `mix` "broad" gives
+    every block type a real share; "encoder" takes the shares the reference
+    encoder picks at distance 0.5. A synthetic frame stands in for the
+    reference encoder's output: encoding 67 MP with butteraugli iterations
+    takes hours on the host."""
     from pik_b200 import synthetic
-    return synthetic.make_highlight_frame(xsize, ysize, seed=seed)
+    shares = synthetic.ENCODER_SHARES_D05 if mix == "encoder" else None
+    return synthetic.make_highlight_frame(xsize, ysize, seed=seed,
+                                          shares=shares)
 
 
 def c5_main(args):
@@ -466,7 +478,7 @@ def c5_main(args):
     if ws > 1:
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    frame = c5_frame()
+    frame = c5_frame(mix=args.mix)
     px = frame.xsize * frame.ysize
     by, bx = frame.blocks
     import ctypes
@@ -584,7 +596,7 @@ def c5_main(args):
     if rank == 0:
         try:
             from oracle import oraclepy
-            sample = c5_frame(4096, 4096)
+            sample = c5_frame(4096, 4096, mix=args.mix)
             t0 = time.perf_counter()
             oraclepy.run(sample, want=("linear",))
             cpu_s = time.perf_counter() - t0
@@ -614,9 +626,9 @@ def c5_main(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "c5_8k: 8192x8192 synthetic frame, "
-                       "distance 0.5, 1% highlights at 4x, every block "
-                       "size, gaborish + EPF on, FP32 linear planes out "
-                       "(805 MB)",
+                       "distance 0.5, 1% highlights at 4x, gaborish + EPF "
+                       "on, FP32 linear planes out (805 MB)",
+                       "mix": C5_MIXES[args.mix],
                        "form": FORM_NAMES[args.form],
                        "l2": "working set > L2 (inputs 403 MB, planes "
                              "805 MB each)",
@@ -662,6 +674,8 @@ def main():
                     choices=sorted(FORM_NAMES))
     ap.add_argument("--workload", default="c2_4k",
                     choices=["c2_4k", "batch64", "adjoint1k", "c5_8k"])
+    ap.add_argument("--mix", default="broad", choices=sorted(C5_MIXES),
+                    help="transform mix of the c5_8k frame")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

@@ -183,9 +183,19 @@ def make_frame(xsize: int, ysize: int, *, seed: int = 0,
         ar_sigma_lut_ids=lut, quantized_dc=dc, quantized_ac=ac)
 
 
+# Shares of 8x8 cells per transform type that the reference encoder picks
+# on the generator images (12 sinusoids, 20 rectangles, noise sigma 3,
+# 1024x1024) at distance 0.5.
+ENCODER_SHARES_D05 = {
+    "DCT16X16": 0.7231, "DCT32X32": 0.2217, "DCT": 0.0528, "DCT4X4": 0.0012,
+    "DCT2X2": 0.0012,
+}
+
+
 def make_highlight_frame(xsize: int, ysize: int, *, seed: int = 0,
                          distance: float = 0.5, highlight_share: float = 0.01,
-                         highlight_gain: float = 4.0) -> "layout.Frame":
+                         highlight_gain: float = 4.0,
+                         shares: dict | None = None) -> "layout.Frame":
     """Synthetic frame of a high-quality encode with highlights.
 
     ``make_frame`` at ``distance``: the quant field scales with 1 / distance
@@ -193,9 +203,10 @@ def make_highlight_frame(xsize: int, ysize: int, *, seed: int = 0,
     axis-aligned rectangles cover ``highlight_share`` of the blocks; their
     light is ``highlight_gain`` x the rest, which in the cube-root XYB domain
     scales their quantized Y DC and their AC by highlight_gain^(1/3).
+    ``shares`` is the transform mix (make_frame's default if None).
     """
     f = make_frame(xsize, ysize, seed=seed, qf_median=18.0 / distance,
-                   ac_scale=1.0 / distance, qf_max=64)
+                   ac_scale=1.0 / distance, qf_max=64, shares=shares)
     by, bx = f.blocks
     rng = np.random.default_rng(seed)
     mask = np.zeros((by, bx), bool)

@@ -131,3 +131,16 @@ def test_highlight_frame_generator(size):
     g = synthetic.make_highlight_frame(w, h, seed=5)
     np.testing.assert_array_equal(f.quantized_ac, g.quantized_ac)
     np.testing.assert_array_equal(f.quantized_dc, g.quantized_dc)
+
+
+def test_highlight_frame_encoder_mix():
+    """The reference encoder's distance-0.5 transform mix, as the 8192x8192
+    workload's `--mix encoder` uses it: valid at the ABI and within 0.02 of
+    the target shares."""
+    f = synthetic.make_highlight_frame(
+        1030, 530, seed=5, shares=synthetic.ENCODER_SHARES_D05)
+    assert native.validate(f)[0] == 0
+    types = f.ac_strategy >> 4
+    for name, share in synthetic.ENCODER_SHARES_D05.items():
+        got = float((types == layout.ACS_TYPES[name]).mean())
+        assert abs(got - share) <= 0.02, (name, got, share)
