@@ -2,10 +2,12 @@
 
     python -m pik_b200.run_frame FRAME.npz [--crop W H] [--reps N]
            [--form fp32|split_bf16|split_bf16x3] [--out linear.npy]
+    python -m pik_b200.run_frame --highlight W H [--mix broad|encoder] ...
 
 `--crop` keeps the top-left W x H pixels (multiples of 64 keep the colour
 tiles and transform placement intact), which makes small cases of a large
-frame for profiling.
+frame for profiling. `--highlight W H` generates a frame of the 8192x8192
+workload's kind at any size instead.
 """
 
 from __future__ import annotations
@@ -17,7 +19,7 @@ import time
 
 import numpy as np
 
-from . import layout, native
+from . import layout, native, synthetic
 
 
 def crop(frame: layout.Frame, w: int, h: int) -> layout.Frame:
@@ -45,17 +47,40 @@ def crop(frame: layout.Frame, w: int, h: int) -> layout.Frame:
         dequant_control_field=frame.dequant_control_field[:ty, :tx].copy())
 
 
-def main(argv=None) -> int:
+def parse_args(argv=None) -> argparse.Namespace:
     ap = argparse.ArgumentParser()
-    ap.add_argument("frame")
+    ap.add_argument("frame", nargs="?", help="frozen frame (.npz)")
+    ap.add_argument("--highlight", nargs=2, type=int, metavar=("W", "H"),
+                    help="instead of a file: a W x H frame from the "
+                         "8192x8192 workload's generator (seed 5)")
+    ap.add_argument("--mix", default="broad", choices=["broad", "encoder"],
+                    help="transform mix of --highlight frames")
     ap.add_argument("--crop", nargs=2, type=int)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--out")
     ap.add_argument("--form", default="fp32", choices=sorted(native.FORMS))
     args = ap.parse_args(argv)
-    frame = layout.Frame.load(args.frame)
+    if (args.frame is None) == (args.highlight is None):
+        ap.error("give either a frame file or --highlight W H")
+    return args
+
+
+def load_frame(args: argparse.Namespace) -> layout.Frame:
+    if args.highlight:
+        shares = (synthetic.ENCODER_SHARES_D05 if args.mix == "encoder"
+                  else None)
+        frame = synthetic.make_highlight_frame(*args.highlight, seed=5,
+                                               shares=shares)
+    else:
+        frame = layout.Frame.load(args.frame)
     if args.crop:
         frame = crop(frame, *args.crop)
+    return frame
+
+
+def main(argv=None) -> int:
+    args = parse_args(argv)
+    frame = load_frame(args)
     ctx = native.Context(0, form=args.form)
     ctx.begin(frame)
     ctx.set_ac()

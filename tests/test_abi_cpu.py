@@ -144,3 +144,17 @@ def test_highlight_frame_encoder_mix():
     for name, share in synthetic.ENCODER_SHARES_D05.items():
         got = float((types == layout.ACS_TYPES[name]).mean())
         assert abs(got - share) <= 0.02, (name, got, share)
+
+
+def test_run_frame_arguments():
+    """The command-line runner takes a frame file or a generated highlight
+    frame (not both), optionally cropped."""
+    from pik_b200 import run_frame
+    a = run_frame.parse_args(["--highlight", "300", "200", "--mix",
+                              "encoder", "--crop", "128", "64"])
+    f = run_frame.load_frame(a)
+    assert (f.xsize, f.ysize) == (128, 64)
+    assert native.validate(f)[0] == 0
+    for bad in ([], ["x.npz", "--highlight", "8", "8"]):
+        with pytest.raises(SystemExit):
+            run_frame.parse_args(bad)
