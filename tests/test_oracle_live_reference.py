@@ -89,3 +89,37 @@ def test_transforms_match_live_reference(t):
             else:
                 assert np.abs(got - ref).max() <= 2e-6 * float(
                     np.abs(ref).max())
+
+
+def test_epf_weights_match_live_reference():
+    """WeightFast + MulTable (pik/epf_target.cc:300-413) for every sigma
+    the filter uses (kMinSigma 16 to kMaxSigma 672) and patch SADs from 0
+    to 3060 in steps of 7, against the reference's scalar build: bit for
+    bit."""
+    L, R = oraclepy.lib(), refpy.lib("scalar")
+    for sigma in range(16, 673):
+        for sad in range(0, 3061, 7):
+            assert (L.pikoracle_epf_weight(sigma, sad) ==
+                    R.pikref_epf_weight(sigma, sad)), (sigma, sad)
+
+
+@pytest.mark.parametrize("t", range(9))
+@pytest.mark.parametrize("which", range(4))
+def test_lf_helpers_match_live_reference(t, which):
+    """LowestFrequenciesFromDC, DC2x2FromLowestFrequencies,
+    DC2x2FromLowFrequencies and LowFrequenciesFromDC2x2
+    (pik/ac_strategy.cc:850-1056) on seeded random 8x32 inputs, against the
+    reference's scalar build: within 2e-6 of the largest output value."""
+    L, R = oraclepy.lib(), refpy.lib("scalar")
+    rng = np.random.default_rng(1000 + 10 * t + which)
+    for _ in range(5):
+        src = (rng.standard_normal((8, 32)) *
+               10.0 ** rng.uniform(-2, 3)).astype(np.float32)
+        got = np.zeros_like(src)
+        ref = np.zeros_like(src)
+        L.pikoracle_lf_helper_f32(t, which, src.ctypes.data, 32,
+                                  got.ctypes.data, 32)
+        R.pikref_lf_helper(t, which, src.ctypes.data, 32, ref.ctypes.data,
+                           32)
+        assert np.abs(got - ref).max() <= 2e-6 * max(
+            1e-30, float(np.abs(ref).max()))
