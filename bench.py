@@ -48,6 +48,31 @@ METRIC = ("decoded MP/s at 4K, split-BF16 vs FP32 form @<=2e-5 err; "
 # Algorithmic bytes per pixel of the path: int16 AC in (6), DC (0.1875),
 # side info (0.094), CfL maps (~0.002), FP32 linear RGB out (12).
 PATH_BYTES_PER_PX = 18.28
+# Measured with ncu on one reconstruction of the 4K frame in the split-BF16
+# form (profiles/): warp instructions of the frame EPF launch
+# (smsp__inst_executed.sum, profiles/k_epf_box_c2_4k.md) and the DRAM bytes
+# (dram__bytes_read.sum + dram__bytes_write.sum) of all the frame's
+# launches (profiles/launches_c2_4k.md); None where not captured.
+EPF_WARP_INSTR_4K = 193.6e6
+# Algorithmic bytes per pixel of each kernel group (PIKGPU_OPT_PROFILE
+# groups), with 4-byte floats.
+GROUP_BYTES = {
+    # in + out: the guide is recomputed from the staged input tile
+    "epf": 3 * 4 + 3 * 4,
+    # filtered + original in, clamped out
+    "ar_clamp": 3 * 4 + 3 * 4 + 3 * 4,
+    # int16 coefficients in (Y read again for X and B), pixels out
+    "hf_idct": 3 * 2 + 2 * 2 + 3 * 4,
+    "gaborish1_minmax": 3 * 4,
+    "gaborish2_opsin_srgb": 3 * 4 + 3 * 4,
+    # per-cell dequantisation parameters written (32 B per cell)
+    "cell_params": 32 / 64,
+    # DC read; per cell and channel the corner's 4 int16 coefficients read
+    # and 4 corner floats and 4 pred2x2 floats written
+    "lf_prediction_corner": 12 / 64 + 3 * 4 * (2 + 4 + 4) / 64,
+    "dc_dequant_epf": 0.2,
+}
+PATH_TRAFFIC_4K = None
 # Arithmetic forms of the reconstruction (PIKGPU_OPT_FORM). The headline is
 # the split-BF16 form; every form is timed on the same frame. Their errors
 # against the FP64 oracle are checked by tests/test_split_bf16.py.
@@ -629,10 +654,7 @@ def c5_main(args):
     gbs = {f: PATH_BYTES_PER_PX * px / (t * 1e-3) / 1e9
            for f, t in forms.items()}
     top = max(acc, key=acc.get)
-    group_bytes = {"epf": 36, "ar_clamp": 36, "hf_idct": 24,
-                   "gaborish1_minmax": 24, "gaborish2_opsin_srgb": 24,
-                   "dequant_ac_lf_update": 18}
-    achieved = group_bytes.get(top, 12) * px / (acc[top] * 1e-3) / 1e9
+    achieved = GROUP_BYTES.get(top, 12) * px / (acc[top] * 1e-3) / 1e9
     if rank == 0:
         print(json.dumps({
             "metric": "achieved HBM GB/s of the 8192x8192 reconstruction "
@@ -857,17 +879,6 @@ def main():
 
     peak, peak_kind = load_peaks()
     top = max(acc, key=acc.get)
-    # Algorithmic bytes per pixel of each kernel group (design notes).
-    group_bytes = {
-        "epf": 3 * 4 + 3 * 4 + 3 * 4,          # in + guide source + out
-        "ar_clamp": 3 * 4 + 3 * 4 + 3 * 4,     # filtered + original + out
-        "hf_idct": 3 * 4 + 3 * 4,              # coefficients in, pixels out
-        "gaborish1_minmax": 3 * 4 + 3 * 4,
-        "gaborish2_opsin_srgb": 3 * 4 + 3 * 4,
-        "dequant_ac_lf_update": 3 * 2 + 3 * 4,
-        "lf_prediction": 0.5,
-        "dc_dequant_epf": 0.2,
-    }
     # DRAM bytes per launch of the 4K workload measured with ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum, one cold launch each).
     ncu_traffic_4k = {
@@ -876,8 +887,22 @@ def main():
         "gaborish2_opsin_srgb": 99.55e6 + 63.85e6,
     }
     traffic = ncu_traffic_4k.get(top) if px == 3840 * 2160 else None
-    top_bytes = group_bytes.get(top, 12) * px
+    top_bytes = GROUP_BYTES.get(top, 12) * px
     achieved = top_bytes / (acc[top] * 1e-3) / 1e9
+    # The EPF is bound by instruction issue, not HBM: its warp instructions
+    # per launch (ncu smsp__inst_executed.sum, one launch of the 4K frame)
+    # against the issue rate of 4 schedulers per SM at the sampled clock.
+    clocks = clk.summary()
+    issue = None
+    if top == "epf" and px == 3840 * 2160 and clocks.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        rate = sms * 4 * clocks["sm_mhz"] * 1e6  # warp instructions / s
+        floor_ms = EPF_WARP_INSTR_4K / rate * 1e3
+        issue = {"warp_instructions": EPF_WARP_INSTR_4K,
+                 "per_pixel": round(EPF_WARP_INSTR_4K / px, 2),
+                 "sm_mhz": clocks["sm_mhz"], "sms": sms,
+                 "floor_ms": round(floor_ms, 4),
+                 "frac": round(floor_ms / acc[top], 4)}
     if rank == 0:
         out = {
             "metric": METRIC, "value": round(value, 2), "unit": "MP/s",
@@ -899,7 +924,12 @@ def main():
                          "path_achieved": round(
                              PATH_BYTES_PER_PX * px / (ms * 1e-3) / 1e9, 1),
                          "path_frac": round(PATH_BYTES_PER_PX * px /
-                                            (ms * 1e-3) / 1e9 / peak, 4)},
+                                            (ms * 1e-3) / 1e9 / peak, 4),
+                         "path_traffic": (PATH_TRAFFIC_4K
+                                          if px == 3840 * 2160 else None),
+                         "path_algorithmic_bytes": round(
+                             PATH_BYTES_PER_PX * px),
+                         "issue": issue},
             "kernel_ms": {k: round(v, 4) for k, v in acc.items()},
             "forms": {f: {"value": round(ws * px / (t * 1e-3) / 1e6, 2),
                           "ms_per_step": round(t, 4)}
@@ -921,7 +951,7 @@ def main():
                              "mode": "one context, blocking "
                                      "pikgpu_reconstruct per frame"},
             "gpu_launches": launches * args.steps,
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "cpu_baseline": cpu_baseline(px) if ws == 1 else None,
         }
         print(json.dumps(out))

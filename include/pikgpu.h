@@ -230,6 +230,16 @@ int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
 #define PIKGPU_OPT_PROFILE 2
 #define PIKGPU_OPT_FORM 3
 #define PIKGPU_OPT_GRAPHS 4
+/* TC_WAIT_POLLS: the tensor-core kernels wait for each batch of MMAs with
+ *               a bounded poll of an mbarrier; if the first wait runs out
+ *               of polls, the kernel drains the MMAs in flight (a second
+ *               bounded wait), stops, and pikgpu_reconstruct fails with
+ *               PIKGPU_ERR_CUDA ("MMA completion wait timed out"); the
+ *               context stays usable. The value is the first wait's number
+ *               of polls: -1 (default) 4194304; 0 makes every first wait
+ *               run out at once, which exercises that error path. No
+ *               counterpart in the reference. */
+#define PIKGPU_OPT_TC_WAIT_POLLS 5
 #define PIKGPU_FORM_FP32 0
 #define PIKGPU_FORM_SPLIT_BF16 1
 #define PIKGPU_FORM_SPLIT_BF16X3 2
@@ -291,14 +301,18 @@ int pikgpu_batch_autotune(pikgpu_batch* batch, float* const* out_linear,
 /* Allocation-free DC reconstruction. No counterpart in the reference: its
  * DequantDC + AdaptiveDCReconstruction (pik/compressed_dc.cc:181-231,
  * pik/adaptive_reconstruction.cc:300-332) allocate their images as they go.
- * This call gives the same result as the DC stage of pikgpu_reconstruct
- * (PIKGPU_STAGE_DC) for callers that must not allocate device memory when
- * they reconstruct: it calls no allocating routine and keeps its
- * intermediates in a static device array of about 6 MiB per device.
- *  quantized_dc: device, 3 planes (X, Y, B) of ysize_blocks x xsize_blocks
- *                int16, contiguous;
- *  dc:           device, 3 planes of ysize_blocks x xsize_blocks floats,
- *                contiguous (output; must not overlap quantized_dc);
+ * This call gives the result of the DC stage of pikgpu_reconstruct
+ * (PIKGPU_STAGE_DC) in the plain FP32 form, bit for bit (the tensor-core
+ * forms' DC EPF uses fused multiply-adds: within 2e-6 of it), for callers
+ * that must not allocate device memory when they reconstruct: it calls no
+ * allocating routine and keeps its intermediates in a static device array
+ * of about 3 MiB per device.
+ *  quantized_dc: device memory of the current device (or managed), 3
+ *                planes (X, Y, B) of ysize_blocks x xsize_blocks int16,
+ *                contiguous;
+ *  dc:           same kind of memory, 3 planes of ysize_blocks x
+ *                xsize_blocks floats, contiguous (output; must not overlap
+ *                quantized_dc);
  *  dc_dequant:   host, DequantMatrix(0, DCT, c)[0] for c = 0..2;
  *  global_scale, quant_dc, ytox_dc, ytob_dc: as in pikgpu_frame_params.
  * Limit: xsize_blocks, ysize_blocks <= 512 (images up to 4096 x 4096);

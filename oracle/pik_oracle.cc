@@ -877,12 +877,16 @@ Img3<F> PadMirror(const Img3<F>& in, int border) {
 // AdaptiveFilter (pik/epf_target.cc:1113-1278). `in` is filtered with
 // weights from `guide_src`; sigma per 8x8 block from qf/strategy/LUT.
 // Decisions may be injected (guide with border, sigma per block).
+// fixed_sigma >= 0: EpfParams::enable_adaptive is false, and every block
+// takes that sigma (Filter, pik/epf_target.cc:1342-1386; FilterWorkers
+// filters every block with it, and sigma 0 copies the image). The guide
+// is formed the same way (MinMax of the guide source, MakeGuide).
 template <typename F>
 Img3<F> AdaptiveFilter(const Img3<F>& guide_src, const Img3<F>& in,
                        const int32_t* qf, const uint8_t* lut_ids,
                        const uint8_t* acs, const uint8_t* guide_in,
                        const int32_t* sigma_in, uint8_t* guide_out,
-                       int32_t* sigma_out) {
+                       int32_t* sigma_out, int fixed_sigma = -1) {
   const int xs = in.xs(), ys = in.ys();
   const int bxs = xs / kBlockDim, bys = ys / kBlockDim;
   const Img3<F> padded_in = PadMirror(in, kBorder);
@@ -925,6 +929,8 @@ Img3<F> AdaptiveFilter(const Img3<F>& guide_src, const Img3<F>& in,
       int sigma;
       if (sigma_in) {
         sigma = sigma_in[bi];
+      } else if (fixed_sigma >= 0) {
+        sigma = fixed_sigma;
       } else {
         const float ac_q = float(qf[bi]);
         const float scale = ARQuantScale(acs[bi] >> 4);
@@ -1608,7 +1614,8 @@ int Run(const pikgpu_frame_params* p, const int16_t* ac, void* const* stages,
     Img3<F> filt = AdaptiveFilter<F>(
         guide_src, idct, p->raw_quant_field, p->ar_sigma_lut_ids,
         p->ac_strategy, dec ? dec->guide : nullptr, dec ? dec->sigma : nullptr,
-        guide_out, sigma_out);
+        guide_out, sigma_out,
+        p->epf_enable_adaptive ? -1 : int(p->epf_sigma));
     CopyOut(filt, stages ? stages[4] : nullptr);
     r.ARClamp(idct, &filt);
     cur = std::move(filt);

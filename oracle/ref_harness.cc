@@ -531,6 +531,43 @@ void* pikref_frozen_from_bitstream(const uint8_t* data, size_t size,
 
 void pikref_frozen_free(void* h) { delete static_cast<Frozen*>(h); }
 
+// The decoder's fixed-sigma override (DecompressParams::epf_sigma > 0,
+// OverridePassFlags, pik/pik_frame.cc:112-115): the EPF runs with one sigma
+// for every block (Filter, pik/epf_target.cc:1342-1386).
+int pikref_frozen_set_fixed_sigma(void* h, int sigma) {
+  Frozen* f = static_cast<Frozen*>(h);
+  if (!f || sigma <= 0) return -1;
+  f->header.epf_params.enable_adaptive = false;
+  f->header.epf_params.sigma = uint32_t(sigma);
+  return 0;
+}
+
+// PikToPixels with DecompressParams::epf_sigma set (0: the bitstream's own
+// EPF parameters), to linear planes (3 * ysize * xsize floats).
+int pikref_decode_epf_sigma(const uint8_t* data, size_t size, int num_threads,
+                            int epf_sigma, float* out_linear,
+                            size_t capacity_floats) {
+  CodecContext context;
+  CodecInOut io(&context);
+  PaddedBytes compressed(size);
+  memcpy(compressed.data(), data, size);
+  DecompressParams dparams;
+  dparams.epf_sigma = epf_sigma;
+  std::unique_ptr<ThreadPool> pool;
+  if (num_threads > 0) pool.reset(new ThreadPool(num_threads));
+  if (!PikToPixels(dparams, compressed, &io, nullptr, pool.get())) {
+    g_error = "PikToPixels failed";
+    return -1;
+  }
+  const Image3F& color = io.color();
+  if (3 * color.xsize() * color.ysize() > capacity_floats) {
+    g_error = "output too small";
+    return -1;
+  }
+  CopyPlaneOut(color, out_linear);
+  return 0;
+}
+
 // Scalars: [0] xsize [1] ysize [2] Bx [3] By [4] flags [5] gaborish
 // [6] predict_lf [7] predict_hf [8] have_ar [9] epf_enable_adaptive
 // [10] epf_sigma [11] epf_use_sharpened [12] global_scale [13] quant_dc

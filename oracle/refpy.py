@@ -56,6 +56,9 @@ def lib(flavour: str = "scalar") -> ctypes.CDLL:
                                     ctypes.POINTER(ctypes.c_void_p),
                                     ctypes.POINTER(ctypes.c_double)]
     L.pikref_frozen_set_ac.argtypes = [P, P, ctypes.c_size_t]
+    L.pikref_frozen_set_fixed_sigma.argtypes = [P, ctypes.c_int]
+    L.pikref_decode_epf_sigma.argtypes = [P, ctypes.c_size_t, ctypes.c_int,
+                                          ctypes.c_int, P, ctypes.c_size_t]
     L.pikref_frozen_encode_dct8.restype = P
     L.pikref_frozen_encode_dct8.argtypes = [P, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_float, ctypes.c_int]
@@ -96,13 +99,15 @@ def encode(linear: np.ndarray, distance: float, *, ar: int = -1,
 
 
 def decode(bitstream: bytes, xsize: int, ysize: int, *, threads: int = 0,
-           flavour: str = "scalar") -> np.ndarray:
-    """Full reference PikToPixels to (3, H, W) linear planes."""
+           flavour: str = "scalar", epf_sigma: int = 0) -> np.ndarray:
+    """Full reference PikToPixels to (3, H, W) linear planes; epf_sigma > 0
+    is the decoder's fixed-sigma EPF override (DecompressParams)."""
     L = lib(flavour)
     out = np.zeros((3, ysize, xsize), np.float32)
     buf = ctypes.create_string_buffer(bitstream, len(bitstream))
-    rc = L.pikref_decode(ctypes.cast(buf, ctypes.c_void_p), len(bitstream),
-                         threads, _ptr(out), out.size)
+    rc = L.pikref_decode_epf_sigma(ctypes.cast(buf, ctypes.c_void_p),
+                                   len(bitstream), threads, epf_sigma,
+                                   _ptr(out), out.size)
     if rc != 0:
         raise RuntimeError(L.pikref_last_error().decode())
     return out
@@ -186,6 +191,12 @@ class Frozen:
             dequant_control_field=self._get("dequant_control_field",
                                             (ty, tx), np.uint8),
             dequant_map=self._get("dequant_map", (16, 256), np.uint8))
+
+    def set_fixed_sigma(self, sigma: int) -> None:
+        """The decoder's fixed-sigma EPF override (sigma > 0)."""
+        if self.L.pikref_frozen_set_fixed_sigma(self.h, sigma) != 0:
+            raise ValueError(f"fixed sigma {sigma}")
+        self.ints[9], self.ints[10] = 0, sigma
 
     def dc_smoothed(self) -> np.ndarray:
         return self._get("dc_smoothed", (3, self.by, self.bx), np.float32)

@@ -1,10 +1,14 @@
 // Allocation-free DC reconstruction (pikgpu_dc_reconstruct_noalloc in
-// include/pikgpu.h). It runs the same kernels, with the same arithmetic, as
-// the DC stage of pikgpu_reconstruct: DequantDC + AdaptiveDCReconstruction
-// (pik/compressed_dc.cc:181-231, pik/adaptive_reconstruction.cc:300-332).
-// The only difference is where the intermediates live. The context path keeps
-// them in cudaMalloc'd buffers. Here they live in one fixed-size file-scope
-// device array, and the caller passes its own input and output buffers.
+// include/pikgpu.h). It runs the kernels, with the arithmetic, of the DC
+// stage of pikgpu_reconstruct in the plain FP32 form: DequantDC +
+// AdaptiveDCReconstruction (pik/compressed_dc.cc:181-231,
+// pik/adaptive_reconstruction.cc:300-332), with the same EPF tile shape
+// choice. Its result is bit-identical to that form's DC stage. The
+// tensor-core forms' DC EPF computes its weighted sums with fused
+// multiply-adds, so their DC stage differs from this result by FP32
+// rounding (within 2e-6). The context path keeps the intermediates in
+// cudaMalloc'd buffers. Here they live in one fixed-size file-scope device
+// array, and the caller passes its own input and output buffers.
 //
 // Who needs it: a caller that must not allocate device memory at the point
 // where it reconstructs DC. Examples are a decoder driven from a real-time or
@@ -19,15 +23,15 @@
 //    at most kNoAllocMaxBlocks x kNoAllocMaxBlocks, so images up to
 //    4096 x 4096 pixels. Larger sizes are rejected with PIKGPU_ERR_INVALID_ARG
 //    before any work is queued.
-//  * The scratch holds two padded DC images (3 x 512 x 512 floats each),
-//    4096 per-block sigmas and the 6 guide min/max words, about 6.02 MiB of
-//    static device memory per device.
+//  * The scratch holds the padded DC image (3 x 512 x 512 floats), 4096
+//    per-block sigmas and the guide min/max words, about 3.02 MiB of static
+//    device memory per device.
 //  * No part of the scratch has to start at zero. Every call first resets
-//    the min/max words with a kernel, then fully writes the padded images
-//    and sigmas before it reads them.
+//    the min/max words with a kernel, then fully writes the padded image
+//    and the sigmas before it reads them.
 //  * The first call on a device does the set-up, with that device current:
 //    it uploads the constant tables, sets the EPF kernel's shared-memory
-//    limit and looks up the scratch address. Make
+//    limit, reads the SM count and looks up the scratch address. Make
 //    that first call before any stream capture on the device.
 //  * All calls on one device share the scratch. Calls that overlap in time
 //    on the same device (other streams, or host threads without ordering)
@@ -40,15 +44,15 @@ namespace {
 constexpr int kNoAllocMaxBlocks = 512;
 constexpr size_t kNoAllocPlane = size_t(kNoAllocMaxBlocks) * kNoAllocMaxBlocks;
 constexpr size_t kNoAllocSigmas = kNoAllocPlane / 64;  // 8x8-block EPF cells
-constexpr size_t kNoAllocPadOff = 0;                   // 3 padded DC planes
-constexpr size_t kNoAllocFiltOff = 3 * kNoAllocPlane;  // 3 filtered planes
-constexpr size_t kNoAllocSigOff = 6 * kNoAllocPlane;   // int32 sigma / cell
-constexpr size_t kNoAllocMmOff = kNoAllocSigOff + kNoAllocSigmas;  // 6 words
+constexpr size_t kNoAllocPadOff = 0;                  // 3 padded DC planes
+constexpr size_t kNoAllocSigOff = 3 * kNoAllocPlane;  // int32 sigma / cell
+constexpr size_t kNoAllocMmOff = kNoAllocSigOff + kNoAllocSigmas;  // 16 words
 constexpr size_t kNoAllocWords = kNoAllocMmOff + 64;
 
 struct NoAllocDevice {
   bool ready = false;
   uint32_t* scratch = nullptr;
+  int num_sms = 148;
 };
 std::mutex g_noalloc_mutex;
 NoAllocDevice g_noalloc[64];
@@ -60,13 +64,17 @@ static __device__ __align__(256) uint32_t g_dc_scratch[kNoAllocWords];
 
 namespace {
 
-bool IsDevicePointer(const void* p) {
+// True for managed memory and for device memory of device `dev` (the
+// kernels run there; another GPU's buffer is refused rather than read
+// through the peer mapping or faulted on).
+bool IsDevicePointer(const void* p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();  // leave no error behind for the caller's next call
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  return a.type == cudaMemoryTypeManaged ||
+         (a.type == cudaMemoryTypeDevice && a.device == dev);
 }
 
 bool Overlaps(const void* a, size_t na, const void* b, size_t nb) {
@@ -98,22 +106,24 @@ int DcNoAlloc(pikgpu_ctx* ctx, const int16_t* quantized_dc, uint32_t bx,
     return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "quant_dc %d", quant_dc);
   }
   const size_t n = size_t(bx) * by;
-  if (!IsDevicePointer(quantized_dc) || !IsDevicePointer(dc)) {
-    return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
-                "quantized_dc and dc must be device pointers");
-  }
-  if (Overlaps(quantized_dc, 3 * n * sizeof(int16_t), dc,
-               3 * n * sizeof(float))) {
-    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "quantized_dc and dc overlap");
-  }
-
   int dev = 0;
   CUDA_TRY(ctx, cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) {
     return Fail(ctx, PIKGPU_ERR_UNSUPPORTED, "device %d", dev);
   }
+  if (!IsDevicePointer(quantized_dc, dev) || !IsDevicePointer(dc, dev)) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                "quantized_dc and dc must be device pointers on the current "
+                "device (%d)",
+                dev);
+  }
+  if (Overlaps(quantized_dc, 3 * n * sizeof(int16_t), dc,
+               3 * n * sizeof(float))) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "quantized_dc and dc overlap");
+  }
   ctx->device = dev;
   uint32_t* scratch = nullptr;
+  int num_sms = 148;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     NoAllocDevice& d = g_noalloc[dev];
@@ -122,10 +132,13 @@ int DcNoAlloc(pikgpu_ctx* ctx, const int16_t* quantized_dc, uint32_t bx,
       if (rc != PIKGPU_OK) return rc;
       void* p = nullptr;
       CUDA_TRY(ctx, cudaGetSymbolAddress(&p, g_dc_scratch));
+      CUDA_TRY(ctx, cudaDeviceGetAttribute(
+                        &d.num_sms, cudaDevAttrMultiProcessorCount, dev));
       d.scratch = static_cast<uint32_t*>(p);
       d.ready = true;
     }
     scratch = d.scratch;
+    num_sms = d.num_sms;
   }
 
   // Same scalars, in the same operation order, as pikgpu_frame_begin.
@@ -151,26 +164,22 @@ int DcNoAlloc(pikgpu_ctx* ctx, const int16_t* quantized_dc, uint32_t bx,
   f.dc = dc;
 
   float* dcpad = reinterpret_cast<float*>(scratch + kNoAllocPadOff);
-  float* dcfilt = reinterpret_cast<float*>(scratch + kNoAllocFiltOff);
   int32_t* sig = reinterpret_cast<int32_t*>(scratch + kNoAllocSigOff);
   uint32_t* mm = scratch + kNoAllocMmOff;
   const int dpw = (g.Bx + 7) / 8 * 8, dph = (g.By + 7) / 8 * 8;
-  const int nb = (dpw / 8) * (dph / 8);
 
-  k_dequant_dc<<<Blocks(n, 256), 256, 0, st>>>(g, f, s);
-  dim3 b(32, 8), gr(Blocks(dpw, 32), Blocks(dph, 8), 3);
-  k_pad_replicate<<<gr, b, 0, st>>>(dc, g.Bx, g.By, dcpad, dpw, dph);
-  k_minmax_init<<<1, 32, 0, st>>>(mm);
-  k_minmax<<<dim3(Blocks(size_t(dpw) * dph, 256 * 8), 3), 256, 0, st>>>(
-      dcpad, size_t(dpw) * dph, mm);
-  k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, nullptr, nullptr, nullptr,
-                                               s.quant_dc / 2, mm, sig);
-  k_epf_box<false, kEpfH><<<Blocks(dpw, kEpfW) * Blocks(dph, kEpfH),
-                            kEpfThreads, kEpfSmemBytes, st>>>(
-      dcpad, dcpad, nullptr, 0, dpw, dph, mm, sig, dcfilt);
-  dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
-  k_dc_clamp<<<gr2, b, 0, st>>>(dc, dcfilt, g.Bx, g.By, dpw, dph,
-                                half_step[0], half_step[1], half_step[2]);
+  // The FP32 form's DC stage of LaunchAll: min/max reset, dequantisation
+  // with the padded copy and its min/max, then the EPF clamping into `dc`.
+  k_frame_init<<<1, 32, 0, st>>>(mm, nullptr, 0);
+  k_dc_prep<<<dim3(Blocks(dpw, 32), Blocks(dph, 8)), 256, 0, st>>>(
+      g, f, s, dcpad, dpw, dph, mm + 8);
+  EpfSigma sgs{};
+  sgs.const_qf = s.quant_dc / 2;
+  sgs.fixed = -1;
+  sgs.out = sig;
+  const EpfDc dco{dc, g.Bx, g.By, half_step[0], half_step[1], half_step[2]};
+  EpfLaunch(st, num_sms, PIKGPU_FORM_FP32, dcpad, dcpad, 0, dpw, dph, mm + 8,
+            sgs, nullptr, nullptr, dco);
   CUDA_TRY(ctx, cudaGetLastError());
   return PIKGPU_OK;
 }

@@ -118,12 +118,71 @@ __device__ __forceinline__ void PatchSads4(const uint32_t* rf,
   }
 }
 
+// Where the per-block sigma comes from. It is computed in the kernel from
+// the guide's stretch (SigmaFromQuant, pik/epf_target.cc:1072-1111):
+// `ovr` (the verification override) if set; else `fixed` if >= 0 (the
+// fixed-sigma EPF, pik/epf_target.cc:1342-1386); else from qf, strategy
+// and LUT per block; or, qf NULL (the DC image), from the constant
+// `const_qf` with a DCT strategy and LUT 0 (AdaptiveDCReconstruction,
+// pik/adaptive_reconstruction.cc:300-318). The sigma used is written to
+// `out` (NULL: not written) by one lane per block.
+struct EpfSigma {
+  const int32_t* ovr;
+  const int32_t* qf;
+  const uint8_t* acs;
+  const uint8_t* lut;
+  int const_qf;
+  int fixed;
+  int32_t* out;
+};
+
+// The DC image's output: instead of storing the filtered value, the clamp
+// of AdaptiveDCReconstruction (pik/adaptive_reconstruction.cc:319-331),
+// dc = max(dc - hs, min(filtered, dc + hs)), into the w x h planes at `dc`
+// (the padding is dropped). dc NULL: the frame EPF, which stores `out`.
+struct EpfDc {
+  float* dc;
+  int w, h;
+  float hs0, hs1, hs2;
+};
+
 // Sigma of this thread's block in the tile at (x0, y0); 0 outside the image.
-__device__ __forceinline__ int EpfLaneSigma(const int32_t* sigma, int w, int h,
-                                            int x0, int y0) {
+__device__ __forceinline__ int EpfLaneSigma(const EpfSigma& s, float stretch,
+                                            int w, int h, int x0, int y0) {
   const int t = threadIdx.x;
   const int px = x0 + (t & 31) + 32 * ((t >> 5) & 1), py0 = y0 + 4 * (t >> 6);
-  return px < w && py0 < h ? sigma[(py0 >> 3) * (w / 8) + (px >> 3)] : 0;
+  if (px >= w || py0 >= h) return 0;
+  const int bi = (py0 >> 3) * (w / 8) + (px >> 3);
+  int sg;
+  if (s.ovr) {
+    sg = s.ovr[bi];
+  } else if (s.fixed >= 0) {
+    sg = s.fixed;
+  } else if (s.qf) {
+    sg = SigmaFromQuant(float(s.qf[bi]), ARQuantScaleOf(s.acs[bi] >> 4),
+                        s.lut[bi], stretch);
+  } else {
+    sg = SigmaFromQuant(float(s.const_qf), 1.0f, 0, stretch);
+  }
+  if (s.out && (px & 7) == 0 && (py0 & 7) == 0) s.out[bi] = sg;
+  return sg;
+}
+
+// Stores the value of channel c at pixel (px, y) of the tile's output.
+__device__ __forceinline__ void EpfStore(float* out, const EpfDc& dco,
+                                         size_t plane, int w, int c, int px,
+                                         int y, float v) {
+  if (dco.dc) {
+    if (px < dco.w && y < dco.h) {
+      float& d = dco.dc[(size_t(c) * dco.h + y) * dco.w + px];
+      const float hs = c == 0 ? dco.hs0 : c == 1 ? dco.hs1 : dco.hs2;
+      const float lo = d - hs, hi = d + hs;
+      const float m = v < hi ? v : hi;
+      d = lo < m ? m : lo;
+    }
+  } else {
+    out[c * plane + size_t(y) * w + px] = v;
+  }
 }
 
 // Tiles whose halo lies inside the image take vector copies and no
@@ -163,9 +222,10 @@ __device__ __forceinline__ void EpfStage(const float* in, int w, int h, int x0,
   }
 }
 
-// Filters the staged tile at (x0, y0) into `out`. The tile's copies are
-// complete in every thread (the first barrier below publishes them); `sig`
-// is EpfLaneSigma of this thread; (amin, mul) quantise the guide
+// Filters the staged tile at (x0, y0) into `out` (or, for the DC image,
+// into dco's clamp). The tile's copies are complete in every thread (the
+// first barrier below publishes them); `sig` is EpfLaneSigma of this
+// thread; (amin, mul) quantise the guide
 // (GuideParams). `sa` holds the aligned guide words while the guide is
 // built. Returns after the tile's last barrier.
 //
@@ -175,8 +235,9 @@ __device__ __forceinline__ void EpfStage(const float* in, int w, int h, int x0,
 template <bool kFma, int TH>
 __device__ __forceinline__ void EpfFilterTile(
     const float* guide_src, const uint8_t* guide_ovr, int gab, int w, int h,
-    float amin, float mul, int sig, float* out, uint32_t* sg, uint32_t* sa,
-    float (*tile)[TH + 10][kEpfTS], int x0, int y0) {
+    float amin, float mul, int sig, float* out, const EpfDc& dco,
+    uint32_t* sg, uint32_t* sa, float (*tile)[TH + 10][kEpfTS], int x0,
+    int y0) {
   constexpr int kGH = TH + 8, kTH = TH + 10;
   constexpr int kGPlane = kGH * kEpfGRow, kThreads = 16 * TH;
   const int tid = threadIdx.x;
@@ -193,9 +254,11 @@ __device__ __forceinline__ void EpfFilterTile(
   // Tiles without filtered blocks are copies (CopyOriginalBlock).
   if (!__syncthreads_or(filtered)) {
     if (inside) {
+#pragma unroll
       for (int c = 0; c < 3; ++c)
+#pragma unroll
         for (int j = 0; j < 4; ++j)
-          out[c * plane + size_t(py0 + j) * w + px] = tile[c][tr0 + j][tc0];
+          EpfStore(out, dco, plane, w, c, px, py0 + j, tile[c][tr0 + j][tc0]);
     }
     return;
   }
@@ -296,9 +359,11 @@ __device__ __forceinline__ void EpfFilterTile(
   // Warps (half a block row of 8 blocks) without filtered blocks copy.
   if (!__any_sync(0xFFFFFFFFu, filtered)) {
     if (inside) {
+#pragma unroll
       for (int c = 0; c < 3; ++c)
+#pragma unroll
         for (int j = 0; j < 4; ++j)
-          out[c * plane + size_t(py0 + j) * w + px] = tile[c][tr0 + j][tc0];
+          EpfStore(out, dco, plane, w, c, px, py0 + j, tile[c][tr0 + j][tc0]);
     }
     return;
   }
@@ -417,8 +482,8 @@ __device__ __forceinline__ void EpfFilterTile(
   for (int c = 0; c < 3; ++c)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      out[c * plane + size_t(py0 + j) * w + px] =
-          filtered ? ws[c][j] / sw[j] : tile[c][tr0 + j][tc0];
+      EpfStore(out, dco, plane, w, c, px, py0 + j,
+               filtered ? ws[c][j] / sw[j] : tile[c][tr0 + j][tc0]);
     }
 }
 
@@ -429,7 +494,7 @@ template <bool kFma, int TH>
 __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
     k_epf_box(const float* in, const float* guide_src,
               const uint8_t* guide_ovr, int gab, int w, int h,
-              const uint32_t* mm, const int32_t* sigma, float* out) {
+              const uint32_t* mm, EpfSigma sgs, float* out, EpfDc dco) {
   extern __shared__ __align__(16) uint32_t epf_smem[];
   uint32_t* sg = epf_smem;  // [3][TH + 8][kEpfGRow]
   auto* tile = reinterpret_cast<float(*)[TH + 10][kEpfTS]>(
@@ -440,11 +505,11 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
   const int y0 = (blockIdx.x / tiles_x) * TH;
   float amin, mul, stretch;
   GuideParams(mm, &amin, &mul, &stretch);
-  const int sig = EpfLaneSigma(sigma, w, h, x0, y0);
   EpfStage<TH>(in, w, h, x0, y0, tile);
+  const int sig = EpfLaneSigma(sgs, stretch, w, h, x0, y0);
   CpAsyncWaitAll();
   EpfFilterTile<kFma, TH>(guide_src, guide_ovr, gab, w, h, amin, mul, sig,
-                          out, sg, sa, tile, x0, y0);
+                          out, dco, sg, sa, tile, x0, y0);
 }
 
 }  // namespace pikgpu

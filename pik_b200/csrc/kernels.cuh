@@ -61,7 +61,6 @@ struct Geo {
 // Per-group bordered arrays: llf (66 x 66) and 2x2 images (132 x 132).
 constexpr int kGB = 66;
 constexpr int kG2 = 132;
-constexpr size_t kLlfGroupFloats = size_t(3) * kGB * kGB;
 constexpr size_t kG2GroupFloats = size_t(3) * kG2 * kG2;
 
 struct FrameScalars {
@@ -74,6 +73,19 @@ struct FrameScalars {
   int have_ar;
   int use_sharpened;
   int quant_dc;
+  // EpfParams::sigma when enable_adaptive is false, else -1.
+  int epf_fixed_sigma;
+};
+
+// Dequant::DoAC's parameters of one 8x8 cell (pik/compressed_image.cc:
+// 636-672): the scaled step inv_global_scale / qf (SafeDiv), the
+// chroma-from-luma multipliers of the cell's colour tile, and the offsets
+// in the dequant table of the cell's three matrix rows (its table, the
+// block's QuantKind, the cell's sub-block). 32 bytes: two 16-byte loads.
+struct CellDq {
+  float scaled, x_cc, b_cc;
+  uint32_t m[3];
+  uint32_t pad[2];
 };
 
 // Device pointers of one frame.
@@ -90,11 +102,17 @@ struct DevFrame {
   const int16_t* qdc;
   const int16_t* qac;
   float* dc;          // 3 x By x Bx
-  float* ac;          // 3 x By x ac_stride
-  float* llf_g;       // groups x 3 x 66 x 66
-  float* lf2x2_g;     // groups x 3 x 132 x 132
+  // The transforms dequantise qac as they load it (cellp), unless ac_in is
+  // set: dequantised AC supplied instead (3 x By x ac_stride). Either way
+  // each block's 2cov x 2cov low-frequency corner (LLF from DC, LF plus
+  // its prediction) comes from `corner`: 3 x By x Bx x 4 floats, element
+  // (r, l) of the block at (bx, by) in cell (bx + l / 2, by + r / 2), slot
+  // 2 (r & 1) + (l & 1).
+  const float* ac_in;
+  const CellDq* cellp;  // By x Bx
+  float* corner;
+  float* ac;          // 3 x By x ac_stride (k_dequant_ac's output)
   float* pred2x2_g;   // groups x 3 x 132 x 132
-  float* tmp2x2_g;    // groups x 3 x 132 x 132
   float* idct;        // 3 x PH x PW
   float* smoothed;    // 3 x PH x PW
   float* filt;        // 3 x PH x PW
@@ -107,6 +125,9 @@ struct DevFrame {
   // Optional clamp tape to follow instead of the computed minimum (same
   // layout; NULL: computed), pikgpu_set_clamp_decisions.
   const uint8_t* clamp_tape_in;
+  // Polls of the tensor-core kernels' first wait on each MMA completion
+  // (tc::WaitMma).
+  uint32_t tc_polls;
 };
 
 }  // namespace pikgpu

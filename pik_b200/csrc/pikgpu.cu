@@ -50,7 +50,7 @@ enum Timed {
   kTDc = 0, kTLf, kTDequant, kTIdct, kTGab1, kTEpf, kTAr, kTFinal, kNumTimed
 };
 const char* kTimedNames[kNumTimed] = {
-    "dc_dequant_epf", "lf_prediction", "dequant_ac_lf_update", "hf_idct",
+    "dc_dequant_epf", "lf_prediction_corner", "cell_params", "hf_idct",
     "gaborish1_minmax", "epf", "ar_clamp", "gaborish2_opsin_srgb"};
 
 struct DevBuf {
@@ -87,7 +87,7 @@ struct pikgpu_ctx {
   std::vector<uint32_t> lists[kNumClasses];
   // device buffers
   DevBuf acs, qf, lut, dq_cf, dq_map, ytox, ytob, table, offsets;
-  DevBuf qdc, qac, dc, dcpad, dcfilt, ac, llf_g, lf2x2_g, pred2x2_g, tmp2x2_g;
+  DevBuf qdc, qac, dc, dcpad, cellp, corner, pred2x2_g;
   DevBuf idct, smoothed, filt, mm, sigma, dc_sigma, list[kNumClasses];
   DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr;
   DevBuf sigma_ovr, counters, active[kNumClasses], tc_err;
@@ -119,6 +119,8 @@ struct pikgpu_ctx {
   cudaEvent_t fork_ev[3] = {}, join_ev[3][kSide] = {};
   int num_sms = 148;
   int tc_ctas_per_sm = kTcCtasPerSm;
+  // PIKGPU_OPT_TC_WAIT_POLLS.
+  uint32_t tc_polls = tc::kMaxPolls;
   float times[kNumTimed] = {};
   float dc_half_step[3] = {};
   int launches = 0;
@@ -245,8 +247,16 @@ int Validate(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
     return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "gaborish strength %u",
                 p->gaborish);
   }
-  if (p->have_adaptive_reconstruction && !p->epf_enable_adaptive) {
-    return Fail(ctx, PIKGPU_ERR_UNSUPPORTED, "fixed-sigma EPF");
+  // Fixed-sigma EPF filters with kMinSigma <= sigma <= kMaxSigma, or copies
+  // when sigma is 0 (FilterWorkers and Filter, pik/epf_target.cc:1295,
+  // 1357-1361).
+  if (p->have_adaptive_reconstruction && !p->epf_enable_adaptive &&
+      p->epf_sigma != 0 &&
+      (p->epf_sigma < uint32_t(kMinSigma) ||
+       p->epf_sigma > uint32_t(kMaxSigma))) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                "fixed EPF sigma %u outside {0} and [%d, %d]", p->epf_sigma,
+                kMinSigma, kMaxSigma);
   }
   if (p->global_scale < 1 || p->global_scale > 32768) {
     return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "global_scale %d",
@@ -361,6 +371,7 @@ void ComputeScalars(const pikgpu_frame_params* p, FrameScalars* s) {
   s->have_ar = p->have_adaptive_reconstruction ? 1 : 0;
   s->use_sharpened = p->epf_use_sharpened ? 1 : 0;
   s->quant_dc = p->quant_dc;
+  s->epf_fixed_sigma = p->epf_enable_adaptive ? -1 : int(p->epf_sigma);
 }
 
 int UploadTables(pikgpu_ctx* ctx) {
@@ -385,6 +396,9 @@ int UploadTables(pikgpu_ctx* ctx) {
                     k_epf_box<true, 8>,
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(EpfSmemBytes(8))));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_lf_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(kLfSmemBytes)));
   if (ctx->device < 64) g_tables_uploaded[ctx->device] = true;
   return PIKGPU_OK;
 }
@@ -413,42 +427,41 @@ void Mark(pikgpu_ctx* ctx, int i) {
   if (ctx->profile) cudaEventRecord(ctx->ev[i], ctx->stream);
 }
 
-// The frame EPF or the DC EPF: minmax of the guide source is expected in
-// ctx->mm already; sigma per block in `sig`. `gab` > 0: the guide is
-// gaborish (that strength) of `in`, computed inside the kernel.
-int RunEpf(pikgpu_ctx* ctx, cudaStream_t st, const float* in,
-           const float* guide_src, int gab, int w, int h, const int32_t* sig,
-           float* out, const uint8_t* guide_ovr) {
+// The frame EPF or the DC EPF: the min/max of the guide source is expected
+// in `mm` already. `sgs`: where the per-block sigma comes from (computed in
+// the kernel); `dco`: the DC image's clamped output instead of `out`.
+// `gab` > 0: the guide is gaborish (that strength) of `in`, computed inside
+// the kernel.
+void EpfLaunch(cudaStream_t st, int num_sms, int form, const float* in,
+               const float* guide_src, int gab, int w, int h,
+               const uint32_t* mm, const EpfSigma& sgs, float* out,
+               const uint8_t* guide_ovr, const EpfDc& dco) {
   // Images that fill fewer than two CTAs per SM with 32-row tiles (the DC
   // image) take 8-row tiles: four times the CTAs, a quarter of the latency.
-  const bool small =
-      Blocks(w, kEpfW) * Blocks(h, kEpfH) < 2 * ctx->num_sms;
-  const bool fma = ctx->form != PIKGPU_FORM_FP32;
-  const uint32_t* mm = P<uint32_t>(ctx->mm);
+  const bool small = Blocks(w, kEpfW) * Blocks(h, kEpfH) < 2 * num_sms;
+  const bool fma = form != PIKGPU_FORM_FP32;
   // One CTA per 64 x th tile.
-  auto grid = [&](int th, int) { return Blocks(w, kEpfW) * Blocks(h, th); };
+  auto grid = [&](int th) { return Blocks(w, kEpfW) * Blocks(h, th); };
   if (small) {
     if (fma) {
-      k_epf_box<true, 8><<<grid(8, 2), 16 * 8, EpfSmemBytes(8), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
+      k_epf_box<true, 8><<<grid(8), 16 * 8, EpfSmemBytes(8), st>>>(
+          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco);
     } else {
-      k_epf_box<false, 8><<<grid(8, 2), 16 * 8, EpfSmemBytes(8), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
+      k_epf_box<false, 8><<<grid(8), 16 * 8, EpfSmemBytes(8), st>>>(
+          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco);
     }
   } else {
     if (fma) {
       // 16-row tiles of 256 threads, three CTAs per SM: the cx-major loop
       // of these forms needs ~85 registers.
-      k_epf_box<true, 16><<<grid(16, 3), 16 * 16, EpfSmemBytes(16), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sig, out);
+      k_epf_box<true, 16><<<grid(16), 16 * 16, EpfSmemBytes(16), st>>>(
+          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco);
     } else {
-      k_epf_box<false, kEpfH><<<grid(kEpfH, 2), kEpfThreads, kEpfSmemBytes,
+      k_epf_box<false, kEpfH><<<grid(kEpfH), kEpfThreads, kEpfSmemBytes,
                                 st>>>(in, guide_src, guide_ovr, gab, w, h, mm,
-                                      sig, out);
+                                      sgs, out, dco);
     }
   }
-  ++ctx->launches;
-  return PIKGPU_OK;
 }
 
 // Concurrent branches of the launch sequence. Fork(i, n) makes side streams
@@ -506,11 +519,14 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   f.qdc = P<int16_t>(ctx->qdc);
   f.qac = P<int16_t>(ctx->qac);
   f.dc = P<float>(ctx->dc);
-  f.ac = P<float>(ctx->ac);
-  f.llf_g = P<float>(ctx->llf_g);
-  f.lf2x2_g = P<float>(ctx->lf2x2_g);
+  // The transforms dequantise the int16 AC as they load it, unless the
+  // caller supplied dequantised AC; k_dequant_ac runs only to export that
+  // stage.
+  f.ac_in = ctx->use_dq_ovr ? P<float>(ctx->dq_ovr) : nullptr;
+  f.cellp = P<CellDq>(ctx->cellp);
+  f.corner = P<float>(ctx->corner);
+  f.ac = ctx->keep_stages ? P<float>(ctx->dbg_dequant) : nullptr;
   f.pred2x2_g = P<float>(ctx->pred2x2_g);
-  f.tmp2x2_g = P<float>(ctx->tmp2x2_g);
   f.idct = P<float>(ctx->idct);
   f.smoothed = P<float>(ctx->smoothed);
   f.filt = P<float>(ctx->filt);
@@ -520,6 +536,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
                    ctx->adj_tape.cap >= nac;
   f.clamp_tape = rec ? P<uint8_t>(ctx->adj_tape) : nullptr;
   f.clamp_tape_in = ctx->use_tape_in ? P<uint8_t>(ctx->tape_in) : nullptr;
+  f.tc_polls = ctx->tc_polls;
   ctx->tape_valid = rec;
   uint32_t* mm = P<uint32_t>(ctx->mm);
   const uint32_t* L[kNumClasses];
@@ -534,56 +551,53 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
 
   ctx->launches = 0;
   ctx->smoothed_valid = false;
+  // Both min/max sets and the clamp's block counters start empty.
+  int* counters = P<int>(ctx->counters);
+  k_frame_init<<<1, 32, 0, st>>>(mm, counters, kNumClasses); ++ctx->launches;
   br.Fork(0, 1);
   Mark(ctx, kTDc);
-  // DC: dequant, EPF on the 8-padded DC image, clamp (side stream 0).
+  // DC (side stream 0): dequantisation, the 8-padded copy and its min/max;
+  // then the EPF on it, which clamps its output into the DC planes.
   cudaStream_t sd = br[0];
-  k_dequant_dc<<<Blocks(size_t(g.Bx) * g.By, 256), 256, 0, sd>>>(g, f, s); ++ctx->launches;
   const int dpw = (g.Bx + 7) / 8 * 8, dph = (g.By + 7) / 8 * 8;
   float* dcpad = P<float>(ctx->dcpad);
-  float* dcfilt = P<float>(ctx->dcfilt);
+  uint32_t* mm_dc = mm + 8;
   {
-    dim3 b(32, 8), gr(Blocks(dpw, 32), Blocks(dph, 8), 3);
-    k_pad_replicate<<<gr, b, 0, sd>>>(f.dc, g.Bx, g.By, dcpad, dpw, dph); ++ctx->launches;
-    k_minmax_init<<<1, 32, 0, sd>>>(mm); ++ctx->launches;
-    k_minmax<<<dim3(Blocks(size_t(dpw) * dph, 256 * 8), 3), 256, 0, sd>>>(
-        dcpad, size_t(dpw) * dph, mm); ++ctx->launches;
-    const int nb = (dpw / 8) * (dph / 8);
-    k_epf_sigma<<<Blocks(nb, 256), 256, 0, sd>>>(
-        nb, nullptr, nullptr, nullptr, s.quant_dc / 2, mm,
-        P<int32_t>(ctx->dc_sigma)); ++ctx->launches;
-    RunEpf(ctx, sd, dcpad, dcpad, 0, dpw, dph, P<int32_t>(ctx->dc_sigma),
-           dcfilt, nullptr);
-    dim3 gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
-    k_dc_clamp<<<gr2, b, 0, sd>>>(f.dc, dcfilt, g.Bx, g.By, dpw, dph,
-                                  ctx->dc_half_step[0], ctx->dc_half_step[1],
-                                  ctx->dc_half_step[2]); ++ctx->launches;
+    k_dc_prep<<<dim3(Blocks(dpw, 32), Blocks(dph, 8)), 256, 0, sd>>>(
+        g, f, s, dcpad, dpw, dph, mm_dc); ++ctx->launches;
+    EpfSigma sgs{};
+    sgs.const_qf = s.quant_dc / 2;
+    sgs.fixed = -1;
+    sgs.out = P<int32_t>(ctx->dc_sigma);
+    const EpfDc dco{f.dc, g.Bx, g.By, ctx->dc_half_step[0],
+                    ctx->dc_half_step[1], ctx->dc_half_step[2]};
+    EpfLaunch(sd, ctx->num_sms, ctx->form, dcpad, dcpad, 0, dpw, dph, mm_dc,
+              sgs, nullptr, nullptr, dco); ++ctx->launches;
   }
   Mark(ctx, kTLf);
-  // Per-group LF prediction (side stream 0, after DC): one CTA per group
-  // and channel.
+  // Per-group LF prediction and every block's low-frequency corner and
+  // pred2x2 (side stream 0, after DC): one CTA per group and channel.
   const int ng = g.Gx * g.Gy;
-  k_lf_chain<<<3 * ng, kLfThreads, 0, sd>>>(g, f, s.predict_lf,
-                                           s.predict_hf); ++ctx->launches;
+  k_lf_chain<<<3 * ng, kLfThreads, kLfSmemBytes, sd>>>(
+      g, f, s, s.predict_lf, s.predict_hf); ++ctx->launches;
   Mark(ctx, kTDequant);
   {
-    // AC dequantisation (main stream, concurrent with DC and LF).
-    dim3 gr(Blocks(g.Bx, kDequantCells), g.By);
-    if (ctx->use_dq_ovr) {
-      cudaMemcpyAsync(f.ac, ctx->dq_ovr.p,
-                      sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
-                      cudaMemcpyDeviceToDevice, st);
-    } else {
-      k_dequant_ac<<<gr, 256, 0, st>>>(g, f, s); ++ctx->launches;
-    }
+    // Dequantisation parameters per cell (main stream, concurrent with DC
+    // and LF).
+    dim3 b2(32, 8), gr1(Blocks(g.Bx, 32), Blocks(g.By, 8));
+    k_cell_params<<<gr1, b2, 0, st>>>(g, f, s); ++ctx->launches;
     if (ctx->keep_stages) {
-      cudaMemcpyAsync(ctx->dbg_dequant.p, f.ac,
-                      sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
-                      cudaMemcpyDeviceToDevice, st);
+      // The dequantised AC for export (PIKGPU_STAGE_DEQUANT_AC).
+      if (ctx->use_dq_ovr) {
+        cudaMemcpyAsync(f.ac, ctx->dq_ovr.p,
+                        sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
+                        cudaMemcpyDeviceToDevice, st);
+      } else {
+        dim3 gr(Blocks(g.Bx, kDequantCells), g.By);
+        k_dequant_ac<<<gr, 256, 0, st>>>(g, f, s); ++ctx->launches;
+      }
     }
     br.Join(0, 1);
-    dim3 b2(32, 8), gr2(Blocks(g.Bx, 32), Blocks(g.By, 8), 3);
-    k_lf_update<<<gr2, b2, 0, st>>>(g, f, s.predict_lf, s.predict_hf); ++ctx->launches;
   }
   Mark(ctx, kTIdct);
   br.Fork(1, ctx->kSide);
@@ -643,7 +657,6 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     // here only its min/max), or the IDCT output itself (sharpened guide,
     // or no gaborish).
     const int gab = s.use_sharpened ? 0 : s.gaborish;
-    k_minmax_init<<<1, 32, 0, st>>>(mm); ++ctx->launches;
     if (gab) {
       const int warps = Blocks(g.PW, 128) * Blocks(g.PH, kGmmRows);
       k_gaborish_minmax<<<dim3(Blocks(warps, 8), 3), 256, 0, st>>>(
@@ -653,17 +666,18 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
                                                                mm); ++ctx->launches;
     }
     Mark(ctx, kTEpf);
-    const int nb = g.Bx * g.By;
     int32_t* sig = P<int32_t>(ctx->sigma);
-    if (ctx->use_sigma_ovr) {
-      cudaMemcpyAsync(sig, ctx->sigma_ovr.p, sizeof(int32_t) * nb,
-                      cudaMemcpyDeviceToDevice, st);
-    } else {
-      k_epf_sigma<<<Blocks(nb, 256), 256, 0, st>>>(nb, f.qf, f.acs, f.lut, 0,
-                                                   mm, sig); ++ctx->launches;
-    }
-    RunEpf(ctx, st, f.idct, f.idct, gab, g.PW, g.PH, sig, f.filt,
-           ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr);
+    EpfSigma sgs{};
+    sgs.ovr = ctx->use_sigma_ovr ? P<int32_t>(ctx->sigma_ovr) : nullptr;
+    sgs.qf = f.qf;
+    sgs.acs = f.acs;
+    sgs.lut = f.lut;
+    sgs.fixed = s.epf_fixed_sigma;
+    sgs.out = sig;
+    EpfLaunch(st, ctx->num_sms, ctx->form, f.idct, f.idct, gab, g.PW, g.PH,
+              mm, sgs, f.filt,
+              ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr,
+              EpfDc{}); ++ctx->launches;
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_epf.p, f.filt, sizeof(float) * 3 * npx,
                       cudaMemcpyDeviceToDevice, st);
@@ -671,8 +685,6 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     Mark(ctx, kTAr);
     // Only blocks the EPF filtered need the clamp (see k_active_blocks).
     if (f.clamp_tape) cudaMemsetAsync(f.clamp_tape, 0, nac, st);
-    int* counters = P<int>(ctx->counters);
-    cudaMemsetAsync(counters, 0, sizeof(int) * kNumClasses, st);
     br.Fork(2, ctx->kSide);
     for (int k = 0; k < kNumClasses; ++k) {
       if (!n[k]) continue;
@@ -895,9 +907,9 @@ int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
                     &ctx->dq_cf,   &ctx->dq_map,    &ctx->ytox,
                     &ctx->ytob,    &ctx->table,     &ctx->offsets,
                     &ctx->qdc,     &ctx->qac,       &ctx->dc,
-                    &ctx->dcpad,   &ctx->dcfilt,    &ctx->ac,
-                    &ctx->llf_g,   &ctx->lf2x2_g,   &ctx->pred2x2_g,
-                    &ctx->tmp2x2_g, &ctx->idct,     &ctx->smoothed,
+                    &ctx->dcpad,   &ctx->cellp,
+                    &ctx->corner,
+                    &ctx->pred2x2_g, &ctx->idct,    &ctx->smoothed,
                     &ctx->filt,    &ctx->mm,        &ctx->sigma,
                     &ctx->dc_sigma, &ctx->out_lin,  &ctx->out_rgb8,
                     &ctx->dbg_dequant, &ctx->dbg_epf, &ctx->dbg_pre,
@@ -964,6 +976,12 @@ int pikgpu_set_option(pikgpu_ctx* ctx, int option, int value) {
         return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "form %d", value);
       }
       ctx->form = value;
+      return PIKGPU_OK;
+    case PIKGPU_OPT_TC_WAIT_POLLS:
+      if (value < -1) {
+        return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "wait polls %d", value);
+      }
+      ctx->tc_polls = value < 0 ? tc::kMaxPolls : uint32_t(value);
       return PIKGPU_OK;
   }
   return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "unknown option %d", option);
@@ -1035,12 +1053,9 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
       {&ctx->qac, 2 * 3 * nac},
       {&ctx->dc, 4 * 3 * nb},
       {&ctx->dcpad, 4 * 3 * size_t(dpw) * dph},
-      {&ctx->dcfilt, 4 * 3 * size_t(dpw) * dph},
-      {&ctx->ac, 4 * 3 * nac},
-      {&ctx->llf_g, 4 * kLlfGroupFloats * ng},
-      {&ctx->lf2x2_g, 4 * kG2GroupFloats * ng},
+      {&ctx->cellp, sizeof(CellDq) * nb},
+      {&ctx->corner, 4 * 3 * 4 * nb},
       {&ctx->pred2x2_g, 4 * kG2GroupFloats * ng},
-      {&ctx->tmp2x2_g, 4 * kG2GroupFloats * ng},
       {&ctx->idct, 4 * 3 * npx},
       {&ctx->filt, 4 * 3 * npx},
       {&ctx->mm, 64},

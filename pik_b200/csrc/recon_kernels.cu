@@ -205,46 +205,6 @@ __device__ __forceinline__ void GroupDims(const Geo& g, int gi, int* x0,
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// DC: DequantDC (pik/compressed_dc.cc:181-231).
-__global__ void k_dequant_dc(Geo g, DevFrame f, FrameScalars s) {
-  const int n = g.Bx * g.By;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float y = float(f.qdc[n + i]) * s.mul_dc[1];
-  f.dc[n + i] = y;
-  f.dc[i] = s.ytox_dc * y + float(f.qdc[i]) * s.mul_dc[0];
-  f.dc[2 * n + i] = s.ytob_dc * y + float(f.qdc[2 * n + i]) * s.mul_dc[2];
-}
-
-// PadImageToMultiple(dc, 8) (pik/image.cc:45-77): replicate the last
-// column/row. out: 3 x ph x pw.
-__global__ void k_pad_replicate(const float* in, int w, int h, float* out,
-                                int pw, int ph) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int c = blockIdx.z;
-  if (x >= pw || y >= ph) return;
-  out[(size_t(c) * ph + y) * pw + x] =
-      in[(size_t(c) * h + min(y, h - 1)) * w + min(x, w - 1)];
-}
-
-// AdaptiveDCReconstruction's final clamp (pik/adaptive_reconstruction.cc:
-// 319-331): dc = max(dc - step, min(denoised, dc + step)).
-__global__ void k_dc_clamp(float* dc, const float* den, int w, int h, int pw,
-                           int ph, float hs0, float hs1, float hs2) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int c = blockIdx.z;
-  if (x >= w || y >= h) return;
-  const float hs = c == 0 ? hs0 : c == 1 ? hs1 : hs2;
-  float& v = dc[(size_t(c) * h + y) * w + x];
-  const float d = den[(size_t(c) * ph + y) * pw + x];
-  const float lo = v - hs, hi = v + hs;
-  const float m = d < hi ? d : hi;
-  v = lo < m ? m : lo;
-}
-
-// ---------------------------------------------------------------------------
 // Min/max of 3 planes (MinMax, pik/epf_target.cc:980-1006): ordered-integer
 // atomics. mm[0..2] = min, mm[3..5] = max (encoded).
 __device__ __forceinline__ uint32_t OrderedBits(float f) {
@@ -262,9 +222,12 @@ __host__ __device__ inline float FromOrderedBits(uint32_t u) {
 #endif
 }
 
-__global__ void k_minmax_init(uint32_t* mm) {
-  if (threadIdx.x < 3) mm[threadIdx.x] = 0xFFFFFFFFu;
-  else if (threadIdx.x < 6) mm[threadIdx.x] = 0u;
+// Start of a frame: the two min/max sets (the frame EPF's at mm[0..5], the
+// DC EPF's at mm[8..13]) reset to empty, and `n` counters to 0.
+__global__ void k_frame_init(uint32_t* mm, int* counters, int n) {
+  const int t = threadIdx.x;
+  if (t < 16) mm[t] = (t & 7) < 3 ? 0xFFFFFFFFu : 0u;
+  if (t < n) counters[t] = 0;
 }
 
 __global__ void __launch_bounds__(256)
@@ -298,6 +261,53 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// DC: DequantDC (pik/compressed_dc.cc:181-231) into `dc`, the 8-padded copy
+// of AdaptiveDCReconstruction (PadImageToMultiple, pik/image.cc:45-77: the
+// last column and row replicated) into `pad` (3 x ph x pw), and its
+// min/max (MinMax, pik/epf_target.cc:980-1006; replication adds no value)
+// into mm[0..5]. One thread per padded position, all three channels.
+__global__ void __launch_bounds__(256)
+    k_dc_prep(Geo g, DevFrame f, FrameScalars s, float* pad, int pw, int ph,
+              uint32_t* mm) {
+  __shared__ uint32_t s_mm[8][6];
+  const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+  uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0, 0, 0};
+  if (x < pw && y < ph) {
+    const int n = g.Bx * g.By;
+    const int i = min(y, g.By - 1) * g.Bx + min(x, g.Bx - 1);
+    const float yv = float(f.qdc[n + i]) * s.mul_dc[1];
+    const float v[3] = {s.ytox_dc * yv + float(f.qdc[i]) * s.mul_dc[0], yv,
+                        s.ytob_dc * yv + float(f.qdc[2 * n + i]) * s.mul_dc[2]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (x < g.Bx && y < g.By) f.dc[c * n + i] = v[c];
+      pad[(size_t(c) * ph + y) * pw + x] = v[c];
+      lo[c] = hi[c] = OrderedBits(v[c]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    for (int off = 16; off; off >>= 1) {
+      lo[c] = min(lo[c], __shfl_xor_sync(0xFFFFFFFFu, lo[c], off));
+      hi[c] = max(hi[c], __shfl_xor_sync(0xFFFFFFFFu, hi[c], off));
+    }
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s_mm[w][c] = lo[c], s_mm[w][3 + c] = hi[c];
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int k = threadIdx.x;
+    uint32_t v = s_mm[0][k];
+    for (int i = 1; i < 8; ++i) v = k < 3 ? min(v, s_mm[i][k]) : max(v, s_mm[i][k]);
+    if (k < 3) atomicMin(&mm[k], v);
+    else atomicMax(&mm[k], v);
+  }
+}
+
 // Stretch and guide multiplier from the min/max (AdaptiveFilter and
 // MakeGuide, pik/epf_target.cc:1040-1047, 1140-1151).
 __device__ __forceinline__ void GuideParams(const uint32_t* mm, float* all_min,
@@ -314,19 +324,10 @@ __device__ __forceinline__ void GuideParams(const uint32_t* mm, float* all_min,
   *stretch = amin == amax ? 1.0f : 255.0f / range;
 }
 
-// SigmaFromQuant (pik/epf_target.cc:1072-1111) per 8x8 block.
-// If qf == nullptr, every block uses `const_qf` with a DCT strategy and LUT 0
-// (AdaptiveDCReconstruction, pik/adaptive_reconstruction.cc:300-318).
-__global__ void k_epf_sigma(int nb, const int32_t* qf, const uint8_t* acs,
-                            const uint8_t* lut, int const_qf,
-                            const uint32_t* mm, int32_t* sigma) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nb) return;
-  float amin, mul, stretch;
-  GuideParams(mm, &amin, &mul, &stretch);
-  const float ac_q = float(qf ? qf[i] : const_qf);
-  const float scale = qf ? ARQuantScaleOf(acs[i] >> 4) : 1.0f;
-  const int lut_id = qf ? lut[i] : 0;
+// SigmaFromQuant (pik/epf_target.cc:1072-1111) of one 8x8 block with raw
+// quant field ac_q, strategy scale (ARQuantScale) and LUT `lut_id`.
+__device__ __forceinline__ int SigmaFromQuant(float ac_q, float scale,
+                                              int lut_id, float stretch) {
   const float quant = ac_q * scale * 0.039324273f;
   float unscaled;
   const float* l = c_t.sigma_lut[lut_id];
@@ -340,130 +341,8 @@ __global__ void k_epf_sigma(int nb, const int32_t* qf, const uint8_t* acs,
     const float frac = pos - float(trunc);
     unscaled = frac * l[trunc + 1] + (1.0f - frac) * l[trunc];
   }
-  const int s = int(unscaled * stretch + 0.5182760822018414f);
-  sigma[i] = min(s, kMaxSigma);
-}
-
-// EPF filter (AdaptiveFilter + WeightedSum, pik/epf_target.cc:526-801,
-// 1113-1278): 16x16 output pixels per CTA, one per thread.
-constexpr int kEpfTile = 16;
-constexpr int kGuideW = kEpfTile + 10;  // x - 4 .. x + 6
-constexpr int kGuideH = kEpfTile + 8;   // y - 4 .. y + 4
-constexpr int kInW = kEpfTile + 7;      // x - 3 .. x + 4
-constexpr int kInH = kEpfTile + 6;      // y - 3 .. y + 3
-
-__device__ __forceinline__ float WeightFast(int mul, int sad) {
-  const int clamped = min(sad, 507);
-  const int prescaled = int(int16_t(clamped << 6));
-  const int unbiased = (prescaled * mul) >> 16;
-  const int biased = int(int16_t(unbiased + (127 << 7)));
-  return __uint_as_float(uint32_t(uint16_t(biased)) << 16);
-}
-
-__global__ void __launch_bounds__(256)
-    k_epf(const float* in, const float* guide_src, const uint8_t* guide_ovr,
-          int w, int h, const uint32_t* mm, const int32_t* sigma,
-          float* out) {
-  __shared__ uint8_t sg[3][kGuideH][kGuideW];
-  __shared__ float si[3][kInH][kInW];
-  const int x0 = blockIdx.x * kEpfTile, y0 = blockIdx.y * kEpfTile;
-  const int tid = threadIdx.x;
-  const size_t plane = size_t(w) * h;
-  const int bw = w / 8;
-  {
-    // Tiles whose 2x2 blocks all have sigma < kMinSigma are plain copies
-    // (CopyOriginalBlock, pik/epf_target.cc:1228-1236).
-    bool any = false;
-    for (int i = 0; i < 4; ++i) {
-      const int bx = x0 / 8 + (i & 1), by = y0 / 8 + (i >> 1);
-      if (bx * 8 < w && by * 8 < h && sigma[by * bw + bx] >= kMinSigma) {
-        any = true;
-      }
-    }
-    if (!any) {
-      const int lx = tid % kEpfTile, ly = tid / kEpfTile;
-      const int x = x0 + lx, y = y0 + ly;
-      if (x < w && y < h) {
-        for (int c = 0; c < 3; ++c) {
-          out[c * plane + size_t(y) * w + x] =
-              in[c * plane + size_t(y) * w + x];
-        }
-      }
-      return;
-    }
-  }
-  float amin, mul, stretch;
-  GuideParams(mm, &amin, &mul, &stretch);
-  const int gw = w + 12;
-  for (int i = tid; i < 3 * kGuideH * kGuideW; i += 256) {
-    const int c = i / (kGuideH * kGuideW);
-    const int r = (i / kGuideW) % kGuideH, col = i % kGuideW;
-    const int gx = x0 - 4 + col, gy = y0 - 4 + r;
-    uint8_t v;
-    if (guide_ovr) {
-      // Positions beyond the 6-pixel border are never used by valid pixels.
-      const bool inside = gx >= -6 && gx < w + 6 && gy >= -6 && gy < h + 6;
-      v = inside ? guide_ovr[(size_t(c) * (h + 12) + gy + 6) * gw + gx + 6]
-                 : uint8_t(0);
-    } else {
-      const float s = guide_src[c * plane + size_t(MirrorIdx(gy, h)) * w +
-                                MirrorIdx(gx, w)];
-      const float scaled = (s - amin) * mul;
-      v = uint8_t(uint32_t(__float2int_rz(scaled)));
-    }
-    sg[c][r][col] = v;
-  }
-  for (int i = tid; i < 3 * kInH * kInW; i += 256) {
-    const int c = i / (kInH * kInW);
-    const int r = (i / kInW) % kInH, col = i % kInW;
-    const int gx = x0 - 3 + col, gy = y0 - 3 + r;
-    si[c][r][col] =
-        in[c * plane + size_t(MirrorIdx(gy, h)) * w + MirrorIdx(gx, w)];
-  }
-  __syncthreads();
-  const int lx = tid % kEpfTile, ly = tid / kEpfTile;
-  const int x = x0 + lx, y = y0 + ly;
-  if (x >= w || y >= h) return;
-  const int sg_ = sigma[(y / 8) * bw + x / 8];
-  if (sg_ < kMinSigma) {
-    for (int c = 0; c < 3; ++c) out[c * plane + size_t(y) * w + x] =
-        si[c][ly + 3][lx + 3];
-    return;
-  }
-  const int m = c_t.mul_table[sg_];
-  // Reference patch (3 x 4 around the pixel, top-left at (-1, -1)).
-  int ref[3][3][4];
-  for (int c = 0; c < 3; ++c)
-    for (int py = 0; py < 3; ++py)
-      for (int px = 0; px < 4; ++px)
-        ref[c][py][px] = sg[c][ly + 4 + py - 1][lx + 4 + px - 1];
-  float ws0 = 0.f, ws1 = 0.f, ws2 = 0.f, sw = 0.f;
-  for (int cy = -3; cy <= 3; ++cy) {
-    for (int cx = -3; cx <= 4; ++cx) {
-      int sad_max = 0;
-      for (int c = 0; c < 3; ++c) {
-        int sad = 0;
-#pragma unroll
-        for (int py = 0; py < 3; ++py) {
-#pragma unroll
-          for (int px = 0; px < 4; ++px) {
-            sad += abs(ref[c][py][px] -
-                       int(sg[c][ly + 4 + cy + py - 1][lx + 4 + cx + px - 1]));
-          }
-        }
-        sad_max = max(sad_max, sad);
-      }
-      float wgt = WeightFast(m, sad_max);
-      if (!(wgt >= 0.05f)) wgt = 0.0f;
-      ws0 += si[0][ly + 3 + cy][lx + 3 + cx] * wgt;
-      ws1 += si[1][ly + 3 + cy][lx + 3 + cx] * wgt;
-      ws2 += si[2][ly + 3 + cy][lx + 3 + cx] * wgt;
-      sw += wgt;
-    }
-  }
-  out[size_t(y) * w + x] = ws0 / sw;
-  out[plane + size_t(y) * w + x] = ws1 / sw;
-  out[2 * plane + size_t(y) * w + x] = ws2 / sw;
+  const int sg = int(unscaled * stretch + 0.5182760822018414f);
+  return min(sg, kMaxSigma);
 }
 
 // Guide decision export (verification hook): u8 guide with the 6-pixel
@@ -583,13 +462,62 @@ __global__ void __launch_bounds__(256) k_dequant_ac(Geo g, DevFrame f,
   d2[1] = make_float4(o2[4], o2[5], o2[6], o2[7]);
 }
 
+// Dequant::DoAC's parameters of cell (bx, by) (pik/compressed_image.cc:
+// 636-672): the operands of k_dequant_ac's arithmetic, formed the same way.
+__device__ __forceinline__ CellDq CellParamsOf(const Geo& g, const DevFrame& f,
+                                               const FrameScalars& s, int bx,
+                                               int by) {
+  const int cell = by * g.Bx + bx;
+  const int qf = f.qf[cell];
+  const int tx = bx >> 3, ty = by >> 3;
+  const int cf = f.dq_cf[ty * g.Tx + tx];
+  const int table = f.dq_map[cf * 256 + (qf - 1)];
+  const int a = f.acs[cell];
+  const int kind = QuantKindOf(a >> 4), blk = a & 0xF;
+  CellDq p;
+  p.scaled = qf == 0 ? 1E10f : s.inv_global_scale / float(qf);
+  p.x_cc = 1.0f * float(f.ytox[ty * g.Tx + tx] - 128) * (1.0f / 256);
+  p.b_cc = 1.0f * float(f.ytob[ty * g.Tx + tx]) * (1.0f / 128);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    p.m[c] = f.offsets[(table * 7 + kind) * 3 + c] + uint32_t(blk) * 64;
+  }
+  p.pad[0] = p.pad[1] = 0;
+  return p;
+}
+
+// Coefficient k of channel c of a cell with parameters p at AC position
+// `pos` (By x ac_stride plane layout): k_dequant_ac's arithmetic and order.
+__device__ __forceinline__ float DequantWith(const Geo& g, const DevFrame& f,
+                                             const CellDq& p, int c,
+                                             size_t pos, int k) {
+  const size_t plane = size_t(g.ac_stride) * g.By;
+  const float dy = AdjustQuantBias(float(f.qac[plane + pos]), c_t.one_bias[1]) *
+                   (f.table[p.m[1] + k] * p.scaled);
+  if (c == 1) return dy;
+  const float dq = AdjustQuantBias(float(f.qac[c * plane + pos]),
+                                   c_t.one_bias[c]) *
+                   (f.table[p.m[c] + k] * p.scaled);
+  return (c == 0 ? p.x_cc : p.b_cc) * dy + dq;
+}
+
+// Element (r, l), r, l < 2 cov, of the low-frequency corner of the block
+// whose first cell is (bx, by) (the layout of DevFrame::corner).
+__device__ __forceinline__ size_t CornerIdx(const Geo& g, int c, int bx,
+                                            int by, int r, int l) {
+  return ((size_t(c) * g.By + by + (r >> 1)) * g.Bx + bx + (l >> 1)) * 4 +
+         (r & 1) * 2 + (l & 1);
+}
+
 // ---------------------------------------------------------------------------
 // Per-group LF prediction (ComputeLlf, PredictLf, pik/ac_predictions.cc:
-// 380-470). Group-local cell (bx, by) in [0, gxs+2) x [0, gys+2); the border
-// ring acts as DCT8; DC from the frame with mirroring (InitializeDecCache,
-// pik/compressed_dc.cc:530-556). One CTA runs all phases of one group and
-// channel (k_lf_chain), with a barrier between phases: the phases are small
-// and were launch- and latency-bound as separate kernels.
+// 380-470) and UpdateLfForDecoder (pik/ac_predictions.cc:560-635,
+// pik/compressed_image.cc:978-1084). Group-local cell (bx, by) in
+// [0, gxs+2) x [0, gys+2); the border ring acts as DCT8; DC from the frame
+// with mirroring (InitializeDecCache, pik/compressed_dc.cc:530-556). One
+// CTA runs all phases of one group and channel (k_lf_chain), with a barrier
+// between phases, and keeps the group's LLF, 2x2 and LF images in shared
+// memory; only pred2x2 and the blocks' corners leave the kernel.
 struct LfGroup {
   int gi, c, x0, y0, gxs, gys;
   __device__ int Acs(const Geo& g, const DevFrame& f, int bx, int by) const {
@@ -598,8 +526,12 @@ struct LfGroup {
   }
 };
 
+// Shared memory of k_lf_chain: the LLF image (kGB x kGB), the 2x2 image
+// before and after LFPredictionBlur (kG2 x kG2 each).
+constexpr size_t kLfSmemBytes = 4 * (size_t(kGB) * kGB + 2 * size_t(kG2) * kG2);
+
 __device__ void LlfCell(const Geo& g, const DevFrame& f, const LfGroup& q,
-                        int bx, int by) {
+                        float* llf, int bx, int by) {
   const int a = q.Acs(g, f, bx, by);
   if (a & 0xF) return;
   const int type = a >> 4, cov = Covered(type);
@@ -610,26 +542,21 @@ __device__ void LlfCell(const Geo& g, const DevFrame& f, const LfGroup& q,
           f.dc[(size_t(q.c) * g.By + MirrorIdx(q.y0 + by - 1 + iy, g.By)) *
                    g.Bx +
                MirrorIdx(q.x0 + bx - 1 + ix, g.Bx)];
-  float* llf = f.llf_g + q.gi * kLlfGroupFloats + q.c * kGB * kGB;
   LowestFreqFromDC(type, dc, 4, llf + by * kGB + bx, kGB);
 }
 
 __device__ void Tmp2x2Cell(const Geo& g, const DevFrame& f, const LfGroup& q,
-                           int bx, int by) {
+                           const float* llf, float* tmp, int bx, int by) {
   const int a = q.Acs(g, f, bx, by);
   if (a & 0xF) return;
-  const float* llf = f.llf_g + q.gi * kLlfGroupFloats + q.c * kGB * kGB;
-  float* tmp = f.tmp2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   DC2x2FromLowestFreq(a >> 4, llf + by * kGB + bx, kGB,
                       tmp + 2 * by * kG2 + 2 * bx, kG2);
 }
 
 // LFPredictionBlur over the group's 2x2 image (ConvolveT<Symmetric3>).
-__device__ void LfBlurPixel(const DevFrame& f, const LfGroup& q, int x,
-                            int y) {
+__device__ void LfBlurPixel(const LfGroup& q, const float* tmp, float* lf,
+                            int x, int y) {
   const int w2 = 2 * (q.gxs + 2), h2 = 2 * (q.gys + 2);
-  const float* tmp = f.tmp2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
-  float* lf = f.lf2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   const float* t = tmp + MirrorIdx(y - 1, h2) * kG2;
   const float* m = tmp + y * kG2;
   const float* b = tmp + MirrorIdx(y + 1, h2) * kG2;
@@ -647,16 +574,16 @@ __device__ void LfBlurPixel(const DevFrame& f, const LfGroup& q, int x,
 }
 
 __device__ void LfFrom2x2Cell(const Geo& g, const DevFrame& f,
-                              const LfGroup& q, int bx, int by) {
+                              const LfGroup& q, float* lf, int bx, int by) {
   const int a = q.Acs(g, f, bx, by);
   if (a & 0xF) return;
-  float* lf = f.lf2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   LowFreqFromDC2x2(a >> 4, lf + 2 * by * kG2 + 2 * bx, kG2);
 }
 
 // Border ring of pred2x2 (pik/compressed_image.cc:978-1039); ring cell i:
 // 2 columns of (gys + 2), then 2 rows of (gxs + 2).
-__device__ void PredBorderCell(const DevFrame& f, const LfGroup& q, int i,
+__device__ void PredBorderCell(const DevFrame& f, const LfGroup& q,
+                               const float* llf, const float* lf, int i,
                                int predict_lf) {
   int x, y;
   if (i < 2 * (q.gys + 2)) {
@@ -667,8 +594,6 @@ __device__ void PredBorderCell(const DevFrame& f, const LfGroup& q, int i,
     y = (j & 1) ? q.gys + 1 : 0;
     x = j >> 1;
   }
-  const float* llf = f.llf_g + q.gi * kLlfGroupFloats + q.c * kGB * kGB;
-  const float* lf = f.lf2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   float* pred = f.pred2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   if (predict_lf) {
     float blk[10];
@@ -684,86 +609,227 @@ __device__ void PredBorderCell(const DevFrame& f, const LfGroup& q, int i,
   }
 }
 
-// 1024 threads (one CTA per SM: 3 x groups CTAs): the phases wait on L2 per
-// cell, and twice the warps hide it better (0.053 -> 0.044 ms at 4K) in
-// spite of a small register spill at 64 registers per thread.
+// UpdateLfForDecoder for the first block at group-local (lbx, lby): its
+// low-frequency corner -- the LLF from DC, the LF coefficients (dequantised
+// here, like Dequant::DoAC) plus the LF prediction -- into DevFrame::corner,
+// and the block's pred2x2 cells from it.
+__device__ void CornerBlock(const Geo& g, const DevFrame& f,
+                            const FrameScalars& s, const LfGroup& q,
+                            const float* llf, const float* lf, int lbx,
+                            int lby, int predict_lf, int predict_hf) {
+  const int bx = q.x0 + lbx, by = q.y0 + lby;
+  const int a = f.acs[by * g.Bx + bx];
+  if (a & 0xF) return;
+  const int type = a >> 4, cov = Covered(type), n = 8 * cov, c = q.c;
+  const size_t plane = size_t(g.ac_stride) * g.By;
+  float cv[8][8];
+  CellDq p{};
+  int pcell = -1;
+  for (int r = 0; r < 2 * cov; ++r) {
+    // Row r of the corner: block row by (r < 8), cell bx + r n / 64 (the
+    // 2 cov columns stay inside it).
+    const int cx = bx + (r * n) / 64;
+    if (!f.ac_in && cx != pcell) {
+      p = CellParamsOf(g, f, s, cx, by);
+      pcell = cx;
+    }
+    for (int l = 0; l < 2 * cov; ++l) {
+      float v;
+      if (r < cov && l < cov) {
+        v = llf[(lby + 1 + r) * kGB + lbx + 1 + l];
+      } else {
+        const int k = (r * n + l) % 64;
+        const size_t pos = size_t(by) * g.ac_stride + size_t(cx) * 64 + k;
+        v = f.ac_in ? f.ac_in[c * plane + pos] : DequantWith(g, f, p, c, pos, k);
+        if (predict_lf) {
+          v += lf[(2 * (lby + 1) + r) * kG2 + 2 * (lbx + 1) + l];
+        }
+      }
+      cv[r][l] = v;
+      f.corner[CornerIdx(g, c, bx, by, r, l)] = v;
+    }
+  }
+  if (predict_hf) {
+    float* pred = f.pred2x2_g + q.gi * kG2GroupFloats + c * kG2 * kG2;
+    DC2x2FromLowFreq(type, [&](int i) { return cv[i / n][i % n]; },
+                     pred + 2 * (lby + 1) * kG2 + 2 * (lbx + 1), kG2);
+  }
+}
+
+// 1024 threads, one CTA per group and channel (blockIdx.x = 3 gi + c).
 constexpr int kLfThreads = 1024;
 
-// All LF prediction phases of one group and channel (blockIdx.x = 3 gi + c):
-// LLF from DC; then, with LF prediction, the 2x2 image, its blur and the LF
-// coefficients from it; then, with HF prediction, the pred2x2 border ring.
+// All LF phases of one group and channel: LLF from DC; then, with LF
+// prediction, the 2x2 image, its blur and the LF coefficients from it;
+// with HF prediction, the pred2x2 border ring; and every first block's
+// corner (and pred2x2 cells).
 __global__ void __launch_bounds__(kLfThreads)
-    k_lf_chain(Geo g, DevFrame f, int predict_lf, int predict_hf) {
+    k_lf_chain(Geo g, DevFrame f, FrameScalars s, int predict_lf,
+               int predict_hf) {
+  extern __shared__ float lf_smem[];
+  float* llf = lf_smem;             // kGB x kGB
+  float* tmp = llf + kGB * kGB;     // kG2 x kG2
+  float* lf = tmp + kG2 * kG2;      // kG2 x kG2
   LfGroup q;
   q.gi = blockIdx.x / 3;
   q.c = blockIdx.x % 3;
   GroupDims(g, q.gi, &q.x0, &q.y0, &q.gxs, &q.gys);
   const int cw = q.gxs + 2, ncell = cw * (q.gys + 2);
   for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
-    LlfCell(g, f, q, i % cw, i / cw);
+    LlfCell(g, f, q, llf, i % cw, i / cw);
   }
   __syncthreads();
   if (predict_lf) {
     for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
-      Tmp2x2Cell(g, f, q, i % cw, i / cw);
+      Tmp2x2Cell(g, f, q, llf, tmp, i % cw, i / cw);
     }
     __syncthreads();
     const int w2 = 2 * cw, n2 = w2 * 2 * (q.gys + 2);
     for (int i = threadIdx.x; i < n2; i += kLfThreads) {
-      LfBlurPixel(f, q, i % w2, i / w2);
+      LfBlurPixel(q, tmp, lf, i % w2, i / w2);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
-      LfFrom2x2Cell(g, f, q, i % cw, i / cw);
+      LfFrom2x2Cell(g, f, q, lf, i % cw, i / cw);
     }
     __syncthreads();
   }
   if (predict_hf) {
     const int nring = 2 * (q.gys + 2) + 2 * (q.gxs + 2);
     for (int i = threadIdx.x; i < nring; i += kLfThreads) {
-      PredBorderCell(f, q, i, predict_lf);
+      PredBorderCell(f, q, llf, lf, i, predict_lf);
+    }
+  }
+  const int nblk = q.gxs * q.gys;
+  for (int i = threadIdx.x; i < nblk; i += kLfThreads) {
+    CornerBlock(g, f, s, q, llf, lf, i % q.gxs, i / q.gxs, predict_lf,
+                predict_hf);
+  }
+}
+
+// Dequant::DoAC's parameters of every cell, for the transforms that
+// dequantise the int16 AC as they load it.
+__global__ void k_cell_params(Geo g, DevFrame f, FrameScalars s) {
+  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int by = blockIdx.y * blockDim.y + threadIdx.y;
+  if (bx >= g.Bx || by >= g.By) return;
+  const CellDq p = CellParamsOf(g, f, s, bx, by);
+  uint4* dst = reinterpret_cast<uint4*>(const_cast<CellDq*>(f.cellp) +
+                                        by * g.Bx + bx);
+  dst[0] = make_uint4(__float_as_uint(p.scaled), __float_as_uint(p.x_cc),
+                      __float_as_uint(p.b_cc), p.m[0]);
+  dst[1] = make_uint4(p.m[1], p.m[2], 0u, 0u);
+}
+
+// Coefficient k of channel c of cell (bx, by), dequantised (k_dequant_ac's
+// arithmetic and order), or taken from the supplied dequantised AC.
+__device__ __forceinline__ float DequantOne(const Geo& g, const DevFrame& f,
+                                            int c, int bx, int by, int k) {
+  const size_t plane = size_t(g.ac_stride) * g.By;
+  const size_t pos = size_t(by) * g.ac_stride + size_t(bx) * 64 + k;
+  if (f.ac_in) return f.ac_in[c * plane + pos];
+  return DequantWith(g, f, f.cellp[by * g.Bx + bx], c, pos, k);
+}
+
+// n consecutive dequantised values: int16 `q` (16-byte aligned) times
+// (matrix row `m` x scaled) after AdjustQuantBias.
+template <int n>
+__device__ __forceinline__ void DequantRun(const int16_t* q, const float* m,
+                                           float scaled, float one_bias,
+                                           float* out) {
+  const bool mvec = (reinterpret_cast<uintptr_t>(m) & 15) == 0;
+#pragma unroll
+  for (int i = 0; i < n; i += 8) {
+    const uint4 raw = *reinterpret_cast<const uint4*>(q + i);
+    float mv[8];
+    if (mvec) {
+      const float4 m0 = *reinterpret_cast<const float4*>(m + i);
+      const float4 m1 = *reinterpret_cast<const float4*>(m + i + 4);
+      mv[0] = m0.x, mv[1] = m0.y, mv[2] = m0.z, mv[3] = m0.w;
+      mv[4] = m1.x, mv[5] = m1.y, mv[6] = m1.z, mv[7] = m1.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) mv[k] = m[i + k];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t word = k < 2 ? raw.x : k < 4 ? raw.y : k < 6 ? raw.z
+                                                                : raw.w;
+      const int16_t qi = int16_t(word >> (16 * (k & 1)));
+      const float mulc = mv[k] * scaled;
+      out[i + k] = AdjustQuantBias(float(qi), one_bias) * mulc;
     }
   }
 }
 
-// UpdateLfForDecoder (pik/ac_predictions.cc:560-635) over first blocks:
-// writes the LLF into the coefficients, adds the LF prediction and forms the
-// block's pred2x2 cells.
-__global__ void k_lf_update(Geo g, DevFrame f, int predict_lf,
-                            int predict_hf) {
-  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int by = blockIdx.y * blockDim.y + threadIdx.y;
-  const int c = blockIdx.z;
-  if (bx >= g.Bx || by >= g.By) return;
-  const int a = f.acs[by * g.Bx + bx];
-  if (a & 0xF) return;
-  const int type = a >> 4, cov = Covered(type);
-  const int gi = (by >> 6) * g.Gx + (bx >> 6);
-  const int lbx = bx & 63, lby = by & 63;
-  const float* llf = f.llf_g + gi * kLlfGroupFloats + c * kGB * kGB;
-  const float* lf = f.lf2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
-  float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
-  float* base = f.ac + size_t(c) * g.ac_stride * g.By +
-                size_t(by) * g.ac_stride + size_t(bx) * 64;
-  const int chunk = 64 * cov;
-  auto at = [&](int i) -> float& {
-    return base[(i / chunk) * size_t(g.ac_stride) + i % chunk];
-  };
-  for (int y = 0; y < cov; ++y)
-    for (int x = 0; x < cov; ++x)
-      at(cov * 8 * y + x) = llf[(lby + 1 + y) * kGB + lbx + 1 + x];
-  if (predict_lf) {
-    for (int y = 0; y < 2 * cov; ++y) {
-      const int start = y < cov ? cov : 0;
-      for (int x = start; x < 2 * cov; ++x) {
-        at(y * cov * 8 + x) += lf[(2 * (lby + 1) + y) * kG2 + 2 * (lbx + 1) + x];
-      }
+// Coefficients k0 .. k0 + n - 1 of channel c of cell (bx, by) (n a multiple
+// of 8, k0 of n): Dequant::DoAC (pik/compressed_image.cc:636-700) applied
+// as they are loaded -- Y, then X and B plus their chroma-from-luma share
+// of Y, in k_dequant_ac's operation order -- or the supplied dequantised AC.
+template <int n>
+__device__ __forceinline__ void CellCoefs(const Geo& g, const DevFrame& f,
+                                          int c, int bx, int by, int k0,
+                                          float* out) {
+  const size_t plane = size_t(g.ac_stride) * g.By;
+  const size_t pos = size_t(by) * g.ac_stride + size_t(bx) * 64 + k0;
+  if (f.ac_in) {
+    const float4* src =
+        reinterpret_cast<const float4*>(f.ac_in + c * plane + pos);
+#pragma unroll
+    for (int i = 0; i < n / 4; ++i) {
+      const float4 v = src[i];
+      out[4 * i] = v.x, out[4 * i + 1] = v.y;
+      out[4 * i + 2] = v.z, out[4 * i + 3] = v.w;
     }
+    return;
   }
-  if (predict_hf) {
-    DC2x2FromLowFreq(type, [&](int i) { return at(i); },
-                     pred + 2 * (lby + 1) * kG2 + 2 * (lbx + 1), kG2);
+  const uint4* pp = reinterpret_cast<const uint4*>(f.cellp + by * g.Bx + bx);
+  const uint4 p0 = pp[0], p1 = pp[1];
+  const float scaled = __uint_as_float(p0.x);
+  const int16_t* qy = f.qac + plane + pos;
+  const float* my = f.table + p1.x + k0;
+  if (c == 1) {
+    DequantRun<n>(qy, my, scaled, c_t.one_bias[1], out);
+    return;
   }
+  const int16_t* qc = f.qac + c * plane + pos;
+  const float* mc = f.table + (c == 0 ? p0.w : p1.y) + k0;
+  const float cc = __uint_as_float(c == 0 ? p0.y : p0.z);
+  // Eight at a time: Y, then this channel plus its share of Y.
+#pragma unroll
+  for (int i = 0; i < n; i += 8) {
+    float dy[8];
+    DequantRun<8>(qy + i, my + i, scaled, c_t.one_bias[1], dy);
+    DequantRun<8>(qc + i, mc + i, scaled, c_t.one_bias[c], out + i);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) out[i + k] = cc * dy[k] + out[i + k];
+  }
+}
+
+
+// Row r of the N x N coefficient matrix of channel c of the block at
+// (bx, by) (GatherCoefficients layout, pik/ac_strategy.h:255-272: block row
+// by + r / 8, offset (r % 8) N, inside one cell), with its low-frequency
+// corner taken from DevFrame::corner.
+template <int N>
+__device__ __forceinline__ void LoadCoefRow(const Geo& g, const DevFrame& f,
+                                            int c, int bx, int by, int r,
+                                            float (&X)[N]) {
+  constexpr int cov = N / 8;
+  const int off = (r % 8) * N;
+  CellCoefs<N>(g, f, c, bx + off / 64, by + r / 8, off % 64, X);
+  if (r < 2 * cov) {
+#pragma unroll
+    for (int l = 0; l < 2 * cov; ++l) X[l] = f.corner[CornerIdx(g, c, bx, by, r, l)];
+  }
+}
+
+// Coefficient e (0..63) of an 8x8-class block (one cell) with its corner.
+__device__ __forceinline__ float CoefAt8(const Geo& g, const DevFrame& f,
+                                         int c, int bx, int by, int e) {
+  const int r = e >> 3, l = e & 7;
+  if (r < 2 && l < 2) return f.corner[CornerIdx(g, c, bx, by, r, l)];
+  return DequantOne(g, f, c, bx, by, e);
 }
 
 constexpr int kDct4Blocks = 4;  // DCT4X4 blocks per CTA (x 64 coefficients)
@@ -923,8 +989,7 @@ __global__ void __launch_bounds__(256)
   }
   const int first = blockIdx.x * NB;
   const int nb = min(NB, count - first);
-  constexpr int cov = N / 8, chunk = 64 * cov;
-  const size_t plane_ac = size_t(g.ac_stride) * g.By;
+  constexpr int cov = N / 8;
   const size_t plane_px = size_t(g.PW) * g.PH;
   __syncthreads();
   for (int c = 0; c < 3; ++c) {
@@ -933,9 +998,12 @@ __global__ void __launch_bounds__(256)
       const int b = i / NN, e = i % NN;
       const uint32_t pk = list[first + b];
       const int bx = pk & 0xFFFF, by = pk >> 16;
-      const float* base = f.ac + c * plane_ac + size_t(by) * g.ac_stride +
-                          size_t(bx) * 64;
-      s_c[i] = base[(e / chunk) * size_t(g.ac_stride) + e % chunk];
+      // Coefficient (y, x) = (e / N, e % N): block row by + y / 8, cell
+      // bx + ((y % 8) N + x) / 64 (GatherCoefficients layout).
+      const int y = e / N, x = e % N, o = (y % 8) * N + x;
+      s_c[i] = y < 2 * cov && x < 2 * cov
+                   ? f.corner[CornerIdx(g, c, bx, by, y, x)]
+                   : DequantOne(g, f, c, bx + o / 64, by + y / 8, o % 64);
       // DCT_NOHF shares this kernel with DCT but takes no HF prediction.
       if (predict_hf && !PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) {
         s_p[i] = 0.f;
@@ -988,7 +1056,6 @@ __global__ void __launch_bounds__(256)
   }
   const int first = blockIdx.x * NB;
   const int nb = min(NB, count - first);
-  const size_t plane_ac = size_t(g.ac_stride) * g.By;
   const size_t plane_px = size_t(g.PW) * g.PH;
   __syncthreads();
   for (int c = 0; c < 3; ++c) {
@@ -996,7 +1063,7 @@ __global__ void __launch_bounds__(256)
       const int b = i / 64, e = i % 64;
       const uint32_t pk = list[first + b];
       const int bx = pk & 0xFFFF, by = pk >> 16;
-      s_c[i] = f.ac[c * plane_ac + size_t(by) * g.ac_stride + bx * 64 + e];
+      s_c[i] = CoefAt8(g, f, c, bx, by, e);
       if (predict_hf && PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) {
         // Sub-block-major pixel layout: sub-block (sy, sx), pixel (py, px).
         const int sb = e / 16, py = (e % 16) / 4, px = e % 4;
@@ -1168,8 +1235,8 @@ __global__ void k_small_idct(Geo g, DevFrame f, const uint32_t* list,
   const uint32_t pk = list[b];
   const int bx = pk & 0xFFFF, by = pk >> 16;
   const int type = f.acs[by * g.Bx + bx] >> 4;
-  const float* cb = f.ac + c * size_t(g.ac_stride) * g.By +
-                    size_t(by) * g.ac_stride + bx * 64;
+  float cb[64];
+  for (int e = 0; e < 64; ++e) cb[e] = CoefAt8(g, f, c, bx, by, e);
   float* px = f.idct + c * size_t(g.PW) * g.PH + size_t(by * 8) * g.PW + bx * 8;
   SmallInverse(type, cb, px, g.PW);
 }

@@ -80,14 +80,6 @@ __device__ __forceinline__ void GetCol(const float* tile, int r, float (&v)[N]) 
   for (int i = 0; i < N; ++i) v[i] = tile[i * (N + 1) + r];
 }
 
-// Pointer to row r of the block's coefficients in the frame layout: row r
-// of the N x N matrix lives in block row (by + r / 8) at column offset
-// bx * 64 + (r % 8) * N (GatherCoefficients layout, pik/ac_strategy.h:255-272).
-__device__ __forceinline__ size_t CoefRowOffset(const Geo& g, int bx, int by,
-                                                int n, int r) {
-  return size_t(by + r / 8) * g.ac_stride + size_t(bx) * 64 + (r % 8) * n;
-}
-
 }  // namespace square
 
 constexpr int kSquareThreads = 128;
@@ -113,14 +105,8 @@ __global__ void __launch_bounds__(kSquareThreads)
   const int b = active ? item / 3 : 0, c = active ? item % 3 : 0;
   const uint32_t pk = list[b];
   const int bx = pk & 0xFFFF, by = pk >> 16;
-  const size_t plane_ac = size_t(g.ac_stride) * g.By;
-  const float* crow = f.ac + c * plane_ac + CoefRowOffset(g, bx, by, N, r);
   float X[N];
-#pragma unroll
-  for (int i = 0; i < N; i += 4) {
-    const float4 v = *reinterpret_cast<const float4*>(crow + i);
-    X[i] = v.x, X[i + 1] = v.y, X[i + 2] = v.z, X[i + 3] = v.w;
-  }
+  LoadCoefRow<N>(g, f, c, bx, by, r, X);
   if (predict_hf) {
     // DCT_NOHF shares the 8x8 class; its prediction is computed but not
     // added, keeping the warp's control flow uniform.

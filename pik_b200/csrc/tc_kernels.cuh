@@ -81,6 +81,22 @@ __device__ __forceinline__ bool TryWait(uint32_t mbar, uint32_t phase) {
   return ok != 0;
 }
 
+// Waits for the commit of the MMAs just issued: at most `polls` polls. If
+// they run out, the wait has failed (the caller reports it through its error
+// flag), and a second wait of at most kMaxPolls polls follows, so that no
+// MMA is left in flight when the caller goes on: its operands and
+// accumulators are reused, and its tensor memory is freed at the end.
+__device__ __forceinline__ bool WaitMma(uint32_t mbar, uint32_t phase,
+                                        uint32_t polls) {
+  for (uint32_t it = 0; it < polls; ++it) {
+    if (TryWait(mbar, phase)) return true;
+  }
+  for (uint32_t it = 0; it < kMaxPolls; ++it) {
+    if (TryWait(mbar, phase)) break;
+  }
+  return false;
+}
+
 // 16 consecutive FP32 columns of this thread's tensor-memory lane.
 __device__ __forceinline__ void Ld16(uint32_t taddr, float* v) {
   uint32_t r[16];
@@ -174,7 +190,8 @@ __device__ __forceinline__ uint32_t AccCol(int c, int j) {
 // of the A operands.
 template <int N, int S>
 __device__ __forceinline__ bool Pass(Smem<N, S>& s, int j, bool a_mn,
-                                     const uint8_t* b, uint32_t& phase) {
+                                     const uint8_t* b, uint32_t& phase,
+                                     uint32_t polls) {
   using Sm = Smem<N, S>;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   FenceBefore();
@@ -206,14 +223,7 @@ __device__ __forceinline__ bool Pass(Smem<N, S>& s, int j, bool a_mn,
         "b64 [%0];" ::"r"(SmemU32(&s.mbar))
         : "memory");
   }
-  const uint32_t mb = SmemU32(&s.mbar);
-  bool ok = false;
-  for (uint32_t it = 0; it < kMaxPolls; ++it) {
-    if (TryWait(mb, phase)) {
-      ok = true;
-      break;
-    }
-  }
+  const bool ok = WaitMma(SmemU32(&s.mbar), phase, polls);
   phase ^= 1u;
   FenceAfter();
   return ok;
@@ -271,7 +281,8 @@ __device__ __forceinline__ void LoadRow1(const Smem1<N, S>& s, uint32_t dcol,
 // (tensor-memory columns j N ..), then waits for it (bounded).
 template <int N, int S>
 __device__ __forceinline__ bool Pass1(Smem1<N, S>& s, int j, bool a_mn,
-                                      const uint8_t* b, uint32_t& phase) {
+                                      const uint8_t* b, uint32_t& phase,
+                                      uint32_t polls) {
   using Sm = Smem1<N, S>;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   FenceBefore();
@@ -298,14 +309,7 @@ __device__ __forceinline__ bool Pass1(Smem1<N, S>& s, int j, bool a_mn,
         "b64 [%0];" ::"r"(SmemU32(&s.mbar))
         : "memory");
   }
-  const uint32_t mb = SmemU32(&s.mbar);
-  bool ok = false;
-  for (uint32_t it = 0; it < kMaxPolls; ++it) {
-    if (TryWait(mb, phase)) {
-      ok = true;
-      break;
-    }
-  }
+  const bool ok = WaitMma(SmemU32(&s.mbar), phase, polls);
   phase ^= 1u;
   FenceAfter();
   return ok;
@@ -387,13 +391,13 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
       }
       PutRowK<N, S>(s.a[c], t, T);  // pixel row y = r of the correction
     }
-    ok = Pass<N, S>(s, 0, false, s.dct, phase);
+    ok = Pass<N, S>(s, 0, false, s.dct, phase, f.tc_polls);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       LoadRow<N, S>(s, AccCol<N>(c, 0), T);  // t_y[k]
       PutColMN<N, S>(s.a[c], N * bl, r, T);
     }
-    ok = Pass<N, S>(s, 1, true, s.dct, phase) && ok;
+    ok = Pass<N, S>(s, 1, true, s.dct, phase, f.tc_polls) && ok;
     float Y[3][N];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -452,13 +456,13 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) PutRowK<N, S>(s.a[c], t, Y[c]);
-    ok = Pass<N, S>(s, 0, false, s.idct, phase) && ok;
+    ok = Pass<N, S>(s, 0, false, s.idct, phase, f.tc_polls) && ok;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       LoadRow<N, S>(s, AccCol<N>(c, 0), T);
       PutColMN<N, S>(s.a[c], N * bl, r, T);
     }
-    ok = Pass<N, S>(s, 1, true, s.idct, phase) && ok;
+    ok = Pass<N, S>(s, 1, true, s.idct, phase, f.tc_polls) && ok;
     ok = __syncthreads_and(ok);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -497,7 +501,6 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
     k_square_idct_tc1(Geo g, DevFrame f, const uint32_t* list, int count,
                       int predict_hf, int* err) {
   using namespace tc;
-  using square::CoefRowOffset;
   static_assert(N == 16, "the HF corner table is for 16x16 blocks");
   constexpr int BPB = 128 / N;  // blocks per batch
   constexpr int cov = N / 8;
@@ -522,7 +525,6 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
   uint32_t phase = 0;
   const int nbat = (count + BPB - 1) / BPB;
   const int nitems = 3 * nbat;
-  const size_t plane_ac = size_t(g.ac_stride) * g.By;
   const size_t plane_px = size_t(g.PW) * g.PH;
   const float inv_nn = 1.0f / float(N * N);
   float cr[6];  // this lane's row of the HF corner table (rows r < 4)
@@ -536,13 +538,11 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
     const int bt = it / 3, ch = it - 3 * bt;
     const int i = bt * BPB + bl;
     const uint32_t pk = list[i < count ? i : 0];
-    const float* crow = f.ac + ch * plane_ac +
-                        CoefRowOffset(g, pk & 0xFFFF, pk >> 16, N, r);
+    if (i < count) {
+      LoadCoefRow<N>(g, f, ch, pk & 0xFFFF, pk >> 16, r, X);
+    } else {
 #pragma unroll
-    for (int j = 0; j < N; j += 4) {
-      const float4 v = i < count ? *reinterpret_cast<const float4*>(crow + j)
-                                 : make_float4(0.f, 0.f, 0.f, 0.f);
-      X[j] = v.x, X[j + 1] = v.y, X[j + 2] = v.z, X[j + 3] = v.w;
+      for (int j = 0; j < N; ++j) X[j] = 0.f;
     }
     return pk;
   };
@@ -614,10 +614,10 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
     float T[N];
     PutRowK<N, S>(s.a, t, X);
     if (item + int(gridDim.x) < nitems) pkd_next = load_row(item + gridDim.x);
-    ok = Pass1<N, S>(s, 0, false, s.idct, phase) && ok;
+    ok = Pass1<N, S>(s, 0, false, s.idct, phase, f.tc_polls) && ok;
     LoadRow1<N, S>(s, 0, T);  // T[k = r][v]
     PutColMN<N, S>(s.a, N * bl, r, T);
-    ok = Pass1<N, S>(s, 1, true, s.idct, phase) && ok;
+    ok = Pass1<N, S>(s, 1, true, s.idct, phase, f.tc_polls) && ok;
     ok = __syncthreads_and(ok);
     LoadRow1<N, S>(s, N, T);  // pixel row v = r
     if (hf) {

@@ -23,6 +23,7 @@ OPT_KEEP_STAGES = 1
 OPT_PROFILE = 2
 OPT_FORM = 3
 OPT_GRAPHS = 4
+OPT_TC_WAIT_POLLS = 5
 FORMS = {"fp32": 0, "split_bf16": 1, "split_bf16x3": 2}
 
 _lib = None
@@ -170,6 +171,9 @@ class Context:
     def _check(self, rc: int) -> None:
         if rc < 0:
             raise PikGpuError(rc, self.L.pikgpu_last_error(self.h).decode())
+
+    def set_option(self, option: int, value: int) -> None:
+        self._check(self.L.pikgpu_set_option(self.h, option, value))
 
     def begin(self, frame: layout.Frame) -> None:
         self._packed = abi.PackedFrame(frame)

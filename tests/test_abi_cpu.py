@@ -47,7 +47,11 @@ def test_valid_frames_pass():
     (lambda f: f.raw_quant_field.__setitem__((1, 1), 257), -1),  # qf > 256
     (lambda f: f.ar_sigma_lut_ids.__setitem__((0, 1), 2), -1),   # LUT id
     (lambda f: setattr(f, "flags", 4), -2),                      # noise
-    (lambda f: setattr(f, "epf_enable_adaptive", 0), -2),        # fixed sigma
+    # fixed sigma: 0 (copy) or in [kMinSigma, kMaxSigma] = [16, 672]
+    (lambda f: (setattr(f, "epf_enable_adaptive", 0),
+                setattr(f, "epf_sigma", 15)), -1),
+    (lambda f: (setattr(f, "epf_enable_adaptive", 0),
+                setattr(f, "epf_sigma", 673)), -1),
     (lambda f: setattr(f, "gaborish", 5), -1),
     (lambda f: setattr(f, "global_scale", 0), -1),
     (lambda f: setattr(f, "quant_dc", 300), -1),
@@ -59,6 +63,12 @@ def test_invalid_fields_rejected(mutate, code):
     mutate(f)
     rc, msg = native.validate(f)
     assert rc == code and msg
+
+
+@pytest.mark.parametrize("sigma", [0, 16, 100, 672])
+def test_fixed_sigma_epf_accepted(sigma):
+    f = _frame(epf_enable_adaptive=0, epf_sigma=sigma)
+    assert native.validate(f) == (0, "")
 
 
 def test_misaligned_and_overlapping_transforms_rejected():

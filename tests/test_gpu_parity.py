@@ -227,3 +227,18 @@ def test_4k_real_frame_against_reference_and_fp64():
     lsb = np.abs(gpu2["srgb8"].transpose(2, 0, 1).astype(np.int32) -
                  golden_cases.srgb8_exact(o64))
     assert lsb.max() <= 1
+
+
+@pytest.mark.parametrize("sigma", [0, 16, 100, 672])
+def test_fixed_sigma_epf_bitexact(sigma):
+    """EpfParams::enable_adaptive = false (Filter, pik/epf_target.cc:
+    1342-1386): every block filtered with one sigma, or copied when it is 0;
+    every stage bit-identical to the FP32 oracle."""
+    frame = synthetic.make_frame(264, 200, seed=sigma + 1, qf_median=9.0)
+    frame.epf_enable_adaptive = 0
+    frame.epf_sigma = sigma
+    gpu = run_gpu(frame)
+    assert np.all(gpu["sigma"] == sigma)
+    assert_bitexact_vs_oracle(frame, gpu)
+    if sigma == 0:
+        np.testing.assert_array_equal(gpu["epf"], gpu["idct"])

@@ -123,3 +123,35 @@ def test_lf_helpers_match_live_reference(t, which):
                            32)
         assert np.abs(got - ref).max() <= 2e-6 * max(
             1e-30, float(np.abs(ref).max()))
+
+
+@pytest.mark.parametrize("sigma", [16, 90, 672])
+def test_fixed_sigma_epf_matches_live_reference(sigma):
+    """The decoder's fixed-sigma EPF (DecompressParams::epf_sigma,
+    pik/pik_frame.cc:112-115; Filter, pik/epf_target.cc:1342-1386): every
+    block filtered with one sigma. The restatement on the reference's guide
+    must give its EPF output and linear output within 2e-5 (the bounds of
+    the adaptive case), and the reference's own full decode with the
+    override must equal its stage-by-stage run."""
+    img = synthetic.srgb8_to_linear255(synthetic.make_image(200, 136,
+                                                            seed=sigma))
+    bs = refpy.encode(img, 1.5, flavour="avx2")
+    fz = refpy.Frozen(bs, flavour="scalar")
+    fz.set_fixed_sigma(sigma)
+    ref, _ = fz.run_stages(threads=1, want=("smoothed", "epf", "linear"))
+    frame = fz.frame()
+    assert frame.epf_enable_adaptive == 0 and frame.epf_sigma == sigma
+    g, _ = decisions.guide_and_stretch(ref["smoothed"])
+    by, bx = frame.blocks
+    s = np.full((by, bx), sigma, np.int32)
+    o = oraclepy.run(frame, precision=32, want=("epf", "linear"), guide=g,
+                     sigma=s)
+    assert np.abs(o["epf"] - ref["epf"]).max() <= 2e-6
+    assert np.abs(o["linear"] - ref["linear"]).max() / 255 <= 2e-5
+    # Without injected decisions the restatement takes the same sigma.
+    o2 = oraclepy.run(frame, precision=32, want=("linear",),
+                      export_decisions=True)
+    np.testing.assert_array_equal(o2["sigma"], s)
+    full = refpy.decode(bs, frame.xsize, frame.ysize, threads=1,
+                        epf_sigma=sigma)
+    np.testing.assert_array_equal(full, ref["linear"])

@@ -60,3 +60,28 @@ def test_dct32_heavy_reference_frame(w, h, distance, seed):
     lsb = np.abs(gpu2["srgb8"].transpose(2, 0, 1).astype(np.int32) -
                  golden_cases.srgb8_exact(ref["linear"]))
     assert lsb.max() <= 1
+
+
+def test_fixed_sigma_reference_frame():
+    """A reference-encoded frame decoded with the decoder's fixed-sigma EPF
+    override (DecompressParams::epf_sigma, pik/pik_frame.cc:112-115): the
+    GPU on the reference's guide is within 2e-5 of the reference's own
+    full decode with the override, and bit-identical to the FP32 oracle."""
+    sigma = 120
+    img = synthetic.srgb8_to_linear255(synthetic.make_image(
+        400, 264, seed=12, sinusoids=12, rectangles=20, noise_sigma=3.0))
+    bs = refpy.encode(img, 1.0, flavour="avx2", threads=os.cpu_count() or 1)
+    fz = refpy.Frozen(bs, flavour="scalar")
+    fz.set_fixed_sigma(sigma)
+    ref, _ = fz.run_stages(threads=1, want=("smoothed", "linear"))
+    full = refpy.decode(bs, fz.xsize, fz.ysize, threads=1, epf_sigma=sigma)
+    np.testing.assert_array_equal(full, ref["linear"])
+    frame = fz.frame()
+    gpu = run_gpu(frame)
+    assert np.all(gpu["sigma"] == sigma)
+    assert_bitexact_vs_oracle(frame, gpu)
+    g, _ = decisions.guide_and_stretch(ref["smoothed"])
+    by, bx = frame.blocks
+    gpu2 = run_gpu(frame, guide=g, sigma=np.full((by, bx), sigma, np.int32),
+                   keep=False)
+    assert np.abs(gpu2["linear"] - full).max() / 255 <= 2e-5

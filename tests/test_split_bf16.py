@@ -1,19 +1,32 @@
 """The split-BF16 tensor-core forms against the FP64 oracle and the plain
-FP32 form. The forms share every discrete decision when the EPF decisions of
-the FP32 form are injected, so the comparison measures arithmetic only.
+FP32 form.
 
 Tolerance on the [0,1]-normalised linear output (the reference value /
-255): 2e-5 against FP64 for both tensor-core forms (two BF16 terms with
-three products, three terms with six); 8-bit sRGB within 1 LSB.
+255): max-abs 2e-5 against FP64 for both tensor-core forms (two BF16 terms
+with three products, three terms with six), and 8-bit sRGB within 1 LSB of
+the exact sRGB encoding of the FP64 output, at every pixel.
 
-One discontinuity remains between forms with different rounding: the
-adaptive-reconstruction clamp treats a DCT correction of exactly +0.0 as
-ratio 0 (SymmetricClamp, pik/adaptive_reconstruction.cc:72-121), so where
-one form computes +0.0 and another a tiny nonzero value the clamp of that
-coefficient differs. On the 4K workload this happens in one 2x2 group of
-DCT4X4 blocks, where the Hadamard of the sub-block DCs cancels exactly.
-Such isolated pixels are bounded by their share (at most 5e-5 of the
-values), the 99.999th percentile by 2e-5."""
+The forms are compared on shared discrete decisions, so the comparison
+measures arithmetic only:
+- the EPF's u8 guide and per-block sigma (MakeGuide / SigmaFromQuant,
+  pik/epf_target.cc:1009-1111);
+- the clamp's branch per coefficient (the clamp tape). SymmetricClamp
+  (pik/adaptive_reconstruction.cc:72-121) treats a correction of exactly
+  +0.0 as ratio 0, so where one form computes +0.0 and another a tiny
+  nonzero value, the clamp of that coefficient differs by O(1). On the 4K
+  workload this happens in one 2x2 group of DCT4X4 blocks whose sub-block
+  DC Hadamard cancels exactly.
+All three are taken from the FP32 form's run and given to the tensor-core
+form and to the FP64 oracle.
+
+A second check runs the tensor-core form on its own decisions, as a
+decoder does. Its bound is statistical, that of the other own-decision
+tests: the 99.9th percentile within 2e-5 of FP64 (on the FP32 form's
+decisions) and at most 1e-3 of the values beyond, with at most 2e-4 of the
+u8 guide bytes flipped and no per-block sigma flipped. A guide value that
+sits on a rounding boundary of the u8 quantisation can flip, and the flip
+changes the weights of the neighbouring pixels by a discrete step
+(measured on the 4K frame: 5e-4 of the values beyond 2e-5)."""
 
 import os
 
@@ -26,51 +39,85 @@ from tests import golden_cases
 
 pytestmark = pytest.mark.gpu
 
-TOL = 2e-5  # the FP32 form against FP64
+TOL = 2e-5  # max-abs against FP64, [0,1] scale
+OUTLIER_SHARE = 1e-3  # own-decision runs only
 
 
-def run(frame, form, guide=None, sigma=None):
+def run(frame, form, guide=None, sigma=None, tape=None):
     ctx = native.Context(0, keep_stages=True, form=form)
     try:
         ctx.begin(frame)
         ctx.set_ac()
         if guide is not None:
             ctx.set_decisions(guide, sigma)
+        if tape is not None:
+            ctx.set_clamp_decisions(tape)
         lin, rgb = ctx.reconstruct(linear=True, srgb8=True)
         out = {"linear": lin, "srgb8": rgb, "idct": ctx.stage("idct")}
         if frame.have_ar:
             out["guide"], out["sigma"] = ctx.decisions()
+            out["tape"] = ctx.clamp_decisions()
         return out
     finally:
         ctx.close()
 
 
-OUTLIER_SHARE = 5e-5
+def fp64_of(frame, guide, sigma, tape):
+    dg, ds = decisions.dc_decisions(frame)
+    return oraclepy.run(frame, precision=64, want=("linear",), guide=guide,
+                        sigma=sigma, dc_guide=dg, dc_sigma=ds,
+                        clamp_tape=tape)["linear"]
+
+
+def lsb_error(srgb8, o64):
+    return np.abs(srgb8.transpose(2, 0, 1).astype(np.int32) -
+                  golden_cases.srgb8_exact(o64))
 
 
 def check_against_fp64(frame, form):
+    """Shared decisions: max-abs bounds at every pixel."""
     fp32 = run(frame, "fp32")
-    g, s = (fp32["guide"], fp32["sigma"]) if frame.have_ar else (None, None)
-    tc = run(frame, form, g, s)
+    g = s = tape = None
+    if frame.have_ar:
+        g, s, tape = fp32["guide"], fp32["sigma"], fp32["tape"]
+    tc = run(frame, form, g, s, tape)
     # IDCT stage (XYB scale): split-BF16 carries about 16 significant bits
     # per operand, so it stays within 1e-4 of the FP32 form.
     d_idct = float(np.abs(tc["idct"] - fp32["idct"]).max())
     assert d_idct <= 1e-4
-    dg, ds = decisions.dc_decisions(frame)
-    o64 = oraclepy.run(frame, precision=64, want=("linear",), guide=g,
-                       sigma=s, dc_guide=dg, dc_sigma=ds)["linear"]
+    o64 = fp64_of(frame, g, s, tape)
     err_tc = np.abs(tc["linear"] - o64) / 255
     err_fp32 = np.abs(fp32["linear"] - o64) / 255
+    lsb = lsb_error(tc["srgb8"], o64)
     print(f"{frame.xsize}x{frame.ysize} {form}: idct diff {d_idct:.3g}, "
-          f"max err vs FP64: {err_tc.max():.3g}, pixels > 2e-5: "
-          f"{int((err_tc > TOL).sum())} (FP32 form {err_fp32.max():.3g})")
+          f"max err vs FP64: {err_tc.max():.3g} (FP32 form "
+          f"{err_fp32.max():.3g}), sRGB-8 max {int(lsb.max())} LSB")
     assert err_fp32.max() <= TOL
-    assert np.quantile(err_tc, 0.99999) <= TOL
-    assert (err_tc > TOL).mean() <= OUTLIER_SHARE
-    lsb = np.abs(tc["srgb8"].transpose(2, 0, 1).astype(np.int32) -
-                 golden_cases.srgb8_exact(o64))
-    assert (lsb > 1).mean() <= OUTLIER_SHARE
+    assert err_tc.max() <= TOL
+    assert lsb.max() <= 1
     return err_tc.max(), err_fp32.max()
+
+
+def check_own_decisions(frame, form):
+    """Each form on its own decisions: percentile bounds."""
+    fp32 = run(frame, "fp32")
+    tc = run(frame, form)
+    g = s = tape = None
+    if frame.have_ar:
+        g, s, tape = fp32["guide"], fp32["sigma"], fp32["tape"]
+    o64 = fp64_of(frame, g, s, tape)
+    err_tc = np.abs(tc["linear"] - o64) / 255
+    lsb = lsb_error(tc["srgb8"], o64)
+    flips = (tc["guide"] != g).mean() if frame.have_ar else 0.0
+    print(f"{frame.xsize}x{frame.ysize} {form} own decisions: max "
+          f"{err_tc.max():.3g}, share > 2e-5 {(err_tc > TOL).mean():.3g}, "
+          f"guide flips {flips:.3g}")
+    if frame.have_ar:
+        np.testing.assert_array_equal(tc["sigma"], s)
+        assert flips <= 2e-4
+    assert np.quantile(err_tc, 0.999) <= TOL
+    assert (err_tc > TOL).mean() <= OUTLIER_SHARE
+    assert (lsb > 1).mean() <= OUTLIER_SHARE
 
 
 FORMS = ["split_bf16x3", "split_bf16"]
@@ -85,6 +132,12 @@ def test_dct16_synthetic(form):
 
 
 @pytest.mark.parametrize("form", FORMS)
+def test_mixed_synthetic(form):
+    frame = synthetic.make_frame(1030, 530, seed=22)
+    check_against_fp64(frame, form)
+
+
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("predict_hf", [0, 1])
 def test_header_variants(form, predict_hf):
     frame = synthetic.make_frame(200, 136, seed=5,
@@ -93,8 +146,16 @@ def test_header_variants(form, predict_hf):
     check_against_fp64(frame, form)
 
 
+def _4k():
+    return layout.Frame.load(os.path.join(golden_cases.GOLDEN,
+                                          "c2_4k_d1_frame.npz"))
+
+
 @pytest.mark.parametrize("form", FORMS)
 def test_4k_real_frame(form):
-    frame = layout.Frame.load(os.path.join(golden_cases.GOLDEN,
-                                           "c2_4k_d1_frame.npz"))
-    check_against_fp64(frame, form)
+    check_against_fp64(_4k(), form)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_4k_real_frame_own_decisions(form):
+    check_own_decisions(_4k(), form)
