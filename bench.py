@@ -61,15 +61,15 @@ GROUP_BYTES = {
     "epf": 3 * 4 + 3 * 4,
     # filtered + original in, clamped out
     "ar_clamp": 3 * 4 + 3 * 4 + 3 * 4,
-    # int16 coefficients in (Y read again for X and B), pixels out
-    "hf_idct": 3 * 2 + 2 * 2 + 3 * 4,
+    # float coefficients in, pixels out
+    "hf_idct": 3 * 4 + 3 * 4,
     "gaborish1_minmax": 3 * 4,
     "gaborish2_opsin_srgb": 3 * 4 + 3 * 4,
-    # per-cell dequantisation parameters written (32 B per cell)
-    "cell_params": 32 / 64,
-    # DC read; per cell and channel the corner's 4 int16 coefficients read
-    # and 4 corner floats and 4 pred2x2 floats written
-    "lf_prediction_corner": 12 / 64 + 3 * 4 * (2 + 4 + 4) / 64,
+    # int16 AC in, float AC out
+    "dequant_ac": 3 * 2 + 3 * 4,
+    # DC read; per cell and channel the corner's 4 floats read and written
+    # and 4 pred2x2 floats written
+    "lf_prediction_update": 12 / 64 + 3 * 4 * (4 + 4 + 4) / 64,
     "dc_dequant_epf": 0.2,
 }
 PATH_TRAFFIC_4K = None

@@ -77,15 +77,13 @@ struct FrameScalars {
   int epf_fixed_sigma;
 };
 
-// Dequant::DoAC's parameters of one 8x8 cell (pik/compressed_image.cc:
-// 636-672): the scaled step inv_global_scale / qf (SafeDiv), the
-// chroma-from-luma multipliers of the cell's colour tile, and the offsets
-// in the dequant table of the cell's three matrix rows (its table, the
-// block's QuantKind, the cell's sub-block). 32 bytes: two 16-byte loads.
-struct CellDq {
-  float scaled, x_cc, b_cc;
-  uint32_t m[3];
-  uint32_t pad[2];
+// The first blocks of each transform class (x | y << 16), their count, and
+// where the clamp's active blocks of the class go.
+constexpr int kMaxClasses = 5;
+struct ClassLists {
+  const uint32_t* list[kMaxClasses];
+  int n[kMaxClasses];
+  uint32_t* active[kMaxClasses];
 };
 
 // Device pointers of one frame.
@@ -102,16 +100,7 @@ struct DevFrame {
   const int16_t* qdc;
   const int16_t* qac;
   float* dc;          // 3 x By x Bx
-  // The transforms dequantise qac as they load it (cellp), unless ac_in is
-  // set: dequantised AC supplied instead (3 x By x ac_stride). Either way
-  // each block's 2cov x 2cov low-frequency corner (LLF from DC, LF plus
-  // its prediction) comes from `corner`: 3 x By x Bx x 4 floats, element
-  // (r, l) of the block at (bx, by) in cell (bx + l / 2, by + r / 2), slot
-  // 2 (r & 1) + (l & 1).
-  const float* ac_in;
-  const CellDq* cellp;  // By x Bx
-  float* corner;
-  float* ac;          // 3 x By x ac_stride (k_dequant_ac's output)
+  float* ac;          // 3 x By x ac_stride
   float* pred2x2_g;   // groups x 3 x 132 x 132
   float* idct;        // 3 x PH x PW
   float* smoothed;    // 3 x PH x PW

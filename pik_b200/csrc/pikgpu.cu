@@ -28,6 +28,12 @@ namespace {
 
 // Block classes launched by separate kernels.
 enum Class { kC8 = 0, kC16, kC32, kC4, kCSmall, kNumClasses };
+// Device counters, zeroed at the start of every frame: the clamp's active
+// blocks per class, then the work counters of the persistent tensor-core
+// transform and clamp kernels.
+constexpr int kWorkIdct = kNumClasses, kWorkAr = kNumClasses + 1;
+constexpr int kNumCounters = kNumClasses + 2;
+static_assert(kNumClasses == kMaxClasses, "ClassLists holds every class");
 int ClassOf(int type) {
   switch (type) {
     case kDCT:
@@ -47,10 +53,10 @@ int ClassOf(int type) {
 
 // Kernel groups timed with events when profiling is on.
 enum Timed {
-  kTDc = 0, kTLf, kTDequant, kTIdct, kTGab1, kTEpf, kTAr, kTFinal, kNumTimed
+  kTDc = 0, kTDequant, kTLf, kTIdct, kTGab1, kTEpf, kTAr, kTFinal, kNumTimed
 };
 const char* kTimedNames[kNumTimed] = {
-    "dc_dequant_epf", "lf_prediction_corner", "cell_params", "hf_idct",
+    "dc_dequant_epf", "dequant_ac", "lf_prediction_update", "hf_idct",
     "gaborish1_minmax", "epf", "ar_clamp", "gaborish2_opsin_srgb"};
 
 struct DevBuf {
@@ -87,7 +93,7 @@ struct pikgpu_ctx {
   std::vector<uint32_t> lists[kNumClasses];
   // device buffers
   DevBuf acs, qf, lut, dq_cf, dq_map, ytox, ytob, table, offsets;
-  DevBuf qdc, qac, dc, dcpad, cellp, corner, pred2x2_g;
+  DevBuf qdc, qac, dc, dcpad, ac, pred2x2_g;
   DevBuf idct, smoothed, filt, mm, sigma, dc_sigma, list[kNumClasses];
   DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr;
   DevBuf sigma_ovr, counters, active[kNumClasses], tc_err;
@@ -397,7 +403,7 @@ int UploadTables(pikgpu_ctx* ctx) {
                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(EpfSmemBytes(8))));
   CUDA_TRY(ctx, cudaFuncSetAttribute(
-                    k_lf_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    k_lf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(kLfSmemBytes)));
   if (ctx->device < 64) g_tables_uploaded[ctx->device] = true;
   return PIKGPU_OK;
@@ -519,13 +525,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   f.qdc = P<int16_t>(ctx->qdc);
   f.qac = P<int16_t>(ctx->qac);
   f.dc = P<float>(ctx->dc);
-  // The transforms dequantise the int16 AC as they load it, unless the
-  // caller supplied dequantised AC; k_dequant_ac runs only to export that
-  // stage.
-  f.ac_in = ctx->use_dq_ovr ? P<float>(ctx->dq_ovr) : nullptr;
-  f.cellp = P<CellDq>(ctx->cellp);
-  f.corner = P<float>(ctx->corner);
-  f.ac = ctx->keep_stages ? P<float>(ctx->dbg_dequant) : nullptr;
+  f.ac = P<float>(ctx->ac);
   f.pred2x2_g = P<float>(ctx->pred2x2_g);
   f.idct = P<float>(ctx->idct);
   f.smoothed = P<float>(ctx->smoothed);
@@ -553,7 +553,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
   ctx->smoothed_valid = false;
   // Both min/max sets and the clamp's block counters start empty.
   int* counters = P<int>(ctx->counters);
-  k_frame_init<<<1, 32, 0, st>>>(mm, counters, kNumClasses); ++ctx->launches;
+  k_frame_init<<<1, 32, 0, st>>>(mm, counters, kNumCounters); ++ctx->launches;
   br.Fork(0, 1);
   Mark(ctx, kTDc);
   // DC (side stream 0): dequantisation, the 8-padded copy and its min/max;
@@ -574,31 +574,33 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     EpfLaunch(sd, ctx->num_sms, ctx->form, dcpad, dcpad, 0, dpw, dph, mm_dc,
               sgs, nullptr, nullptr, dco); ++ctx->launches;
   }
-  Mark(ctx, kTLf);
-  // Per-group LF prediction and every block's low-frequency corner and
-  // pred2x2 (side stream 0, after DC): one CTA per group and channel.
-  const int ng = g.Gx * g.Gy;
-  k_lf_chain<<<3 * ng, kLfThreads, kLfSmemBytes, sd>>>(
-      g, f, s, s.predict_lf, s.predict_hf); ++ctx->launches;
   Mark(ctx, kTDequant);
   {
-    // Dequantisation parameters per cell (main stream, concurrent with DC
-    // and LF).
-    dim3 b2(32, 8), gr1(Blocks(g.Bx, 32), Blocks(g.By, 8));
-    k_cell_params<<<gr1, b2, 0, st>>>(g, f, s); ++ctx->launches;
+    // AC dequantisation (main stream, concurrent with DC).
+    if (ctx->use_dq_ovr) {
+      cudaMemcpyAsync(f.ac, ctx->dq_ovr.p,
+                      sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
+                      cudaMemcpyDeviceToDevice, st);
+    } else {
+      dim3 gr(Blocks(g.Bx, kDequantCells), g.By);
+      k_dequant_ac<<<gr, 256, 0, st>>>(g, f, s); ++ctx->launches;
+    }
     if (ctx->keep_stages) {
-      // The dequantised AC for export (PIKGPU_STAGE_DEQUANT_AC).
-      if (ctx->use_dq_ovr) {
-        cudaMemcpyAsync(f.ac, ctx->dq_ovr.p,
-                        sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
-                        cudaMemcpyDeviceToDevice, st);
-      } else {
-        dim3 gr(Blocks(g.Bx, kDequantCells), g.By);
-        k_dequant_ac<<<gr, 256, 0, st>>>(g, f, s); ++ctx->launches;
-      }
+      cudaMemcpyAsync(ctx->dbg_dequant.p, f.ac,
+                      sizeof(float) * 3 * size_t(g.ac_stride) * g.By,
+                      cudaMemcpyDeviceToDevice, st);
     }
     br.Join(0, 1);
   }
+  Mark(ctx, kTLf);
+  // Per-group LF prediction and the LF update of every block's dequantised
+  // coefficients, with its pred2x2 (after DC and the dequantisation): one
+  // CTA per tile of 32 x 32 cells of a group and channel.
+  const int ng = g.Gx * g.Gy;
+  constexpr int kTilesPerGroup = (64 + kLfTile - 1) / kLfTile;
+  k_lf_tile<<<dim3(kTilesPerGroup * kTilesPerGroup, ng, 3), kLfThreads,
+              kLfSmemBytes, st>>>(g, f, s.predict_lf, s.predict_hf);
+  ++ctx->launches;
   Mark(ctx, kTIdct);
   br.Fork(1, ctx->kSide);
   {
@@ -607,6 +609,25 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       const int warps = (items + upw - 1) / upw;
       return (warps * 32 + kSquareThreads - 1) / kSquareThreads;
     };
+    // The classes with few blocks first, so that their CTAs are resident
+    // before the persistent tensor-core kernel fills the SMs (which takes
+    // its work from a counter and leaves those SMs' share to the others).
+    if (n[kCSmall]) {
+      k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, cls(kCSmall)>>>(
+          g, f, L[kCSmall], n[kCSmall]);
+      ++ctx->launches;
+    }
+    if (n[kC4]) {
+      k_dct4_idct<<<Blocks(n[kC4], kDct4Blocks), 256, 0, cls(kC4)>>>(
+          g, f, L[kC4], n[kC4], s.predict_hf);
+      ++ctx->launches;
+    }
+    if (n[kC32]) {
+      // One 256-thread CTA per block.
+      k_square_idct<32><<<n[kC32], 256, 0, cls(kC32)>>>(g, f, L[kC32], n[kC32],
+                                                       s.predict_hf);
+      ++ctx->launches;
+    }
     if (n[kC8]) {
       k_square_idct_rows<8><<<rows_grid(3 * n[kC8], 8), kSquareThreads, 0,
                               cls(kC8)>>>(g, f, L[kC8], n[kC8], s.predict_hf);
@@ -619,32 +640,18 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
           std::min(3 * items, ctx->num_sms * 2 * ctx->tc_ctas_per_sm);
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
         k_square_idct_tc1<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
-            g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
+            g, f, L[kC16], n[kC16], s.predict_hf, counters + kWorkIdct,
+            P<int>(ctx->tc_err));
       } else {
         k_square_idct_tc1<16, 3><<<grid, tc::kThreads, 0, cls(kC16)>>>(
-            g, f, L[kC16], n[kC16], s.predict_hf, P<int>(ctx->tc_err));
+            g, f, L[kC16], n[kC16], s.predict_hf, counters + kWorkIdct,
+            P<int>(ctx->tc_err));
       }
       ++ctx->launches;
     } else if (n[kC16]) {
       k_square_idct_rows<16><<<rows_grid(3 * n[kC16], 16), kSquareThreads, 0,
                                cls(kC16)>>>(g, f, L[kC16], n[kC16],
                                             s.predict_hf);
-      ++ctx->launches;
-    }
-    if (n[kC32]) {
-      // One 256-thread CTA per block.
-      k_square_idct<32><<<n[kC32], 256, 0, cls(kC32)>>>(g, f, L[kC32], n[kC32],
-                                                       s.predict_hf);
-      ++ctx->launches;
-    }
-    if (n[kC4]) {
-      k_dct4_idct<<<Blocks(n[kC4], kDct4Blocks), 256, 0, cls(kC4)>>>(
-          g, f, L[kC4], n[kC4], s.predict_hf);
-      ++ctx->launches;
-    }
-    if (n[kCSmall]) {
-      k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, cls(kCSmall)>>>(
-          g, f, L[kCSmall], n[kCSmall]);
       ++ctx->launches;
     }
   }
@@ -685,19 +692,45 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     Mark(ctx, kTAr);
     // Only blocks the EPF filtered need the clamp (see k_active_blocks).
     if (f.clamp_tape) cudaMemsetAsync(f.clamp_tape, 0, nac, st);
-    br.Fork(2, ctx->kSide);
-    for (int k = 0; k < kNumClasses; ++k) {
-      if (!n[k]) continue;
-      k_active_blocks<<<Blocks(n[k], 256), 256, 0, cls(k)>>>(
-          g, sig, f.acs, L[k], n[k], P<uint32_t>(ctx->active[k]),
-          counters + k);
-      ++ctx->launches;
+    // Every class's filtered blocks in one pass (main stream), then the
+    // classes' clamps, the ones with few blocks first (see the transforms).
+    {
+      ClassLists cl{};
+      int total = 0;
+      for (int k = 0; k < kNumClasses; ++k) {
+        cl.list[k] = L[k];
+        cl.n[k] = n[k];
+        cl.active[k] = P<uint32_t>(ctx->active[k]);
+        total += n[k];
+      }
+      if (total) {
+        k_active_blocks<<<Blocks(total, 256), 256, 0, st>>>(g, sig, f.acs, cl,
+                                                            counters);
+        ++ctx->launches;
+      }
     }
+    br.Fork(2, ctx->kSide);
     auto rows_grid = [](int items, int nn) {
       const int upw = 32 / nn;
       const int warps = (items + upw - 1) / upw;
       return (warps * 32 + kSquareThreads - 1) / kSquareThreads;
     };
+    if (n[kCSmall]) {
+      k_small_ar<<<Blocks(n[kCSmall], kSmallArBlocks), 3 * kSmallArBlocks, 0,
+                   cls(kCSmall)>>>(
+          g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
+      ++ctx->launches;
+    }
+    if (n[kC4]) {
+      k_dct4_ar<<<Blocks(n[kC4], kDct4Blocks), 256, 0, cls(kC4)>>>(
+          g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
+      ++ctx->launches;
+    }
+    if (n[kC32]) {
+      k_square_ar<32><<<n[kC32], 256, 0, cls(kC32)>>>(
+          g, f, s, P<uint32_t>(ctx->active[kC32]), counters + kC32);
+      ++ctx->launches;
+    }
     if (n[kC8]) {
       k_square_ar_rows<8><<<rows_grid(n[kC8], 8), kSquareThreads, 0,
                             cls(kC8)>>>(g, f, s, P<uint32_t>(ctx->active[kC8]),
@@ -710,11 +743,11 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
         k_square_ar_tc<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
-            P<int>(ctx->tc_err));
+            counters + kWorkAr, P<int>(ctx->tc_err));
       } else {
         k_square_ar_tc<16, 3><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
-            P<int>(ctx->tc_err));
+            counters + kWorkAr, P<int>(ctx->tc_err));
       }
       ++ctx->launches;
     } else if (n[kC16]) {
@@ -722,22 +755,6 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
                              cls(kC16)>>>(g, f, s,
                                           P<uint32_t>(ctx->active[kC16]),
                                           counters + kC16);
-      ++ctx->launches;
-    }
-    if (n[kC32]) {
-      k_square_ar<32><<<n[kC32], 256, 0, cls(kC32)>>>(
-          g, f, s, P<uint32_t>(ctx->active[kC32]), counters + kC32);
-      ++ctx->launches;
-    }
-    if (n[kC4]) {
-      k_dct4_ar<<<Blocks(n[kC4], kDct4Blocks), 256, 0, cls(kC4)>>>(
-          g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
-      ++ctx->launches;
-    }
-    if (n[kCSmall]) {
-      k_small_ar<<<Blocks(n[kCSmall], kSmallArBlocks), 3 * kSmallArBlocks, 0,
-                   cls(kCSmall)>>>(
-          g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
       ++ctx->launches;
     }
     br.Join(2, ctx->kSide);
@@ -907,8 +924,7 @@ int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
                     &ctx->dq_cf,   &ctx->dq_map,    &ctx->ytox,
                     &ctx->ytob,    &ctx->table,     &ctx->offsets,
                     &ctx->qdc,     &ctx->qac,       &ctx->dc,
-                    &ctx->dcpad,   &ctx->cellp,
-                    &ctx->corner,
+                    &ctx->dcpad,   &ctx->ac,
                     &ctx->pred2x2_g, &ctx->idct,    &ctx->smoothed,
                     &ctx->filt,    &ctx->mm,        &ctx->sigma,
                     &ctx->dc_sigma, &ctx->out_lin,  &ctx->out_rgb8,
@@ -1053,8 +1069,7 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
       {&ctx->qac, 2 * 3 * nac},
       {&ctx->dc, 4 * 3 * nb},
       {&ctx->dcpad, 4 * 3 * size_t(dpw) * dph},
-      {&ctx->cellp, sizeof(CellDq) * nb},
-      {&ctx->corner, 4 * 3 * 4 * nb},
+      {&ctx->ac, 4 * 3 * nac},
       {&ctx->pred2x2_g, 4 * kG2GroupFloats * ng},
       {&ctx->idct, 4 * 3 * npx},
       {&ctx->filt, 4 * 3 * npx},
@@ -1084,7 +1099,7 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
     }
   }
   cudaStream_t st = ctx->stream;
-  if ((rc = Ensure(ctx, &ctx->counters, sizeof(int) * kNumClasses))) {
+  if ((rc = Ensure(ctx, &ctx->counters, sizeof(int) * kNumCounters))) {
     return rc;
   }
   for (int k = 0; k < kNumClasses; ++k) {

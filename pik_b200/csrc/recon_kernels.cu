@@ -26,6 +26,8 @@ __device__ __forceinline__ const float* DctMat(int n) {
 // Single-thread transforms used by the small LF kernels (n <= 8).
 
 // tsIDCT (pik/dct.h:441-507): out = A C^T A^T (C row = horizontal freq).
+// Runtime size n <= 8: compact loops (these run once per block in the LF
+// kernels, where code size and registers matter more than unrolling).
 __device__ void TsIdct1(int n, const float* in, int is, float* out, int os) {
   const float* a = IdctMat(n);
   float tmp[64];
@@ -66,34 +68,105 @@ __device__ void TsDct1(int n, const float* in, int is, float* out, int os) {
   }
 }
 
-// ReinterpretingDCT / ReinterpretingIDCT (pik/ac_strategy.cc:270-311).
-__device__ void ReinterpDct(int dctn, int n, const float* in, int is,
-                            float* out, int os) {
-  float block[64], res[64];
-  for (int y = 0; y < n; ++y) {
-    for (int x = 0; x < n; ++x) block[y * n + x] = in[y * is + x];
+// The same two transforms for N <= 4, unrolled into registers (the same
+// sums in the same order).
+template <int N>
+__device__ __forceinline__ void TsIdctSmall(const float* in, int is,
+                                            float* out, int os) {
+  const float* a = IdctMat(N);
+  float tmp[N * N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+#pragma unroll
+    for (int v = 0; v < N; ++v) {
+      float s = 0.f;
+#pragma unroll
+      for (int l = 0; l < N; ++l) s += in[k * is + l] * a[v * N + l];
+      tmp[k * N + v] = s;
+    }
   }
-  TsDct1(n, block, n, res, n);
-  const int sn = SizeIndex(n), sd = SizeIndex(dctn);
-  for (int y = 0; y < n; ++y) {
-    for (int x = 0; x < n; ++x) {
-      out[y * os + x] = res[y * n + x] * c_t.total_scale[sn][y][x] *
+#pragma unroll
+  for (int v = 0; v < N; ++v) {
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+      float s = 0.f;
+#pragma unroll
+      for (int k = 0; k < N; ++k) s += a[u * N + k] * tmp[k * N + v];
+      out[v * os + u] = s;
+    }
+  }
+}
+template <int N>
+__device__ __forceinline__ void TsDctSmall(const float* in, int is, float* out,
+                                           int os) {
+  const float* b = DctMat(N);
+  float tmp[N * N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+#pragma unroll
+    for (int y = 0; y < N; ++y) {
+      float s = 0.f;
+#pragma unroll
+      for (int x = 0; x < N; ++x) s += b[k * N + x] * in[y * is + x];
+      tmp[k * N + y] = s;
+    }
+  }
+  const float scale = 1.0f / float(N * N);
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      float s = 0.f;
+#pragma unroll
+      for (int y = 0; y < N; ++y) s += tmp[k * N + y] * b[l * N + y];
+      out[k * os + l] = s * scale;
+    }
+  }
+}
+
+// ReinterpretingDCT / ReinterpretingIDCT (pik/ac_strategy.cc:270-311).
+template <int DCTN, int N>
+__device__ void ReinterpDct(const float* in, int is, float* out, int os) {
+  float block[N * N], res[N * N];
+#pragma unroll
+  for (int y = 0; y < N; ++y) {
+#pragma unroll
+    for (int x = 0; x < N; ++x) block[y * N + x] = in[y * is + x];
+  }
+  if constexpr (N <= 4) {
+    TsDctSmall<N>(block, N, res, N);
+  } else {
+    TsDct1(N, block, N, res, N);
+  }
+  constexpr int sn = SizeIndex(N), sd = SizeIndex(DCTN);
+#pragma unroll
+  for (int y = 0; y < N; ++y) {
+#pragma unroll
+    for (int x = 0; x < N; ++x) {
+      out[y * os + x] = res[y * N + x] * c_t.total_scale[sn][y][x] *
                         c_t.inv_total_scale[sd][y][x];
     }
   }
 }
-__device__ void ReinterpIdct(int dctn, int lf, int n, const float* in, int is,
-                             float* out, int os) {
-  float block[64];
-  for (int i = 0; i < n * n; ++i) block[i] = 0.f;
-  const int sn = SizeIndex(n), sd = SizeIndex(dctn);
-  for (int y = 0; y < lf; ++y) {
-    for (int x = 0; x < lf; ++x) {
-      block[y * n + x] = in[y * is + x] * c_t.inv_total_scale[sn][y][x] *
+template <int DCTN, int LF, int N>
+__device__ void ReinterpIdct(const float* in, int is, float* out, int os) {
+  float block[N * N];
+#pragma unroll
+  for (int i = 0; i < N * N; ++i) block[i] = 0.f;
+  constexpr int sn = SizeIndex(N), sd = SizeIndex(DCTN);
+#pragma unroll
+  for (int y = 0; y < LF; ++y) {
+#pragma unroll
+    for (int x = 0; x < LF; ++x) {
+      block[y * N + x] = in[y * is + x] * c_t.inv_total_scale[sn][y][x] *
                          c_t.total_scale[sd][y][x];
     }
   }
-  TsIdct1(n, block, n, out, os);
+  if constexpr (N <= 4) {
+    TsIdctSmall<N>(block, N, out, os);
+  } else {
+    TsIdct1(N, block, N, out, os);
+  }
 }
 
 // AcStrategy LLF/LF helpers (pik/ac_strategy.cc:850-1056).
@@ -101,12 +174,12 @@ __device__ void LowestFreqFromDC(int type, const float* dc, int ds, float* llf,
                                  int ls) {
   if (type == kDCT16X16) {
     float t[4];
-    ReinterpDct(16, 2, dc, ds, t, 2);
+    ReinterpDct<16, 2>(dc, ds, t, 2);
     for (int y = 0; y < 2; ++y)
       for (int x = 0; x < 2; ++x) llf[y * ls + x] = t[y * 2 + x];
   } else if (type == kDCT32X32) {
     float t[16];
-    ReinterpDct(32, 4, dc, ds, t, 4);
+    ReinterpDct<32, 4>(dc, ds, t, 4);
     for (int y = 0; y < 4; ++y)
       for (int x = 0; x < 4; ++x) llf[y * ls + x] = t[y * 4 + x];
   } else {
@@ -117,7 +190,7 @@ __device__ void LowestFreqFromDC(int type, const float* dc, int ds, float* llf,
 __device__ void DC2x2FromLowestFreq(int type, const float* llf, int ls,
                                     float* d, int dstr) {
   if (type == kDCT || type == kDCT_NOHF || type == kLINES) {
-    ReinterpIdct(8, 1, 2, llf, 0, d, dstr);
+    ReinterpIdct<8, 1, 2>(llf, 0, d, dstr);
   } else if (type == kDCT16X16) {
     float dest[16];
     for (int i = 0; i < 16; ++i) dest[i] = 0.f;
@@ -125,13 +198,13 @@ __device__ void DC2x2FromLowestFreq(int type, const float* llf, int ls,
     dest[1] = llf[1];
     dest[4] = llf[ls];
     dest[5] = llf[ls + 1];
-    ReinterpIdct(16, 2, 4, dest, 4, d, dstr);
+    ReinterpIdct<16, 2, 4>(dest, 4, d, dstr);
   } else if (type == kDCT32X32) {
     float dest[64];
     for (int i = 0; i < 64; ++i) dest[i] = 0.f;
     for (int iy = 0; iy < 4; ++iy)
       for (int ix = 0; ix < 4; ++ix) dest[iy * 8 + ix] = llf[iy * ls + ix];
-    ReinterpIdct(32, 4, 8, dest, 8, d, dstr);
+    ReinterpIdct<32, 4, 8>(dest, 8, d, dstr);
   } else {
     d[0] = llf[0];
     d[1] = llf[0];
@@ -146,17 +219,17 @@ __device__ void DC2x2FromLowFreq(int type, const Blk& blk, float* d,
                                  int dstr) {
   if (type == kDCT || type == kDCT_NOHF || type == kLINES) {
     float in[4] = {blk(0), blk(1), blk(8), blk(9)};
-    ReinterpIdct(8, 2, 2, in, 2, d, dstr);
+    ReinterpIdct<8, 2, 2>(in, 2, d, dstr);
   } else if (type == kDCT16X16) {
     float dest[16];
     for (int y = 0; y < 4; ++y)
       for (int x = 0; x < 4; ++x) dest[4 * y + x] = blk(16 * y + x);
-    ReinterpIdct(16, 4, 4, dest, 4, d, dstr);
+    ReinterpIdct<16, 4, 4>(dest, 4, d, dstr);
   } else if (type == kDCT32X32) {
     float dest[64];
     for (int y = 0; y < 8; ++y)
       for (int x = 0; x < 8; ++x) dest[8 * y + x] = blk(32 * y + x);
-    ReinterpIdct(32, 8, 8, dest, 8, d, dstr);
+    ReinterpIdct<32, 8, 8>(dest, 8, d, dstr);
   } else {
     const float b00 = blk(0), b01 = blk(1), b10 = blk(8), b11 = blk(9);
     d[0] = b00 + b01 + b10 + b11;
@@ -169,19 +242,19 @@ __device__ void DC2x2FromLowFreq(int type, const Blk& blk, float* d,
 __device__ void LowFreqFromDC2x2(int type, float* d, int dstr) {
   if (type == kDCT || type == kDCT_NOHF || type == kLINES) {
     float out[4];
-    ReinterpDct(8, 2, d, dstr, out, 2);
+    ReinterpDct<8, 2>(d, dstr, out, 2);
     d[0] = out[0];
     d[1] = out[1];
     d[dstr] = out[2];
     d[dstr + 1] = out[3];
   } else if (type == kDCT16X16) {
     float out[16];
-    ReinterpDct(16, 4, d, dstr, out, 4);
+    ReinterpDct<16, 4>(d, dstr, out, 4);
     for (int y = 0; y < 4; ++y)
       for (int x = 0; x < 4; ++x) d[dstr * y + x] = out[y * 4 + x];
   } else if (type == kDCT32X32) {
     float out[64];
-    ReinterpDct(32, 8, d, dstr, out, 8);
+    ReinterpDct<32, 8>(d, dstr, out, 8);
     for (int y = 0; y < 8; ++y)
       for (int x = 0; x < 8; ++x) d[dstr * y + x] = out[y * 8 + x];
   } else {
@@ -462,62 +535,21 @@ __global__ void __launch_bounds__(256) k_dequant_ac(Geo g, DevFrame f,
   d2[1] = make_float4(o2[4], o2[5], o2[6], o2[7]);
 }
 
-// Dequant::DoAC's parameters of cell (bx, by) (pik/compressed_image.cc:
-// 636-672): the operands of k_dequant_ac's arithmetic, formed the same way.
-__device__ __forceinline__ CellDq CellParamsOf(const Geo& g, const DevFrame& f,
-                                               const FrameScalars& s, int bx,
-                                               int by) {
-  const int cell = by * g.Bx + bx;
-  const int qf = f.qf[cell];
-  const int tx = bx >> 3, ty = by >> 3;
-  const int cf = f.dq_cf[ty * g.Tx + tx];
-  const int table = f.dq_map[cf * 256 + (qf - 1)];
-  const int a = f.acs[cell];
-  const int kind = QuantKindOf(a >> 4), blk = a & 0xF;
-  CellDq p;
-  p.scaled = qf == 0 ? 1E10f : s.inv_global_scale / float(qf);
-  p.x_cc = 1.0f * float(f.ytox[ty * g.Tx + tx] - 128) * (1.0f / 256);
-  p.b_cc = 1.0f * float(f.ytob[ty * g.Tx + tx]) * (1.0f / 128);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    p.m[c] = f.offsets[(table * 7 + kind) * 3 + c] + uint32_t(blk) * 64;
-  }
-  p.pad[0] = p.pad[1] = 0;
-  return p;
-}
-
-// Coefficient k of channel c of a cell with parameters p at AC position
-// `pos` (By x ac_stride plane layout): k_dequant_ac's arithmetic and order.
-__device__ __forceinline__ float DequantWith(const Geo& g, const DevFrame& f,
-                                             const CellDq& p, int c,
-                                             size_t pos, int k) {
-  const size_t plane = size_t(g.ac_stride) * g.By;
-  const float dy = AdjustQuantBias(float(f.qac[plane + pos]), c_t.one_bias[1]) *
-                   (f.table[p.m[1] + k] * p.scaled);
-  if (c == 1) return dy;
-  const float dq = AdjustQuantBias(float(f.qac[c * plane + pos]),
-                                   c_t.one_bias[c]) *
-                   (f.table[p.m[c] + k] * p.scaled);
-  return (c == 0 ? p.x_cc : p.b_cc) * dy + dq;
-}
-
-// Element (r, l), r, l < 2 cov, of the low-frequency corner of the block
-// whose first cell is (bx, by) (the layout of DevFrame::corner).
-__device__ __forceinline__ size_t CornerIdx(const Geo& g, int c, int bx,
-                                            int by, int r, int l) {
-  return ((size_t(c) * g.By + by + (r >> 1)) * g.Bx + bx + (l >> 1)) * 4 +
-         (r & 1) * 2 + (l & 1);
-}
-
 // ---------------------------------------------------------------------------
-// Per-group LF prediction (ComputeLlf, PredictLf, pik/ac_predictions.cc:
-// 380-470) and UpdateLfForDecoder (pik/ac_predictions.cc:560-635,
-// pik/compressed_image.cc:978-1084). Group-local cell (bx, by) in
-// [0, gxs+2) x [0, gys+2); the border ring acts as DCT8; DC from the frame
-// with mirroring (InitializeDecCache, pik/compressed_dc.cc:530-556). One
-// CTA runs all phases of one group and channel (k_lf_chain), with a barrier
-// between phases, and keeps the group's LLF, 2x2 and LF images in shared
-// memory; only pred2x2 and the blocks' corners leave the kernel.
+// LF prediction (ComputeLlf, PredictLf, pik/ac_predictions.cc:380-470) and
+// UpdateLfForDecoder (pik/ac_predictions.cc:560-635,
+// pik/compressed_image.cc:978-1084), per 512x512 group as the reference
+// computes them. Group-local cell (X, Y) in [0, gxs+2) x [0, gys+2): the
+// group's cells shifted by one, with a border ring that acts as DCT8; DC
+// from the frame with mirroring (InitializeDecCache,
+// pik/compressed_dc.cc:530-556). The 2x2 image of the group is
+// 2 (gxs + 2) x 2 (gys + 2), mirrored at its edges by the blur.
+//
+// A CTA (k_lf_tile) takes one channel of a tile of kLfTile x kLfTile cells
+// of a group and keeps the images it needs in shared memory: the LLF and
+// 2x2 images of every block that reaches the tile's blurred range (one
+// cell beyond the tile, and the ring where the tile touches it), so its
+// first cell may lie up to 3 cells before that range (DCT32X32).
 struct LfGroup {
   int gi, c, x0, y0, gxs, gys;
   __device__ int Acs(const Geo& g, const DevFrame& f, int bx, int by) const {
@@ -526,14 +558,35 @@ struct LfGroup {
   }
 };
 
-// Shared memory of k_lf_chain: the LLF image (kGB x kGB), the 2x2 image
-// before and after LFPredictionBlur (kG2 x kG2 each).
-constexpr size_t kLfSmemBytes = 4 * (size_t(kGB) * kGB + 2 * size_t(kG2) * kG2);
+constexpr int kLfTile = 32;           // cells per tile side
+constexpr int kLfWin = kLfTile + 12;  // shared-memory window, cells
+constexpr int kLfWin2 = 2 * kLfWin;   // the 2x2 images' window, pixels
+constexpr int kLfThreads = 256;
+// Shared memory of k_lf_tile: the LLF image, the 2x2 image before and after
+// LFPredictionBlur, over the window, and the list of the window's first
+// cells.
+constexpr size_t kLfSmemBytes =
+    4 * (2 * size_t(kLfWin) * kLfWin + 2 * size_t(kLfWin2) * kLfWin2);
+
+// The window of a tile: cell (X, Y) of the group is at (X - ex, Y - ey).
+struct LfWin {
+  int ex, ey;
+  float* llf;  // kLfWin x kLfWin
+  float* tmp;  // kLfWin2 x kLfWin2
+  float* lf;   // kLfWin2 x kLfWin2
+  __device__ float* Llf(int X, int Y) const {
+    return llf + (Y - ey) * kLfWin + (X - ex);
+  }
+  __device__ float* Tmp(int X2, int Y2) const {
+    return tmp + (Y2 - 2 * ey) * kLfWin2 + (X2 - 2 * ex);
+  }
+  __device__ float* Lf(int X2, int Y2) const {
+    return lf + (Y2 - 2 * ey) * kLfWin2 + (X2 - 2 * ex);
+  }
+};
 
 __device__ void LlfCell(const Geo& g, const DevFrame& f, const LfGroup& q,
-                        float* llf, int bx, int by) {
-  const int a = q.Acs(g, f, bx, by);
-  if (a & 0xF) return;
+                        const LfWin& w, int a, int bx, int by) {
   const int type = a >> 4, cov = Covered(type);
   float dc[16];
   for (int iy = 0; iy < cov; ++iy)
@@ -542,294 +595,193 @@ __device__ void LlfCell(const Geo& g, const DevFrame& f, const LfGroup& q,
           f.dc[(size_t(q.c) * g.By + MirrorIdx(q.y0 + by - 1 + iy, g.By)) *
                    g.Bx +
                MirrorIdx(q.x0 + bx - 1 + ix, g.Bx)];
-  LowestFreqFromDC(type, dc, 4, llf + by * kGB + bx, kGB);
+  LowestFreqFromDC(type, dc, 4, w.Llf(bx, by), kLfWin);
 }
 
-__device__ void Tmp2x2Cell(const Geo& g, const DevFrame& f, const LfGroup& q,
-                           const float* llf, float* tmp, int bx, int by) {
-  const int a = q.Acs(g, f, bx, by);
-  if (a & 0xF) return;
-  DC2x2FromLowestFreq(a >> 4, llf + by * kGB + bx, kGB,
-                      tmp + 2 * by * kG2 + 2 * bx, kG2);
-}
-
-// LFPredictionBlur over the group's 2x2 image (ConvolveT<Symmetric3>).
-__device__ void LfBlurPixel(const LfGroup& q, const float* tmp, float* lf,
-                            int x, int y) {
+// LFPredictionBlur over the group's 2x2 image (ConvolveT<Symmetric3>,
+// mirrored at the image's edges) for the run of up to 8 pixels x0 ..
+// x0 + n - 1 of row y: the 3 x (n + 2) inputs are loaded once, and each
+// output keeps Symmetric3's operation order.
+__device__ void LfBlurRun(const LfGroup& q, const LfWin& w, int x0, int y,
+                          int n) {
   const int w2 = 2 * (q.gxs + 2), h2 = 2 * (q.gys + 2);
-  const float* t = tmp + MirrorIdx(y - 1, h2) * kG2;
-  const float* m = tmp + y * kG2;
-  const float* b = tmp + MirrorIdx(y + 1, h2) * kG2;
-  const int xl = MirrorIdx(x - 1, w2), xr = MirrorIdx(x + 1, w2);
-  const float w0 = c_t.lf_blur[0], w1 = c_t.lf_blur[1], w2_ = c_t.lf_blur[2];
-  const float sum_tb = t[x] + b[x];
-  const float mul0 = m[x] * w0;
-  const float sum_lr = m[xl] + m[xr];
-  const float x1 = sum_tb + sum_lr;
-  const float mul1 = x1 * w1 + mul0;
-  const float sum_t2 = t[xl] + t[xr];
-  const float sum_b2 = b[xl] + b[xr];
-  const float x2 = sum_t2 + sum_b2;
-  lf[y * kG2 + x] = x2 * w2_ + mul1;
-}
-
-__device__ void LfFrom2x2Cell(const Geo& g, const DevFrame& f,
-                              const LfGroup& q, float* lf, int bx, int by) {
-  const int a = q.Acs(g, f, bx, by);
-  if (a & 0xF) return;
-  LowFreqFromDC2x2(a >> 4, lf + 2 * by * kG2 + 2 * bx, kG2);
-}
-
-// Border ring of pred2x2 (pik/compressed_image.cc:978-1039); ring cell i:
-// 2 columns of (gys + 2), then 2 rows of (gxs + 2).
-__device__ void PredBorderCell(const DevFrame& f, const LfGroup& q,
-                               const float* llf, const float* lf, int i,
-                               int predict_lf) {
-  int x, y;
-  if (i < 2 * (q.gys + 2)) {
-    x = (i & 1) ? q.gxs + 1 : 0;
-    y = i >> 1;
-  } else {
-    const int j = i - 2 * (q.gys + 2);
-    y = (j & 1) ? q.gys + 1 : 0;
-    x = j >> 1;
+  const int yr[3] = {MirrorIdx(y - 1, h2), y, MirrorIdx(y + 1, h2)};
+  float v[3][10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    if (i < n + 2) {
+      const int x = MirrorIdx(x0 - 1 + i, w2);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) v[j][i] = *w.Tmp(x, yr[j]);
+    }
   }
+  const float w0 = c_t.lf_blur[0], w1 = c_t.lf_blur[1], w2_ = c_t.lf_blur[2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    if (i < n) {
+      const float sum_tb = v[0][i + 1] + v[2][i + 1];
+      const float mul0 = v[1][i + 1] * w0;
+      const float sum_lr = v[1][i] + v[1][i + 2];
+      const float x1 = sum_tb + sum_lr;
+      const float mul1 = x1 * w1 + mul0;
+      const float sum_t2 = v[0][i] + v[0][i + 2];
+      const float sum_b2 = v[2][i] + v[2][i + 2];
+      const float x2 = sum_t2 + sum_b2;
+      *w.Lf(x0 + i, y) = x2 * w2_ + mul1;
+    }
+  }
+}
+
+// Ring cell (x, y) of pred2x2 (pik/compressed_image.cc:978-1039).
+__device__ void PredBorderCell(const DevFrame& f, const LfGroup& q,
+                               const LfWin& w, int x, int y,
+                               int predict_lf) {
   float* pred = f.pred2x2_g + q.gi * kG2GroupFloats + q.c * kG2 * kG2;
   if (predict_lf) {
     float blk[10];
-    blk[0] = llf[y * kGB + x];
-    blk[1] = lf[2 * y * kG2 + 2 * x + 1];
-    blk[8] = lf[(2 * y + 1) * kG2 + 2 * x];
-    blk[9] = lf[(2 * y + 1) * kG2 + 2 * x + 1];
+    blk[0] = *w.Llf(x, y);
+    blk[1] = *w.Lf(2 * x + 1, 2 * y);
+    blk[8] = *w.Lf(2 * x, 2 * y + 1);
+    blk[9] = *w.Lf(2 * x + 1, 2 * y + 1);
     DC2x2FromLowFreq(kDCT, [&](int k) { return blk[k]; },
                      pred + 2 * y * kG2 + 2 * x, kG2);
   } else {
-    DC2x2FromLowestFreq(kDCT, llf + y * kGB + x, kGB,
+    DC2x2FromLowestFreq(kDCT, w.Llf(x, y), kLfWin,
                         pred + 2 * y * kG2 + 2 * x, kG2);
   }
 }
 
-// UpdateLfForDecoder for the first block at group-local (lbx, lby): its
-// low-frequency corner -- the LLF from DC, the LF coefficients (dequantised
-// here, like Dequant::DoAC) plus the LF prediction -- into DevFrame::corner,
-// and the block's pred2x2 cells from it.
-__device__ void CornerBlock(const Geo& g, const DevFrame& f,
-                            const FrameScalars& s, const LfGroup& q,
-                            const float* llf, const float* lf, int lbx,
-                            int lby, int predict_lf, int predict_hf) {
-  const int bx = q.x0 + lbx, by = q.y0 + lby;
-  const int a = f.acs[by * g.Bx + bx];
-  if (a & 0xF) return;
-  const int type = a >> 4, cov = Covered(type), n = 8 * cov, c = q.c;
-  const size_t plane = size_t(g.ac_stride) * g.By;
-  float cv[8][8];
-  CellDq p{};
-  int pcell = -1;
-  for (int r = 0; r < 2 * cov; ++r) {
-    // Row r of the corner: block row by (r < 8), cell bx + r n / 64 (the
-    // 2 cov columns stay inside it).
-    const int cx = bx + (r * n) / 64;
-    if (!f.ac_in && cx != pcell) {
-      p = CellParamsOf(g, f, s, cx, by);
-      pcell = cx;
-    }
-    for (int l = 0; l < 2 * cov; ++l) {
-      float v;
-      if (r < cov && l < cov) {
-        v = llf[(lby + 1 + r) * kGB + lbx + 1 + l];
-      } else {
-        const int k = (r * n + l) % 64;
-        const size_t pos = size_t(by) * g.ac_stride + size_t(cx) * 64 + k;
-        v = f.ac_in ? f.ac_in[c * plane + pos] : DequantWith(g, f, p, c, pos, k);
-        if (predict_lf) {
-          v += lf[(2 * (lby + 1) + r) * kG2 + 2 * (lbx + 1) + l];
-        }
+// UpdateLfForDecoder for the first block at group cell (X, Y), in place on
+// the dequantised AC: the LLF from DC into the block's corner, the LF
+// prediction added to the LF coefficients, and the block's pred2x2 cells
+// from the updated corner.
+__device__ void LfUpdateBlock(const Geo& g, const DevFrame& f,
+                              const LfGroup& q, const LfWin& w, int type,
+                              int X, int Y, int predict_lf, int predict_hf) {
+  const int bx = q.x0 + X - 1, by = q.y0 + Y - 1, c = q.c;
+  const int cov = Covered(type);
+  float* base = f.ac + size_t(c) * g.ac_stride * g.By +
+                size_t(by) * g.ac_stride + size_t(bx) * 64;
+  const int chunk = 64 * cov;
+  auto at = [&](int i) -> float& {
+    return base[(i / chunk) * size_t(g.ac_stride) + i % chunk];
+  };
+  for (int y = 0; y < cov; ++y)
+    for (int x = 0; x < cov; ++x) at(cov * 8 * y + x) = *w.Llf(X + x, Y + y);
+  if (predict_lf) {
+    for (int y = 0; y < 2 * cov; ++y) {
+      const int start = y < cov ? cov : 0;
+      for (int x = start; x < 2 * cov; ++x) {
+        at(y * cov * 8 + x) += *w.Lf(2 * X + x, 2 * Y + y);
       }
-      cv[r][l] = v;
-      f.corner[CornerIdx(g, c, bx, by, r, l)] = v;
     }
   }
   if (predict_hf) {
     float* pred = f.pred2x2_g + q.gi * kG2GroupFloats + c * kG2 * kG2;
-    DC2x2FromLowFreq(type, [&](int i) { return cv[i / n][i % n]; },
-                     pred + 2 * (lby + 1) * kG2 + 2 * (lbx + 1), kG2);
+    DC2x2FromLowFreq(type, [&](int i) { return at(i); },
+                     pred + 2 * Y * kG2 + 2 * X, kG2);
   }
 }
 
-// 1024 threads, one CTA per group and channel (blockIdx.x = 3 gi + c).
-constexpr int kLfThreads = 1024;
-
-// All LF phases of one group and channel: LLF from DC; then, with LF
-// prediction, the 2x2 image, its blur and the LF coefficients from it;
-// with HF prediction, the pred2x2 border ring; and every first block's
-// corner (and pred2x2 cells).
-__global__ void __launch_bounds__(kLfThreads)
-    k_lf_chain(Geo g, DevFrame f, FrameScalars s, int predict_lf,
-               int predict_hf) {
+// One channel of one tile: blockIdx.x = tile, blockIdx.y = group,
+// blockIdx.z = channel. Phases (a barrier between them): LLF and the 2x2
+// image of every block whose first cell is in [lo - 4, hi + 1) (the blur
+// reads cells lo - 1 .. hi), then the blur and LowFrequenciesFromDC2x2 over
+// [lo, hi) -- the tile plus the ring cells beside it -- then the ring's
+// pred2x2 and the update of the tile's blocks.
+__global__ void __launch_bounds__(kLfThreads, 2)
+    k_lf_tile(Geo g, DevFrame f, int predict_lf, int predict_hf) {
   extern __shared__ float lf_smem[];
-  float* llf = lf_smem;             // kGB x kGB
-  float* tmp = llf + kGB * kGB;     // kG2 x kG2
-  float* lf = tmp + kG2 * kG2;      // kG2 x kG2
   LfGroup q;
-  q.gi = blockIdx.x / 3;
-  q.c = blockIdx.x % 3;
+  q.gi = blockIdx.y;
+  q.c = blockIdx.z;
   GroupDims(g, q.gi, &q.x0, &q.y0, &q.gxs, &q.gys);
-  const int cw = q.gxs + 2, ncell = cw * (q.gys + 2);
-  for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
-    LlfCell(g, f, q, llf, i % cw, i / cw);
+  const int ntx = (q.gxs + kLfTile - 1) / kLfTile;
+  const int tx = blockIdx.x % ntx, ty = blockIdx.x / ntx;
+  if (ty * kLfTile >= q.gys) return;
+  // The tile's cells [X0, X1) x [Y0, Y1); the LF range adds the ring.
+  const int X0 = 1 + tx * kLfTile, X1 = min(X0 + kLfTile, q.gxs + 1);
+  const int Y0 = 1 + ty * kLfTile, Y1 = min(Y0 + kLfTile, q.gys + 1);
+  const int lx = X0 == 1 ? 0 : X0, hx = X1 == q.gxs + 1 ? q.gxs + 2 : X1;
+  const int ly = Y0 == 1 ? 0 : Y0, hy = Y1 == q.gys + 1 ? q.gys + 2 : Y1;
+  __shared__ int s_count;
+  LfWin w;
+  w.ex = lx - 4;
+  w.ey = ly - 4;
+  w.llf = lf_smem;
+  w.tmp = w.llf + kLfWin * kLfWin;
+  w.lf = w.tmp + kLfWin2 * kLfWin2;
+  // The first cells of the blocks reaching cells lx - 1 .. hx (clipped to
+  // the group's ring), listed as X | Y << 10 | strategy byte << 20, so that
+  // the per-block phases below give every lane a block (a cell-per-lane
+  // loop leaves the lanes of the other cells of multi-block transforms
+  // idle).
+  int* first = reinterpret_cast<int*>(w.lf + kLfWin2 * kLfWin2);
+  if (threadIdx.x == 0) s_count = 0;
+  __syncthreads();
+  const int sx = max(lx - 4, 0), sy = max(ly - 4, 0);
+  const int nx = min(hx + 1, q.gxs + 2) - sx, ny = min(hy + 1, q.gys + 2) - sy;
+  for (int i = threadIdx.x; i < nx * ny; i += kLfThreads) {
+    const int X = sx + i % nx, Y = sy + i / nx;
+    const int a = q.Acs(g, f, X, Y);
+    if (a & 0xF) continue;
+    first[atomicAdd(&s_count, 1)] = X | (Y << 10) | (a << 20);
+  }
+  __syncthreads();
+  const int nfirst = s_count;
+  for (int i = threadIdx.x; i < nfirst; i += kLfThreads) {
+    const int e = first[i];
+    const int X = e & 1023, Y = (e >> 10) & 1023, a = e >> 20;
+    LlfCell(g, f, q, w, a, X, Y);
+    if (predict_lf) {
+      DC2x2FromLowestFreq(a >> 4, w.Llf(X, Y), kLfWin, w.Tmp(2 * X, 2 * Y),
+                          kLfWin2);
+    }
   }
   __syncthreads();
   if (predict_lf) {
-    for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
-      Tmp2x2Cell(g, f, q, llf, tmp, i % cw, i / cw);
-    }
-    __syncthreads();
-    const int w2 = 2 * cw, n2 = w2 * 2 * (q.gys + 2);
+    // Runs of 8 pixels of the blurred range's rows.
+    const int w2 = 2 * (hx - lx), runs = (w2 + 7) / 8;
+    const int n2 = runs * 2 * (hy - ly);
     for (int i = threadIdx.x; i < n2; i += kLfThreads) {
-      LfBlurPixel(q, tmp, lf, i % w2, i / w2);
+      const int r = i % runs, y = 2 * ly + i / runs;
+      LfBlurRun(q, w, 2 * lx + 8 * r, y, min(8, w2 - 8 * r));
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < ncell; i += kLfThreads) {
-      LfFrom2x2Cell(g, f, q, lf, i % cw, i / cw);
+    for (int i = threadIdx.x; i < nfirst; i += kLfThreads) {
+      const int e = first[i];
+      const int X = e & 1023, Y = (e >> 10) & 1023, a = e >> 20;
+      if (X < lx || X >= hx || Y < ly || Y >= hy) continue;
+      LowFreqFromDC2x2(a >> 4, w.Lf(2 * X, 2 * Y), kLfWin2);
     }
     __syncthreads();
   }
   if (predict_hf) {
-    const int nring = 2 * (q.gys + 2) + 2 * (q.gxs + 2);
-    for (int i = threadIdx.x; i < nring; i += kLfThreads) {
-      PredBorderCell(f, q, llf, lf, i, predict_lf);
+    // Ring cells beside the tile: left/right columns, then top/bottom rows.
+    const int rows = hy - ly, cols = hx - lx;
+    for (int i = threadIdx.x; i < 2 * rows + 2 * cols; i += kLfThreads) {
+      int X, Y;
+      if (i < 2 * rows) {
+        X = (i & 1) ? q.gxs + 1 : 0;
+        Y = ly + (i >> 1);
+        if ((X == 0 && lx != 0) || (X != 0 && hx != q.gxs + 2)) continue;
+      } else {
+        const int j = i - 2 * rows;
+        Y = (j & 1) ? q.gys + 1 : 0;
+        X = lx + (j >> 1);
+        if ((Y == 0 && ly != 0) || (Y != 0 && hy != q.gys + 2)) continue;
+        // Corner cells belong to the columns' pass.
+        if (X == 0 || X == q.gxs + 1) continue;
+      }
+      PredBorderCell(f, q, w, X, Y, predict_lf);
     }
   }
-  const int nblk = q.gxs * q.gys;
-  for (int i = threadIdx.x; i < nblk; i += kLfThreads) {
-    CornerBlock(g, f, s, q, llf, lf, i % q.gxs, i / q.gxs, predict_lf,
-                predict_hf);
+  for (int i = threadIdx.x; i < nfirst; i += kLfThreads) {
+    const int e = first[i];
+    const int X = e & 1023, Y = (e >> 10) & 1023, a = e >> 20;
+    if (X < X0 || X >= X1 || Y < Y0 || Y >= Y1) continue;
+    LfUpdateBlock(g, f, q, w, a >> 4, X, Y, predict_lf, predict_hf);
   }
-}
-
-// Dequant::DoAC's parameters of every cell, for the transforms that
-// dequantise the int16 AC as they load it.
-__global__ void k_cell_params(Geo g, DevFrame f, FrameScalars s) {
-  const int bx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int by = blockIdx.y * blockDim.y + threadIdx.y;
-  if (bx >= g.Bx || by >= g.By) return;
-  const CellDq p = CellParamsOf(g, f, s, bx, by);
-  uint4* dst = reinterpret_cast<uint4*>(const_cast<CellDq*>(f.cellp) +
-                                        by * g.Bx + bx);
-  dst[0] = make_uint4(__float_as_uint(p.scaled), __float_as_uint(p.x_cc),
-                      __float_as_uint(p.b_cc), p.m[0]);
-  dst[1] = make_uint4(p.m[1], p.m[2], 0u, 0u);
-}
-
-// Coefficient k of channel c of cell (bx, by), dequantised (k_dequant_ac's
-// arithmetic and order), or taken from the supplied dequantised AC.
-__device__ __forceinline__ float DequantOne(const Geo& g, const DevFrame& f,
-                                            int c, int bx, int by, int k) {
-  const size_t plane = size_t(g.ac_stride) * g.By;
-  const size_t pos = size_t(by) * g.ac_stride + size_t(bx) * 64 + k;
-  if (f.ac_in) return f.ac_in[c * plane + pos];
-  return DequantWith(g, f, f.cellp[by * g.Bx + bx], c, pos, k);
-}
-
-// n consecutive dequantised values: int16 `q` (16-byte aligned) times
-// (matrix row `m` x scaled) after AdjustQuantBias.
-template <int n>
-__device__ __forceinline__ void DequantRun(const int16_t* q, const float* m,
-                                           float scaled, float one_bias,
-                                           float* out) {
-  const bool mvec = (reinterpret_cast<uintptr_t>(m) & 15) == 0;
-#pragma unroll
-  for (int i = 0; i < n; i += 8) {
-    const uint4 raw = *reinterpret_cast<const uint4*>(q + i);
-    float mv[8];
-    if (mvec) {
-      const float4 m0 = *reinterpret_cast<const float4*>(m + i);
-      const float4 m1 = *reinterpret_cast<const float4*>(m + i + 4);
-      mv[0] = m0.x, mv[1] = m0.y, mv[2] = m0.z, mv[3] = m0.w;
-      mv[4] = m1.x, mv[5] = m1.y, mv[6] = m1.z, mv[7] = m1.w;
-    } else {
-#pragma unroll
-      for (int k = 0; k < 8; ++k) mv[k] = m[i + k];
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const uint32_t word = k < 2 ? raw.x : k < 4 ? raw.y : k < 6 ? raw.z
-                                                                : raw.w;
-      const int16_t qi = int16_t(word >> (16 * (k & 1)));
-      const float mulc = mv[k] * scaled;
-      out[i + k] = AdjustQuantBias(float(qi), one_bias) * mulc;
-    }
-  }
-}
-
-// Coefficients k0 .. k0 + n - 1 of channel c of cell (bx, by) (n a multiple
-// of 8, k0 of n): Dequant::DoAC (pik/compressed_image.cc:636-700) applied
-// as they are loaded -- Y, then X and B plus their chroma-from-luma share
-// of Y, in k_dequant_ac's operation order -- or the supplied dequantised AC.
-template <int n>
-__device__ __forceinline__ void CellCoefs(const Geo& g, const DevFrame& f,
-                                          int c, int bx, int by, int k0,
-                                          float* out) {
-  const size_t plane = size_t(g.ac_stride) * g.By;
-  const size_t pos = size_t(by) * g.ac_stride + size_t(bx) * 64 + k0;
-  if (f.ac_in) {
-    const float4* src =
-        reinterpret_cast<const float4*>(f.ac_in + c * plane + pos);
-#pragma unroll
-    for (int i = 0; i < n / 4; ++i) {
-      const float4 v = src[i];
-      out[4 * i] = v.x, out[4 * i + 1] = v.y;
-      out[4 * i + 2] = v.z, out[4 * i + 3] = v.w;
-    }
-    return;
-  }
-  const uint4* pp = reinterpret_cast<const uint4*>(f.cellp + by * g.Bx + bx);
-  const uint4 p0 = pp[0], p1 = pp[1];
-  const float scaled = __uint_as_float(p0.x);
-  const int16_t* qy = f.qac + plane + pos;
-  const float* my = f.table + p1.x + k0;
-  if (c == 1) {
-    DequantRun<n>(qy, my, scaled, c_t.one_bias[1], out);
-    return;
-  }
-  const int16_t* qc = f.qac + c * plane + pos;
-  const float* mc = f.table + (c == 0 ? p0.w : p1.y) + k0;
-  const float cc = __uint_as_float(c == 0 ? p0.y : p0.z);
-  // Eight at a time: Y, then this channel plus its share of Y.
-#pragma unroll
-  for (int i = 0; i < n; i += 8) {
-    float dy[8];
-    DequantRun<8>(qy + i, my + i, scaled, c_t.one_bias[1], dy);
-    DequantRun<8>(qc + i, mc + i, scaled, c_t.one_bias[c], out + i);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) out[i + k] = cc * dy[k] + out[i + k];
-  }
-}
-
-
-// Row r of the N x N coefficient matrix of channel c of the block at
-// (bx, by) (GatherCoefficients layout, pik/ac_strategy.h:255-272: block row
-// by + r / 8, offset (r % 8) N, inside one cell), with its low-frequency
-// corner taken from DevFrame::corner.
-template <int N>
-__device__ __forceinline__ void LoadCoefRow(const Geo& g, const DevFrame& f,
-                                            int c, int bx, int by, int r,
-                                            float (&X)[N]) {
-  constexpr int cov = N / 8;
-  const int off = (r % 8) * N;
-  CellCoefs<N>(g, f, c, bx + off / 64, by + r / 8, off % 64, X);
-  if (r < 2 * cov) {
-#pragma unroll
-    for (int l = 0; l < 2 * cov; ++l) X[l] = f.corner[CornerIdx(g, c, bx, by, r, l)];
-  }
-}
-
-// Coefficient e (0..63) of an 8x8-class block (one cell) with its corner.
-__device__ __forceinline__ float CoefAt8(const Geo& g, const DevFrame& f,
-                                         int c, int bx, int by, int e) {
-  const int r = e >> 3, l = e & 7;
-  if (r < 2 && l < 2) return f.corner[CornerIdx(g, c, bx, by, r, l)];
-  return DequantOne(g, f, c, bx, by, e);
 }
 
 constexpr int kDct4Blocks = 4;  // DCT4X4 blocks per CTA (x 64 coefficients)
@@ -989,7 +941,8 @@ __global__ void __launch_bounds__(256)
   }
   const int first = blockIdx.x * NB;
   const int nb = min(NB, count - first);
-  constexpr int cov = N / 8;
+  constexpr int cov = N / 8, chunk = 64 * cov;
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
   const size_t plane_px = size_t(g.PW) * g.PH;
   __syncthreads();
   for (int c = 0; c < 3; ++c) {
@@ -998,12 +951,9 @@ __global__ void __launch_bounds__(256)
       const int b = i / NN, e = i % NN;
       const uint32_t pk = list[first + b];
       const int bx = pk & 0xFFFF, by = pk >> 16;
-      // Coefficient (y, x) = (e / N, e % N): block row by + y / 8, cell
-      // bx + ((y % 8) N + x) / 64 (GatherCoefficients layout).
-      const int y = e / N, x = e % N, o = (y % 8) * N + x;
-      s_c[i] = y < 2 * cov && x < 2 * cov
-                   ? f.corner[CornerIdx(g, c, bx, by, y, x)]
-                   : DequantOne(g, f, c, bx + o / 64, by + y / 8, o % 64);
+      const float* base = f.ac + c * plane_ac + size_t(by) * g.ac_stride +
+                          size_t(bx) * 64;
+      s_c[i] = base[(e / chunk) * size_t(g.ac_stride) + e % chunk];
       // DCT_NOHF shares this kernel with DCT but takes no HF prediction.
       if (predict_hf && !PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) {
         s_p[i] = 0.f;
@@ -1056,6 +1006,7 @@ __global__ void __launch_bounds__(256)
   }
   const int first = blockIdx.x * NB;
   const int nb = min(NB, count - first);
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
   const size_t plane_px = size_t(g.PW) * g.PH;
   __syncthreads();
   for (int c = 0; c < 3; ++c) {
@@ -1063,7 +1014,7 @@ __global__ void __launch_bounds__(256)
       const int b = i / 64, e = i % 64;
       const uint32_t pk = list[first + b];
       const int bx = pk & 0xFFFF, by = pk >> 16;
-      s_c[i] = CoefAt8(g, f, c, bx, by, e);
+      s_c[i] = f.ac[c * plane_ac + size_t(by) * g.ac_stride + bx * 64 + e];
       if (predict_hf && PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) {
         // Sub-block-major pixel layout: sub-block (sy, sx), pixel (py, px).
         const int sb = e / 16, py = (e % 16) / 4, px = e % 4;
@@ -1235,8 +1186,8 @@ __global__ void k_small_idct(Geo g, DevFrame f, const uint32_t* list,
   const uint32_t pk = list[b];
   const int bx = pk & 0xFFFF, by = pk >> 16;
   const int type = f.acs[by * g.Bx + bx] >> 4;
-  float cb[64];
-  for (int e = 0; e < 64; ++e) cb[e] = CoefAt8(g, f, c, bx, by, e);
+  const float* cb = f.ac + c * size_t(g.ac_stride) * g.By +
+                    size_t(by) * g.ac_stride + bx * 64;
   float* px = f.idct + c * size_t(g.PW) * g.PH + size_t(by * 8) * g.PW + bx * 8;
   SmallInverse(type, cb, px, g.PW);
 }
@@ -1705,16 +1656,16 @@ template __global__ void k_square_idct_rows<32>(Geo, DevFrame,
                                                 const uint32_t*, int, int);
 template __global__ void k_square_idct_tc1<16, 2>(Geo, DevFrame,
                                                   const uint32_t*, int, int,
-                                                  int*);
+                                                  int*, int*);
 template __global__ void k_square_idct_tc1<16, 3>(Geo, DevFrame,
                                                   const uint32_t*, int, int,
-                                                  int*);
+                                                  int*, int*);
 template __global__ void k_square_ar_tc<16, 2>(Geo, DevFrame, FrameScalars,
                                                const uint32_t*, const int*,
-                                               int*);
+                                               int*, int*);
 template __global__ void k_square_ar_tc<16, 3>(Geo, DevFrame, FrameScalars,
                                                const uint32_t*, const int*,
-                                               int*);
+                                               int*, int*);
 template __global__ void k_square_ar_rows<8>(Geo, DevFrame, FrameScalars,
                                              const uint32_t*, const int*);
 template __global__ void k_square_ar_rows<16>(Geo, DevFrame, FrameScalars,

@@ -80,6 +80,14 @@ __device__ __forceinline__ void GetCol(const float* tile, int r, float (&v)[N]) 
   for (int i = 0; i < N; ++i) v[i] = tile[i * (N + 1) + r];
 }
 
+// Pointer to row r of the block's coefficients in the frame layout: row r
+// of the N x N matrix lives in block row (by + r / 8) at column offset
+// bx * 64 + (r % 8) * N (GatherCoefficients layout, pik/ac_strategy.h:255-272).
+__device__ __forceinline__ size_t CoefRowOffset(const Geo& g, int bx, int by,
+                                                int n, int r) {
+  return size_t(by + r / 8) * g.ac_stride + size_t(bx) * 64 + (r % 8) * n;
+}
+
 }  // namespace square
 
 constexpr int kSquareThreads = 128;
@@ -105,8 +113,14 @@ __global__ void __launch_bounds__(kSquareThreads)
   const int b = active ? item / 3 : 0, c = active ? item % 3 : 0;
   const uint32_t pk = list[b];
   const int bx = pk & 0xFFFF, by = pk >> 16;
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
+  const float* crow = f.ac + c * plane_ac + CoefRowOffset(g, bx, by, N, r);
   float X[N];
-  LoadCoefRow<N>(g, f, c, bx, by, r, X);
+#pragma unroll
+  for (int i = 0; i < N; i += 4) {
+    const float4 v = *reinterpret_cast<const float4*>(crow + i);
+    X[i] = v.x, X[i + 1] = v.y, X[i + 2] = v.z, X[i + 3] = v.w;
+  }
   if (predict_hf) {
     // DCT_NOHF shares the 8x8 class; its prediction is computed but not
     // added, keeping the warp's control flow uniform.
@@ -144,22 +158,25 @@ __global__ void __launch_bounds__(kSquareThreads)
   }
 }
 
-// Keeps the blocks of `list` that the EPF filtered (some cell has sigma >=
-// kMinSigma); for the others the clamp stage is an exact no-op because the
-// filtered block equals the original.
+// Keeps the blocks of each class's list that the EPF filtered (some cell
+// has sigma >= kMinSigma) in that class's active list (counter k); for the
+// others the clamp stage is an exact no-op because the filtered block
+// equals the original. One thread per block of all the classes.
 __global__ void k_active_blocks(Geo g, const int32_t* sigma,
-                                const uint8_t* acs, const uint32_t* list,
-                                int count, uint32_t* out, int* counter) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const uint32_t pk = list[i];
+                                const uint8_t* acs, ClassLists cl,
+                                int* counters) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = 0;
+  while (k < kMaxClasses && i >= cl.n[k]) i -= cl.n[k++];
+  if (k == kMaxClasses) return;
+  const uint32_t pk = cl.list[k][i];
   const int bx = pk & 0xFFFF, by = pk >> 16;
   const int cov = Covered(acs[by * g.Bx + bx] >> 4);
   bool any = false;
   for (int y = 0; y < cov; ++y)
     for (int x = 0; x < cov; ++x)
       any |= sigma[(by + y) * g.Bx + bx + x] >= kMinSigma;
-  if (any) out[atomicAdd(counter, 1)] = pk;
+  if (any) cl.active[k][atomicAdd(&counters[k], 1)] = pk;
 }
 
 // AdaptiveReconstruction clamp for square DCT blocks, one unit per block

@@ -326,11 +326,12 @@ __device__ __forceinline__ bool Pass1(Smem1<N, S>& s, int j, bool a_mn,
 template <int N, int S>
 __global__ void __launch_bounds__(tc::kThreads, 4)
     k_square_ar_tc(Geo g, DevFrame f, FrameScalars sc, const uint32_t* list,
-                   const int* count_ptr, int* err) {
+                   const int* count_ptr, int* work, int* err) {
   using namespace tc;
   constexpr int BPB = 128 / N;
   constexpr int cov = N / 8;
   __shared__ Smem<N, S> s;
+  __shared__ int s_next[2];
   const int t = threadIdx.x, bl = t / N, r = t % N;
   if (t < 32) {
     asm volatile(
@@ -355,7 +356,15 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
   const size_t plane = size_t(g.PW) * g.PH;
   const float inv_nn = 1.0f / float(N * N);
   bool ok = true;
-  for (int batch = blockIdx.x; batch < nbat && ok; batch += gridDim.x) {
+  // Batches are taken from a work counter, one at a time: a CTA that
+  // starts late (its SM busy with another class's kernel) takes fewer.
+  // The next batch is fetched at the start of a batch and read after the
+  // batch's last barrier.
+  if (t == 0) s_next[0] = atomicAdd(work, 1);
+  __syncthreads();
+  int batch = s_next[0];
+  for (int k = 1; batch < nbat && ok; ++k) {
+    if (t == 0) s_next[k & 1] = atomicAdd(work, 1);
     const int idx = batch * BPB + bl;
     const bool active = idx < count;
     const uint32_t pkd = list[active ? idx : 0];
@@ -464,6 +473,7 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
     }
     ok = Pass<N, S>(s, 1, true, s.idct, phase, f.tc_polls) && ok;
     ok = __syncthreads_and(ok);
+    const int next = s_next[k & 1];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       LoadRow<N, S>(s, AccCol<N>(c, 1), T);  // pixel row v = r
@@ -478,6 +488,7 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
         }
       }
     }
+    batch = next;
   }
   if (!ok && t == 0) atomicExch(err, 1);
   FenceBefore();
@@ -499,12 +510,14 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
 template <int N, int S>
 __global__ void __launch_bounds__(tc::kThreads, 8)
     k_square_idct_tc1(Geo g, DevFrame f, const uint32_t* list, int count,
-                      int predict_hf, int* err) {
+                      int predict_hf, int* work, int* err) {
   using namespace tc;
+  using square::CoefRowOffset;
   static_assert(N == 16, "the HF corner table is for 16x16 blocks");
   constexpr int BPB = 128 / N;  // blocks per batch
   constexpr int cov = N / 8;
   __shared__ Smem1<N, S> s;
+  __shared__ int s_first[2], s_next[2];
   const int t = threadIdx.x, bl = t / N, r = t % N;
   if (t < 32) {
     asm volatile(
@@ -525,6 +538,7 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
   uint32_t phase = 0;
   const int nbat = (count + BPB - 1) / BPB;
   const int nitems = 3 * nbat;
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
   const size_t plane_px = size_t(g.PW) * g.PH;
   const float inv_nn = 1.0f / float(N * N);
   float cr[6];  // this lane's row of the HF corner table (rows r < 4)
@@ -538,16 +552,29 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
     const int bt = it / 3, ch = it - 3 * bt;
     const int i = bt * BPB + bl;
     const uint32_t pk = list[i < count ? i : 0];
-    if (i < count) {
-      LoadCoefRow<N>(g, f, ch, pk & 0xFFFF, pk >> 16, r, X);
-    } else {
+    const float* crow = f.ac + ch * plane_ac +
+                        CoefRowOffset(g, pk & 0xFFFF, pk >> 16, N, r);
 #pragma unroll
-      for (int j = 0; j < N; ++j) X[j] = 0.f;
+    for (int j = 0; j < N; j += 4) {
+      const float4 v = i < count ? *reinterpret_cast<const float4*>(crow + j)
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+      X[j] = v.x, X[j + 1] = v.y, X[j + 2] = v.z, X[j + 3] = v.w;
     }
     return pk;
   };
-  uint32_t pkd_next = blockIdx.x < nitems ? load_row(blockIdx.x) : 0u;
-  for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+  // Items are taken from a work counter, so that a CTA that starts late
+  // (its SM busy with another class's kernel) takes fewer. Two are known
+  // ahead: the current one and the next, whose coefficient row is loaded
+  // during the current item's passes; the one after that is fetched during
+  // the current item and read after its first pass's barrier.
+  if (t == 0) {
+    s_first[0] = atomicAdd(work, 1);
+    s_first[1] = atomicAdd(work, 1);
+  }
+  __syncthreads();
+  int item = s_first[0], item_next = s_first[1];
+  uint32_t pkd_next = item < nitems ? load_row(item) : 0u;
+  for (int k = 0; item < nitems && ok; ++k) {
     const int batch = item / 3, c = item - 3 * batch;
     const int idx = batch * BPB + bl;
     const bool active = idx < count;
@@ -613,8 +640,10 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
     }
     float T[N];
     PutRowK<N, S>(s.a, t, X);
-    if (item + int(gridDim.x) < nitems) pkd_next = load_row(item + gridDim.x);
+    if (item_next < nitems) pkd_next = load_row(item_next);
+    if (t == 0) s_next[k & 1] = atomicAdd(work, 1);
     ok = Pass1<N, S>(s, 0, false, s.idct, phase, f.tc_polls) && ok;
+    const int item_after = s_next[k & 1];
     LoadRow1<N, S>(s, 0, T);  // T[k = r][v]
     PutColMN<N, S>(s.a, N * bl, r, T);
     ok = Pass1<N, S>(s, 1, true, s.idct, phase, f.tc_polls) && ok;
@@ -632,6 +661,8 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
             make_float4(T[i], T[i + 1], T[i + 2], T[i + 3]);
       }
     }
+    item = item_next;
+    item_next = item_after;
   }
   if (!ok && t == 0) atomicExch(err, 1);
   FenceBefore();
