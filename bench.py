@@ -78,10 +78,11 @@ PATH_TRAFFIC_4K = None
 # against the FP64 oracle are checked by tests/test_split_bf16.py.
 FORM_NAMES = {
     "fp32": "plain FP32 on CUDA cores (bit-exact to the FP32 oracle)",
-    "split_bf16": "16x16 transforms on tcgen05 tensor cores, split-BF16 "
-                  "(hi+lo, 3 products, FP32 accumulate)",
-    "split_bf16x3": "16x16 transforms on tcgen05 tensor cores, split-BF16 "
-                    "(hi+mid+lo, 6 products, FP32 accumulate)",
+    "split_bf16": "16x16 and 32x32 transforms on tcgen05 tensor cores, "
+                  "split-BF16 with FP32 accumulate (16-point: hi+lo, 3 "
+                  "products; 32-point: hi+mid+lo, 6 products)",
+    "split_bf16x3": "16x16 and 32x32 transforms on tcgen05 tensor cores, "
+                    "split-BF16 (hi+mid+lo, 6 products, FP32 accumulate)",
 }
 
 
@@ -508,6 +509,57 @@ def c5_frame(xsize=8192, ysize=8192, seed=5, mix="broad"):
                                           shares=shares)
 
 
+def c5_summary(local, steps, warmup, mix="encoder"):
+    """Device time per frame of the 8192x8192 workload (`mix`) in the plain
+    FP32 and split-BF16 forms, inputs resident and outputs into device
+    planes, with the achieved HBM GB/s of 18.28 algorithmic B/px. Reported
+    in the default line beside the 4K figures."""
+    import ctypes
+    import torch
+    from pik_b200 import native
+    dev = torch.device("cuda", local)
+    frame = c5_frame(mix=mix)
+    px = frame.xsize * frame.ysize
+    by, bx = frame.blocks
+    ac_dev = torch.from_numpy(frame.quantized_ac).to(dev)
+    planes = (ctypes.c_void_p * 3)(*[ac_dev[c].data_ptr() for c in range(3)])
+    lin = torch.empty((3, frame.ysize, frame.xsize), dtype=torch.float32,
+                      device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    out = {"workload": "c5_8k: 8192x8192 synthetic highlight frame, "
+                       "distance 0.5, gaborish + EPF on, FP32 planes out",
+           "mix": C5_MIXES[mix]}
+    for form in ("fp32", "split_bf16"):
+        ctx = native.Context(local, form=form)
+        ctx.begin(frame)
+        ctx.L.pikgpu_set_stream(ctx.h, stream.cuda_stream)
+
+        def step():
+            ctx._check(ctx.L.pikgpu_frame_set_ac_device(ctx.h, planes,
+                                                        bx * 64))
+            ctx.reconstruct_device(lin.data_ptr(), frame.xsize)
+
+        for _ in range(max(3, warmup)):
+            step()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        ctx.close()
+        out[form] = {"ms_per_frame": round(ms, 4),
+                     "megapixels_per_s": round(px / (ms * 1e-3) / 1e6, 1),
+                     "hbm_gbs": round(PATH_BYTES_PER_PX * px / (ms * 1e-3)
+                                      / 1e9, 1)}
+    out["split_over_fp32"] = round(out["fp32"]["ms_per_frame"] /
+                                   out["split_bf16"]["ms_per_frame"], 3)
+    return out
+
+
 def c5_main(args):
     """Achieved HBM GB/s of the 8192x8192 reconstruction (FP32 linear planes
     out, 805 MB) in the split-BF16 and plain FP32 forms: 18.28 algorithmic
@@ -715,6 +767,8 @@ def main():
                     choices=["c2_4k", "batch64", "adjoint1k", "c5_8k"])
     ap.add_argument("--mix", default="broad", choices=sorted(C5_MIXES),
                     help="transform mix of the c5_8k frame")
+    ap.add_argument("--no-c5", action="store_true",
+                    help="leave the 8192x8192 summary out of the 4K line")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -954,6 +1008,9 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu_baseline(px) if ws == 1 else None,
         }
+        if ws == 1 and not args.no_c5:
+            out["c5_8k"] = c5_summary(local, min(args.steps, 10),
+                                      args.warmup)
         print(json.dumps(out))
     if ws > 1:
         dist.barrier()

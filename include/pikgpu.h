@@ -211,12 +211,16 @@ int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
  *               (pikgpu_last_kernel_times);
  *  FORM:        PIKGPU_FORM_FP32 (default): every stage in FP32 on the CUDA
  *               cores in the reference's operation order;
- *               PIKGPU_FORM_SPLIT_BF16: the 16x16 transforms on the tensor
- *               cores as split-BF16 GEMMs with FP32 accumulation, operands
- *               split in two BF16 terms (hi + lo, three products; about
- *               16 significant bits);
- *               PIKGPU_FORM_SPLIT_BF16X3: the same with three terms
- *               (hi + mid + lo, six products; FP32-level error).
+ *               PIKGPU_FORM_SPLIT_BF16: the 16x16 and 32x32 transforms
+ *               (the IDCT with HF prediction and the clamp's DCT pair) on
+ *               the tensor cores as split-BF16 GEMMs with FP32
+ *               accumulation; 16-point operands split in two BF16 terms
+ *               (hi + lo, three products; about 16 significant bits) --
+ *               in three for the IDCT of frames without HF prediction --
+ *               and 32-point operands in three (hi + mid + lo, six
+ *               products);
+ *               PIKGPU_FORM_SPLIT_BF16X3: three terms for both sizes
+ *               (FP32-level error).
  *               The tensor-core forms are not bit-identical to the FP32
  *               form;
  *  GRAPHS:      1 (default): when pikgpu_reconstruct is called again with

@@ -32,7 +32,8 @@ enum Class { kC8 = 0, kC16, kC32, kC4, kCSmall, kNumClasses };
 // blocks per class, then the work counters of the persistent tensor-core
 // transform and clamp kernels.
 constexpr int kWorkIdct = kNumClasses, kWorkAr = kNumClasses + 1;
-constexpr int kNumCounters = kNumClasses + 2;
+constexpr int kWorkIdct32 = kNumClasses + 2, kWorkAr32 = kNumClasses + 3;
+constexpr int kNumCounters = kNumClasses + 4;
 static_assert(kNumClasses == kMaxClasses, "ClassLists holds every class");
 int ClassOf(int type) {
   switch (type) {
@@ -405,6 +406,18 @@ int UploadTables(pikgpu_ctx* ctx) {
   CUDA_TRY(ctx, cudaFuncSetAttribute(
                     k_lf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
                     int(kLfSmemBytes)));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_square_ar_tc<16, 2>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(ArTcSmemBytes<16, 2>())));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_square_ar_tc<16, 3>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(ArTcSmemBytes<16, 3>())));
+  CUDA_TRY(ctx, cudaFuncSetAttribute(
+                    k_square_ar_tc<32, 3>,
+                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    int(ArTcSmemBytes<32, 3>())));
   if (ctx->device < 64) g_tables_uploaded[ctx->device] = true;
   return PIKGPU_OK;
 }
@@ -622,7 +635,18 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
           g, f, L[kC4], n[kC4], s.predict_hf);
       ++ctx->launches;
     }
-    if (n[kC32]) {
+    if (n[kC32] && ctx->form != PIKGPU_FORM_FP32) {
+      // One channel per CTA: four blocks of 32 rows per batch, up to
+      // tc_ctas_per_sm CTAs per SM (registers). Both tensor-core forms
+      // split the 32-point operands in three BF16 terms: with two, a frame
+      // without HF prediction reached 3.0e-5 against FP64.
+      const int items = 3 * ((n[kC32] + 3) / 4);
+      const int grid = std::min(items, ctx->num_sms * ctx->tc_ctas_per_sm);
+      k_square_idct_tc1<32, 3><<<grid, tc::kThreads, 0, cls(kC32)>>>(
+          g, f, L[kC32], n[kC32], s.predict_hf, counters + kWorkIdct32,
+          P<int>(ctx->tc_err));
+      ++ctx->launches;
+    } else if (n[kC32]) {
       // One 256-thread CTA per block.
       k_square_idct<32><<<n[kC32], 256, 0, cls(kC32)>>>(g, f, L[kC32], n[kC32],
                                                        s.predict_hf);
@@ -638,7 +662,10 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       // One channel per CTA: up to 2 tc_ctas_per_sm CTAs per SM.
       const int grid =
           std::min(3 * items, ctx->num_sms * 2 * ctx->tc_ctas_per_sm);
-      if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
+      // Two BF16 terms hold 2e-5 against FP64 only when the HF prediction
+      // carries the bulk of the coefficients (it is added in FP32 outside
+      // the tensor cores); frames without it take three terms.
+      if (ctx->form == PIKGPU_FORM_SPLIT_BF16 && s.predict_hf) {
         k_square_idct_tc1<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
             g, f, L[kC16], n[kC16], s.predict_hf, counters + kWorkIdct,
             P<int>(ctx->tc_err));
@@ -726,7 +753,17 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
           g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
       ++ctx->launches;
     }
-    if (n[kC32]) {
+    if (n[kC32] && ctx->form != PIKGPU_FORM_FP32) {
+      // Four blocks per batch; two CTAs per SM (256 tensor-memory columns
+      // each); three BF16 terms in both tensor-core forms (see the
+      // transforms).
+      const int grid = std::min((n[kC32] + 3) / 4, ctx->num_sms * 2);
+      k_square_ar_tc<32, 3><<<grid, tc::kThreads, ArTcSmemBytes<32, 3>(),
+                              cls(kC32)>>>(
+          g, f, s, P<uint32_t>(ctx->active[kC32]), counters + kC32,
+          counters + kWorkAr32, P<int>(ctx->tc_err));
+      ++ctx->launches;
+    } else if (n[kC32]) {
       k_square_ar<32><<<n[kC32], 256, 0, cls(kC32)>>>(
           g, f, s, P<uint32_t>(ctx->active[kC32]), counters + kC32);
       ++ctx->launches;
@@ -741,11 +778,13 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       const int grid =
           std::min((n[kC16] + 7) / 8, ctx->num_sms * ctx->tc_ctas_per_sm);
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
-        k_square_ar_tc<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
+        k_square_ar_tc<16, 2><<<grid, tc::kThreads, ArTcSmemBytes<16, 2>(),
+                                cls(kC16)>>>(
             g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
             counters + kWorkAr, P<int>(ctx->tc_err));
       } else {
-        k_square_ar_tc<16, 3><<<grid, tc::kThreads, 0, cls(kC16)>>>(
+        k_square_ar_tc<16, 3><<<grid, tc::kThreads, ArTcSmemBytes<16, 3>(),
+                                cls(kC16)>>>(
             g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
             counters + kWorkAr, P<int>(ctx->tc_err));
       }

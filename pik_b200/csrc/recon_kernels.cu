@@ -1666,6 +1666,12 @@ template __global__ void k_square_ar_tc<16, 2>(Geo, DevFrame, FrameScalars,
 template __global__ void k_square_ar_tc<16, 3>(Geo, DevFrame, FrameScalars,
                                                const uint32_t*, const int*,
                                                int*, int*);
+template __global__ void k_square_idct_tc1<32, 3>(Geo, DevFrame,
+                                                  const uint32_t*, int, int,
+                                                  int*, int*);
+template __global__ void k_square_ar_tc<32, 3>(Geo, DevFrame, FrameScalars,
+                                               const uint32_t*, const int*,
+                                               int*, int*);
 template __global__ void k_square_ar_rows<8>(Geo, DevFrame, FrameScalars,
                                              const uint32_t*, const int*);
 template __global__ void k_square_ar_rows<16>(Geo, DevFrame, FrameScalars,

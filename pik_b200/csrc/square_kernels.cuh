@@ -168,15 +168,30 @@ __global__ void k_active_blocks(Geo g, const int32_t* sigma,
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int k = 0;
   while (k < kMaxClasses && i >= cl.n[k]) i -= cl.n[k++];
-  if (k == kMaxClasses) return;
-  const uint32_t pk = cl.list[k][i];
-  const int bx = pk & 0xFFFF, by = pk >> 16;
-  const int cov = Covered(acs[by * g.Bx + bx] >> 4);
   bool any = false;
-  for (int y = 0; y < cov; ++y)
-    for (int x = 0; x < cov; ++x)
-      any |= sigma[(by + y) * g.Bx + bx + x] >= kMinSigma;
-  if (any) cl.active[k][atomicAdd(&counters[k], 1)] = pk;
+  uint32_t pk = 0;
+  if (k < kMaxClasses) {
+    pk = cl.list[k][i];
+    const int bx = pk & 0xFFFF, by = pk >> 16;
+    const int cov = Covered(acs[by * g.Bx + bx] >> 4);
+    for (int y = 0; y < cov; ++y)
+      for (int x = 0; x < cov; ++x)
+        any |= sigma[(by + y) * g.Bx + bx + x] >= kMinSigma;
+  }
+  // One atomic per warp and class: the lanes of a class take consecutive
+  // slots after the first of them reserves them all.
+  const int lane = threadIdx.x & 31;
+  for (int kk = 0; kk < kMaxClasses; ++kk) {
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, any && k == kk);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&counters[kk], __popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (any && k == kk) {
+      cl.active[kk][base + __popc(m & ((1u << lane) - 1))] = pk;
+    }
+  }
 }
 
 // AdaptiveReconstruction clamp for square DCT blocks, one unit per block

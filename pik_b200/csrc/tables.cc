@@ -128,6 +128,18 @@ void BuildTables(DevTables* t) {
         }
         t->hf_corner16[k][m] = float(acc);
       }
+    const float* b32 = t->dct + MatOffset(32);
+    for (int k = 0; k < 8; ++k)
+      for (int m = 0; m < 10; ++m) {
+        double acc = 0.0;
+        for (int x = 0; x < 32; ++x) {
+          const int i = m - x / 4;
+          if (i >= 0 && i <= 2) {
+            acc += double(b32[k * 32 + x]) * double(t->ub4[i][x % 4]);
+          }
+        }
+        t->hf_corner32[k][m] = float(acc);
+      }
   }
   t->lf_blur[0] = 0.41459272584128337f;
   t->lf_blur[1] = 0.25489157325704559f;

@@ -47,6 +47,8 @@ struct DevTables {
   // of the 2-D DCT of the upsampled prediction is C * Pred * C^T with Pred
   // the block's 6x6 window of 2x2-cell values.
   float hf_corner16[4][6];
+  // The same for a 32x32 block: its 8x8 corner from the 10x10 window.
+  float hf_corner32[8][10];
   // LFPredictionBlur (pik/ac_predictions.cc:120-133) w0, w1, w2.
   float lf_blur[3];
   // Gaborish weights per strength 1..4 (pik/gaborish.cc:16-88): w0, w1, w2.

@@ -31,7 +31,6 @@ namespace pikgpu {
 namespace tc {
 
 constexpr int kThreads = 128;            // one row of D per thread
-constexpr int kTmemCols = 128;           // 3 channels x 2 accumulators
 constexpr uint32_t kMaxPolls = 1u << 22;  // bounded mbarrier wait
 
 __device__ __forceinline__ uint32_t SmemU32(const void* p) {
@@ -256,17 +255,38 @@ __device__ __forceinline__ void PutMatrix(uint8_t* base, const float* m) {
 // channels of a block are independent in the IDCT), so a thread holds a
 // third of the registers of the three-channel kernels and more CTAs share
 // an SM, each with its own MMA round trips.
+// Side of a block's window of 2x2-cell prediction values: the block's 2 cov
+// cells and one on each side (the upsampling's 3 taps).
+template <int N>
+__host__ __device__ constexpr int HfWin() {
+  return N / 4 + 2;
+}
 template <int N, int S>
 struct Smem1 {
   static constexpr int kOpBytes = 128 * N * 2;
   static constexpr int kMatBytes = N * N * 2;
   alignas(128) uint8_t a[S * kOpBytes];
   alignas(128) uint8_t idct[S * kMatBytes];
-  float win[128 / N][36];  // HF prediction: each block's 6x6 cell window
+  // HF prediction: each block's window of cell values.
+  float win[128 / N][HfWin<N>() * HfWin<N>()];
   alignas(8) uint64_t mbar;
   uint32_t tmem;
 };
-constexpr int kTmemCols1 = 32;  // 2 accumulators x N = 16
+// Tensor-memory columns: the one-channel kernel's 2 accumulators of N
+// columns, the three-channel kernel's 6 (rounded up to a power of two).
+template <int N>
+__host__ __device__ constexpr int TmemCols1() {
+  return 2 * N;
+}
+template <int N>
+__host__ __device__ constexpr int TmemCols3() {
+  return N == 16 ? 128 : 256;
+}
+// The HF corner table of an N x N block: 2 cov rows of HfWin<N>() taps.
+template <int N>
+__device__ __forceinline__ const float* HfCorner() {
+  return N == 16 ? &c_t.hf_corner16[0][0] : &c_t.hf_corner32[0][0];
+}
 
 // This thread's row of D (N FP32 columns from dcol).
 template <int N, int S>
@@ -323,21 +343,31 @@ __device__ __forceinline__ bool Pass1(Smem1<N, S>& s, int j, bool a_mn,
 // the clamp ratio of each coefficient (minimum over X, Y, B) in registers,
 // then the IDCT of the scaled correction added to the original. `count` is
 // read from device memory (the compacted list of k_active_blocks).
+// Dynamic shared memory of k_square_ar_tc: its Smem and room to align it
+// to 128 bytes.
 template <int N, int S>
-__global__ void __launch_bounds__(tc::kThreads, 4)
+constexpr size_t ArTcSmemBytes() {
+  return sizeof(tc::Smem<N, S>) + 128;
+}
+
+template <int N, int S>
+__global__ void __launch_bounds__(tc::kThreads, N == 16 ? 4 : 2)
     k_square_ar_tc(Geo g, DevFrame f, FrameScalars sc, const uint32_t* list,
                    const int* count_ptr, int* work, int* err) {
   using namespace tc;
   constexpr int BPB = 128 / N;
   constexpr int cov = N / 8;
-  __shared__ Smem<N, S> s;
+  constexpr int kCols = TmemCols3<N>();
+  extern __shared__ uint8_t ar_tc_smem[];
+  Smem<N, S>& s = *reinterpret_cast<Smem<N, S>*>(
+      (reinterpret_cast<uintptr_t>(ar_tc_smem) + 127) & ~uintptr_t(127));
   __shared__ int s_next[2];
   const int t = threadIdx.x, bl = t / N, r = t % N;
   if (t < 32) {
     asm volatile(
         "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
             "r"(SmemU32(&s.tmem)),
-        "r"(kTmemCols));
+        "r"(kCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (t == 0) {
@@ -372,9 +402,9 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
     const size_t row0 = size_t(by * 8 + r) * g.PW + bx * 8;
     // The block's clamp intervals (a chain of dependent table loads) are
     // looked up first, so that the loads resolve during the DCT passes. The
-    // class holds only DCT16X16 blocks.
-    static_assert(N == 16, "the class of this kernel is DCT16X16");
-    constexpr int type = kDCT16X16;
+    // class holds only blocks of one type.
+    static_assert(N == 16 || N == 32, "DCT16X16 or DCT32X32");
+    constexpr int type = N == 16 ? kDCT16X16 : kDCT32X32;
     const int qac = f.qf[by * g.Bx + bx];
     const float inv_quant_ac =
         ClampInvQuantAc(g, f, sc.inv_global_scale, bx, by, qac);
@@ -496,26 +526,29 @@ __global__ void __launch_bounds__(tc::kThreads, 4)
   if (t < 32) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
                      s.tmem),
-                 "r"(kTmemCols));
+                 "r"(kCols));
   }
 }
 
-// HF prediction + AddBlockExceptLFAndLLFTo + IDCT for 16x16 DCT blocks on
-// the tensor cores (split-BF16 form of k_square_idct_rows). Persistent CTAs
-// of 128 threads; an item is one channel of a batch of 128 / N blocks
-// ((batch, channel) pairs, batch-major; the channels of a block are
-// independent here). A thread holds one row of one channel, so eight CTAs
-// share an SM, each with its own MMA round trips; the next item's
-// coefficient row is loaded while this item's passes run.
+// HF prediction + AddBlockExceptLFAndLLFTo + IDCT for 16x16 and 32x32 DCT
+// blocks on the tensor cores (split-BF16 form of k_square_idct_rows and
+// k_square_idct). Persistent CTAs of 128 threads; an item is one channel
+// of a batch of 128 / N blocks ((batch, channel) pairs, batch-major; the
+// channels of a block are independent here). A thread holds one row of one
+// channel, so several CTAs share an SM (eight for N = 16, four for
+// N = 32), each with its own MMA round trips; the next item's coefficient
+// row is loaded while this item's passes run.
 template <int N, int S>
-__global__ void __launch_bounds__(tc::kThreads, 8)
+__global__ void __launch_bounds__(tc::kThreads, N == 16 ? 8 : 4)
     k_square_idct_tc1(Geo g, DevFrame f, const uint32_t* list, int count,
                       int predict_hf, int* work, int* err) {
   using namespace tc;
   using square::CoefRowOffset;
-  static_assert(N == 16, "the HF corner table is for 16x16 blocks");
+  static_assert(N == 16 || N == 32, "DCT16X16 or DCT32X32");
   constexpr int BPB = 128 / N;  // blocks per batch
   constexpr int cov = N / 8;
+  constexpr int W = HfWin<N>();  // prediction window side (cells)
+  constexpr int kCols = TmemCols1<N>();
   __shared__ Smem1<N, S> s;
   __shared__ int s_first[2], s_next[2];
   const int t = threadIdx.x, bl = t / N, r = t % N;
@@ -523,7 +556,7 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
     asm volatile(
         "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
             "r"(SmemU32(&s.tmem)),
-        "r"(kTmemCols1));
+        "r"(kCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (t == 0) {
@@ -541,9 +574,11 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
   const size_t plane_ac = size_t(g.ac_stride) * g.By;
   const size_t plane_px = size_t(g.PW) * g.PH;
   const float inv_nn = 1.0f / float(N * N);
-  float cr[6];  // this lane's row of the HF corner table (rows r < 4)
+  // This lane's row of the HF corner table (rows r < 2 cov).
+  const float* ctab = HfCorner<N>();
+  float cr[W];
 #pragma unroll
-  for (int m = 0; m < 6; ++m) cr[m] = c_t.hf_corner16[r & 3][m];
+  for (int m = 0; m < W; ++m) cr[m] = ctab[(r & (2 * cov - 1)) * W + m];
   bool ok = true;
   // The next item's coefficient row is loaded while this item's passes
   // run (the CTAs of an SM otherwise wait for their loads in step).
@@ -584,13 +619,13 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
     // 2cov x 2cov corner and transforming back equals transforming the
     // coefficients minus that corner of DCT(P) and adding P (IDCT(DCT(P))
     // = P). The upsampled prediction P of this pixel row is the 3-tap
-    // vertical blend of three rows of the 2x2-cell grid (6 columns), then
+    // vertical blend of three rows of the 2x2-cell grid (W columns), then
     // the 3-tap horizontal blend; its DCT corner is C Pred C^T over the
-    // block's 6x6 cell window (C = hf_corner16), of which lanes r < 4
-    // subtract row r. The class holds only DCT16X16 blocks, which predict
-    // HF. The block's 16 lanes first stage its 6x6 cell window in shared
-    // memory (up to three loads per lane instead of 18 to 54 scalar loads
-    // of cells that the lanes share).
+    // block's W x W cell window (C = HfCorner<N>), of which lanes
+    // r < 2 cov subtract row r. The class holds only DCT16X16 (DCT32X32)
+    // blocks, which predict HF. The block's N lanes first stage its cell
+    // window in shared memory (a few loads per lane instead of tens of
+    // scalar loads of cells that the lanes share).
     float P[N];
     const bool hf = active && predict_hf;
     if (predict_hf) {
@@ -598,19 +633,21 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
       const int rb = (by & 63) * 2, q0 = (bx & 63) * 2;
       const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2 +
                           (rb + 1) * kG2 + q0 + 1;
-      for (int e = r; e < 36; e += N) s.win[bl][e] = pred[(e / 6) * kG2 + e % 6];
+      for (int e = r; e < W * W; e += N) {
+        s.win[bl][e] = pred[(e / W) * kG2 + e % W];
+      }
       __syncwarp();
     }
     if (hf) {
       const float* w = s.win[bl];
       const int iy = r & 3;
-      const float* w0 = w + (r >> 2) * 6;
+      const float* w0 = w + (r >> 2) * W;
       const float v0 = c_t.ub4[0][iy], v1 = c_t.ub4[1][iy],
                   v2 = c_t.ub4[2][iy];
-      float col[6];
+      float col[W];
 #pragma unroll
-      for (int m = 0; m < 6; ++m) {
-        col[m] = fmaf(w0[12 + m], v2, fmaf(w0[6 + m], v1, w0[m] * v0));
+      for (int m = 0; m < W; ++m) {
+        col[m] = fmaf(w0[2 * W + m], v2, fmaf(w0[W + m], v1, w0[m] * v0));
       }
 #pragma unroll
       for (int x = 0; x < N; ++x) {
@@ -619,20 +656,20 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
                     fmaf(col[q + 1], c_t.ub4[1][ix], col[q] * c_t.ub4[0][ix]));
       }
       if (r < 2 * cov) {
-        float u[6];
+        float u[W];
 #pragma unroll
-        for (int rho = 0; rho < 6; ++rho) {
+        for (int rho = 0; rho < W; ++rho) {
           float a = 0.f;
 #pragma unroll
-          for (int m = 0; m < 6; ++m) a = fmaf(w[rho * 6 + m], cr[m], a);
+          for (int m = 0; m < W; ++m) a = fmaf(w[rho * W + m], cr[m], a);
           u[rho] = a;
         }
 #pragma unroll
         for (int l = 0; l < 2 * cov; ++l) {
           float v = 0.f;
 #pragma unroll
-          for (int rho = 0; rho < 6; ++rho) {
-            v = fmaf(c_t.hf_corner16[l][rho], u[rho], v);
+          for (int rho = 0; rho < W; ++rho) {
+            v = fmaf(ctab[l * W + rho], u[rho], v);
           }
           X[l] -= v * inv_nn;
         }
@@ -670,7 +707,7 @@ __global__ void __launch_bounds__(tc::kThreads, 8)
   if (t < 32) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
                      s.tmem),
-                 "r"(kTmemCols1));
+                 "r"(kCols));
   }
 }
 

@@ -23,6 +23,7 @@ from oracle import decisions, refpy
 from pik_b200 import synthetic
 from tests import golden_cases
 from tests.test_gpu_parity import assert_bitexact_vs_oracle, run_gpu
+from tests.test_split_bf16 import check_against_fp64
 
 pytestmark = [
     pytest.mark.gpu,
@@ -60,6 +61,10 @@ def test_dct32_heavy_reference_frame(w, h, distance, seed):
     lsb = np.abs(gpu2["srgb8"].transpose(2, 0, 1).astype(np.int32) -
                  golden_cases.srgb8_exact(ref["linear"]))
     assert lsb.max() <= 1
+    # The tensor-core forms, whose DCT32X32 transforms and clamp run on
+    # tcgen05, against FP64 on the FP32 form's decisions.
+    for form in ("split_bf16", "split_bf16x3"):
+        check_against_fp64(frame, form)
 
 
 def test_fixed_sigma_reference_frame():

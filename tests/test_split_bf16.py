@@ -132,6 +132,24 @@ def test_dct16_synthetic(form):
 
 
 @pytest.mark.parametrize("form", FORMS)
+def test_dct32_synthetic(form):
+    frame = synthetic.make_frame(1030, 530, seed=23,
+                                 shares={"DCT32X32": 0.9, "DCT": 0.1},
+                                 qf_median=8.0)
+    check_against_fp64(frame, form)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("predict_hf", [0, 1])
+def test_dct32_header_variants(form, predict_hf):
+    frame = synthetic.make_frame(264, 136, seed=6,
+                                 shares={"DCT32X32": 0.7, "DCT16X16": 0.2,
+                                         "DCT": 0.1})
+    frame.predict_hf = predict_hf
+    check_against_fp64(frame, form)
+
+
+@pytest.mark.parametrize("form", FORMS)
 def test_mixed_synthetic(form):
     frame = synthetic.make_frame(1030, 530, seed=22)
     check_against_fp64(frame, form)

@@ -18,7 +18,8 @@ pytestmark = pytest.mark.gpu
 
 def _frame():
     return synthetic.make_frame(520, 264, seed=11,
-                                shares={"DCT16X16": 0.8, "DCT": 0.2})
+                                shares={"DCT32X32": 0.4, "DCT16X16": 0.4,
+                                        "DCT": 0.2})
 
 
 def _reconstruct(ctx, frame):
