@@ -179,6 +179,25 @@ int pikgpu_reconstruct_async(pikgpu_ctx* ctx, float* const out_linear[3],
  * there is none) and returns its status. */
 int pikgpu_wait(pikgpu_ctx* ctx);
 
+/* Output-format step of dpik's writer (WriteOutput, pik/dpik.cc:196-223;
+ * EncodeImagePNM and EncodeHeader, pik/codec_pnm.cc:179-196,260-294;
+ * ExternalImage's casts, pik/external_image.cc), run on the device for the
+ * frame of the last pikgpu_reconstruct that wrote linear planes: the image
+ * of a PPM file ("P6", 8 or 16 bits per sample, big-endian samples) or a
+ * PFM file ("PF", 32-bit little-endian floats, scale -1: sample values
+ * x 255), header included, rows top to bottom, RGB interleaved.
+ *  transfer: PIKGPU_TF_SRGB encodes with TF_SRGB (what dpik writes for an
+ *            sRGB original), PIKGPU_TF_LINEAR keeps linear light;
+ *  8 / 16 bits clamp to [0, 1] and round like ExternalImage::CopyTo.
+ * `out`: `capacity` bytes of host memory (device memory if out_on_device).
+ * The file's size is written to *size; with out NULL only the size is
+ * computed. Blocks until the bytes are written. */
+#define PIKGPU_TF_LINEAR 0
+#define PIKGPU_TF_SRGB 1
+int pikgpu_encode_pnm(pikgpu_ctx* ctx, int bits_per_sample, int transfer,
+                      uint8_t* out, size_t capacity, size_t* size,
+                      int out_on_device);
+
 /* Intermediate planes for stage-by-stage parity checks, valid after
  * pikgpu_reconstruct. Each is 3 planes in host memory. */
 #define PIKGPU_STAGE_DC 0          /* Bx x By: DC after AdaptiveDCRecon. */

@@ -35,6 +35,7 @@
 #include "pik/ans_decode.h"
 #include "pik/block_dictionary.h"
 #include "pik/codec.h"
+#include "pik/codec_pnm.h"
 #include "pik/color_correlation.h"
 #include "pik/common.h"
 #include "pik/compressed_dc.h"
@@ -530,6 +531,41 @@ void* pikref_frozen_from_bitstream(const uint8_t* data, size_t size,
 }
 
 void pikref_frozen_free(void* h) { delete static_cast<Frozen*>(h); }
+
+// The reference's PNM writer (EncodeImagePNM, pik/codec_pnm.cc:260-294) on
+// linear planes (0..255 scale, as PikToPixels leaves io.color()), written
+// in sRGB (to_srgb) or linear light with bits_per_sample 8, 16 or 32. The
+// sRGB transfer runs through oracle/ref_shim.cc's colour management (the
+// reference's skip-lcms route); the container, casts and rounding are the
+// reference's own. Returns 0 and the file's size in *size.
+int pikref_encode_pnm(const float* planes, int xsize, int ysize, int bits,
+                      int to_srgb, uint8_t* out, size_t capacity,
+                      size_t* size) {
+  CodecContext context;
+  CodecInOut io(&context);
+  Image3F img(xsize, ysize);
+  for (int c = 0; c < 3; ++c) {
+    for (int y = 0; y < ysize; ++y) {
+      memcpy(img.PlaneRow(c, y), planes + (size_t(c) * ysize + y) * xsize,
+             xsize * sizeof(float));
+    }
+  }
+  io.SetFromImage(std::move(img), context.c_linear_srgb[0]);
+  PaddedBytes bytes;
+  const ColorEncoding& c_out =
+      to_srgb ? context.c_srgb[0] : context.c_linear_srgb[0];
+  if (!EncodeImagePNM(&io, c_out, bits, nullptr, &bytes)) {
+    g_error = "EncodeImagePNM failed";
+    return -1;
+  }
+  *size = bytes.size();
+  if (bytes.size() > capacity) {
+    g_error = "output too small";
+    return -1;
+  }
+  memcpy(out, bytes.data(), bytes.size());
+  return 0;
+}
 
 // The decoder's fixed-sigma override (DecompressParams::epf_sigma > 0,
 // OverridePassFlags, pik/pik_frame.cc:112-115): the EPF runs with one sigma

@@ -57,6 +57,10 @@ def lib(flavour: str = "scalar") -> ctypes.CDLL:
                                     ctypes.POINTER(ctypes.c_double)]
     L.pikref_frozen_set_ac.argtypes = [P, P, ctypes.c_size_t]
     L.pikref_frozen_set_fixed_sigma.argtypes = [P, ctypes.c_int]
+    L.pikref_encode_pnm.argtypes = [P, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, P,
+                                    ctypes.c_size_t,
+                                    ctypes.POINTER(ctypes.c_size_t)]
     L.pikref_decode_epf_sigma.argtypes = [P, ctypes.c_size_t, ctypes.c_int,
                                           ctypes.c_int, P, ctypes.c_size_t]
     L.pikref_frozen_encode_dct8.restype = P
@@ -111,6 +115,23 @@ def decode(bitstream: bytes, xsize: int, ysize: int, *, threads: int = 0,
     if rc != 0:
         raise RuntimeError(L.pikref_last_error().decode())
     return out
+
+
+def encode_pnm(linear: np.ndarray, bits: int, srgb: bool = True,
+               flavour: str = "scalar") -> bytes:
+    """The reference's PNM writer (EncodeImagePNM) on (3, H, W) linear
+    planes (0..255): PPM for 8/16 bits, PFM for 32."""
+    L = lib(flavour)
+    img = np.ascontiguousarray(linear, dtype=np.float32)
+    _, h, w = img.shape
+    cap = 64 + 3 * w * h * max(1, bits // 8)
+    out = np.zeros(cap, np.uint8)
+    n = ctypes.c_size_t()
+    rc = L.pikref_encode_pnm(_ptr(img), w, h, bits, int(srgb), _ptr(out),
+                             cap, ctypes.byref(n))
+    if rc != 0:
+        raise RuntimeError(L.pikref_last_error().decode())
+    return out[:n.value].tobytes()
 
 
 def encode_dct8(linear: np.ndarray, quant: float, *, gaborish: int = 2,

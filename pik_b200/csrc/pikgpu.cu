@@ -96,7 +96,11 @@ struct pikgpu_ctx {
   DevBuf acs, qf, lut, dq_cf, dq_map, ytox, ytob, table, offsets;
   DevBuf qdc, qac, dc, dcpad, ac, pred2x2_g;
   DevBuf idct, smoothed, filt, mm, sigma, dc_sigma, list[kNumClasses];
-  DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr;
+  DevBuf out_lin, out_rgb8, dbg_dequant, dbg_epf, dbg_pre, guide_ovr, pnm;
+  // Linear planes of the last reconstruction (device; NULL if it wrote
+  // none), for pikgpu_encode_pnm.
+  const float* last_lin = nullptr;
+  size_t last_lin_stride = 0;
   DevBuf sigma_ovr, counters, active[kNumClasses], tc_err;
   bool use_guide_ovr = false, use_sigma_ovr = false;
   // Dequantised AC supplied by the caller instead of Dequant::DoAC, and the
@@ -973,7 +977,7 @@ int pikgpu_ctx_destroy(pikgpu_ctx* ctx) {
                     &ctx->adj_c,   &ctx->adj_coef,  &ctx->adj_pred,
                     &ctx->adj_qf,  &ctx->adj_guide, &ctx->adj_partial,
                     &ctx->adj_jac, &ctx->adj_target, &ctx->adj_tape,
-                    &ctx->tape_in};
+                    &ctx->tape_in, &ctx->pnm};
   for (DevBuf* b : bufs) FreeBuf(b);
   for (auto& b : ctx->list) FreeBuf(&b);
   for (auto& b : ctx->active) FreeBuf(&b);
@@ -1327,6 +1331,8 @@ int EnqueueReconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
   }
   rc = RunFrame(ctx, lin, lin_stride, rgb8, rgb8_stride);
   if (rc != PIKGPU_OK) return rc;
+  ctx->last_lin = lin;
+  ctx->last_lin_stride = lin_stride;
   if (!outputs_on_device) {
     if (out_linear) {
       for (int c = 0; c < 3; ++c) {
@@ -1541,6 +1547,67 @@ int pikgpu_last_kernel_times(pikgpu_ctx* ctx, float* ms, int n) {
   if (!ctx->profile) return Fail(ctx, PIKGPU_ERR_STATE, "profiling is off");
   for (int i = 0; i < n && i < kNumTimed; ++i) ms[i] = ctx->times[i];
   return kNumTimed;
+}
+
+int pikgpu_encode_pnm(pikgpu_ctx* ctx, int bits_per_sample, int transfer,
+                      uint8_t* out, size_t capacity, size_t* size,
+                      int out_on_device) {
+  if (!ctx) return PIKGPU_ERR_INVALID_ARG;
+  PIKGPU_NOT_PENDING(ctx);
+  if (!ctx->have_result || !ctx->last_lin) {
+    return Fail(ctx, PIKGPU_ERR_STATE,
+                "no reconstruction with linear planes to encode");
+  }
+  if (bits_per_sample != 8 && bits_per_sample != 16 &&
+      bits_per_sample != 32) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "bits per sample %d",
+                bits_per_sample);
+  }
+  if (transfer != PIKGPU_TF_LINEAR && transfer != PIKGPU_TF_SRGB) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "transfer %d", transfer);
+  }
+  if (!size) return Fail(ctx, PIKGPU_ERR_INVALID_ARG, "size is NULL");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const Geo& g = ctx->g;
+  // EncodeHeader (pik/codec_pnm.cc:179-196): PFM with the scale's sign
+  // giving the byte order (little-endian: -1), PPM with the maximum value.
+  char hdr[96];
+  int hlen;
+  if (bits_per_sample == 32) {
+    hlen = snprintf(hdr, sizeof(hdr), "PF %zu %zu\n%f\n", size_t(g.W),
+                    size_t(g.H), -1.0);
+  } else {
+    hlen = snprintf(hdr, sizeof(hdr), "P6\n%zu %zu\n%u\n", size_t(g.W),
+                    size_t(g.H), (1u << bits_per_sample) - 1);
+  }
+  const size_t body = size_t(g.W) * g.H * 3 * (bits_per_sample / 8);
+  *size = size_t(hlen) + body;
+  if (!out) return PIKGPU_OK;
+  if (capacity < *size) {
+    return Fail(ctx, PIKGPU_ERR_INVALID_ARG,
+                "output of %zu bytes is smaller than the file (%zu)",
+                capacity, *size);
+  }
+  uint8_t* dst = out + hlen;
+  if (!out_on_device) {
+    int rc = Ensure(ctx, &ctx->pnm, body);
+    if (rc != PIKGPU_OK) return rc;
+    dst = P<uint8_t>(ctx->pnm);
+  }
+  k_encode_pnm<<<dim3(Blocks(g.W, 128), g.H), 128, 0, ctx->stream>>>(
+      ctx->last_lin, ctx->last_lin_stride, g.W, g.H, bits_per_sample,
+      transfer == PIKGPU_TF_SRGB, dst);
+  CUDA_TRY(ctx, cudaGetLastError());
+  if (out_on_device) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(out, hdr, hlen, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+  } else {
+    memcpy(out, hdr, hlen);
+    CUDA_TRY(ctx, cudaMemcpyAsync(out + hlen, dst, body,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return PIKGPU_OK;
 }
 
 int pikgpu_last_launch_count(const pikgpu_ctx* ctx) {

@@ -438,6 +438,26 @@ __global__ void k_export_guide(const float* src, int w, int h,
 // polynomial (pik/color_management.cc:323-345) and the rounding of
 // ExternalImage::CopyTo (pik/external_image.cc:1205). The gaborish / opsin
 // stencil kernels are in stencil_kernels.cuh.
+// TF_SRGB::EncodedFromDisplay of a linear value on the 0..255 scale after
+// Image3ToTemp01's x (1 / 255) (pik/external_image.cc:79-90).
+__device__ __forceinline__ float SrgbEncoded(float lin255) {
+  const float x = lin255 * (1.0f / 255);
+  const float a = fabsf(x);
+  float mag;
+  if (a > 0.0031308f) {
+    const float s = sqrtf(a);
+    float yp = c_t.srgb_p[4], yq = c_t.srgb_q[4];
+    for (int i = 3; i >= 0; --i) {
+      yp = yp * s + c_t.srgb_p[i];
+      yq = yq * s + c_t.srgb_q[i];
+    }
+    mag = yp / yq;
+  } else {
+    mag = a * 12.92f;
+  }
+  return copysignf(mag, x);
+}
+
 __device__ __forceinline__ uint8_t Srgb8(float lin255) {
   const float x = lin255 * (1.0f / 255);
   const float a = fabsf(x);
@@ -457,6 +477,48 @@ __device__ __forceinline__ uint8_t Srgb8(float lin255) {
   const float cl = fminf(fmaxf(0.0f, e), 1.0f);
   const float sample = cl * 255.0f + 0.0f;
   return uint8_t(int(sample + 0.5f));
+}
+
+// ---------------------------------------------------------------------------
+// The output-format step of dpik's writer (EncodeImagePNM,
+// pik/codec_pnm.cc:260-294, through ExternalImage, pik/external_image.cc):
+// the body of a PPM (8 or 16 bits per sample, big-endian) or PFM (32-bit
+// little-endian floats) file, rows top to bottom, RGB interleaved, from the
+// linear planes (0..255 scale, row stride `stride` floats). Each sample is
+// Image3ToTemp01's value (x (1 / 255)), transfer-encoded to sRGB if
+// `srgb` (else kept linear), then:
+//  8 / 16 bits: CastClip01 (clamp to [0, 1], x (2^bits - 1) + 0) and
+//               ToExternal's int(sample + 0.5f) (pik/external_image.cc:
+//               192-205, 666-696);
+//  32 bits:     CastFloat01's x 255 (pik/external_image.cc:754-773).
+// One thread per pixel.
+__global__ void k_encode_pnm(const float* lin, size_t stride, int w, int h,
+                             int bits, int srgb, uint8_t* out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= w) return;
+  const size_t plane = stride * h;
+  const size_t p = size_t(y) * w + x;
+  for (int c = 0; c < 3; ++c) {
+    const float v = lin[c * plane + size_t(y) * stride + x];
+    const float e = srgb ? SrgbEncoded(v) : v * (1.0f / 255);
+    if (bits == 32) {
+      const uint32_t u = __float_as_uint(e * 255.0f);
+      uint8_t* o = out + 4 * (3 * p + c);
+      o[0] = uint8_t(u), o[1] = uint8_t(u >> 8);
+      o[2] = uint8_t(u >> 16), o[3] = uint8_t(u >> 24);
+    } else {
+      const float width = bits == 8 ? 255.0f : 65535.0f;
+      const float cl = fminf(fmaxf(0.0f, e), 1.0f);
+      const int q = int(cl * width + 0.0f + 0.5f);
+      if (bits == 8) {
+        out[3 * p + c] = uint8_t(q);
+      } else {
+        out[2 * (3 * p + c)] = uint8_t(q >> 8);
+        out[2 * (3 * p + c) + 1] = uint8_t(q);
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -73,6 +73,8 @@ def lib() -> ctypes.CDLL:
         P, ctypes.c_int32, ctypes.c_int32, P, P, ctypes.c_char_p, S]
     L.pikgpu_adjoint.argtypes = [P, P, P, P, P, ctypes.c_int]
     L.pikgpu_graph_stats.argtypes = [P, P, P]
+    L.pikgpu_encode_pnm.argtypes = [P, ctypes.c_int, ctypes.c_int, P, S,
+                                    ctypes.POINTER(S), ctypes.c_int]
     L.pikgpu_reconstruct_async.argtypes = [P, ctypes.POINTER(P), S, P, S,
                                            ctypes.c_int]
     L.pikgpu_wait.argtypes = [P]
@@ -280,6 +282,18 @@ class Context:
             g_ac.ctypes.data if grads else None,
             g_qf.ctypes.data if grads else None, 0))
         return float(loss[0]), g_ac, g_qf
+
+    def encode_pnm(self, bits: int = 8, srgb: bool = True) -> bytes:
+        """pikgpu_encode_pnm of the last reconstruction: the bytes of a PPM
+        (8 or 16 bits) or PFM (32) file."""
+        n = ctypes.c_size_t()
+        self._check(self.L.pikgpu_encode_pnm(self.h, bits, int(srgb), None,
+                                             0, ctypes.byref(n), 0))
+        buf = np.zeros(n.value, np.uint8)
+        self._check(self.L.pikgpu_encode_pnm(self.h, bits, int(srgb),
+                                             buf.ctypes.data, n.value,
+                                             ctypes.byref(n), 0))
+        return buf.tobytes()
 
     def clamp_decisions(self) -> np.ndarray:
         """The clamp tape of the last recording forward pass, (By, Bx*64)
