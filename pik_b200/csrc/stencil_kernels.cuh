@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kTileThreads)
 // and each output follows Sym3's operation order, so the min/max equal
 // those of k_gaborish_tile. Grid: (warps of a plane / 8, 3).
 constexpr int kGmmRows = 8;
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     k_gaborish_minmax(const float* in, int w, int h, int strength,
                       uint32_t* mm) {
   constexpr int R = kGmmRows;
