@@ -49,11 +49,12 @@ METRIC = ("decoded MP/s at 4K, split-BF16 vs FP32 form @<=2e-5 err; "
 # side info (0.094), CfL maps (~0.002), FP32 linear RGB out (12).
 PATH_BYTES_PER_PX = 18.28
 # Measured with ncu on one reconstruction of the 4K frame in the split-BF16
-# form (profiles/): warp instructions of the frame EPF launch
-# (smsp__inst_executed.sum, profiles/k_epf_box_c2_4k.md) and the DRAM bytes
-# (dram__bytes_read.sum + dram__bytes_write.sum) of all the frame's
-# launches (profiles/launches_c2_4k.md); None where not captured.
-EPF_WARP_INSTR_4K = 193.6e6
+# form: warp instructions of the frame EPF launch (smsp__inst_executed.sum,
+# profiles/k_epf_box_c2_4k.md) and the DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum) of all the frame's 17 launches, run one after
+# another with the caches kept between them (profiles/traffic_c2_4k.md).
+EPF_WARP_INSTR_4K = 199.0e6
+PATH_TRAFFIC_4K = 828.3e6
 # Algorithmic bytes per pixel of each kernel group (PIKGPU_OPT_PROFILE
 # groups), with 4-byte floats.
 GROUP_BYTES = {
@@ -72,7 +73,6 @@ GROUP_BYTES = {
     "lf_prediction_update": 12 / 64 + 3 * 4 * (4 + 4 + 4) / 64,
     "dc_dequant_epf": 0.2,
 }
-PATH_TRAFFIC_4K = None
 # Arithmetic forms of the reconstruction (PIKGPU_OPT_FORM). The headline is
 # the split-BF16 form; every form is timed on the same frame. Their errors
 # against the FP64 oracle are checked by tests/test_split_bf16.py.
@@ -936,7 +936,7 @@ def main():
     # DRAM bytes per launch of the 4K workload measured with ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum, one cold launch each).
     ncu_traffic_4k = {
-        "epf": 100.09e6 + 65.80e6,
+        "epf": 100.51e6 + 63.73e6,
         "gaborish1_minmax": 99.54e6 + 64.64e6,
         "gaborish2_opsin_srgb": 99.55e6 + 63.85e6,
     }

@@ -630,13 +630,14 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     // before the persistent tensor-core kernel fills the SMs (which takes
     // its work from a counter and leaves those SMs' share to the others).
     if (n[kCSmall]) {
-      k_small_idct<<<Blocks(3 * n[kCSmall], 64), 64, 0, cls(kCSmall)>>>(
+      k_small_idct<<<Blocks(3 * n[kCSmall], kSmallIdctThreads),
+                     kSmallIdctThreads, 0, cls(kCSmall)>>>(
           g, f, L[kCSmall], n[kCSmall]);
       ++ctx->launches;
     }
     if (n[kC4]) {
-      k_dct4_idct<<<Blocks(n[kC4], kDct4Blocks), 256, 0, cls(kC4)>>>(
-          g, f, L[kC4], n[kC4], s.predict_hf);
+      k_dct4_idct<<<Blocks(3 * n[kC4], kDct4Threads / 8), kDct4Threads, 0,
+                    cls(kC4)>>>(g, f, L[kC4], n[kC4], s.predict_hf);
       ++ctx->launches;
     }
     if (n[kC32] && ctx->form != PIKGPU_FORM_FP32) {
@@ -1141,6 +1142,15 @@ int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* p) {
       ctx->lists[ClassOf(a >> 4)].push_back(uint32_t(x) | (uint32_t(y) << 16));
     }
   }
+  // The small-transform class in type order: its inverse runs one thread
+  // per block, and warps of one type do not diverge.
+  std::stable_sort(ctx->lists[kCSmall].begin(), ctx->lists[kCSmall].end(),
+                   [&](uint32_t u, uint32_t v) {
+                     const auto type = [&](uint32_t q) {
+                       return p->ac_strategy[(q >> 16) * g.Bx + (q & 0xFFFF)];
+                     };
+                     return type(u) < type(v);
+                   });
   cudaStream_t st = ctx->stream;
   if ((rc = Ensure(ctx, &ctx->counters, sizeof(int) * kNumCounters))) {
     return rc;

@@ -626,9 +626,13 @@ constexpr int kLfWin2 = 2 * kLfWin;   // the 2x2 images' window, pixels
 constexpr int kLfThreads = 256;
 // Shared memory of k_lf_tile: the LLF image, the 2x2 image before and after
 // LFPredictionBlur, over the window, and the list of the window's first
-// cells.
+// cells (by block size: 8x8-class blocks, then 16x16, then 32x32).
+constexpr int kLfList1 = kLfWin * kLfWin;
+constexpr int kLfList2 = (kLfWin / 2 + 1) * (kLfWin / 2 + 1);
+constexpr int kLfList4 = (kLfWin / 4 + 1) * (kLfWin / 4 + 1);
 constexpr size_t kLfSmemBytes =
-    4 * (2 * size_t(kLfWin) * kLfWin + 2 * size_t(kLfWin2) * kLfWin2);
+    4 * (size_t(kLfWin) * kLfWin + 2 * size_t(kLfWin2) * kLfWin2 + kLfList1 +
+         kLfList2 + kLfList4);
 
 // The window of a tile: cell (X, Y) of the group is at (X - ex, Y - ey).
 struct LfWin {
@@ -766,7 +770,6 @@ __global__ void __launch_bounds__(kLfThreads, 2)
   const int Y0 = 1 + ty * kLfTile, Y1 = min(Y0 + kLfTile, q.gys + 1);
   const int lx = X0 == 1 ? 0 : X0, hx = X1 == q.gxs + 1 ? q.gxs + 2 : X1;
   const int ly = Y0 == 1 ? 0 : Y0, hy = Y1 == q.gys + 1 ? q.gys + 2 : Y1;
-  __shared__ int s_count;
   LfWin w;
   w.ex = lx - 4;
   w.ey = ly - 4;
@@ -777,9 +780,15 @@ __global__ void __launch_bounds__(kLfThreads, 2)
   // the group's ring), listed as X | Y << 10 | strategy byte << 20, so that
   // the per-block phases below give every lane a block (a cell-per-lane
   // loop leaves the lanes of the other cells of multi-block transforms
-  // idle).
-  int* first = reinterpret_cast<int*>(w.lf + kLfWin2 * kLfWin2);
-  if (threadIdx.x == 0) s_count = 0;
+  // idle). One list per block size, read as one after the other, so that a
+  // warp's lanes mostly take the same transform sizes (the 32x32 blocks'
+  // LF transforms are far longer than the others').
+  __shared__ int s_n[3];
+  int* lists[3];
+  lists[0] = reinterpret_cast<int*>(w.lf + kLfWin2 * kLfWin2);
+  lists[1] = lists[0] + kLfList1;
+  lists[2] = lists[1] + kLfList2;
+  if (threadIdx.x < 3) s_n[threadIdx.x] = 0;
   __syncthreads();
   const int sx = max(lx - 4, 0), sy = max(ly - 4, 0);
   const int nx = min(hx + 1, q.gxs + 2) - sx, ny = min(hy + 1, q.gys + 2) - sy;
@@ -787,12 +796,17 @@ __global__ void __launch_bounds__(kLfThreads, 2)
     const int X = sx + i % nx, Y = sy + i / nx;
     const int a = q.Acs(g, f, X, Y);
     if (a & 0xF) continue;
-    first[atomicAdd(&s_count, 1)] = X | (Y << 10) | (a << 20);
+    const int cov = Covered(a >> 4), k = cov == 1 ? 0 : cov == 2 ? 1 : 2;
+    lists[k][atomicAdd(&s_n[k], 1)] = X | (Y << 10) | (a << 20);
   }
   __syncthreads();
-  const int nfirst = s_count;
+  const int n0 = s_n[0], n01 = n0 + s_n[1], nfirst = n01 + s_n[2];
+  auto first_at = [&](int i) {
+    return i < n0 ? lists[0][i] : i < n01 ? lists[1][i - n0]
+                                          : lists[2][i - n01];
+  };
   for (int i = threadIdx.x; i < nfirst; i += kLfThreads) {
-    const int e = first[i];
+    const int e = first_at(i);
     const int X = e & 1023, Y = (e >> 10) & 1023, a = e >> 20;
     LlfCell(g, f, q, w, a, X, Y);
     if (predict_lf) {
@@ -811,7 +825,7 @@ __global__ void __launch_bounds__(kLfThreads, 2)
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nfirst; i += kLfThreads) {
-      const int e = first[i];
+      const int e = first_at(i);
       const int X = e & 1023, Y = (e >> 10) & 1023, a = e >> 20;
       if (X < lx || X >= hx || Y < ly || Y >= hy) continue;
       LowFreqFromDC2x2(a >> 4, w.Lf(2 * X, 2 * Y), kLfWin2);
@@ -839,7 +853,7 @@ __global__ void __launch_bounds__(kLfThreads, 2)
     }
   }
   for (int i = threadIdx.x; i < nfirst; i += kLfThreads) {
-    const int e = first[i];
+    const int e = first_at(i);
     const int X = e & 1023, Y = (e >> 10) & 1023, a = e >> 20;
     if (X < X0 || X >= X1 || Y < Y0 || Y >= Y1) continue;
     LfUpdateBlock(g, f, q, w, a >> 4, X, Y, predict_lf, predict_hf);
@@ -1054,88 +1068,120 @@ __global__ void __launch_bounds__(256)
 
 // DCT4X4 (and _NOHF): four 4x4 transforms with interleaved coefficients
 // (AcStrategy::TransformFromPixels/ToPixels, pik/ac_strategy.cc:604-629,
-// 762-790). kDct4Blocks blocks per CTA, one thread per coefficient: few
-// blocks per CTA spread the (few) DCT4X4 blocks of a frame over many SMs.
-__global__ void __launch_bounds__(256)
+// 762-790), with the HF prediction (UpSample4x4BlurDCT,
+// pik/ac_predictions.cc:263-374). A unit of 8 lanes takes one block and
+// channel; lane j = 4 sy + k holds row sy + 2 k of the block's 64
+// coefficients, which is row k of the coefficient matrices of sub-blocks
+// (sy, 0) and (sy, 1) (columns sx + 2 l), and in the pixel domain pixel
+// row 4 sy + k. The 4x4 transforms' second passes need the other rows of a
+// sub-block: they go through a small shared-memory transpose per unit.
+// Every sum has the operation order of TsIdct / TsDct (CoopTsIdct,
+// CoopTsDct), so the result is bit-identical to the CTA-wide form.
+constexpr int kDct4Threads = 128;
+__global__ void __launch_bounds__(kDct4Threads)
     k_dct4_idct(Geo g, DevFrame f, const uint32_t* list, int count,
                 int predict_hf) {
-  constexpr int NB = kDct4Blocks;
-  __shared__ float s_a[16], s_b[16];
-  __shared__ float s_c[NB * 64], s_p[NB * 64], s_t[NB * 64], s_q[NB * 64];
-  if (threadIdx.x < 16) {
-    s_a[threadIdx.x] = c_t.idct[MatOffset(4) + threadIdx.x];
-    s_b[threadIdx.x] = c_t.dct[MatOffset(4) + threadIdx.x];
+  constexpr int kUnits = kDct4Threads / 8;
+  __shared__ float s_t[kUnits][2][2][4][5];  // per unit: [sy][sx][row][col]
+  const int unit = threadIdx.x >> 3, j = threadIdx.x & 7;
+  const int sy = j >> 2, k = j & 3;
+  const int item = blockIdx.x * kUnits + unit;
+  const bool active = item < 3 * count;
+  const int b = active ? item / 3 : 0, c = active ? item % 3 : 0;
+  const uint32_t mask = 0xFFu << (threadIdx.x & 24);  // the unit's lanes
+  const uint32_t pk = list[b];
+  const int bx = pk & 0xFFFF, by = pk >> 16;
+  const float* A = IdctMat(4);
+  const float* B = DctMat(4);
+  float (*t)[4][5] = s_t[unit][sy];
+  // Coefficient row sy + 2 k: C_{sy,sx}[k][l] = cr[sx + 2 l].
+  const float* crow = f.ac + c * size_t(g.ac_stride) * g.By +
+                      size_t(by) * g.ac_stride + bx * 64 + (sy + 2 * k) * 8;
+  float cr[8];
+  {
+    const float4 v0 = *reinterpret_cast<const float4*>(crow);
+    const float4 v1 = *reinterpret_cast<const float4*>(crow + 4);
+    cr[0] = v0.x, cr[1] = v0.y, cr[2] = v0.z, cr[3] = v0.w;
+    cr[4] = v1.x, cr[5] = v1.y, cr[6] = v1.z, cr[7] = v1.w;
   }
-  const int first = blockIdx.x * NB;
-  const int nb = min(NB, count - first);
-  const size_t plane_ac = size_t(g.ac_stride) * g.By;
-  const size_t plane_px = size_t(g.PW) * g.PH;
-  __syncthreads();
-  for (int c = 0; c < 3; ++c) {
-    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
-      const int b = i / 64, e = i % 64;
-      const uint32_t pk = list[first + b];
-      const int bx = pk & 0xFFFF, by = pk >> 16;
-      s_c[i] = f.ac[c * plane_ac + size_t(by) * g.ac_stride + bx * 64 + e];
-      if (predict_hf && PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) {
-        // Sub-block-major pixel layout: sub-block (sy, sx), pixel (py, px).
-        const int sb = e / 16, py = (e % 16) / 4, px = e % 4;
-        const int sy = sb / 2, sx = sb % 2;
-        const int gi = (by >> 6) * g.Gx + (bx >> 6);
-        const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
-        s_p[i] = Upsample(pred, (bx & 63) * 8 + sx * 4 + px,
-                          (by & 63) * 8 + sy * 4 + py);
-      } else {
-        s_p[i] = 0.f;
+  if (predict_hf && PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) {
+    // Prediction pixel row y = k of sub-blocks (sy, 0..1).
+    const int gi = (by >> 6) * g.Gx + (bx >> 6);
+    const float* pred = f.pred2x2_g + gi * kG2GroupFloats + c * kG2 * kG2;
+    float P[8];
+    UpsampleRow<8>(pred, (bx & 63) * 8, (by & 63) * 8 + 4 * sy + k, P);
+    // TsDct pass 1: tmp[kk][y = k] = sum_x B[kk][x] P[y][x], to the tile.
+#pragma unroll
+    for (int sx = 0; sx < 2; ++sx) {
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        float sum = 0.f;
+#pragma unroll
+        for (int x = 0; x < 4; ++x) sum += B[kk * 4 + x] * P[4 * sx + x];
+        t[sx][kk][k] = sum;
       }
     }
-    __syncthreads();
-    if (predict_hf) {
-      CoopTsDct(4, nb * 4, s_b, s_p, s_t, s_q);
-      // Scatter to interleaved coefficient positions, skipping the LF
-      // corner (positions 0, 1, 8, 9 hold the sub-block DCs).
-      for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
-        const int b = i / 64, e = i % 64;
-        const int sb = e / 16, iy = (e % 16) / 4, ix = e % 4;
-        const int sy = sb / 2, sx = sb % 2;
-        const int pos = (sy + iy * 2) * 8 + sx + ix * 2;
-        if (pos == 0 || pos == 1 || pos == 8 || pos == 9) continue;
-        const uint32_t pk = list[first + b];
-        const int bx = pk & 0xFFFF, by = pk >> 16;
-        if (!PredictHFOf(f.acs[by * g.Bx + bx] >> 4)) continue;
-        s_c[b * 64 + pos] += s_q[i];
+    __syncwarp(mask);
+    // Pass 2: out[kk = k][l] = (sum_y tmp[k][y] B[l][y]) / 16, added to
+    // coefficient (k, l) except the sub-blocks' DCs (positions 0, 1, 8, 9).
+#pragma unroll
+    for (int sx = 0; sx < 2; ++sx) {
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        float sum = 0.f;
+#pragma unroll
+        for (int y = 0; y < 4; ++y) sum += t[sx][k][y] * B[l * 4 + y];
+        const float q = sum * (1.0f / 16.0f);
+        if (k != 0 || l != 0) cr[sx + 2 * l] += q;
       }
-      __syncthreads();
     }
-    // Gather sub-block inputs: DCs from the Hadamard of 0, 1, 8, 9.
-    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
-      const int b = i / 64, e = i % 64;
-      const int sb = e / 16, iy = (e % 16) / 4, ix = e % 4;
-      const int sy = sb / 2, sx = sb % 2;
-      const float* cb = s_c + b * 64;
-      float v;
-      if (iy == 0 && ix == 0) {
-        const float b00 = cb[0], b01 = cb[1], b10 = cb[8], b11 = cb[9];
-        const float d[4] = {b00 + b01 + b10 + b11, b00 + b01 - b10 - b11,
-                            b00 - b01 + b10 - b11, b00 - b01 - b10 + b11};
-        v = d[sy * 2 + sx];
-      } else {
-        v = cb[(sy + iy * 2) * 8 + sx + ix * 2];
-      }
-      s_q[i] = v;
+    __syncwarp(mask);
+  }
+  // The sub-blocks' DCs: the 2x2 Hadamard of positions 0, 1, 8, 9 (rows 0
+  // and 1, held by lanes 0 and 4 of the unit).
+  {
+    const int base = threadIdx.x & 24;
+    const float b00 = __shfl_sync(mask, cr[0], base);
+    const float b01 = __shfl_sync(mask, cr[1], base);
+    const float b10 = __shfl_sync(mask, cr[0], base + 4);
+    const float b11 = __shfl_sync(mask, cr[1], base + 4);
+    if (k == 0) {
+      const float d[4] = {b00 + b01 + b10 + b11, b00 + b01 - b10 - b11,
+                          b00 - b01 + b10 - b11, b00 - b01 - b10 + b11};
+      cr[0] = d[sy * 2];
+      cr[1] = d[sy * 2 + 1];
     }
-    __syncthreads();
-    CoopTsIdct(4, nb * 4, s_a, s_q, s_t, s_p);
-    for (int i = threadIdx.x; i < nb * 64; i += blockDim.x) {
-      const int b = i / 64, e = i % 64;
-      const int sb = e / 16, py = (e % 16) / 4, px = e % 4;
-      const int sy = sb / 2, sx = sb % 2;
-      const uint32_t pk = list[first + b];
-      const int bx = pk & 0xFFFF, by = pk >> 16;
-      f.idct[c * plane_px + size_t(by * 8 + sy * 4 + py) * g.PW + bx * 8 +
-             sx * 4 + px] = s_p[i];
+  }
+  // TsIdct pass 1: tmp[k][v] = sum_l C[k][l] A[v][l], to the tile.
+#pragma unroll
+  for (int sx = 0; sx < 2; ++sx) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      float sum = 0.f;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) sum += cr[sx + 2 * l] * A[v * 4 + l];
+      t[sx][k][v] = sum;
     }
-    __syncthreads();
+  }
+  __syncwarp(mask);
+  // Pass 2: pixel row v = k: out[v][u] = sum_k A[u][k] tmp[k][v].
+  float px[8];
+#pragma unroll
+  for (int sx = 0; sx < 2; ++sx) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      float sum = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) sum += A[u * 4 + kk] * t[sx][kk][k];
+      px[4 * sx + u] = sum;
+    }
+  }
+  if (active) {
+    float* out = f.idct + c * size_t(g.PW) * g.PH +
+                 size_t(by * 8 + 4 * sy + k) * g.PW + bx * 8;
+    *reinterpret_cast<float4*>(out) = make_float4(px[0], px[1], px[2], px[3]);
+    *reinterpret_cast<float4*>(out + 4) =
+        make_float4(px[4], px[5], px[6], px[7]);
   }
 }
 
@@ -1240,18 +1286,56 @@ __device__ void SmallInverse(int type, const float* cb, float* px, int ps) {
   }
 }
 
-__global__ void k_small_idct(Geo g, DevFrame f, const uint32_t* list,
-                             int count) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 3 * count) return;
-  const int b = i / 3, c = i % 3;
-  const uint32_t pk = list[b];
-  const int bx = pk & 0xFFFF, by = pk >> 16;
-  const int type = f.acs[by * g.Bx + bx] >> 4;
-  const float* cb = f.ac + c * size_t(g.ac_stride) * g.By +
-                    size_t(by) * g.ac_stride + bx * 64;
-  float* px = f.idct + c * size_t(g.PW) * g.PH + size_t(by * 8) * g.PW + bx * 8;
-  SmallInverse(type, cb, px, g.PW);
+// One thread per block and channel computes the inverse transform from
+// shared memory; the warp stages its 32 items' coefficients and pixels with
+// coalesced 16-byte accesses (the block list of this class is ordered by
+// transform type, so a warp rarely holds more than one type).
+constexpr int kSmallIdctThreads = 64;
+__global__ void __launch_bounds__(kSmallIdctThreads)
+    k_small_idct(Geo g, DevFrame f, const uint32_t* list, int count) {
+  __shared__ float s_in[kSmallIdctThreads][65];
+  __shared__ float s_out[kSmallIdctThreads][65];
+  const int lane = threadIdx.x & 31, w0 = threadIdx.x & ~31;
+  const int base = blockIdx.x * kSmallIdctThreads + w0;  // the warp's items
+  const int items = 3 * count;
+  const size_t plane_ac = size_t(g.ac_stride) * g.By;
+  const size_t plane_px = size_t(g.PW) * g.PH;
+#pragma unroll 4
+  for (int r = 0; r < 16; ++r) {  // two items of 16 float4 per step
+    const int it = 2 * r + (lane >> 4), e = (lane & 15) * 4;
+    const int item = base + it;
+    if (item < items) {
+      const int b = item / 3, c = item % 3;
+      const uint32_t pk = list[b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      const float4 v = *reinterpret_cast<const float4*>(
+          f.ac + c * plane_ac + size_t(by) * g.ac_stride + bx * 64 + e);
+      float* d = s_in[w0 + it] + e;
+      d[0] = v.x, d[1] = v.y, d[2] = v.z, d[3] = v.w;
+    }
+  }
+  __syncwarp();
+  if (base + lane < items) {
+    const uint32_t pk = list[(base + lane) / 3];
+    const int bx = pk & 0xFFFF, by = pk >> 16;
+    SmallInverse(f.acs[by * g.Bx + bx] >> 4, s_in[w0 + lane],
+                 s_out[w0 + lane], 8);
+  }
+  __syncwarp();
+#pragma unroll 4
+  for (int r = 0; r < 16; ++r) {  // two items of 8 rows x 2 float4 per step
+    const int it = 2 * r + (lane >> 4), y = (lane >> 1) & 7, h = lane & 1;
+    const int item = base + it;
+    if (item < items) {
+      const int b = item / 3, c = item % 3;
+      const uint32_t pk = list[b];
+      const int bx = pk & 0xFFFF, by = pk >> 16;
+      const float* o = s_out[w0 + it] + y * 8 + 4 * h;
+      *reinterpret_cast<float4*>(f.idct + c * plane_px +
+                                 size_t(by * 8 + y) * g.PW + bx * 8 + 4 * h) =
+          make_float4(o[0], o[1], o[2], o[3]);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

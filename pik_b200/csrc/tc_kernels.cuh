@@ -363,6 +363,18 @@ __global__ void __launch_bounds__(tc::kThreads, N == 16 ? 4 : 2)
       (reinterpret_cast<uintptr_t>(ar_tc_smem) + 127) & ~uintptr_t(127));
   __shared__ int s_next[2];
   const int t = threadIdx.x, bl = t / N, r = t % N;
+  const int count = *count_ptr;
+  const int nbat = (count + BPB - 1) / BPB;
+  // Batches are taken from a work counter, one at a time: a CTA that
+  // starts late (its SM busy with another class's kernel) takes fewer. The
+  // first is taken before the set-up, which a CTA without work skips (the
+  // grid is sized for all of the class's blocks, the active ones are
+  // counted on the device). The next batch is fetched at the start of a
+  // batch and read after the batch's last barrier.
+  if (t == 0) s_next[0] = atomicAdd(work, 1);
+  __syncthreads();
+  int batch = s_next[0];
+  if (batch >= nbat) return;
   if (t < 32) {
     asm volatile(
         "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
@@ -381,18 +393,9 @@ __global__ void __launch_bounds__(tc::kThreads, N == 16 ? 4 : 2)
   __syncthreads();
   FenceAfter();
   uint32_t phase = 0;
-  const int count = *count_ptr;
-  const int nbat = (count + BPB - 1) / BPB;
   const size_t plane = size_t(g.PW) * g.PH;
   const float inv_nn = 1.0f / float(N * N);
   bool ok = true;
-  // Batches are taken from a work counter, one at a time: a CTA that
-  // starts late (its SM busy with another class's kernel) takes fewer.
-  // The next batch is fetched at the start of a batch and read after the
-  // batch's last barrier.
-  if (t == 0) s_next[0] = atomicAdd(work, 1);
-  __syncthreads();
-  int batch = s_next[0];
   for (int k = 1; batch < nbat && ok; ++k) {
     if (t == 0) s_next[k & 1] = atomicAdd(work, 1);
     const int idx = batch * BPB + bl;
@@ -552,6 +555,20 @@ __global__ void __launch_bounds__(tc::kThreads, N == 16 ? 8 : 4)
   __shared__ Smem1<N, S> s;
   __shared__ int s_first[2], s_next[2];
   const int t = threadIdx.x, bl = t / N, r = t % N;
+  const int nitems = 3 * ((count + BPB - 1) / BPB);
+  // Items are taken from a work counter, so that a CTA that starts late
+  // (its SM busy with another class's kernel) takes fewer; a CTA without
+  // work skips the set-up. Two are known ahead: the current one and the
+  // next, whose coefficient row is loaded during the current item's
+  // passes; the one after that is fetched during the current item and read
+  // after its first pass's barrier.
+  if (t == 0) {
+    s_first[0] = atomicAdd(work, 1);
+    s_first[1] = atomicAdd(work, 1);
+  }
+  __syncthreads();
+  int item = s_first[0], item_next = s_first[1];
+  if (item >= nitems) return;
   if (t < 32) {
     asm volatile(
         "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
@@ -569,8 +586,6 @@ __global__ void __launch_bounds__(tc::kThreads, N == 16 ? 8 : 4)
   __syncthreads();
   FenceAfter();
   uint32_t phase = 0;
-  const int nbat = (count + BPB - 1) / BPB;
-  const int nitems = 3 * nbat;
   const size_t plane_ac = size_t(g.ac_stride) * g.By;
   const size_t plane_px = size_t(g.PW) * g.PH;
   const float inv_nn = 1.0f / float(N * N);
@@ -597,17 +612,6 @@ __global__ void __launch_bounds__(tc::kThreads, N == 16 ? 8 : 4)
     }
     return pk;
   };
-  // Items are taken from a work counter, so that a CTA that starts late
-  // (its SM busy with another class's kernel) takes fewer. Two are known
-  // ahead: the current one and the next, whose coefficient row is loaded
-  // during the current item's passes; the one after that is fetched during
-  // the current item and read after its first pass's barrier.
-  if (t == 0) {
-    s_first[0] = atomicAdd(work, 1);
-    s_first[1] = atomicAdd(work, 1);
-  }
-  __syncthreads();
-  int item = s_first[0], item_next = s_first[1];
   uint32_t pkd_next = item < nitems ? load_row(item) : 0u;
   for (int k = 0; item < nitems && ok; ++k) {
     const int batch = item / 3, c = item - 3 * batch;
