@@ -34,6 +34,10 @@ enum Class { kC8 = 0, kC16, kC32, kC4, kCSmall, kNumClasses };
 constexpr int kWorkIdct = kNumClasses, kWorkAr = kNumClasses + 1;
 constexpr int kWorkIdct32 = kNumClasses + 2, kWorkAr32 = kNumClasses + 3;
 constexpr int kNumCounters = kNumClasses + 4;
+// Up to this many small-transform blocks per SM, the small classes run one
+// CTA per block (short latency: one or two waves); above it, one thread per
+// block and channel (throughput).
+constexpr int kSmallCtaMax = 16;
 static_assert(kNumClasses == kMaxClasses, "ClassLists holds every class");
 int ClassOf(int type) {
   switch (type) {
@@ -630,9 +634,14 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     // before the persistent tensor-core kernel fills the SMs (which takes
     // its work from a counter and leaves those SMs' share to the others).
     if (n[kCSmall]) {
-      k_small_idct<<<Blocks(3 * n[kCSmall], kSmallIdctThreads),
-                     kSmallIdctThreads, 0, cls(kCSmall)>>>(
-          g, f, L[kCSmall], n[kCSmall]);
+      if (n[kCSmall] <= kSmallCtaMax * ctx->num_sms) {
+        k_small_idct_cta<<<n[kCSmall], kSmallCtaThreads, 0, cls(kCSmall)>>>(
+            g, f, L[kCSmall], n[kCSmall]);
+      } else {
+        k_small_idct<<<Blocks(3 * n[kCSmall], kSmallIdctThreads),
+                       kSmallIdctThreads, 0, cls(kCSmall)>>>(
+            g, f, L[kCSmall], n[kCSmall]);
+      }
       ++ctx->launches;
     }
     if (n[kC4]) {
@@ -748,13 +757,19 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       return (warps * 32 + kSquareThreads - 1) / kSquareThreads;
     };
     if (n[kCSmall]) {
-      k_small_ar<<<Blocks(n[kCSmall], kSmallArBlocks), 3 * kSmallArBlocks, 0,
-                   cls(kCSmall)>>>(
-          g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
+      if (n[kCSmall] <= kSmallCtaMax * ctx->num_sms) {
+        k_small_ar_cta<<<n[kCSmall], kSmallCtaThreads, 0, cls(kCSmall)>>>(
+            g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
+      } else {
+        k_small_ar<<<Blocks(n[kCSmall], kSmallArBlocks), 3 * kSmallArBlocks,
+                     0, cls(kCSmall)>>>(
+            g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
+      }
       ++ctx->launches;
     }
     if (n[kC4]) {
-      k_dct4_ar<<<Blocks(n[kC4], kDct4Blocks), 256, 0, cls(kC4)>>>(
+      k_dct4_ar<<<Blocks(n[kC4], kDct4ArThreads / 8), kDct4ArThreads, 0,
+                  cls(kC4)>>>(
           g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
       ++ctx->launches;
     }

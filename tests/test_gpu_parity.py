@@ -92,6 +92,20 @@ def test_every_transform_type_bitexact(name):
     assert_bitexact_vs_oracle(frame, run_gpu(frame))
 
 
+@pytest.mark.parametrize("shares", [
+    {"DCT2X2": 0.4, "IDENTITY": 0.3, "LINES": 0.3},
+    {"DCT4X4": 0.5, "DCT4X4_NOHF": 0.5},
+])
+def test_many_small_blocks_bitexact(shares):
+    """4225 small-transform blocks: more than the one-CTA-per-block forms of
+    the DCT2X2 / IDENTITY / LINES inverse and clamp take (16 blocks per SM),
+    so the one-thread-per-block-and-channel forms run; the frames above run
+    the others."""
+    frame = synthetic.make_frame(520, 520, seed=13, shares=shares,
+                                 qf_median=9.0)
+    assert_bitexact_vs_oracle(frame, run_gpu(frame))
+
+
 @pytest.mark.parametrize("size", [(8, 8), (1, 1), (13, 7), (520, 9),
                                   (1030, 530), (64, 520)])
 def test_sizes_and_group_borders(size):
