@@ -1,0 +1,372 @@
+// dpik_gpu: the reference decoder (PikToPixels, pik/pik.cc:92-131, built
+// from its unmodified sources into oracle/_ref/libpikref_scalar.so) with its
+// reconstruction swapped for libpikgpu at the reference's own function
+// boundaries. Nothing of the reference is copied or patched: this
+// executable defines four of the library's exported functions, and the
+// dynamic linker binds the library's calls to these definitions (symbol
+// interposition; the library is built with -fPIC and default visibility,
+// so its cross-file calls go through the PLT / GOT). The overrides reach the
+// library's own definitions through dlsym(RTLD_NEXT).
+//
+// The hook points are those of an `#ifdef PIKGPU` build of the decoder:
+//  * AdaptiveDCReconstruction (called by DecodeDCGroups,
+//    pik/compressed_dc.cc:549): keeps a copy of the frame's dequantised DC
+//    (DequantDC's output, pik/compressed_dc.cc:181-225), then runs the
+//    reference's own smoothing for the CPU caches.
+//  * DecodeFromBitstream<true> (pik/compressed_image.cc:720-813, called per
+//    group from the ThreadPool, pik/pik_frame.cc:906-916): runs the
+//    reference's entropy decoding and un-scattering, then -- the first call
+//    under std::call_once -- starts the GPU frame from the decoder's frame
+//    state (pikgpu_frame_begin) and hands the group's int16 coefficients to
+//    the GPU (pikgpu_frame_set_group_ac), from the pool thread.
+//  * ReconOpsinImage (pik/pik_frame.cc:925-928): skipped; the GPU
+//    reconstructs the whole frame.
+//  * FinalizeFrameDecoding (pik/pik_frame.cc:1149-1152): one
+//    pikgpu_reconstruct into the decoder's opsin image, which the reference
+//    then treats as linear sRGB, as after its own FinalizeFrameDecoding.
+//
+// The reference keeps only the dequantised DC (DequantDC runs inside
+// compressed_dc.cc's anonymous namespace, out of reach), while the ABI takes
+// the quantised DC. It is recovered by inverting DequantDC's two steps
+// (q_Y = dc_Y / mul_Y; q_XB = (dc_XB - ytox_dc * dc_Y) / mul_XB, rounded to
+// the nearest integer) and accepted only if recomputing DequantDC from the
+// recovered integers reproduces every dequantised value bit for bit.
+//
+// Usage: dpik_gpu in.pik out.f32 [fp32|split_bf16|split_bf16x3] [threads]
+// out.f32: int32 xsize, int32 ysize, then 3 planes of ysize x xsize floats
+// (linear RGB, 0..255 scale, as PikToPixels leaves io.color()). Prints the
+// number of calls each override took.
+
+#include <dlfcn.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pik/adaptive_reconstruction.h"
+#include "pik/block_dictionary.h"
+#include "pik/codec.h"
+#include "pik/color_correlation.h"
+#include "pik/compressed_image.h"
+#include "pik/compressed_image_fwd.h"
+#include "pik/data_parallel.h"
+#include "pik/headers.h"
+#include "pik/image.h"
+#include "pik/noise.h"
+#include "pik/pik.h"
+#include "pik/pik_info.h"
+#include "pik/pik_params.h"
+#include "pik/quant_weights.h"
+#include "pik/quantizer.h"
+
+#include "pikgpu.h"
+
+namespace {
+
+pikgpu_ctx* g_ctx = nullptr;
+// The image size from the file header (read in main before decoding):
+// pikgpu_frame_begin needs it before the decoder reaches
+// FinalizeFrameDecoding, which is the first hook that is given it.
+uint32_t g_xsize = 0, g_ysize = 0;
+std::once_flag g_begin_once;
+int g_begin_rc = 0;
+std::string g_error;
+pik::Image3F g_dc_dequant;  // frame DC after DequantDC
+std::atomic<int> g_calls_dc{0}, g_calls_groups{0}, g_calls_recon{0},
+    g_calls_finalize{0};
+
+void* Next(const char* symbol) {
+  void* p = dlsym(RTLD_NEXT, symbol);
+  if (!p) {
+    fprintf(stderr, "dpik_gpu: %s not found in the reference library\n",
+            symbol);
+    abort();
+  }
+  return p;
+}
+
+template <typename T>
+std::vector<T> Pack(const pik::Image<T>& img) {
+  std::vector<T> v(img.xsize() * img.ysize());
+  for (size_t y = 0; y < img.ysize(); ++y) {
+    memcpy(v.data() + y * img.xsize(), img.ConstRow(y),
+           img.xsize() * sizeof(T));
+  }
+  return v;
+}
+
+// The quantised DC from the dequantised one (see the file comment); false if
+// any value does not round-trip.
+bool RecoverQuantizedDC(const pik::Quantizer& quantizer,
+                        const pik::ColorCorrelationMap& cmap,
+                        std::vector<int16_t>* q) {
+  const pik::Image3F& dc = g_dc_dequant;
+  const size_t bx = dc.xsize(), by = dc.ysize();
+  float mul_dc[3];
+  for (int c = 0; c < 3; ++c) {
+    mul_dc[c] = quantizer.DequantMatrix(0, pik::kQuantKindDCT8, c)[0] *
+                quantizer.inv_quant_dc();
+  }
+  const float y_mul[3] = {
+      pik::ColorCorrelationMap::YtoX(1.0f, cmap.ytox_dc), 0.f,
+      pik::ColorCorrelationMap::YtoB(1.0f, cmap.ytob_dc)};
+  q->assign(3 * bx * by, 0);
+  for (size_t y = 0; y < by; ++y) {
+    const float* row_y = dc.ConstPlaneRow(1, y);
+    for (int c : {1, 0, 2}) {
+      const float* row = dc.ConstPlaneRow(c, y);
+      int16_t* out = q->data() + (c * by + y) * bx;
+      for (size_t x = 0; x < bx; ++x) {
+        const float rest = c == 1 ? row[x] : row[x] - y_mul[c] * row_y[x];
+        const long v = lrintf(rest / mul_dc[c]);
+        if (v < -32768 || v > 32767) return false;
+        out[x] = int16_t(v);
+        // DequantDC's arithmetic: q * mul (Y), y_mul * Y + q * mul (X, B).
+        const float dq = float(out[x]) * mul_dc[c];
+        const float back = c == 1 ? dq : y_mul[c] * row_y[x] + dq;
+        if (memcmp(&back, &row[x], sizeof(float)) != 0) return false;
+      }
+    }
+  }
+  return true;
+}
+
+int BeginFrame(const pik::FrameHeader& hd, const pik::Quantizer& quantizer,
+               const pik::ColorCorrelationMap& cmap,
+               const pik::FrameDecCache& fdc) {
+  std::vector<int16_t> qdc;
+  if (!RecoverQuantizedDC(quantizer, cmap, &qdc)) {
+    g_error = "the quantised DC did not round-trip through DequantDC";
+    return -1;
+  }
+  const pik::DequantMatrices& m = fdc.matrices;
+  std::vector<uint32_t> offsets(pik::kNumPredefinedTables *
+                                pik::kNumQuantKinds * 3);
+  for (size_t t = 0; t < pik::kNumPredefinedTables; ++t) {
+    for (size_t k = 0; k < pik::kNumQuantKinds; ++k) {
+      for (int c = 0; c < 3; ++c) {
+        offsets[(t * pik::kNumQuantKinds + k) * 3 + c] =
+            m.MatrixOffset(t, k, c);
+      }
+    }
+  }
+  const auto cf = Pack(fdc.dequant_control_field);
+  const auto ytox = Pack(cmap.ytox_map), ytob = Pack(cmap.ytob_map);
+  const auto acs = Pack(fdc.ac_strategy.ConstRaw());
+  const auto qf = Pack(fdc.raw_quant_field);
+  const auto lut = Pack(fdc.ar_sigma_lut_ids);
+  pikgpu_frame_params p = {};
+  p.xsize = g_xsize;
+  p.ysize = g_ysize;
+  p.flags = hd.flags;
+  p.gaborish = static_cast<uint32_t>(hd.gaborish);
+  p.predict_lf = hd.predict_lf;
+  p.predict_hf = hd.predict_hf;
+  p.have_adaptive_reconstruction = hd.have_adaptive_reconstruction;
+  p.epf_enable_adaptive = hd.epf_params.enable_adaptive;
+  p.epf_sigma = hd.epf_params.sigma;
+  p.epf_use_sharpened = hd.epf_params.use_sharpened;
+  // Quantizer::global_scale_ from its inverse (pik/quantizer.h:131-139).
+  p.global_scale = int(65536.0f / quantizer.InvGlobalScale() + 0.5f);
+  p.quant_dc = quantizer.QuantDC();
+  p.dequant_table = m.Matrix(0, pik::kQuantKindDCT8, 0) -
+                    m.MatrixOffset(0, pik::kQuantKindDCT8, 0);
+  p.dequant_table_size = uint32_t(m.Size());
+  p.dequant_offsets = offsets.data();
+  p.num_dequant_tables = pik::kNumPredefinedTables;
+  p.dequant_control_field = cf.data();
+  p.dequant_map = &fdc.dequant_map[0][0];
+  p.ytox_map = ytox.data();
+  p.ytob_map = ytob.data();
+  p.ytox_dc = cmap.ytox_dc;
+  p.ytob_dc = cmap.ytob_dc;
+  p.ac_strategy = acs.data();
+  p.raw_quant_field = qf.data();
+  p.ar_sigma_lut_ids = lut.data();
+  p.quantized_dc = qdc.data();
+  return pikgpu_frame_begin(g_ctx, &p);
+}
+
+}  // namespace
+
+namespace pik {
+
+void AdaptiveDCReconstruction(Image3F& dc, const Quantizer& quantizer,
+                              ThreadPool* pool) {
+  using Fn = void (*)(Image3F&, const Quantizer&, ThreadPool*);
+  static const Fn next = reinterpret_cast<Fn>(
+      Next("_ZN3pik24AdaptiveDCReconstructionERNS_6Image3IfEERKNS_9"
+           "QuantizerEPNS_10ThreadPoolE"));
+  g_dc_dequant = CopyImage(dc);
+  ++g_calls_dc;
+  next(dc, quantizer, pool);
+}
+
+template <>
+bool DecodeFromBitstream<true>(
+    const FrameHeader& frame_header, const GroupHeader& header,
+    const PaddedBytes& compressed, BitReader* reader, const Rect& group_rect,
+    MultipassHandler* handler, const size_t xsize_blocks,
+    const size_t ysize_blocks, const ColorCorrelationMap& cmap,
+    const Rect& cmap_rect, NoiseParams* noise_params,
+    const Quantizer& quantizer, FrameDecCache* PIK_RESTRICT frame_dec_cache,
+    GroupDecCache* PIK_RESTRICT group_dec_cache, PikInfo* aux_out) {
+  using Fn = bool (*)(const FrameHeader&, const GroupHeader&,
+                      const PaddedBytes&, BitReader*, const Rect&,
+                      MultipassHandler*, size_t, size_t,
+                      const ColorCorrelationMap&, const Rect&, NoiseParams*,
+                      const Quantizer&, FrameDecCache*, GroupDecCache*,
+                      PikInfo*);
+  static const Fn next = reinterpret_cast<Fn>(Next(
+      "_ZN3pik19DecodeFromBitstreamILb1EEEbRKNS_11FrameHeaderERKNS_11"
+      "GroupHeaderERKNS_11PaddedBytesEPNS_9BitReaderERKNS_4RectEPNS_16"
+      "MultipassHandlerEmmRKNS_19ColorCorrelationMapESE_PNS_11NoiseParamsE"
+      "RKNS_9QuantizerEPNS_13FrameDecCacheEPNS_13GroupDecCacheEPNS_7"
+      "PikInfoE"));
+  if (!next(frame_header, header, compressed, reader, group_rect, handler,
+            xsize_blocks, ysize_blocks, cmap, cmap_rect, noise_params,
+            quantizer, frame_dec_cache, group_dec_cache, aux_out)) {
+    return false;
+  }
+  std::call_once(g_begin_once, [&] {
+    g_begin_rc = BeginFrame(frame_header, quantizer, cmap, *frame_dec_cache);
+  });
+  if (g_begin_rc != 0) return false;
+  // group_rect: the group's pixels (512x512 groups, row-major).
+  const uint32_t groups_x = (g_xsize + 511) / 512;
+  const uint32_t gi = uint32_t(group_rect.y0() / 512) * groups_x +
+                      uint32_t(group_rect.x0() / 512);
+  const Image3S& q = group_dec_cache->quantized_ac;
+  const int16_t* planes[3] = {q.ConstPlaneRow(0, 0), q.ConstPlaneRow(1, 0),
+                              q.ConstPlaneRow(2, 0)};
+  ++g_calls_groups;
+  return pikgpu_frame_set_group_ac(g_ctx, gi, planes, q.PixelsPerRow()) ==
+         PIKGPU_OK;
+}
+
+void ReconOpsinImage(const FrameHeader& frame_header,
+                     const GroupHeader& header, const Quantizer& quantizer,
+                     const Rect& block_group_rect,
+                     FrameDecCache* PIK_RESTRICT frame_dec_cache,
+                     GroupDecCache* PIK_RESTRICT group_dec_cache,
+                     Image3F* PIK_RESTRICT idct, const Rect& idct_rect,
+                     PikInfo* aux_out, size_t downsample) {
+  ++g_calls_recon;  // the GPU reconstructs the frame at the end
+}
+
+Status FinalizeFrameDecoding(Image3F* PIK_RESTRICT idct, size_t xsize,
+                             size_t ysize, const FrameHeader& frame_header,
+                             const NoiseParams& noise_params,
+                             const Quantizer& quantizer,
+                             const BlockDictionary& dictionary,
+                             ThreadPool* pool, FrameDecCache* frame_dec_cache,
+                             PikInfo* aux_out, size_t downsample) {
+  ++g_calls_finalize;
+  if (downsample != 1) return PIK_FAILURE("dpik_gpu: downsampling");
+  {
+    // A frame whose block dictionary adds dots is not on the GPU path.
+    Image3F probe(idct->xsize(), idct->ysize());
+    ZeroFillImage(&probe);
+    dictionary.AddTo(&probe, 1);
+    for (int c = 0; c < 3; ++c) {
+      for (size_t y = 0; y < probe.ysize(); ++y) {
+        const float* row = probe.ConstPlaneRow(c, y);
+        for (size_t x = 0; x < probe.xsize(); ++x) {
+          if (row[x] != 0.0f) return PIK_FAILURE("dpik_gpu: block dictionary");
+        }
+      }
+    }
+  }
+  if (xsize != g_xsize || ysize != g_ysize) {
+    return PIK_FAILURE("dpik_gpu: image size differs from the header's");
+  }
+  float* rows[3] = {idct->PlaneRow(0, 0), idct->PlaneRow(1, 0),
+                    idct->PlaneRow(2, 0)};
+  if (pikgpu_reconstruct(g_ctx, rows, idct->PixelsPerRow(), nullptr, 0,
+                         /*outputs_on_device=*/0) != PIKGPU_OK) {
+    g_error = pikgpu_last_error(g_ctx);
+    return PIK_FAILURE("dpik_gpu: pikgpu_reconstruct failed");
+  }
+  idct->ShrinkTo(xsize, ysize);
+  return true;
+}
+
+}  // namespace pik
+
+int main(int argc, char** argv) {
+  if (argc < 3) {
+    fprintf(stderr,
+            "usage: dpik_gpu in.pik out.f32 [fp32|split_bf16|split_bf16x3] "
+            "[threads]\n");
+    return 2;
+  }
+  FILE* f = fopen(argv[1], "rb");
+  if (!f) return 2;
+  fseek(f, 0, SEEK_END);
+  const long size = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  pik::PaddedBytes compressed(size);
+  if (fread(compressed.data(), 1, size, f) != size_t(size)) return 2;
+  fclose(f);
+  int form = PIKGPU_FORM_FP32;
+  if (argc > 3 && !strcmp(argv[3], "split_bf16")) form = PIKGPU_FORM_SPLIT_BF16;
+  if (argc > 3 && !strcmp(argv[3], "split_bf16x3")) {
+    form = PIKGPU_FORM_SPLIT_BF16X3;
+  }
+  const int threads = argc > 4 ? atoi(argv[4]) : 8;
+
+  // The image size (the file header's), which pikgpu_frame_begin needs
+  // before the decoder reaches FinalizeFrameDecoding.
+  {
+    pik::BitReader reader(compressed.data(), compressed.size());
+    pik::FileHeader container;
+    if (!pik::ReadFileHeader(&reader, &container)) {
+      fprintf(stderr, "dpik_gpu: cannot read the file header\n");
+      return 1;
+    }
+    g_xsize = uint32_t(container.xsize());
+    g_ysize = uint32_t(container.ysize());
+  }
+  if (pikgpu_ctx_create(0, &g_ctx) != PIKGPU_OK ||
+      pikgpu_set_option(g_ctx, PIKGPU_OPT_FORM, form) != PIKGPU_OK) {
+    fprintf(stderr, "dpik_gpu: context: %s\n",
+            g_ctx ? pikgpu_last_error(g_ctx) : "create failed");
+    return 1;
+  }
+
+  pik::CodecContext context;
+  pik::CodecInOut io(&context);
+  pik::DecompressParams dparams;
+  std::unique_ptr<pik::ThreadPool> pool;
+  if (threads > 0) pool.reset(new pik::ThreadPool(threads));
+  const bool ok = pik::PikToPixels(dparams, compressed, &io, nullptr,
+                                   pool.get());
+  printf("overrides: AdaptiveDCReconstruction %d, DecodeFromBitstream %d, "
+         "ReconOpsinImage %d, FinalizeFrameDecoding %d\n",
+         g_calls_dc.load(), g_calls_groups.load(), g_calls_recon.load(),
+         g_calls_finalize.load());
+  if (!ok) {
+    fprintf(stderr, "dpik_gpu: PikToPixels failed: %s\n", g_error.c_str());
+    pikgpu_ctx_destroy(g_ctx);
+    return 1;
+  }
+  const pik::Image3F& color = io.color();
+  FILE* out = fopen(argv[2], "wb");
+  if (!out) return 2;
+  const int32_t dims[2] = {int32_t(color.xsize()), int32_t(color.ysize())};
+  fwrite(dims, sizeof(dims), 1, out);
+  for (int c = 0; c < 3; ++c) {
+    for (size_t y = 0; y < color.ysize(); ++y) {
+      fwrite(color.ConstPlaneRow(c, y), sizeof(float), color.xsize(), out);
+    }
+  }
+  fclose(out);
+  pikgpu_ctx_destroy(g_ctx);
+  return 0;
+}

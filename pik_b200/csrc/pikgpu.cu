@@ -768,7 +768,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       ++ctx->launches;
     }
     if (n[kC4]) {
-      k_dct4_ar<<<Blocks(n[kC4], kDct4ArThreads / 8), kDct4ArThreads, 0,
+      k_dct4_ar<<<Blocks(n[kC4], kDct4ArThreads / 32), kDct4ArThreads, 0,
                   cls(kC4)>>>(
           g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
       ++ctx->launches;

@@ -1386,14 +1386,16 @@ __device__ void SmallInversePar(int type, int c, int e, float (*co)[64],
       const int y = e >> 1, x = e & 1;
       const float* cb = co[c];
       const float b00 = cb[0], b01 = cb[1], b10 = cb[8], b11 = cb[9];
-      const float dcs[4] = {b00 + b01 + b10 + b11, b00 + b01 - b10 - b11,
-                            b00 - b01 + b10 - b11, b00 - b01 - b10 + b11};
+      const float dc = e == 0   ? b00 + b01 + b10 + b11
+                       : e == 1 ? b00 + b01 - b10 - b11
+                       : e == 2 ? b00 - b01 + b10 - b11
+                                : b00 - b01 - b10 + b11;
       float residual_sum = 0.f;
       for (int iy = 0; iy < 4; ++iy)
         for (int ix = 0; ix < 4; ++ix)
           if (ix != 0 || iy != 0)
             residual_sum += cb[(y + iy * 2) * 8 + x + ix * 2];
-      aux[c][e] = dcs[y * 2 + x] - residual_sum * (1.0f / 16);
+      aux[c][e] = dc - residual_sum * (1.0f / 16);
     }
     __syncthreads();
     const int y = Y >> 2, iy = Y & 3, x = X >> 2, ix = X & 3;
@@ -1755,170 +1757,165 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Clamp for DCT4X4 blocks. A unit of 8 lanes takes one block and all three
-// channels: lane j = 4 sy + k holds pixel row 4 sy + k of the correction
-// (filtered - original) and, after the forward 4x4 transforms, coefficient
-// row sy + 2 k of each channel, so the minimum ratio over the channels is
-// taken inside the lane. The second pass of each 4x4 transform reads the
-// other rows of its sub-block through a shared-memory transpose. Every sum
-// has the operation order of TsDct / TsIdct (CoopTsDct, CoopTsIdct).
+// Clamp for DCT4X4 blocks: one warp per block, lanes 8 c + j (c < 3) on
+// channel c. Lane j = 4 sy + k of a channel holds pixel row 4 sy + k of the
+// correction (filtered - original) and, after the forward 4x4 transforms,
+// coefficient row sy + 2 k; the minimum ratio over the channels is read
+// from the lanes j, j + 8, j + 16 of the other channels. The second pass
+// of each 4x4 transform reads the other rows of its sub-block through a
+// shared-memory transpose. Every sum has the operation order of TsDct /
+// TsIdct (CoopTsDct, CoopTsIdct). Lanes 24..31 repeat channel 2 and store
+// nothing.
 constexpr int kDct4ArThreads = 128;
 __global__ void __launch_bounds__(kDct4ArThreads)
     k_dct4_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
               const int* count_ptr) {
-  constexpr int kUnits = kDct4ArThreads / 8;
+  constexpr int kWarps = kDct4ArThreads / 32;
   const int count = *count_ptr;
-  if (int(blockIdx.x) * kUnits >= count) return;  // whole CTA
-  __shared__ float s_t[kUnits][2][2][4][5];  // per unit: [sy][sx][row][col]
-  const int unit = threadIdx.x >> 3, j = threadIdx.x & 7;
+  if (int(blockIdx.x) * kWarps >= count) return;  // whole CTA
+  __shared__ float s_t[kWarps][4][2][2][4][5];  // [warp][c][sy][sx][row][col]
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = min(lane >> 3, 2), j = lane & 7;
+  const bool owner = lane < 24;
   const int sy = j >> 2, k = j & 3;
-  const int b = blockIdx.x * kUnits + unit;
+  const int b = blockIdx.x * kWarps + w;
   const bool active = b < count;
-  const uint32_t mask = 0xFFu << (threadIdx.x & 24);
-  const int base = threadIdx.x & 24;  // lane of the unit's row 0
+  const int base = c * 8;  // lane of the channel's coefficient row 0
   const uint32_t pk = list[active ? b : 0];
   const int bx = pk & 0xFFFF, by = pk >> 16;
   const float* A = IdctMat(4);
   const float* B = DctMat(4);
-  float (*t)[4][5] = s_t[unit][sy];
+  float (*t)[4][5] = s_t[w][lane >> 3][sy];
   const size_t plane = size_t(g.PW) * g.PH;
-  const size_t row = size_t(by * 8 + 4 * sy + k) * g.PW + bx * 8;
-  // The clamp intervals of the lane's 24 coefficients, loaded first (a
-  // chain of dependent loads whose latency the transforms then hide).
-  float interval[3][8];
+  const size_t row = c * plane + size_t(by * 8 + 4 * sy + k) * g.PW + bx * 8;
+  // The clamp intervals of the lane's 8 coefficients, loaded first (a chain
+  // of dependent loads whose latency the forward transform then hides).
+  float interval[8];
   {
     const int type = f.acs[by * g.Bx + bx] >> 4;
     const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
+    const float* dm = c == 0 ? info.dm[0] : c == 1 ? info.dm[1] : info.dm[2];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int col = 0; col < 8; ++col) {
-        const int e = (sy + 2 * k) * 8 + col;
-        interval[c][col] =
-            e == 0 ? 1.0f * s.mul_dc[c] : info.dm[c][e] * info.inv_quant_ac;
-      }
-  }
-  float co[3][8], iv[3][8];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    float d[8];
-    {
-      const float* fp = f.filt + c * plane + row;
-      const float* ip = f.idct + c * plane + row;
-      const float4 f0 = *reinterpret_cast<const float4*>(fp);
-      const float4 f1 = *reinterpret_cast<const float4*>(fp + 4);
-      const float4 i0 = *reinterpret_cast<const float4*>(ip);
-      const float4 i1 = *reinterpret_cast<const float4*>(ip + 4);
-      iv[c][0] = i0.x, iv[c][1] = i0.y, iv[c][2] = i0.z, iv[c][3] = i0.w;
-      iv[c][4] = i1.x, iv[c][5] = i1.y, iv[c][6] = i1.z, iv[c][7] = i1.w;
-      d[0] = f0.x - i0.x, d[1] = f0.y - i0.y, d[2] = f0.z - i0.z;
-      d[3] = f0.w - i0.w, d[4] = f1.x - i1.x, d[5] = f1.y - i1.y;
-      d[6] = f1.z - i1.z, d[7] = f1.w - i1.w;
+    for (int col = 0; col < 8; ++col) {
+      const int e = (sy + 2 * k) * 8 + col;
+      interval[col] = e == 0 ? 1.0f * s.mul_dc[c] : dm[e] * info.inv_quant_ac;
     }
-    // TsDct pass 1 (pixel row y = k): tmp[kk][k] = sum_x B[kk][x] d[x].
+  }
+  float co[8], iv[8], d[8];
+  {
+    const float4 f0 = *reinterpret_cast<const float4*>(f.filt + row);
+    const float4 f1 = *reinterpret_cast<const float4*>(f.filt + row + 4);
+    const float4 i0 = *reinterpret_cast<const float4*>(f.idct + row);
+    const float4 i1 = *reinterpret_cast<const float4*>(f.idct + row + 4);
+    iv[0] = i0.x, iv[1] = i0.y, iv[2] = i0.z, iv[3] = i0.w;
+    iv[4] = i1.x, iv[5] = i1.y, iv[6] = i1.z, iv[7] = i1.w;
+    d[0] = f0.x - i0.x, d[1] = f0.y - i0.y, d[2] = f0.z - i0.z;
+    d[3] = f0.w - i0.w, d[4] = f1.x - i1.x, d[5] = f1.y - i1.y;
+    d[6] = f1.z - i1.z, d[7] = f1.w - i1.w;
+  }
+  // TsDct pass 1 (pixel row y = k): tmp[kk][k] = sum_x B[kk][x] d[x].
 #pragma unroll
-    for (int sx = 0; sx < 2; ++sx)
+  for (int sx = 0; sx < 2; ++sx)
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        float sum = 0.f;
+    for (int kk = 0; kk < 4; ++kk) {
+      float sum = 0.f;
 #pragma unroll
-        for (int x = 0; x < 4; ++x) sum += B[kk * 4 + x] * d[4 * sx + x];
-        t[sx][kk][k] = sum;
-      }
-    __syncwarp(mask);
-    // Pass 2: coefficient (k, l) of sub-block (sy, sx), at column sx + 2 l
-    // of coefficient row sy + 2 k.
+      for (int x = 0; x < 4; ++x) sum += B[kk * 4 + x] * d[4 * sx + x];
+      t[sx][kk][k] = sum;
+    }
+  __syncwarp();
+  // Pass 2: coefficient (k, l) of sub-block (sy, sx), at column sx + 2 l of
+  // coefficient row sy + 2 k.
 #pragma unroll
-    for (int sx = 0; sx < 2; ++sx)
+  for (int sx = 0; sx < 2; ++sx)
 #pragma unroll
-      for (int l = 0; l < 4; ++l) {
-        float sum = 0.f;
+    for (int l = 0; l < 4; ++l) {
+      float sum = 0.f;
 #pragma unroll
-        for (int y = 0; y < 4; ++y) sum += t[sx][k][y] * B[l * 4 + y];
-        co[c][sx + 2 * l] = sum * (1.0f / 16.0f);
-      }
-    __syncwarp(mask);
-    // The 2x2 Hadamard of the sub-block DCs (positions 0, 1, 8, 9) x 0.25.
-    const float b00 = __shfl_sync(mask, co[c][0], base);
-    const float b01 = __shfl_sync(mask, co[c][1], base);
-    const float b10 = __shfl_sync(mask, co[c][0], base + 4);
-    const float b11 = __shfl_sync(mask, co[c][1], base + 4);
+      for (int y = 0; y < 4; ++y) sum += t[sx][k][y] * B[l * 4 + y];
+      co[sx + 2 * l] = sum * (1.0f / 16.0f);
+    }
+  __syncwarp();
+  // The 2x2 Hadamard of the sub-block DCs (positions 0, 1, 8, 9) x 0.25.
+  {
+    const float b00 = __shfl_sync(~0u, co[0], base);
+    const float b01 = __shfl_sync(~0u, co[1], base);
+    const float b10 = __shfl_sync(~0u, co[0], base + 4);
+    const float b11 = __shfl_sync(~0u, co[1], base + 4);
     if (k == 0) {
       if (sy == 0) {
-        co[c][0] = (b00 + b01 + b10 + b11) * 0.25f;
-        co[c][1] = (b00 + b01 - b10 - b11) * 0.25f;
+        co[0] = (b00 + b01 + b10 + b11) * 0.25f;
+        co[1] = (b00 + b01 - b10 - b11) * 0.25f;
       } else {
-        co[c][0] = (b00 - b01 + b10 - b11) * 0.25f;
-        co[c][1] = (b00 - b01 - b10 + b11) * 0.25f;
+        co[0] = (b00 - b01 + b10 - b11) * 0.25f;
+        co[1] = (b00 - b01 - b10 + b11) * 0.25f;
       }
     }
   }
   // Clamp ratios, their minimum over X, Y, B, and the scaled corrections.
+#pragma unroll
+  for (int col = 0; col < 8; ++col) {
+    const float r = ClampRatio(co[col], interval[col]);
+    float rt[3], cv[3];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      rt[cc] = __shfl_sync(~0u, r, cc * 8 + j);
+      cv[cc] = __shfl_sync(~0u, co[col], cc * 8 + j);
+    }
+    float mr = 1.0f;
+    int arg = -1;
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      if (rt[cc] < mr) mr = rt[cc], arg = cc;
+    }
+    const int e = (sy + 2 * k) * 8 + col;
+    const size_t to = CoefOffset(g, bx, by, 1, e);
+    const float ca = arg == 0 ? cv[0] : arg == 1 ? cv[1] : cv[2];
+    uint8_t code = ClampTapeCode(arg, arg < 0 ? 0.f : ca);
+    if (f.clamp_tape_in) {
+      code = f.clamp_tape_in[to];
+      mr = TapeRatio(code, rt[0], rt[1], rt[2]);
+    }
+    if (active && lane < 8 && f.clamp_tape) f.clamp_tape[to] = code;
+    co[col] = co[col] * mr;
+  }
+  // Inverse: sub-block DCs from the Hadamard of 0, 1, 8, 9, then TsIdct;
+  // the result is added to the original.
   {
-#pragma unroll
-    for (int col = 0; col < 8; ++col) {
-      const int e = (sy + 2 * k) * 8 + col;
-      float mr = 1.0f, rt[3];
-      int arg = -1;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        rt[c] = ClampRatio(co[c][col], interval[c][col]);
-        if (rt[c] < mr) mr = rt[c], arg = c;
-      }
-      const size_t to = CoefOffset(g, bx, by, 1, e);
-      const float ca = arg == 0 ? co[0][col] : arg == 1 ? co[1][col]
-                                                        : co[2][col];
-      uint8_t code = ClampTapeCode(arg, arg < 0 ? 0.f : ca);
-      if (f.clamp_tape_in) {
-        code = f.clamp_tape_in[to];
-        mr = TapeRatio(code, rt[0], rt[1], rt[2]);
-      }
-      if (active && f.clamp_tape) f.clamp_tape[to] = code;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) co[c][col] = co[c][col] * mr;
+    const float b00 = __shfl_sync(~0u, co[0], base);
+    const float b01 = __shfl_sync(~0u, co[1], base);
+    const float b10 = __shfl_sync(~0u, co[0], base + 4);
+    const float b11 = __shfl_sync(~0u, co[1], base + 4);
+    if (k == 0) {
+      co[0] = sy == 0 ? b00 + b01 + b10 + b11 : b00 - b01 + b10 - b11;
+      co[1] = sy == 0 ? b00 + b01 - b10 - b11 : b00 - b01 - b10 + b11;
     }
   }
-  // Inverse per channel: sub-block DCs from the Hadamard of 0, 1, 8, 9,
-  // then TsIdct; the result is added to the original.
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const float b00 = __shfl_sync(mask, co[c][0], base);
-    const float b01 = __shfl_sync(mask, co[c][1], base);
-    const float b10 = __shfl_sync(mask, co[c][0], base + 4);
-    const float b11 = __shfl_sync(mask, co[c][1], base + 4);
-    if (k == 0) {
-      const float dd[4] = {b00 + b01 + b10 + b11, b00 + b01 - b10 - b11,
-                           b00 - b01 + b10 - b11, b00 - b01 - b10 + b11};
-      co[c][0] = dd[sy * 2];
-      co[c][1] = dd[sy * 2 + 1];
+  for (int sx = 0; sx < 2; ++sx)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      float sum = 0.f;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) sum += co[sx + 2 * l] * A[v * 4 + l];
+      t[sx][k][v] = sum;
     }
+  __syncwarp();
+  float px[8];
 #pragma unroll
-    for (int sx = 0; sx < 2; ++sx)
+  for (int sx = 0; sx < 2; ++sx)
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        float sum = 0.f;
+    for (int u = 0; u < 4; ++u) {
+      float sum = 0.f;
 #pragma unroll
-        for (int l = 0; l < 4; ++l) sum += co[c][sx + 2 * l] * A[v * 4 + l];
-        t[sx][k][v] = sum;
-      }
-    __syncwarp(mask);
-    float px[8];
-#pragma unroll
-    for (int sx = 0; sx < 2; ++sx)
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        float sum = 0.f;
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) sum += A[u * 4 + kk] * t[sx][kk][k];
-        px[4 * sx + u] = sum + iv[c][4 * sx + u];
-      }
-    __syncwarp(mask);
-    if (active) {
-      float* fp = f.filt + c * plane + row;
-      *reinterpret_cast<float4*>(fp) = make_float4(px[0], px[1], px[2], px[3]);
-      *reinterpret_cast<float4*>(fp + 4) =
-          make_float4(px[4], px[5], px[6], px[7]);
+      for (int kk = 0; kk < 4; ++kk) sum += A[u * 4 + kk] * t[sx][kk][k];
+      px[4 * sx + u] = sum + iv[4 * sx + u];
     }
+  if (active && owner) {
+    *reinterpret_cast<float4*>(f.filt + row) =
+        make_float4(px[0], px[1], px[2], px[3]);
+    *reinterpret_cast<float4*>(f.filt + row + 4) =
+        make_float4(px[4], px[5], px[6], px[7]);
   }
 }
 
@@ -2043,8 +2040,9 @@ __global__ void __launch_bounds__(kSmallCtaThreads)
   const int bx = pk & 0xFFFF, by = pk >> 16;
   const int type = f.acs[by * g.Bx + bx] >> 4;
   const ArBlockInfo info = ArInfo(g, f, s, bx, by, type);
+  const float* dm = c == 0 ? info.dm[0] : c == 1 ? info.dm[1] : info.dm[2];
   const float interval =
-      e == 0 ? 1.0f * s.mul_dc[c] : info.dm[c][e] * info.inv_quant_ac;
+      e == 0 ? 1.0f * s.mul_dc[c] : dm[e] * info.inv_quant_ac;
   const size_t o = c * size_t(g.PW) * g.PH +
                    size_t(by * 8 + (e >> 3)) * g.PW + bx * 8 + (e & 7);
   const float iv = f.idct[o];
