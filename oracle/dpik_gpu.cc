@@ -2,7 +2,7 @@
 // from its unmodified sources into oracle/_ref/libpikref_scalar.so) with its
 // reconstruction swapped for libpikgpu at the reference's own function
 // boundaries. Nothing of the reference is copied or patched: this
-// executable defines four of the library's exported functions, and the
+// executable defines five of the library's exported functions, and the
 // dynamic linker binds the library's calls to these definitions (symbol
 // interposition; the library is built with -fPIC and default visibility,
 // so its cross-file calls go through the PLT / GOT). The overrides reach the
@@ -15,10 +15,18 @@
 //    reference's own smoothing for the CPU caches.
 //  * DecodeFromBitstream<true> (pik/compressed_image.cc:720-813, called per
 //    group from the ThreadPool, pik/pik_frame.cc:906-916): runs the
-//    reference's entropy decoding and un-scattering, then -- the first call
-//    under std::call_once -- starts the GPU frame from the decoder's frame
-//    state (pikgpu_frame_begin) and hands the group's int16 coefficients to
-//    the GPU (pikgpu_frame_set_group_ac), from the pool thread.
+//    reference's own, then -- the first call under std::call_once -- starts
+//    the GPU frame from the decoder's frame state (pikgpu_frame_begin) and
+//    hands the group's int16 coefficients to the GPU
+//    (pikgpu_frame_set_group_ac), from the pool thread.
+//  * DecodeAC (pik/entropy_coder.cc:1149, called per 64x64 tile by
+//    DecodeFromBitstream, :775-779): the reference decodes the tile into a
+//    tile-sized buffer that the next tile overwrites, so the hook copies
+//    each decoded tile into the group's coefficient planes, applying the
+//    reference's un-scatter step (:780-801, with its own
+//    AcStrategy::GatherCoefficients) to the copy. The reference's DoAC still
+//    runs on the CPU (it is inlined into DecodeFromBitstream, out of reach
+//    of the dynamic linker); a patched build of the decoder drops it.
 //  * ReconOpsinImage (pik/pik_frame.cc:925-928): skipped; the GPU
 //    reconstructs the whole frame.
 //  * FinalizeFrameDecoding (pik/pik_frame.cc:1149-1152): one
@@ -32,10 +40,16 @@
 // the nearest integer) and accepted only if recomputing DequantDC from the
 // recovered integers reproduces every dequantised value bit for bit.
 //
-// Usage: dpik_gpu in.pik out.f32 [fp32|split_bf16|split_bf16x3] [threads]
+// Usage: dpik_gpu in.pik out.f32 [fp32|split_bf16|split_bf16x3|validate]
+//                 [threads]
 // out.f32: int32 xsize, int32 ysize, then 3 planes of ysize x xsize floats
 // (linear RGB, 0..255 scale, as PikToPixels leaves io.color()). Prints the
-// number of calls each override took.
+// number of calls each override took. `validate` needs no GPU: it builds
+// the frame parameters from the decoder state, recovers the quantised DC
+// and checks them with pikgpu_validate, then stops before the
+// reconstruction (printing "validated" and exiting 0 if they pass); its
+// out.f32 holds int32 Bx, By, the quantised DC (3 x By x Bx int16) and the
+// coefficients the groups would upload (3 x By x Bx * 64 int16).
 
 #include <dlfcn.h>
 #include <math.h>
@@ -49,13 +63,16 @@
 #include <string>
 #include <vector>
 
+#include "pik/ac_strategy.h"
 #include "pik/adaptive_reconstruction.h"
+#include "pik/ans_decode.h"
 #include "pik/block_dictionary.h"
 #include "pik/codec.h"
 #include "pik/color_correlation.h"
 #include "pik/compressed_image.h"
 #include "pik/compressed_image_fwd.h"
 #include "pik/data_parallel.h"
+#include "pik/entropy_coder.h"
 #include "pik/headers.h"
 #include "pik/image.h"
 #include "pik/noise.h"
@@ -78,6 +95,24 @@ std::once_flag g_begin_once;
 int g_begin_rc = 0;
 std::string g_error;
 pik::Image3F g_dc_dequant;  // frame DC after DequantDC
+
+// The group a pool thread is decoding (set by the DecodeFromBitstream hook
+// for the DecodeAC hooks it calls): its block rectangle in the frame, the
+// frame's strategies, and its un-scattered coefficients (3 planes of
+// ysize rows x xsize * 64 int16).
+struct GroupCapture {
+  size_t x0_blocks, y0_blocks, xsize_blocks, ysize_blocks;
+  const pik::FrameDecCache* fdc;
+  std::vector<int16_t> ac[3];
+  pik::Image3S tile;  // scratch for the un-scatter
+};
+thread_local GroupCapture* t_cap = nullptr;
+
+// Validation only: the frame's quantised DC and coefficients as the hooks
+// pass them to the ABI (written to the output file for comparison).
+bool g_validate_only = false;
+std::vector<int16_t> g_qdc, g_frame_ac;
+size_t g_bx = 0, g_by = 0;
 std::atomic<int> g_calls_dc{0}, g_calls_groups{0}, g_calls_recon{0},
     g_calls_finalize{0};
 
@@ -190,7 +225,22 @@ int BeginFrame(const pik::FrameHeader& hd, const pik::Quantizer& quantizer,
   p.raw_quant_field = qf.data();
   p.ar_sigma_lut_ids = lut.data();
   p.quantized_dc = qdc.data();
-  return pikgpu_frame_begin(g_ctx, &p);
+  char msg[256] = {0};
+  if (pikgpu_validate(&p, msg, sizeof(msg)) != PIKGPU_OK) {
+    g_error = std::string("pikgpu_validate: ") + msg;
+    return -1;
+  }
+  if (g_validate_only) {
+    g_qdc = qdc;
+    g_bx = (g_xsize + 7) / 8, g_by = (g_ysize + 7) / 8;
+    g_frame_ac.assign(3 * g_by * g_bx * 64, 0);
+    return 0;
+  }
+  if (pikgpu_frame_begin(g_ctx, &p) != PIKGPU_OK) {
+    g_error = pikgpu_last_error(g_ctx);
+    return -1;
+  }
+  return 0;
 }
 
 }  // namespace
@@ -229,11 +279,20 @@ bool DecodeFromBitstream<true>(
       "MultipassHandlerEmmRKNS_19ColorCorrelationMapESE_PNS_11NoiseParamsE"
       "RKNS_9QuantizerEPNS_13FrameDecCacheEPNS_13GroupDecCacheEPNS_7"
       "PikInfoE"));
-  if (!next(frame_header, header, compressed, reader, group_rect, handler,
-            xsize_blocks, ysize_blocks, cmap, cmap_rect, noise_params,
-            quantizer, frame_dec_cache, group_dec_cache, aux_out)) {
-    return false;
-  }
+  thread_local GroupCapture cap;
+  cap.x0_blocks = group_rect.x0() / kBlockDim;
+  cap.y0_blocks = group_rect.y0() / kBlockDim;
+  cap.fdc = frame_dec_cache;
+  cap.xsize_blocks = xsize_blocks;
+  cap.ysize_blocks = ysize_blocks;
+  for (auto& plane : cap.ac) plane.assign(ysize_blocks * xsize_blocks * 64, 0);
+  t_cap = &cap;
+  const bool ok = next(frame_header, header, compressed, reader, group_rect,
+                       handler, xsize_blocks, ysize_blocks, cmap, cmap_rect,
+                       noise_params, quantizer, frame_dec_cache,
+                       group_dec_cache, aux_out);
+  t_cap = nullptr;
+  if (!ok) return false;
   std::call_once(g_begin_once, [&] {
     g_begin_rc = BeginFrame(frame_header, quantizer, cmap, *frame_dec_cache);
   });
@@ -242,12 +301,90 @@ bool DecodeFromBitstream<true>(
   const uint32_t groups_x = (g_xsize + 511) / 512;
   const uint32_t gi = uint32_t(group_rect.y0() / 512) * groups_x +
                       uint32_t(group_rect.x0() / 512);
-  const Image3S& q = group_dec_cache->quantized_ac;
-  const int16_t* planes[3] = {q.ConstPlaneRow(0, 0), q.ConstPlaneRow(1, 0),
-                              q.ConstPlaneRow(2, 0)};
+  const int16_t* planes[3] = {cap.ac[0].data(), cap.ac[1].data(),
+                              cap.ac[2].data()};
   ++g_calls_groups;
-  return pikgpu_frame_set_group_ac(g_ctx, gi, planes, q.PixelsPerRow()) ==
-         PIKGPU_OK;
+  if (g_validate_only) {
+    for (int c = 0; c < 3; ++c) {
+      for (size_t by = 0; by < ysize_blocks; ++by) {
+        memcpy(g_frame_ac.data() +
+                   ((c * g_by) + cap.y0_blocks + by) * g_bx * 64 +
+                   cap.x0_blocks * 64,
+               planes[c] + by * xsize_blocks * 64,
+               xsize_blocks * 64 * sizeof(int16_t));
+      }
+    }
+    return true;
+  }
+  if (pikgpu_frame_set_group_ac(g_ctx, gi, planes, xsize_blocks * 64) !=
+      PIKGPU_OK) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    g_error = pikgpu_last_error(g_ctx);
+    return false;
+  }
+  return true;
+}
+
+bool DecodeAC(const std::vector<uint8_t>& context_map,
+              const int32_t* PIK_RESTRICT coeff_order,
+              BitReader* PIK_RESTRICT br, ANSSymbolReader* decoder,
+              Image3S* PIK_RESTRICT ac, const Rect& rect,
+              Image3I* PIK_RESTRICT tmp_num_nzeroes) {
+  using Fn = bool (*)(const std::vector<uint8_t>&, const int32_t*,
+                      BitReader*, ANSSymbolReader*, Image3S*, const Rect&,
+                      Image3I*);
+  static const Fn next = reinterpret_cast<Fn>(
+      Next("_ZN3pik8DecodeACERKSt6vectorIhSaIhEEPKiPNS_9BitReaderEPNS_15"
+           "ANSSymbolReaderEPNS_6Image3IsEERKNS_4RectEPNSB_IiEE"));
+  if (!next(context_map, coeff_order, br, decoder, ac, rect,
+            tmp_num_nzeroes)) {
+    return false;
+  }
+  GroupCapture* cap = t_cap;
+  if (!cap) return true;
+  // The tile (rect: block units within the group) sits at the top left of
+  // `ac`. Copy it, un-scatter the copy as the reference does, and place it.
+  const size_t row_len = rect.xsize() * kDCTBlockSize;
+  if (cap->tile.xsize() < ac->xsize() || cap->tile.ysize() < ac->ysize()) {
+    cap->tile = Image3S(ac->xsize(), ac->ysize());
+  }
+  for (int c = 0; c < 3; ++c) {
+    for (size_t by = 0; by < rect.ysize(); ++by) {
+      memcpy(cap->tile.PlaneRow(c, by), ac->ConstPlaneRow(c, by),
+             row_len * sizeof(int16_t));
+    }
+  }
+  const size_t stride = cap->tile.PixelsPerRow();
+  const Rect acs_rect(cap->x0_blocks, cap->y0_blocks, cap->xsize_blocks,
+                      cap->ysize_blocks);
+  SIMD_ALIGN int16_t unscattered[AcStrategy::kMaxCoeffArea];
+  for (int c = 0; c < 3; ++c) {
+    for (size_t by = 0; by < rect.ysize(); ++by) {
+      AcStrategyRow acs_row =
+          cap->fdc->ac_strategy.ConstRow(acs_rect, by + rect.y0());
+      int16_t* PIK_RESTRICT row = cap->tile.PlaneRow(c, by);
+      for (size_t bx = 0; bx < rect.xsize(); ++bx) {
+        AcStrategy acs = acs_row[bx + rect.x0()];
+        if (!acs.IsFirstBlock()) continue;
+        int16_t* block = row + bx * kDCTBlockSize;
+        acs.GatherCoefficients(block, stride, unscattered,
+                               acs.covered_blocks_x() * kDCTBlockSize);
+        for (size_t i = 0; i < acs.covered_blocks_y(); i++) {
+          memcpy(block + stride * i,
+                 unscattered + acs.covered_blocks_x() * kDCTBlockSize * i,
+                 sizeof(int16_t) * acs.covered_blocks_x() * kDCTBlockSize);
+        }
+      }
+    }
+    for (size_t by = 0; by < rect.ysize(); ++by) {
+      memcpy(cap->ac[c].data() +
+                 (rect.y0() + by) * cap->xsize_blocks * kDCTBlockSize +
+                 rect.x0() * kDCTBlockSize,
+             cap->tile.ConstPlaneRow(c, by), row_len * sizeof(int16_t));
+    }
+  }
+  return true;
 }
 
 void ReconOpsinImage(const FrameHeader& frame_header,
@@ -286,6 +423,10 @@ Status FinalizeFrameDecoding(Image3F* PIK_RESTRICT idct, size_t xsize,
   if (xsize != g_xsize || ysize != g_ysize) {
     return PIK_FAILURE("dpik_gpu: image size differs from the header's");
   }
+  if (g_validate_only) {
+    g_error = "validation only";
+    return false;
+  }
   float* rows[3] = {idct->PlaneRow(0, 0), idct->PlaneRow(1, 0),
                     idct->PlaneRow(2, 0)};
   if (pikgpu_reconstruct(g_ctx, rows, idct->PixelsPerRow(), nullptr, 0,
@@ -319,6 +460,8 @@ int main(int argc, char** argv) {
   if (argc > 3 && !strcmp(argv[3], "split_bf16x3")) {
     form = PIKGPU_FORM_SPLIT_BF16X3;
   }
+  const bool validate_only = argc > 3 && !strcmp(argv[3], "validate");
+  g_validate_only = validate_only;
   const int threads = argc > 4 ? atoi(argv[4]) : 8;
 
   // The image size (the file header's), which pikgpu_frame_begin needs
@@ -333,8 +476,9 @@ int main(int argc, char** argv) {
     g_xsize = uint32_t(container.xsize());
     g_ysize = uint32_t(container.ysize());
   }
-  if (pikgpu_ctx_create(0, &g_ctx) != PIKGPU_OK ||
-      pikgpu_set_option(g_ctx, PIKGPU_OPT_FORM, form) != PIKGPU_OK) {
+  if (!validate_only &&
+      (pikgpu_ctx_create(0, &g_ctx) != PIKGPU_OK ||
+       pikgpu_set_option(g_ctx, PIKGPU_OPT_FORM, form) != PIKGPU_OK)) {
     fprintf(stderr, "dpik_gpu: context: %s\n",
             g_ctx ? pikgpu_last_error(g_ctx) : "create failed");
     return 1;
@@ -351,6 +495,20 @@ int main(int argc, char** argv) {
          "ReconOpsinImage %d, FinalizeFrameDecoding %d\n",
          g_calls_dc.load(), g_calls_groups.load(), g_calls_recon.load(),
          g_calls_finalize.load());
+  if (validate_only) {
+    const bool passed = g_begin_rc == 0 && g_calls_finalize.load() == 1;
+    printf("%s%s\n", passed ? "validated" : "not validated: ",
+           passed ? "" : g_error.c_str());
+    if (!passed) return 1;
+    FILE* out = fopen(argv[2], "wb");
+    if (!out) return 2;
+    const int32_t dims[2] = {int32_t(g_bx), int32_t(g_by)};
+    fwrite(dims, sizeof(dims), 1, out);
+    fwrite(g_qdc.data(), sizeof(int16_t), g_qdc.size(), out);
+    fwrite(g_frame_ac.data(), sizeof(int16_t), g_frame_ac.size(), out);
+    fclose(out);
+    return 0;
+  }
   if (!ok) {
     fprintf(stderr, "dpik_gpu: PikToPixels failed: %s\n", g_error.c_str());
     pikgpu_ctx_destroy(g_ctx);
