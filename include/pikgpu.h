@@ -75,7 +75,9 @@ typedef struct pikgpu_frame_params {
   uint32_t predict_lf, predict_hf;
   uint32_t have_adaptive_reconstruction;
   /* EpfParams (pik/epf.h:19-40); used iff have_adaptive_reconstruction. */
-  uint32_t epf_enable_adaptive; /* 0 (fixed sigma) is UNSUPPORTED */
+  /* 0: the fixed-sigma EPF (Filter, pik/epf_target.cc:1342-1386) with
+   * epf_sigma for every block (0: a copy; else within [16, 672]). */
+  uint32_t epf_enable_adaptive;
   uint32_t epf_sigma;
   uint32_t epf_use_sharpened;
 
@@ -121,8 +123,9 @@ const char* pikgpu_last_error(const pikgpu_ctx* ctx);
  * Errors: INVALID_ARG for strategy > 8 (pik/ac_strategy.h:95-97), sub-block
  * indices inconsistent with the strategy, qf outside [1,256]
  * (pik/quantizer.h:125-128), LUT id > 1, dequant_map entries >= the number
- * of tables, offsets past the table; UNSUPPORTED for any FrameHeader flag
- * (noise, gradient map, grayscale, ...) and fixed-sigma EPF. */
+ * of tables, offsets past the table, a fixed sigma outside {0} U [16, 672];
+ * UNSUPPORTED for any FrameHeader flag (noise, gradient map, grayscale,
+ * ...) and for multi-block transforms not aligned to their size. */
 int pikgpu_frame_begin(pikgpu_ctx* ctx, const pikgpu_frame_params* params);
 
 /* Supplies the whole frame's quantized AC after entropy decoding and
