@@ -15,7 +15,7 @@
 //    reference's own smoothing for the CPU caches.
 //  * DecodeFromBitstream<true> (pik/compressed_image.cc:720-813, called per
 //    group from the ThreadPool, pik/pik_frame.cc:906-916): runs the
-//    reference's own, then -- the first call under std::call_once -- starts
+//    reference's own, then -- the first call of the decode, under a mutex -- starts
 //    the GPU frame from the decoder's frame state (pikgpu_frame_begin) and
 //    hands the group's int16 coefficients to the GPU
 //    (pikgpu_frame_set_group_ac), from the pool thread.
@@ -41,10 +41,11 @@
 // recovered integers reproduces every dequantised value bit for bit.
 //
 // Usage: dpik_gpu in.pik out.f32 [fp32|split_bf16|split_bf16x3|validate]
-//                 [threads]
+//                 [threads] [reps]
 // out.f32: int32 xsize, int32 ysize, then 3 planes of ysize x xsize floats
 // (linear RGB, 0..255 scale, as PikToPixels leaves io.color()). Prints the
-// number of calls each override took. `validate` needs no GPU: it builds
+// number of calls each override took, and with reps > 1 the wall time of
+// each PikToPixels call (the output is the last one's). `validate` needs no GPU: it builds
 // the frame parameters from the decoder state, recovers the quantised DC
 // and checks them with pikgpu_validate, then stops before the
 // reconstruction (printing "validated" and exiting 0 if they pass); its
@@ -57,7 +58,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -91,7 +94,8 @@ pikgpu_ctx* g_ctx = nullptr;
 // pikgpu_frame_begin needs it before the decoder reaches
 // FinalizeFrameDecoding, which is the first hook that is given it.
 uint32_t g_xsize = 0, g_ysize = 0;
-std::once_flag g_begin_once;
+std::mutex g_begin_mu;
+bool g_begun = false;  // pikgpu_frame_begin done for the current decode
 int g_begin_rc = 0;
 std::string g_error;
 pik::Image3F g_dc_dequant;  // frame DC after DequantDC
@@ -164,7 +168,11 @@ bool RecoverQuantizedDC(const pik::Quantizer& quantizer,
         out[x] = int16_t(v);
         // DequantDC's arithmetic: q * mul (Y), y_mul * Y + q * mul (X, B).
         const float dq = float(out[x]) * mul_dc[c];
+#if defined(__FMA__)  // the AVX2 flavour's mul_add is fused
+        const float back = c == 1 ? dq : fmaf(y_mul[c], row_y[x], dq);
+#else
         const float back = c == 1 ? dq : y_mul[c] * row_y[x] + dq;
+#endif
         if (memcmp(&back, &row[x], sizeof(float)) != 0) return false;
       }
     }
@@ -293,10 +301,15 @@ bool DecodeFromBitstream<true>(
                        group_dec_cache, aux_out);
   t_cap = nullptr;
   if (!ok) return false;
-  std::call_once(g_begin_once, [&] {
-    g_begin_rc = BeginFrame(frame_header, quantizer, cmap, *frame_dec_cache);
-  });
-  if (g_begin_rc != 0) return false;
+  {
+    std::lock_guard<std::mutex> lock(g_begin_mu);
+    if (!g_begun) {
+      g_begin_rc =
+          BeginFrame(frame_header, quantizer, cmap, *frame_dec_cache);
+      g_begun = true;
+    }
+    if (g_begin_rc != 0) return false;
+  }
   // group_rect: the group's pixels (512x512 groups, row-major).
   const uint32_t groups_x = (g_xsize + 511) / 512;
   const uint32_t gi = uint32_t(group_rect.y0() / 512) * groups_x +
@@ -406,19 +419,11 @@ Status FinalizeFrameDecoding(Image3F* PIK_RESTRICT idct, size_t xsize,
                              PikInfo* aux_out, size_t downsample) {
   ++g_calls_finalize;
   if (downsample != 1) return PIK_FAILURE("dpik_gpu: downsampling");
-  {
-    // A frame whose block dictionary adds dots is not on the GPU path.
-    Image3F probe(idct->xsize(), idct->ysize());
-    ZeroFillImage(&probe);
-    dictionary.AddTo(&probe, 1);
-    for (int c = 0; c < 3; ++c) {
-      for (size_t y = 0; y < probe.ysize(); ++y) {
-        const float* row = probe.ConstPlaneRow(c, y);
-        for (size_t x = 0; x < probe.xsize(); ++x) {
-          if (row[x] != 0.0f) return PIK_FAILURE("dpik_gpu: block dictionary");
-        }
-      }
-    }
+  // A frame whose block dictionary places blocks (dots) is not on the GPU
+  // path. The dictionary's members are private; its encoding equals the
+  // empty dictionary's exactly when it has no entries and no positions.
+  if (dictionary.Encode(nullptr) != BlockDictionary().Encode(nullptr)) {
+    return PIK_FAILURE("dpik_gpu: block dictionary");
   }
   if (xsize != g_xsize || ysize != g_ysize) {
     return PIK_FAILURE("dpik_gpu: image size differs from the header's");
@@ -443,8 +448,8 @@ Status FinalizeFrameDecoding(Image3F* PIK_RESTRICT idct, size_t xsize,
 int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr,
-            "usage: dpik_gpu in.pik out.f32 [fp32|split_bf16|split_bf16x3] "
-            "[threads]\n");
+            "usage: dpik_gpu in.pik out.f32 "
+            "[fp32|split_bf16|split_bf16x3|validate] [threads] [reps]\n");
     return 2;
   }
   FILE* f = fopen(argv[1], "rb");
@@ -489,8 +494,22 @@ int main(int argc, char** argv) {
   pik::DecompressParams dparams;
   std::unique_ptr<pik::ThreadPool> pool;
   if (threads > 0) pool.reset(new pik::ThreadPool(threads));
-  const bool ok = pik::PikToPixels(dparams, compressed, &io, nullptr,
-                                   pool.get());
+  const int reps = argc > 5 ? std::max(1, atoi(argv[5])) : 1;
+  bool ok = true;
+  std::vector<double> ms;
+  for (int r = 0; r < reps && ok; ++r) {
+    g_begun = false;
+    g_calls_dc = g_calls_groups = g_calls_recon = g_calls_finalize = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    ok = pik::PikToPixels(dparams, compressed, &io, nullptr, pool.get());
+    const auto t1 = std::chrono::steady_clock::now();
+    ms.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
+  }
+  if (reps > 1) {
+    printf("PikToPixels ms:");
+    for (double v : ms) printf(" %.3f", v);
+    printf("\n");
+  }
   printf("overrides: AdaptiveDCReconstruction %d, DecodeFromBitstream %d, "
          "ReconOpsinImage %d, FinalizeFrameDecoding %d\n",
          g_calls_dc.load(), g_calls_groups.load(), g_calls_recon.load(),
