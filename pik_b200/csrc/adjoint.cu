@@ -1130,14 +1130,13 @@ int pikgpu_adjoint(pikgpu_ctx* ctx, const float* target, double* loss,
                       sizeof(double), kind, st));
   }
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  if (ctx->form != PIKGPU_FORM_FP32) {
-    int tc_err = 0;
-    CUDA_TRY(ctx, cudaMemcpy(&tc_err, ctx->tc_err.p, sizeof(int),
+  {
+    int code = 0;
+    CUDA_TRY(ctx, cudaMemcpy(&code, ctx->tc_err.p, sizeof(int),
                              cudaMemcpyDeviceToHost));
-    if (tc_err) {
+    if (code) {
       cudaMemset(ctx->tc_err.p, 0, sizeof(int));
-      return Fail(ctx, PIKGPU_ERR_CUDA,
-                  "tensor-core transform: MMA completion wait timed out");
+      return Fail(ctx, PIKGPU_ERR_CUDA, "%s", WaitTimeoutMessage(code));
     }
   }
   ctx->have_result = true;

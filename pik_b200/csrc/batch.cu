@@ -28,8 +28,19 @@ struct pikgpu_batch {
   int chains = 0;  // 0: one branch per frame
   int tc_ctas = kTcCtasPerSm;
   bool exec_valid_for_shape = false;  // the graph was captured with these
+  // The frames' wait-timeout flags, gathered (and cleared) by one kernel
+  // after each replay and read back with one copy.
+  int** flag_ptrs = nullptr;  // device: each frame's flag
+  int* flags = nullptr;       // device: the gathered values
+  int* flags_host = nullptr;  // pinned
   std::string err;
 };
+
+// Copies and clears the frames' wait-timeout flags.
+__global__ void k_gather_flags(int* const* src, int n, int* dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = atomicExch(src[i], 0);
+}
 
 namespace {
 
@@ -144,6 +155,17 @@ int pikgpu_batch_create(int device, int num_frames, pikgpu_batch** out) {
     ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) ==
                    cudaSuccess;
   }
+  if (ok) {
+    std::vector<int*> ptrs;
+    for (auto* ctx : b->frames) ptrs.push_back(P<int>(ctx->tc_err));
+    ok = cudaMalloc(&b->flag_ptrs, sizeof(int*) * num_frames) ==
+             cudaSuccess &&
+         cudaMalloc(&b->flags, sizeof(int) * num_frames) == cudaSuccess &&
+         cudaMallocHost(&b->flags_host, sizeof(int) * num_frames) ==
+             cudaSuccess &&
+         cudaMemcpy(b->flag_ptrs, ptrs.data(), sizeof(int*) * num_frames,
+                    cudaMemcpyHostToDevice) == cudaSuccess;
+  }
   if (!ok) {
     pikgpu_batch_destroy(b);
     return PIKGPU_ERR_CUDA;
@@ -161,6 +183,9 @@ int pikgpu_batch_destroy(pikgpu_batch* b) {
     if (e) cudaEventDestroy(e);
   }
   if (b->fork) cudaEventDestroy(b->fork);
+  if (b->flag_ptrs) cudaFree(b->flag_ptrs);
+  if (b->flags) cudaFree(b->flags);
+  if (b->flags_host) cudaFreeHost(b->flags_host);
   if (b->stream) cudaStreamDestroy(b->stream);
   for (auto* ctx : b->frames) pikgpu_ctx_destroy(ctx);
   delete b;
@@ -215,27 +240,24 @@ int pikgpu_batch_reconstruct(pikgpu_batch* b, float* const* out_linear,
   }
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
   CUDA_TRY_B(b, cudaGraphLaunch(b->exec, st));
+  k_gather_flags<<<Blocks(n, 256), 256, 0, st>>>(b->flag_ptrs, int(n),
+                                                  b->flags);
+  CUDA_TRY_B(b, cudaMemcpyAsync(b->flags_host, b->flags, sizeof(int) * n,
+                                cudaMemcpyDeviceToHost, st));
   CUDA_TRY_B(b, cudaStreamSynchronize(st));
   for (size_t i = 0; i < n; ++i) {
-    pikgpu_ctx* ctx = b->frames[i];
-    if (ctx->form != PIKGPU_FORM_FP32) {
-      int tc_err = 0;
-      CUDA_TRY_B(b, cudaMemcpy(&tc_err, ctx->tc_err.p, sizeof(int),
-                               cudaMemcpyDeviceToHost));
-      if (tc_err) {
-        cudaMemset(ctx->tc_err.p, 0, sizeof(int));
-        return BatchFail(b, PIKGPU_ERR_CUDA, "frame %zu: tensor-core "
-                         "transform: MMA completion wait timed out", i);
-      }
+    if (const int code = b->flags_host[i]) {
+      return BatchFail(b, PIKGPU_ERR_CUDA, "frame %zu: %s", i,
+                       WaitTimeoutMessage(code));
     }
-    ctx->have_result = true;
+    b->frames[i]->have_result = true;
   }
   return PIKGPU_OK;
 }
 
 int pikgpu_batch_launch_count(const pikgpu_batch* b) {
   if (!b) return PIKGPU_ERR_INVALID_ARG;
-  int n = 0;
+  int n = 1;  // k_gather_flags
   for (const auto* ctx : b->frames) n += ctx->launches;
   return n;
 }

@@ -179,7 +179,7 @@ int DcNoAlloc(pikgpu_ctx* ctx, const int16_t* quantized_dc, uint32_t bx,
   sgs.out = sig;
   const EpfDc dco{dc, g.Bx, g.By, half_step[0], half_step[1], half_step[2]};
   EpfLaunch(st, num_sms, PIKGPU_FORM_FP32, dcpad, dcpad, 0, dpw, dph, mm + 8,
-            sgs, nullptr, nullptr, dco);
+            sgs, nullptr, nullptr, dco, /*err=*/nullptr);
   CUDA_TRY(ctx, cudaGetLastError());
   return PIKGPU_OK;
 }

@@ -50,7 +50,11 @@ constexpr int kEpfAligned = kEpfGBytes / 4;  // aligned guide words per row
 constexpr size_t EpfSmemBytes(int th) {
   return size_t(3) * (th + 8) * kEpfGRow * 4 +
          size_t(3) * (th + 10) * kEpfTS * 4 +
-         size_t(3) * (th + 8) * kEpfAligned * 4;
+         size_t(3) * (th + 8) * kEpfAligned * 4 + 16;  // + the TMA mbarrier
+}
+// Bytes of one tile's TMA copy (three planes of TH + 10 rows of kEpfTW).
+__host__ __device__ constexpr uint32_t EpfTileBytes(int th) {
+  return uint32_t(3 * (th + 10) * kEpfTW * 4);
 }
 constexpr size_t kEpfSmemBytes = EpfSmemBytes(kEpfH);
 
@@ -490,24 +494,70 @@ __device__ __forceinline__ void EpfFilterTile(
 // One CTA per 64 x TH tile (1-D grid, row-major tile order). More CTAs
 // than resident slots balance the uneven tiles (copies, border tiles)
 // better than CTAs that loop over tiles.
+//
+// Interior tiles are staged by the Tensor Memory Accelerator when `tmap`
+// is valid (use_tma): one thread issues a 3-D tiled bulk copy
+// (cp.async.bulk.tensor, a tensor map over this GPU's input planes, no
+// multicast) of the tile's rows y0 - 5 .. y0 + TH + 4, columns
+// x0 - 12 .. x0 + 75 of the three planes, straight into `tile` (whose
+// layout is the copy's box), completing on an mbarrier with the byte count.
+// The innermost coordinate x0 - 12 is a multiple of 4 floats (x0 is a
+// multiple of 64), as the copy requires. The wait is bounded: if it runs
+// out, the kernel sets *err = 2 (the host reports the frame as failed) and
+// waits once more, bounded, so that no copy is in flight when the CTA
+// exits. Border tiles, and all tiles without a tensor map, are staged with
+// cp.async (EpfStage).
 template <bool kFma, int TH>
 __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
     k_epf_box(const float* in, const float* guide_src,
               const uint8_t* guide_ovr, int gab, int w, int h,
-              const uint32_t* mm, EpfSigma sgs, float* out, EpfDc dco) {
-  extern __shared__ __align__(16) uint32_t epf_smem[];
+              const uint32_t* mm, EpfSigma sgs, float* out, EpfDc dco,
+              const __grid_constant__ CUtensorMap tmap, int use_tma,
+              int* err) {
+  extern __shared__ __align__(128) uint32_t epf_smem[];
   uint32_t* sg = epf_smem;  // [3][TH + 8][kEpfGRow]
   auto* tile = reinterpret_cast<float(*)[TH + 10][kEpfTS]>(
       epf_smem + 3 * (TH + 8) * kEpfGRow);
   uint32_t* sa = epf_smem + 3 * (TH + 8) * kEpfGRow + 3 * (TH + 10) * kEpfTS;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sa + 3 * (TH + 8) * kEpfAligned);
   const int tiles_x = (w + kEpfW - 1) / kEpfW;
   const int x0 = (blockIdx.x % tiles_x) * kEpfW;
   const int y0 = (blockIdx.x / tiles_x) * TH;
   float amin, mul, stretch;
   GuideParams(mm, &amin, &mul, &stretch);
-  EpfStage<TH>(in, w, h, x0, y0, tile);
+  const uint32_t tile_s = tc::SmemU32(tile), mbar_s = tc::SmemU32(mbar);
+  const bool tma = use_tma && EpfInterior<TH>(w, h, x0, y0) &&
+                   (tile_s & 127u) == 0;
+  if (tma) {
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_s)
+                   : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile(
+          "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+              mbar_s),
+          "r"(EpfTileBytes(TH))
+          : "memory");
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::"
+          "complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(tile_s),
+          "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(x0 - 12), "r"(y0 - 5),
+          "r"(0), "r"(mbar_s)
+          : "memory");
+    }
+  } else {
+    EpfStage<TH>(in, w, h, x0, y0, tile);
+  }
   const int sig = EpfLaneSigma(sgs, stretch, w, h, x0, y0);
-  CpAsyncWaitAll();
+  if (tma) {
+    __syncthreads();  // the mbarrier is initialised before anyone waits
+    // (tc::WaitMma is the bounded mbarrier wait of the tensor-core kernels)
+    if (!tc::WaitMma(mbar_s, 0, tc::kMaxPolls) && threadIdx.x == 0) {
+      atomicExch(err, 2);
+    }
+  } else {
+    CpAsyncWaitAll();
+  }
   EpfFilterTile<kFma, TH>(guide_src, guide_ovr, gab, w, h, amin, mul, sig,
                           out, dco, sg, sa, tile, x0, y0);
 }

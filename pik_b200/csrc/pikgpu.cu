@@ -18,6 +18,9 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "../../include/pikgpu.h"
 #include "recon_kernels.cu"
 #include "tables.cc"
@@ -170,7 +173,7 @@ struct pikgpu_ctx {
   int* tc_err_host = nullptr;
   // pikgpu_reconstruct_async enqueued work that pikgpu_wait has not yet
   // finished (with the tensor-core flag to check).
-  bool pending = false, pending_tc = false;
+  bool pending = false;
 };
 
 namespace {
@@ -459,34 +462,88 @@ void Mark(pikgpu_ctx* ctx, int i) {
 // the kernel); `dco`: the DC image's clamped output instead of `out`.
 // `gab` > 0: the guide is gaborish (that strength) of `in`, computed inside
 // the kernel.
+// The wait that ran out, from the context's timeout flag: 1 from the
+// tensor-core kernels' MMA completion waits, 2 from the EPF's tile copy.
+const char* WaitTimeoutMessage(int code) {
+  return code == 2 ? "EPF: TMA tile copy wait timed out"
+                   : "tensor-core transform: MMA completion wait timed out";
+}
+
+// cuTensorMapEncodeTiled from the driver, found through the runtime's
+// entry-point query (no link-time dependency on libcuda); NULL if the
+// driver has none.
+PFN_cuTensorMapEncodeTiled_v12000 TensorMapEncoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p,
+                                cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      return PFN_cuTensorMapEncodeTiled_v12000(nullptr);
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// The EPF's tile map over the three w x h planes at `in` (boxes of th + 10
+// rows x kEpfTW columns x 3 planes, the layout of k_epf_box's staged tile).
+// False if it cannot be made: no driver entry point, `in` not 16-byte
+// aligned, rows not a multiple of 16 bytes, or the encoder refuses.
+bool EpfTileMap(CUtensorMap* m, const float* in, int w, int h, int th) {
+  const auto enc = TensorMapEncoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(in) & 15) || (w % 4) ||
+      w < kEpfTW || h < th + 10) {
+    return false;
+  }
+  const cuuint64_t dims[3] = {cuuint64_t(w), cuuint64_t(h), 3};
+  const cuuint64_t strides[2] = {cuuint64_t(w) * 4,
+                                 cuuint64_t(w) * cuuint64_t(h) * 4};
+  const cuuint32_t box[3] = {cuuint32_t(kEpfTW), cuuint32_t(th + 10), 3};
+  const cuuint32_t elem[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(in),
+             dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// `err`: the context's wait-timeout flag (k_epf_box's TMA wait sets 2);
+// NULL: no TMA staging.
 void EpfLaunch(cudaStream_t st, int num_sms, int form, const float* in,
                const float* guide_src, int gab, int w, int h,
                const uint32_t* mm, const EpfSigma& sgs, float* out,
-               const uint8_t* guide_ovr, const EpfDc& dco) {
+               const uint8_t* guide_ovr, const EpfDc& dco, int* err) {
   // Images that fill fewer than two CTAs per SM with 32-row tiles (the DC
   // image) take 8-row tiles: four times the CTAs, a quarter of the latency.
   const bool small = Blocks(w, kEpfW) * Blocks(h, kEpfH) < 2 * num_sms;
   const bool fma = form != PIKGPU_FORM_FP32;
   // One CTA per 64 x th tile.
   auto grid = [&](int th) { return Blocks(w, kEpfW) * Blocks(h, th); };
+  const int th = small ? 8 : fma ? 16 : kEpfH;
+  CUtensorMap map;
+  memset(&map, 0, sizeof(map));
+  const int tma = err && EpfTileMap(&map, in, w, h, th) ? 1 : 0;
   if (small) {
     if (fma) {
       k_epf_box<true, 8><<<grid(8), 16 * 8, EpfSmemBytes(8), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco);
+          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
+          err);
     } else {
       k_epf_box<false, 8><<<grid(8), 16 * 8, EpfSmemBytes(8), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco);
+          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
+          err);
     }
   } else {
     if (fma) {
       // 16-row tiles of 256 threads, three CTAs per SM: the cx-major loop
       // of these forms needs ~85 registers.
       k_epf_box<true, 16><<<grid(16), 16 * 16, EpfSmemBytes(16), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco);
+          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
+          err);
     } else {
       k_epf_box<false, kEpfH><<<grid(kEpfH), kEpfThreads, kEpfSmemBytes,
                                 st>>>(in, guide_src, guide_ovr, gab, w, h, mm,
-                                      sgs, out, dco);
+                                      sgs, out, dco, map, tma, err);
     }
   }
 }
@@ -593,7 +650,8 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     const EpfDc dco{f.dc, g.Bx, g.By, ctx->dc_half_step[0],
                     ctx->dc_half_step[1], ctx->dc_half_step[2]};
     EpfLaunch(sd, ctx->num_sms, ctx->form, dcpad, dcpad, 0, dpw, dph, mm_dc,
-              sgs, nullptr, nullptr, dco); ++ctx->launches;
+              sgs, nullptr, nullptr, dco, P<int>(ctx->tc_err));
+    ++ctx->launches;
   }
   Mark(ctx, kTDequant);
   {
@@ -725,7 +783,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     EpfLaunch(st, ctx->num_sms, ctx->form, f.idct, f.idct, gab, g.PW, g.PH,
               mm, sgs, f.filt,
               ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr,
-              EpfDc{}); ++ctx->launches;
+              EpfDc{}, P<int>(ctx->tc_err)); ++ctx->launches;
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_epf.p, f.filt, sizeof(float) * 3 * npx,
                       cudaMemcpyDeviceToDevice, st);
@@ -1374,28 +1432,21 @@ int EnqueueReconstruct(pikgpu_ctx* ctx, float* const out_linear[3],
                                       cudaMemcpyDeviceToHost, ctx->stream));
     }
   }
-  // The tensor-core error flag comes back with the same synchronisation.
-  const bool tc = ctx->form != PIKGPU_FORM_FP32;
-  if (tc) {
-    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->tc_err_host, ctx->tc_err.p,
-                                  sizeof(int), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
-  }
+  // The wait-timeout flag comes back with the same synchronisation.
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->tc_err_host, ctx->tc_err.p, sizeof(int),
+                                cudaMemcpyDeviceToHost, ctx->stream));
   ctx->pending = true;
-  ctx->pending_tc = tc;
   return PIKGPU_OK;
 }
 
 // Waits for the enqueued reconstruction and checks it.
 int FinishReconstruct(pikgpu_ctx* ctx) {
   ctx->pending = false;
-  const bool tc = ctx->pending_tc;
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  if (tc && *ctx->tc_err_host) {
+  if (const int code = *ctx->tc_err_host) {
     *ctx->tc_err_host = 0;
     cudaMemset(ctx->tc_err.p, 0, sizeof(int));
-    return Fail(ctx, PIKGPU_ERR_CUDA,
-                "tensor-core transform: MMA completion wait timed out");
+    return Fail(ctx, PIKGPU_ERR_CUDA, "%s", WaitTimeoutMessage(code));
   }
   if (ctx->profile) {
     for (int i = 0; i < kNumTimed; ++i) {
