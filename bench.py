@@ -358,35 +358,28 @@ def batch_main(args):
 # overlaps the upload and kernels of the next two.
 STREAM_CONTEXTS = 3
 
-ADJ_SHARES = {"DCT": 0.3, "DCT16X16": 0.3, "DCT32X32": 0.2, "DCT4X4": 0.05,
-              "DCT2X2": 0.05, "IDENTITY": 0.04, "LINES": 0.03,
-              "DCT_NOHF": 0.02, "DCT4X4_NOHF": 0.01}
-
-
 def adjoint_main(args):
     """Gradient evaluations of sum((pre_opsin - target)^2) with respect to
     the dequantised AC and the quant field (pikgpu_adjoint: forward pass
-    with the clamp tape, then the backward kernels) on a 1024x1024 frame at
-    distance 1.5 with every block size and the EPF on. Synthetic frame; the
-    target is its own reconstruction plus N(0, 0.01) noise."""
+    with the clamp tape, then the backward kernels) on a 1024x1024 frame
+    encoded by the reference encoder at distance 1.5
+    (tests/golden/c4_1k_d15_frame.npz; EPF on, the encoder's transform mix).
+    The target is the XYB of the frame's source image (the generator image
+    synthetic.ADJOINT_SOURCE through pik_b200.xyb.linear_to_xyb, the
+    encoder's own opsin transform), i.e. the loss an encoder minimises."""
     import ctypes
     import torch
-    from pik_b200 import native, synthetic
+    from pik_b200 import layout, native, synthetic, xyb
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    frame = synthetic.make_frame(1024, 1024, seed=4, qf_median=12.0,
-                                 shares=ADJ_SHARES)
+    frame = layout.Frame.load(os.path.join(ROOT, "tests", "golden",
+                                           "c4_1k_d15_frame.npz"))
     px = frame.xsize * frame.ysize
     by, bx = frame.blocks
-    probe = native.Context(local, keep_stages=True, form=args.form)
-    probe.begin(frame)
-    probe.set_ac()
-    probe.reconstruct()
-    pre = probe.stage("pre_opsin")
-    probe.close()
-    rng = np.random.default_rng(0)
-    target = (pre + rng.normal(0, 0.01, pre.shape)).astype(np.float32)
+    src = dict(synthetic.ADJOINT_SOURCE)
+    img = synthetic.make_image(src.pop("xsize"), src.pop("ysize"), **src)
+    target = xyb.linear_to_xyb(synthetic.srgb8_to_linear255(img))
     stream = torch.cuda.Stream(device=dev)
     ctx = native.Context(local, form=args.form)
     ctx.begin(frame)
@@ -468,10 +461,13 @@ def adjoint_main(args):
             "value": round(px / (ms_adj * 1e-3) / 1e6, 2), "unit": "MP/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms_adj, 4), "higher_is_better": True,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "adjoint1k: 1024x1024 synthetic frame, "
-                       "distance 1.5 (quant field ~12), every block size, "
-                       "gaborish + EPF on",
+            "dtype": "f32",
+            "data": "generator image (seeded, synthetic) encoded by the "
+                    "reference encoder; target = the source's XYB",
+            "config": {"workload": "adjoint1k: 1024x1024 generator image "
+                       "reference-encoded at distance 1.5 (63% DCT16X16, "
+                       "30% DCT32X32, 6% DCT8; gaborish + EPF on), loss "
+                       "sum((pre_opsin - XYB(source))^2)",
                        "form": FORM_NAMES[args.form]},
             "forward_only": {"value": round(px / (ms_fwd * 1e-3) / 1e6, 2),
                              "ms_per_step": round(ms_fwd, 4)},

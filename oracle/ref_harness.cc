@@ -493,6 +493,16 @@ int pikref_encode(const float* planes, int xsize, int ysize, float distance,
 
 void pikref_free(void* p) { free(p); }
 
+// LinearToXyb (pik/opsin_image.cc:34-47), the encoder's opsin transform, on
+// n pixels of planar linear sRGB (0..255): planar XYB out.
+int pikref_linear_to_xyb(const float* lin, size_t n, float* xyb) {
+  for (size_t i = 0; i < n; ++i) {
+    LinearToXyb(lin[i], lin[n + i], lin[2 * n + i], &xyb[i], &xyb[n + i],
+                &xyb[2 * n + i]);
+  }
+  return 0;
+}
+
 // Full reference decode (PikToPixels, pik/pik.cc:92-131) to linear planes
 // (3 * ysize * xsize floats).
 int pikref_decode(const uint8_t* data, size_t size, int num_threads,

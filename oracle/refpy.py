@@ -46,6 +46,7 @@ def lib(flavour: str = "scalar") -> ctypes.CDLL:
     L.pikref_free.argtypes = [P]
     L.pikref_decode.argtypes = [P, ctypes.c_size_t, ctypes.c_int, P,
                                 ctypes.c_size_t]
+    L.pikref_linear_to_xyb.argtypes = [P, ctypes.c_size_t, P]
     L.pikref_frozen_from_bitstream.restype = P
     L.pikref_frozen_from_bitstream.argtypes = [P, ctypes.c_size_t,
                                                ctypes.c_int, ctypes.c_int]
@@ -100,6 +101,15 @@ def encode(linear: np.ndarray, distance: float, *, ar: int = -1,
     data = ctypes.string_at(out, n.value)
     L.pikref_free(out)
     return data
+
+
+def linear_to_xyb(linear: np.ndarray, flavour: str = "scalar") -> np.ndarray:
+    """The reference's LinearToXyb on (3, H, W) linear planes (0..255)."""
+    L = lib(flavour)
+    lin = np.ascontiguousarray(linear, dtype=np.float32)
+    out = np.empty_like(lin)
+    L.pikref_linear_to_xyb(_ptr(lin), lin[0].size, _ptr(out))
+    return out
 
 
 def decode(bitstream: bytes, xsize: int, ysize: int, *, threads: int = 0,

@@ -291,7 +291,53 @@ __device__ __forceinline__ void EpfFilterTile(
   // (bytes 4 wd .. 4 wd + 3 of a row) first, into `sa` (row-major, one
   // row of kEpfAligned words per channel and guide row).
   constexpr int kAligned = kEpfAligned;
-  for (int i = tid; i < 3 * kGH * kAligned; i += kThreads) {
+  // Interior tiles with the smoothed guide: each thread takes a vertical
+  // strip of kStrip words of one channel and column, with its three input
+  // rows rolling down the strip, so that each input row is loaded once and
+  // its pair sums v[i] + v[i + 2] (Sym3's left/right and corner sums) are
+  // formed once for the three output rows that use them. The arithmetic of
+  // each value is Sym3Rows', in its order.
+  constexpr int kStrip = (3 * kGH * kAligned + kThreads - 1) / kThreads;
+  static_assert(kGH % kStrip == 0, "whole strips");
+  constexpr int kStrips = kGH / kStrip;
+  const bool strips = interior && !guide_ovr && gab;
+  if (strips && tid < 3 * kAligned * kStrips) {
+    const int wd = tid % kAligned, c = (tid / kAligned) % 3;
+    const int r0 = (tid / (3 * kAligned)) * kStrip;
+    const int lx = 4 * wd + 4;
+    float t[6], m[6], b[6], ht[4], hm[4], hb[4];
+    auto load = [&](int r, float* v, float* hv) {
+      const float* row = &tile[c][r][lx];
+      const float4 q = *reinterpret_cast<const float4*>(row);
+      v[0] = row[-1];
+      v[1] = q.x, v[2] = q.y, v[3] = q.z, v[4] = q.w;
+      v[5] = row[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) hv[i] = v[i] + v[i + 2];
+    };
+    load(r0, t, ht);
+    load(r0 + 1, m, hm);
+#pragma unroll
+    for (int j = 0; j < kStrip; ++j) {
+      load(r0 + j + 2, b, hb);
+      uint32_t word = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float sum_tb = t[i + 1] + b[i + 1];
+        const float mul0 = m[i + 1] * gw[0];
+        const float x1 = sum_tb + hm[i];
+        const float mul1 = x1 * gw[1] + mul0;
+        const float x2 = ht[i] + hb[i];
+        word |= quant(x2 * gw[2] + mul1) << (8 * i);
+      }
+      sa[(c * kGH + r0 + j) * kAligned + wd] = word;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) t[i] = m[i], m[i] = b[i];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) ht[i] = hm[i], hm[i] = hb[i];
+    }
+  }
+  for (int i = tid; i < 3 * kGH * kAligned && !strips; i += kThreads) {
     const int cr = i / kAligned, wd = i - cr * kAligned;
     const int c = cr / kGH, r = cr - c * kGH;
     const int gy = y0 - 4 + r;

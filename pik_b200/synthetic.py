@@ -186,6 +186,12 @@ def make_frame(xsize: int, ysize: int, *, seed: int = 0,
 # Shares of 8x8 cells per transform type that the reference encoder picks
 # on the generator images (12 sinusoids, 20 rectangles, noise sigma 3,
 # 1024x1024) at distance 0.5.
+# The adjoint workload's source image (make_image arguments): its
+# reference-encoded frame (distance 1.5) is tests/golden/c4_1k_d15_frame.npz,
+# and its XYB (pik_b200.xyb) is the loss target.
+ADJOINT_SOURCE = dict(xsize=1024, ysize=1024, seed=4, sinusoids=12,
+                      rectangles=20, noise_sigma=3)
+
 ENCODER_SHARES_D05 = {
     "DCT16X16": 0.7231, "DCT32X32": 0.2217, "DCT": 0.0528, "DCT4X4": 0.0012,
     "DCT2X2": 0.0012,

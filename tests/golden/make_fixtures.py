@@ -19,6 +19,10 @@ Fixtures (all seeded, reproducible):
                     (seed 0) encoded by the reference encoder at distance 1.0.
   c2_4k_d1_frame.npz  that bitstream decoded to the reconstruction boundary
                     by the reference's own decoding functions (bench input).
+  c4_1k_d15_frame.npz  the adjoint workload's frame: a 1024x1024
+                    generator image (synthetic.ADJOINT_SOURCE) encoded by the reference
+                    encoder at distance 1.5 and decoded to the
+                    reconstruction boundary.
   probes.npz        single-function outputs of the reference: every
                     AcStrategy transform on seeded random blocks, the LLF/LF
                     helpers, EPF weights, the opsin inverse matrix and
@@ -83,6 +87,21 @@ def c2_4k() -> None:
     print("c2_4k_d1: bitstream", len(bs), "bytes")
 
 
+# The adjoint workload's source image (synthetic.ADJOINT_SOURCE): the bench
+# regenerates it and takes its XYB (pik_b200.xyb) as the loss target.
+C4_DISTANCE = 1.5
+
+
+def c4() -> None:
+    src = dict(synthetic.ADJOINT_SOURCE)
+    img = synthetic.make_image(src.pop("xsize"), src.pop("ysize"), **src)
+    bs = refpy.encode(synthetic.srgb8_to_linear255(img), C4_DISTANCE,
+                      threads=8)
+    fz = refpy.Frozen(bs, flavour="scalar")
+    fz.frame().save(os.path.join(HERE, "c4_1k_d15_frame.npz"))
+    print("c4_1k_d15: bitstream", len(bs), "bytes")
+
+
 def probes() -> None:
     L = refpy.lib("scalar")
     rng = np.random.default_rng(7)
@@ -129,6 +148,6 @@ def probes() -> None:
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["c1", "c2_small", "c2_4k", "probes"]
+    which = sys.argv[1:] or ["c1", "c2_small", "c2_4k", "c4", "probes"]
     for w in which:
         globals()[w]()

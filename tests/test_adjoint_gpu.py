@@ -172,6 +172,32 @@ def test_adjoint_1024_distance_1_5():
     finite_differences(frame, n_ac=256, n_qf=64, seed=6)
 
 
+def test_adjoint_reference_encoded_frame_source_target():
+    """The adjoint workload itself: the 1024 x 1024 generator image encoded
+    by the reference encoder at distance 1.5 (tests/golden/
+    c4_1k_d15_frame.npz), with the source image's XYB as the target (the
+    loss an encoder minimises). Full gradient against the FP64 reference."""
+    import os
+    from pik_b200 import layout, xyb
+    from tests import golden_cases
+    frame = layout.Frame.load(os.path.join(golden_cases.GOLDEN,
+                                           "c4_1k_d15_frame.npz"))
+    src = dict(synthetic.ADJOINT_SOURCE)
+    img = synthetic.make_image(src.pop("xsize"), src.pop("ysize"), **src)
+    target = xyb.linear_to_xyb(synthetic.srgb8_to_linear255(img))
+    ctx, dec, pre = forward(frame)
+    try:
+        loss, g_ac, g_qf = ctx.adjoint(target)
+    finally:
+        ctx.close()
+    loss_r, g_ac_r, g_qf_r = reference(frame, target, dec)
+    print(f"loss {loss:.9g} ref {loss_r:.9g} (per pixel "
+          f"{loss / pre[0].size:.3g})")
+    assert abs(loss - loss_r) <= 1e-4 * loss_r
+    compare("grad_ac", g_ac, g_ac_r)
+    compare("grad_qf", g_qf, g_qf_r)
+
+
 def test_own_branches_differ_only_by_branch_flips():
     """With its own clamp branches the FP64 reference gradient differs from
     the CUDA one only on blocks where the two precisions' clamp branches
