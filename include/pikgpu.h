@@ -256,15 +256,17 @@ int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
 #define PIKGPU_OPT_PROFILE 2
 #define PIKGPU_OPT_FORM 3
 #define PIKGPU_OPT_GRAPHS 4
-/* TC_WAIT_POLLS: the tensor-core kernels wait for each batch of MMAs with
- *               a bounded poll of an mbarrier; if the first wait runs out
- *               of polls, the kernel drains the MMAs in flight (a second
- *               bounded wait), stops, and pikgpu_reconstruct fails with
- *               PIKGPU_ERR_CUDA ("MMA completion wait timed out"); the
- *               context stays usable. The value is the first wait's number
- *               of polls: -1 (default) 4194304; 0 makes every first wait
- *               run out at once, which exercises that error path. No
- *               counterpart in the reference. */
+/* TC_WAIT_POLLS: the device's bounded waits on an mbarrier -- the
+ *               tensor-core kernels' wait for each batch of MMAs, and the
+ *               EPF's wait for each tile copied by the Tensor Memory
+ *               Accelerator. If a first wait runs out of polls, the kernel
+ *               drains what is in flight (a second bounded wait), stops,
+ *               and pikgpu_reconstruct fails with PIKGPU_ERR_CUDA ("MMA
+ *               completion wait timed out" / "EPF: TMA tile copy wait
+ *               timed out"); the context stays usable. The value is the
+ *               first wait's number of polls: -1 (default) 4194304; 0
+ *               makes every first wait run out at once, which exercises
+ *               that error path. No counterpart in the reference. */
 #define PIKGPU_OPT_TC_WAIT_POLLS 5
 #define PIKGPU_FORM_FP32 0
 #define PIKGPU_FORM_SPLIT_BF16 1

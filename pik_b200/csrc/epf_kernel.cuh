@@ -548,10 +548,10 @@ __device__ __forceinline__ void EpfFilterTile(
 // x0 - 12 .. x0 + 75 of the three planes, straight into `tile` (whose
 // layout is the copy's box), completing on an mbarrier with the byte count.
 // The innermost coordinate x0 - 12 is a multiple of 4 floats (x0 is a
-// multiple of 64), as the copy requires. The wait is bounded: if it runs
-// out, the kernel sets *err = 2 (the host reports the frame as failed) and
-// waits once more, bounded, so that no copy is in flight when the CTA
-// exits. Border tiles, and all tiles without a tensor map, are staged with
+// multiple of 64), as the copy requires. The wait is bounded (`polls`, the
+// context's PIKGPU_OPT_TC_WAIT_POLLS): if it runs out, the kernel sets
+// *err = 2 (the host reports the frame as failed) and waits once more,
+// bounded, so that no copy is in flight when the CTA exits. Border tiles, and all tiles without a tensor map, are staged with
 // cp.async (EpfStage).
 template <bool kFma, int TH>
 __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
               const uint8_t* guide_ovr, int gab, int w, int h,
               const uint32_t* mm, EpfSigma sgs, float* out, EpfDc dco,
               const __grid_constant__ CUtensorMap tmap, int use_tma,
-              int* err) {
+              int* err, uint32_t polls) {
   extern __shared__ __align__(128) uint32_t epf_smem[];
   uint32_t* sg = epf_smem;  // [3][TH + 8][kEpfGRow]
   auto* tile = reinterpret_cast<float(*)[TH + 10][kEpfTS]>(
@@ -598,7 +598,7 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
   if (tma) {
     __syncthreads();  // the mbarrier is initialised before anyone waits
     // (tc::WaitMma is the bounded mbarrier wait of the tensor-core kernels)
-    if (!tc::WaitMma(mbar_s, 0, tc::kMaxPolls) && threadIdx.x == 0) {
+    if (!tc::WaitMma(mbar_s, 0, polls) && threadIdx.x == 0) {
       atomicExch(err, 2);
     }
   } else {

@@ -507,12 +507,13 @@ bool EpfTileMap(CUtensorMap* m, const float* in, int w, int h, int th) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// `err`: the context's wait-timeout flag (k_epf_box's TMA wait sets 2);
-// NULL: no TMA staging.
+// `err`: the context's wait-timeout flag (k_epf_box's TMA wait sets 2),
+// `polls` the first wait's limit; err NULL: no TMA staging.
 void EpfLaunch(cudaStream_t st, int num_sms, int form, const float* in,
                const float* guide_src, int gab, int w, int h,
                const uint32_t* mm, const EpfSigma& sgs, float* out,
-               const uint8_t* guide_ovr, const EpfDc& dco, int* err) {
+               const uint8_t* guide_ovr, const EpfDc& dco, int* err,
+               uint32_t polls = tc::kMaxPolls) {
   // Images that fill fewer than two CTAs per SM with 32-row tiles (the DC
   // image) take 8-row tiles: four times the CTAs, a quarter of the latency.
   const bool small = Blocks(w, kEpfW) * Blocks(h, kEpfH) < 2 * num_sms;
@@ -527,11 +528,11 @@ void EpfLaunch(cudaStream_t st, int num_sms, int form, const float* in,
     if (fma) {
       k_epf_box<true, 8><<<grid(8), 16 * 8, EpfSmemBytes(8), st>>>(
           in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
-          err);
+          err, polls);
     } else {
       k_epf_box<false, 8><<<grid(8), 16 * 8, EpfSmemBytes(8), st>>>(
           in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
-          err);
+          err, polls);
     }
   } else {
     if (fma) {
@@ -539,11 +540,11 @@ void EpfLaunch(cudaStream_t st, int num_sms, int form, const float* in,
       // of these forms needs ~85 registers.
       k_epf_box<true, 16><<<grid(16), 16 * 16, EpfSmemBytes(16), st>>>(
           in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
-          err);
+          err, polls);
     } else {
       k_epf_box<false, kEpfH><<<grid(kEpfH), kEpfThreads, kEpfSmemBytes,
                                 st>>>(in, guide_src, guide_ovr, gab, w, h, mm,
-                                      sgs, out, dco, map, tma, err);
+                                      sgs, out, dco, map, tma, err, polls);
     }
   }
 }
@@ -650,7 +651,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     const EpfDc dco{f.dc, g.Bx, g.By, ctx->dc_half_step[0],
                     ctx->dc_half_step[1], ctx->dc_half_step[2]};
     EpfLaunch(sd, ctx->num_sms, ctx->form, dcpad, dcpad, 0, dpw, dph, mm_dc,
-              sgs, nullptr, nullptr, dco, P<int>(ctx->tc_err));
+              sgs, nullptr, nullptr, dco, P<int>(ctx->tc_err), ctx->tc_polls);
     ++ctx->launches;
   }
   Mark(ctx, kTDequant);
@@ -783,7 +784,8 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     EpfLaunch(st, ctx->num_sms, ctx->form, f.idct, f.idct, gab, g.PW, g.PH,
               mm, sgs, f.filt,
               ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr,
-              EpfDc{}, P<int>(ctx->tc_err)); ++ctx->launches;
+              EpfDc{}, P<int>(ctx->tc_err), ctx->tc_polls);
+    ++ctx->launches;
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_epf.p, f.filt, sizeof(float) * 3 * npx,
                       cudaMemcpyDeviceToDevice, st);
