@@ -528,12 +528,19 @@ __device__ __forceinline__ void EpfFilterTile(
     }
   }
   if (!inside) return;
+  // The normalisation: an IEEE division in the FP32 form (the reference's
+  // rounding); in the tensor-core forms one reciprocal per row (the weight
+  // sum is in [1, 56]) and a multiply per channel, within 2 ulp.
+  float inv[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) inv[j] = kFma ? __frcp_rn(sw[j]) : 0.f;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
+      const float v = kFma ? ws[c][j] * inv[j] : ws[c][j] / sw[j];
       EpfStore(out, dco, plane, w, c, px, py0 + j,
-               filtered ? ws[c][j] / sw[j] : tile[c][tr0 + j][tc0]);
+               filtered ? v : tile[c][tr0 + j][tc0]);
     }
 }
 
