@@ -151,10 +151,11 @@ struct EpfDc {
 };
 
 // Sigma of this thread's block in the tile at (x0, y0); 0 outside the image.
-__device__ __forceinline__ int EpfLaneSigma(const EpfSigma& s, float stretch,
-                                            int w, int h, int x0, int y0) {
-  const int t = threadIdx.x;
-  const int px = x0 + (t & 31) + 32 * ((t >> 5) & 1), py0 = y0 + 4 * (t >> 6);
+// Sigma of the block holding pixel (px, py0) (0 outside the image); `store`:
+// also write it to s.out.
+__device__ __forceinline__ int EpfBlockSigma(const EpfSigma& s, float stretch,
+                                             int w, int h, int px, int py0,
+                                             bool store) {
   if (px >= w || py0 >= h) return 0;
   const int bi = (py0 >> 3) * (w / 8) + (px >> 3);
   int sg;
@@ -168,8 +169,16 @@ __device__ __forceinline__ int EpfLaneSigma(const EpfSigma& s, float stretch,
   } else {
     sg = SigmaFromQuant(float(s.const_qf), 1.0f, 0, stretch);
   }
-  if (s.out && (px & 7) == 0 && (py0 & 7) == 0) s.out[bi] = sg;
+  if (s.out && store) s.out[bi] = sg;
   return sg;
+}
+
+__device__ __forceinline__ int EpfLaneSigma(const EpfSigma& s, float stretch,
+                                            int w, int h, int x0, int y0) {
+  const int t = threadIdx.x;
+  const int px = x0 + (t & 31) + 32 * ((t >> 5) & 1), py0 = y0 + 4 * (t >> 6);
+  return EpfBlockSigma(s, stretch, w, h, px, py0,
+                       (px & 7) == 0 && (py0 & 7) == 0);
 }
 
 // Stores the value of channel c at pixel (px, y) of the tile's output.
@@ -200,13 +209,13 @@ __device__ __forceinline__ bool EpfInterior(int w, int h, int x0, int y0) {
 // the three planes into `tile` by asynchronous copies: 16 bytes each for
 // interior tiles, 4 bytes per mirrored coordinate at the image border. The
 // caller commits them and waits.
-template <int TH>
+template <int TH, int NT = 16 * TH>
 __device__ __forceinline__ void EpfStage(const float* in, int w, int h, int x0,
                                          int y0,
-                                         float (*tile)[TH + 10][kEpfTS]) {
-  constexpr int kTH = TH + 10, kThreads = 16 * TH;
+                                         float (*tile)[TH + 10][kEpfTS],
+                                         int tid) {
+  constexpr int kTH = TH + 10, kThreads = NT;
   const size_t plane = size_t(w) * h;
-  const int tid = threadIdx.x;
   if (EpfInterior<TH>(w, h, x0, y0)) {
     constexpr int Q = kEpfTW / 4;
     for (int i = tid; i < 3 * kTH * Q; i += kThreads) {
@@ -226,47 +235,18 @@ __device__ __forceinline__ void EpfStage(const float* in, int w, int h, int x0,
   }
 }
 
-// Filters the staged tile at (x0, y0) into `out` (or, for the DC image,
-// into dco's clamp). The tile's copies are complete in every thread (the
-// first barrier below publishes them); `sig` is EpfLaneSigma of this
-// thread; (amin, mul) quantise the guide
-// (GuideParams). `sa` holds the aligned guide words while the guide is
-// built. Returns after the tile's last barrier.
-//
-// kFma: the weighted sums with fused multiply-adds (the tensor-core forms,
-// which are not bound to the reference's rounding); otherwise every product
-// and sum is rounded separately, as the reference does.
-template <bool kFma, int TH>
-__device__ __forceinline__ void EpfFilterTile(
-    const float* guide_src, const uint8_t* guide_ovr, int gab, int w, int h,
-    float amin, float mul, int sig, float* out, const EpfDc& dco,
-    uint32_t* sg, uint32_t* sa, float (*tile)[TH + 10][kEpfTS], int x0,
-    int y0) {
+// Builds the tile's u8 guide (MakeGuide, pik/epf_target.cc:1009-1070) in
+// shared memory: the aligned words into `sa`, then one word per byte offset
+// into `sg`. NT threads take part (this thread is `tid` of them), and
+// `sync` is their barrier; the tile's copies are complete and published.
+// Returns after the last barrier.
+template <int TH, int NT, typename Sync>
+__device__ __forceinline__ void EpfBuildGuide(
+    int tid, Sync sync, const float* guide_src, const uint8_t* guide_ovr,
+    int gab, int w, int h, float amin, float mul, uint32_t* sg, uint32_t* sa,
+    float (*tile)[TH + 10][kEpfTS], int x0, int y0) {
   constexpr int kGH = TH + 8, kTH = TH + 10;
-  constexpr int kGPlane = kGH * kEpfGRow, kThreads = 16 * TH;
-  const int tid = threadIdx.x;
-  const int lane = tid & 31, wp = tid >> 5;
-  // 4-row band of the warp and its first column (tile-local).
-  const int band = wp >> 1, col0 = 32 * (wp & 1);
   const size_t plane = size_t(w) * h;
-  const int px = x0 + lane + col0, py0 = y0 + 4 * band;
-  const bool inside = px < w && py0 < h;  // w and h are multiples of 8
-  const bool filtered = sig >= kMinSigma;
-  // Tile position of the pixel (px, py0).
-  const int tr0 = 4 * band + 3 + kEpfTRow0, tc0 = lane + col0 + 3 + kEpfTCol0;
-
-  // Tiles without filtered blocks are copies (CopyOriginalBlock).
-  if (!__syncthreads_or(filtered)) {
-    if (inside) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          EpfStore(out, dco, plane, w, c, px, py0 + j, tile[c][tr0 + j][tc0]);
-    }
-    return;
-  }
-
   const bool interior = EpfInterior<TH>(w, h, x0, y0);
   const float* gw = c_t.gaborish[gab];
   auto quant = [&](float v) {
@@ -297,7 +277,7 @@ __device__ __forceinline__ void EpfFilterTile(
   // its pair sums v[i] + v[i + 2] (Sym3's left/right and corner sums) are
   // formed once for the three output rows that use them. The arithmetic of
   // each value is Sym3Rows', in its order.
-  constexpr int kStrip = (3 * kGH * kAligned + kThreads - 1) / kThreads;
+  constexpr int kStrip = (3 * kGH * kAligned + NT - 1) / NT;
   static_assert(kGH % kStrip == 0, "whole strips");
   constexpr int kStrips = kGH / kStrip;
   const bool strips = interior && !guide_ovr && gab;
@@ -337,7 +317,7 @@ __device__ __forceinline__ void EpfFilterTile(
       for (int i = 0; i < 4; ++i) ht[i] = hm[i], hm[i] = hb[i];
     }
   }
-  for (int i = tid; i < 3 * kGH * kAligned && !strips; i += kThreads) {
+  for (int i = tid; i < 3 * kGH * kAligned && !strips; i += NT) {
     const int cr = i / kAligned, wd = i - cr * kAligned;
     const int c = cr / kGH, r = cr - c * kGH;
     const int gy = y0 - 4 + r;
@@ -393,10 +373,10 @@ __device__ __forceinline__ void EpfFilterTile(
     }
     sa[i] = word;
   }
-  __syncthreads();
+  sync();
   // The words of offsets 4 wd .. 4 wd + 3 from the two aligned neighbours
   // (bytes past the row end read as 0), one 16-byte store each.
-  for (int i = tid; i < 3 * kGH * kAligned; i += kThreads) {
+  for (int i = tid; i < 3 * kGH * kAligned; i += NT) {
     const int cr = i / kAligned, wd = i - cr * kAligned;
     const uint32_t lo = sa[i];
     const uint32_t hi = wd + 1 < kAligned ? sa[i + 1] : 0u;
@@ -404,7 +384,28 @@ __device__ __forceinline__ void EpfFilterTile(
         make_uint4(lo, __funnelshift_r(lo, hi, 8), __funnelshift_r(lo, hi, 16),
                    __funnelshift_r(lo, hi, 24));
   }
-  __syncthreads();
+  sync();
+
+}
+
+// Filters the tile from its staged input and guide (this thread's pixels:
+// `tid` < 16 TH of the tile's filtering threads), with `sig` the sigma of
+// this thread's block, and stores the result. No CTA barrier.
+template <bool kFma, int TH>
+__device__ __forceinline__ void EpfFilterCore(
+    int tid, int sig, float* out, const EpfDc& dco, int w, int h,
+    const uint32_t* sg, float (*tile)[TH + 10][kEpfTS], int x0, int y0) {
+  constexpr int kGH = TH + 8;
+  constexpr int kGPlane = kGH * kEpfGRow;
+  const int lane = tid & 31, wp = tid >> 5;
+  // 4-row band of the warp and its first column (tile-local).
+  const int band = wp >> 1, col0 = 32 * (wp & 1);
+  const size_t plane = size_t(w) * h;
+  const int px = x0 + lane + col0, py0 = y0 + 4 * band;
+  const bool inside = px < w && py0 < h;  // w and h are multiples of 8
+  const bool filtered = sig >= kMinSigma;
+  // Tile position of the pixel (px, py0).
+  const int tr0 = 4 * band + 3 + kEpfTRow0, tc0 = lane + col0 + 3 + kEpfTCol0;
 
   // Warps (half a block row of 8 blocks) without filtered blocks copy.
   if (!__any_sync(0xFFFFFFFFu, filtered)) {
@@ -544,6 +545,46 @@ __device__ __forceinline__ void EpfFilterTile(
     }
 }
 
+// Filters the staged tile at (x0, y0) into `out` (or, for the DC image,
+// into dco's clamp), with every thread of the CTA: the guide, then the
+// filter. The tile's copies are complete in every thread (the first
+// barrier below publishes them); `sig` is EpfLaneSigma of this thread;
+// (amin, mul) quantise the guide (GuideParams). `sa` holds the aligned
+// guide words while the guide is built.
+//
+// kFma: the weighted sums with fused multiply-adds (the tensor-core forms,
+// which are not bound to the reference's rounding); otherwise every product
+// and sum is rounded separately, as the reference does.
+template <bool kFma, int TH>
+__device__ __forceinline__ void EpfFilterTile(
+    const float* guide_src, const uint8_t* guide_ovr, int gab, int w, int h,
+    float amin, float mul, int sig, float* out, const EpfDc& dco,
+    uint32_t* sg, uint32_t* sa, float (*tile)[TH + 10][kEpfTS], int x0,
+    int y0) {
+  const int tid = threadIdx.x;
+  // Tiles without filtered blocks are copies (CopyOriginalBlock).
+  if (!__syncthreads_or(sig >= kMinSigma)) {
+    const int lane = tid & 31, wp = tid >> 5;
+    const int band = wp >> 1, col0 = 32 * (wp & 1);
+    const size_t plane = size_t(w) * h;
+    const int px = x0 + lane + col0, py0 = y0 + 4 * band;
+    const int tr0 = 4 * band + 3 + kEpfTRow0;
+    const int tc0 = lane + col0 + 3 + kEpfTCol0;
+    if (px < w && py0 < h) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          EpfStore(out, dco, plane, w, c, px, py0 + j, tile[c][tr0 + j][tc0]);
+    }
+    return;
+  }
+  EpfBuildGuide<TH, 16 * TH>(tid, [] { __syncthreads(); }, guide_src,
+                             guide_ovr, gab, w, h, amin, mul, sg, sa, tile,
+                             x0, y0);
+  EpfFilterCore<kFma, TH>(tid, sig, out, dco, w, h, sg, tile, x0, y0);
+}
+
 // One CTA per 64 x TH tile (1-D grid, row-major tile order). More CTAs
 // than resident slots balance the uneven tiles (copies, border tiles)
 // better than CTAs that loop over tiles.
@@ -599,7 +640,7 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
           : "memory");
     }
   } else {
-    EpfStage<TH>(in, w, h, x0, y0, tile);
+    EpfStage<TH>(in, w, h, x0, y0, tile, threadIdx.x);
   }
   const int sig = EpfLaneSigma(sgs, stretch, w, h, x0, y0);
   if (tma) {
