@@ -147,7 +147,13 @@ int pikgpu_frame_set_group_ac(pikgpu_ctx* ctx, uint32_t group_index,
                               const int16_t* const planes[3], size_t stride);
 
 /* Device-resident variant of pikgpu_frame_set_ac: `planes` are device
- * pointers on the context's device; no host copy is made. */
+ * pointers on the context's device; no host copy is made. Planes in the
+ * context's own layout -- stride Bx * 64, the three planes consecutive
+ * (planes[c] = planes[0] + c * By * Bx * 64), planes[0] 16-byte aligned --
+ * are read in place by every later pikgpu_reconstruct of this frame (no
+ * device copy either): they must stay valid until the last reconstruction
+ * that uses them has completed, and changing their contents between calls
+ * changes the next result. Other layouts are copied into the context. */
 int pikgpu_frame_set_ac_device(pikgpu_ctx* ctx, const int16_t* const planes[3],
                                size_t stride);
 

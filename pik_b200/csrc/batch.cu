@@ -92,7 +92,8 @@ int Capture(pikgpu_batch* b, float* const* out, const size_t* strides) {
     cudaStream_t user = ctx->stream;
     ctx->stream = b->frames[i % k]->own_stream;
     ctx->tc_ctas_per_sm = b->tc_ctas;
-    rc = LaunchAll(ctx, out[i], strides[i], nullptr, 0);
+    rc = LaunchAll(ctx, out[i], strides[i], nullptr, 0,
+                   /*single_stream=*/true);
     if (rc != PIKGPU_OK) BatchFail(b, rc, "frame %zu: %s", i, ctx->err.c_str());
     ctx->stream = user;
   }

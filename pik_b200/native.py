@@ -189,6 +189,13 @@ class Context:
         self._check(self.L.pikgpu_frame_set_ac(self.h, _planes(a),
                                                a.shape[-1]))
 
+    def set_ac_device(self, plane_ptrs, stride: int) -> None:
+        """pikgpu_frame_set_ac_device: three device pointers (int16 planes
+        of By rows, `stride` elements apart). The context's own layout is
+        read in place by later reconstructions; others are copied."""
+        planes = (ctypes.c_void_p * 3)(*plane_ptrs)
+        self._check(self.L.pikgpu_frame_set_ac_device(self.h, planes, stride))
+
     def set_group_ac(self, group: int, planes: np.ndarray) -> None:
         a = np.ascontiguousarray(planes, np.int16)
         self._check(self.L.pikgpu_frame_set_group_ac(self.h, group,
