@@ -620,10 +620,10 @@ struct LfGroup {
   }
 };
 
-constexpr int kLfTile = 32;           // cells per tile side
+constexpr int kLfTile = 16;           // cells per tile side
 constexpr int kLfWin = kLfTile + 12;  // shared-memory window, cells
 constexpr int kLfWin2 = 2 * kLfWin;   // the 2x2 images' window, pixels
-constexpr int kLfThreads = 256;
+constexpr int kLfThreads = 128;
 // Shared memory of k_lf_tile: the LLF image, the 2x2 image before and after
 // LFPredictionBlur, over the window, and the list of the window's first
 // cells (by block size: 8x8-class blocks, then 16x16, then 32x32).
@@ -755,7 +755,7 @@ __device__ void LfUpdateBlock(const Geo& g, const DevFrame& f,
 // reads cells lo - 1 .. hi), then the blur and LowFrequenciesFromDC2x2 over
 // [lo, hi) -- the tile plus the ring cells beside it -- then the ring's
 // pred2x2 and the update of the tile's blocks.
-__global__ void __launch_bounds__(kLfThreads, 2)
+__global__ void __launch_bounds__(kLfThreads, 4)
     k_lf_tile(Geo g, DevFrame f, int predict_lf, int predict_hf) {
   extern __shared__ float lf_smem[];
   LfGroup q;
