@@ -18,7 +18,8 @@ groups + FinalizeFrameDecoding.
          memory and reads the FP32 linear planes back; three contexts take
          the frames in turn with the non-blocking call, so one frame's
          copies overlap the other's kernels (the blocking one-context figure
-         is "e2e_blocking").
+         is "e2e_blocking"; "e2e_srgb8" reads back the 8-bit sRGB output
+         instead).
 
 `--impl reference` times the reference's own CPU implementation (built from
 its sources into oracle/_ref/, AVX2 flavour, all host threads) on the same
@@ -924,6 +925,36 @@ def main():
     stream_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     stream_ms = max_over_ranks(stream_ms, dev)
     e2e = ws * px / (stream_ms * 1e-3) / 1e6
+
+    # The same streaming run with the 8-bit sRGB output only (interleaved
+    # RGB bytes, ExternalImage::CopyTo's rounding: what dpik writes to an
+    # 8-bit PPM) read back instead of the linear float planes.
+    pin_rgbs = [torch.empty((frame.ysize, frame.xsize, 3),
+                            dtype=torch.uint8).pin_memory()
+                for _ in range(STREAM_CONTEXTS)]
+
+    def stream_step8(i):
+        c = ctxs[i % STREAM_CONTEXTS]
+        c.wait()
+        c._check(c.L.pikgpu_frame_begin(c.h, packed.ref))
+        c._check(c.L.pikgpu_frame_set_ac(c.h, ac_planes, bx * 64))
+        c.reconstruct_async(None, 0, pin_rgbs[i % STREAM_CONTEXTS].data_ptr(),
+                            3 * frame.xsize)
+
+    for i in range(max(3, args.warmup)):
+        stream_step8(i)
+    for c in ctxs:
+        c.wait()
+    if ws > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        stream_step8(i)
+    for c in ctxs:
+        c.wait()
+    stream8_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    stream8_ms = max_over_ranks(stream8_ms, dev)
+    e2e8 = ws * px / (stream8_ms * 1e-3) / 1e6
     for c in ctxs:
         c.close()
 
@@ -932,7 +963,7 @@ def main():
     # DRAM bytes per launch of the 4K workload measured with ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum, one cold launch each).
     ncu_traffic_4k = {
-        "epf": 100.51e6 + 63.73e6,
+        "epf": 100.38e6 + 63.28e6,
         "gaborish1_minmax": 99.54e6 + 64.64e6,
         "gaborish2_opsin_srgb": 99.55e6 + 63.85e6,
     }
@@ -1000,6 +1031,12 @@ def main():
             "e2e_blocking": {"value": round(e2e_blocking, 2), "unit": "MP/s",
                              "mode": "one context, blocking "
                                      "pikgpu_reconstruct per frame"},
+            "e2e_srgb8": {"value": round(e2e8, 2), "unit": "MP/s",
+                          "h2d_bytes_per_step": int(h2d),
+                          "d2h_bytes_per_step": int(3 * px),
+                          "mode": "as e2e, with the 8-bit sRGB output (what "
+                                  "dpik writes to an 8-bit PPM) read back "
+                                  "instead of the linear planes"},
             "gpu_launches": launches * args.steps,
             "clocks": clocks,
             "cpu_baseline": cpu_baseline(px) if ws == 1 else None,
