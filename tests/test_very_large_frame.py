@@ -13,19 +13,25 @@ generator, through the C ABI.
 - On its own decisions, as a decoder runs it, the split-BF16 form stays
   within 2e-5 of the FP32 form at the 99.999th percentile, with at most
   5e-5 of the values beyond (an isolated guide byte, sigma or clamp branch
-  can flip)."""
+  can flip).
+
+The FP64 oracle of this frame holds about 10 GB of host memory, so the
+check runs in a child process of its own (its memory is returned when it
+exits, whatever the test session holds) and compares the outputs one
+channel at a time."""
+
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
-
-from oracle import decisions, oraclepy
-from pik_b200 import native, synthetic
-from tests.test_split_bf16 import lsb_error
 
 pytestmark = pytest.mark.gpu
 
 
 def _run(frame, form, guide=None, sigma=None, tape=None, record=False):
+    from pik_b200 import native
     ctx = native.Context(0, form=form, keep_stages=record)
     try:
         ctx.begin(frame)
@@ -42,24 +48,34 @@ def _run(frame, form, guide=None, sigma=None, tape=None, record=False):
         ctx.close()
 
 
-@pytest.mark.timeout(1200)
-def test_8192_frame_fp32_bitexact_and_split_bf16_bounded():
+def check_8192() -> None:
+    """The whole check (run in the child process)."""
+    from oracle import decisions, oraclepy
+    from pik_b200 import synthetic
+    from tests import golden_cases
     frame = synthetic.make_highlight_frame(8192, 8192, seed=5)
     lin, rgb, guide, sigma, tape = _run(frame, "fp32", record=True)
     o = oraclepy.run(frame, precision=32, want=("linear", "srgb8"),
                      export_decisions=True)
     np.testing.assert_array_equal(guide, o["guide"])
     np.testing.assert_array_equal(sigma, o["sigma"])
-    np.testing.assert_array_equal(lin, o["linear"])
+    for c in range(3):
+        np.testing.assert_array_equal(lin[c], o["linear"][c])
     np.testing.assert_array_equal(rgb, o["srgb8"])
-    del o
+    del o, rgb
     # Own decisions against the FP32 form.
     tc = _run(frame, "split_bf16")[0]
-    d = np.abs(tc - lin) / 255
+    d = np.empty(lin.shape, np.float32)
+    for c in range(3):
+        np.subtract(tc[c], lin[c], out=d[c])
+    np.abs(d, out=d)
+    d *= np.float32(1 / 255)
+    q = float(np.quantile(d, 0.99999))
+    share = float((d > 2e-5).mean())
     print(f"8192x8192 split-BF16 vs FP32 form (own decisions): max "
-          f"{d.max():.3g}, share > 2e-5: {(d > 2e-5).mean():.3g}")
-    assert np.quantile(d, 0.99999) <= 2e-5
-    assert (d > 2e-5).mean() <= 5e-5
+          f"{float(d.max()):.3g}, share > 2e-5: {share:.3g}")
+    assert q <= 2e-5
+    assert share <= 5e-5
     del tc, d
     # Shared decisions against FP64.
     tc, tc_rgb = _run(frame, "split_bf16", guide, sigma, tape)[:2]
@@ -67,11 +83,29 @@ def test_8192_frame_fp32_bitexact_and_split_bf16_bounded():
     o64 = oraclepy.run(frame, precision=64, want=("linear",), guide=guide,
                        sigma=sigma, dc_guide=dg, dc_sigma=ds,
                        clamp_tape=tape)["linear"]
-    err_tc = np.abs(tc - o64) / 255
-    err_fp32 = np.abs(lin - o64) / 255
-    lsb = lsb_error(tc_rgb, o64)
+    err_tc = err_fp32 = 0.0
+    lsb = 0
+    for c in range(3):
+        err_tc = max(err_tc, float(np.abs(tc[c] - o64[c]).max()) / 255)
+        err_fp32 = max(err_fp32, float(np.abs(lin[c] - o64[c]).max()) / 255)
+        exact = golden_cases.srgb8_exact(o64[c])
+        lsb = max(lsb, int(np.abs(tc_rgb[:, :, c].astype(np.int32) -
+                                  exact).max()))
+        del exact
     print(f"8192x8192 vs FP64 (shared decisions): split-BF16 max "
-          f"{err_tc.max():.3g}, FP32 form max {err_fp32.max():.3g}, "
-          f"sRGB-8 max {int(lsb.max())} LSB")
-    assert err_tc.max() <= 2e-5
-    assert lsb.max() <= 1
+          f"{err_tc:.3g}, FP32 form max {err_fp32:.3g}, "
+          f"sRGB-8 max {lsb} LSB")
+    assert err_tc <= 2e-5
+    assert lsb <= 1
+
+
+@pytest.mark.timeout(1300)
+def test_8192_frame_fp32_bitexact_and_split_bf16_bounded():
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, PYTHONPATH=root)
+    r = subprocess.run(
+        [sys.executable, "-c",
+         "from tests.test_very_large_frame import check_8192; check_8192()"],
+        capture_output=True, text=True, timeout=1200, cwd=root, env=env)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr[-3000:]
