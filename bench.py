@@ -55,7 +55,7 @@ PATH_BYTES_PER_PX = 18.28
 # dram__bytes_write.sum) of all the frame's 17 launches, run one after
 # another with the caches kept between them (profiles/traffic_c2_4k.md).
 EPF_WARP_INSTR_4K = 175.5e6
-PATH_TRAFFIC_4K = 834.1e6
+PATH_TRAFFIC_4K = 835.2e6
 # Algorithmic bytes per pixel of each kernel group (PIKGPU_OPT_PROFILE
 # groups), with 4-byte floats.
 GROUP_BYTES = {
