@@ -48,6 +48,25 @@ __host__ __device__ inline int MirrorIdx(int x, int size) {
   return x;
 }
 
+// Programmatic dependent launch (PTX griddepcontrol, sm_90 and later). The
+// transform classes, and the clamp classes, run as a chain of kernels on
+// one stream, each launched as a programmatic dependent of the one before
+// it: a dependent may start once every CTA of its predecessor has executed
+// PdlLaunchDependents (or exited), which the chain kernels do first thing.
+// The classes write disjoint blocks, so the one order kept is completion:
+// PdlTail, declared at the top of a chain kernel, waits for the
+// predecessor's completion (and the visibility of its writes) on every
+// return path, so the chain's last kernel completes after all of them.
+// Both instructions do nothing in a launch without such a dependency.
+__device__ __forceinline__ void PdlLaunchDependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+struct PdlTail {
+  __device__ __forceinline__ ~PdlTail() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+  }
+};
+
 // Frame geometry.
 struct Geo {
   int W, H;       // pixels

@@ -581,14 +581,51 @@ struct Branches {
   }
 };
 
+// The transform classes other than DCT8 (and later their clamps) as one
+// chain of kernels on one stream. Each kernel after the first is launched
+// as a programmatic dependent of the one before it
+// (cudaLaunchAttributeProgrammaticStreamSerialization): it may start once
+// every CTA of its predecessor has begun, and it waits for the
+// predecessor's completion before it exits (PdlLaunchDependents and
+// PdlTail in the kernels). The first is an ordinary launch, so the chain
+// starts after everything before it. Launched in the order given, the
+// few-block classes are resident before the persistent tensor-core kernels
+// take the SMs, in a graph replay too, whose branches start in an order of
+// the runtime's choosing.
+struct ClassChain {
+  cudaStream_t st;
+  int* launches;
+  bool started = false;
+  cudaError_t err = cudaSuccess;
+  template <typename... KArgs, typename... Args>
+  void operator()(void (*kernel)(KArgs...), int grid, int block, size_t smem,
+                  Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr = {};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = started ? &attr : nullptr;
+    cfg.numAttrs = started ? 1 : 0;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+    if (e != cudaSuccess && err == cudaSuccess) err = e;
+    started = true;
+    ++*launches;
+  }
+};
+
 // The launch sequence of one frame. Its DAG:
-//   side 0: DC dequant, DC EPF and clamp, then the per-group LF prediction
+//   side 0: DC dequant, DC EPF and clamp
 //   main:   AC dequantisation            (both from the inputs only)
 //   main:   LLF / LF update, pred2x2      (joins the two)
-//   main + sides: the inverse transforms, one transform class each (their
+//   main:   the DCT8 inverse transforms, beside
+//   side 0: the other classes' inverse transforms (ClassChain; the classes'
 //           blocks are disjoint)
 //   main:   gaborish minmax, sigma, EPF
-//   main + sides: the clamp, one transform class each
+//   main + side 0: the clamp, split the same way
 //   main:   gaborish #2, opsin, outputs
 //
 // `single_stream`: everything on the main stream (the events become no-ops).
@@ -634,9 +671,6 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     L[k] = P<uint32_t>(ctx->list[k]);
     n[k] = int(ctx->lists[k].size());
   }
-  // Side stream of each transform class's branch (the main stream takes
-  // DCT8, usually the most blocks).
-  auto cls = [&](int k) { return k == kC8 ? st : br[k - 1]; };
 
   ctx->launches = 0;
   ctx->smoothed_valid = false;
@@ -692,31 +726,36 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
               kLfSmemBytes, st>>>(g, f, s.predict_lf, s.predict_hf);
   ++ctx->launches;
   Mark(ctx, kTIdct);
-  br.Fork(1, ctx->kSide);
+  br.Fork(1, 1);
   {
     auto rows_grid = [](int items, int n) {
       const int upw = 32 / n;
       const int warps = (items + upw - 1) / upw;
       return (warps * 32 + kSquareThreads - 1) / kSquareThreads;
     };
-    // The classes with few blocks first, so that their CTAs are resident
-    // before the persistent tensor-core kernel fills the SMs (which takes
-    // its work from a counter and leaves those SMs' share to the others).
-    if (n[kCSmall]) {
-      if (n[kCSmall] <= kSmallCtaMax * ctx->num_sms) {
-        k_small_idct_cta<<<n[kCSmall], kSmallCtaThreads, 0, cls(kCSmall)>>>(
-            g, f, L[kCSmall], n[kCSmall]);
-      } else {
-        k_small_idct<<<Blocks(3 * n[kCSmall], kSmallIdctThreads),
-                       kSmallIdctThreads, 0, cls(kCSmall)>>>(
-            g, f, L[kCSmall], n[kCSmall]);
-      }
+    // DCT8 on the main stream; the other classes as one chain on a side
+    // stream, the classes with few blocks first, so that their CTAs are
+    // resident before the persistent tensor-core kernels fill the SMs
+    // (which take their work from a counter and leave those SMs' share to
+    // the others).
+    if (n[kC8]) {
+      k_square_idct_rows<8><<<rows_grid(3 * n[kC8], 8), kSquareThreads, 0,
+                              st>>>(g, f, L[kC8], n[kC8], s.predict_hf);
       ++ctx->launches;
     }
+    ClassChain ch{br[0], &ctx->launches};
+    if (n[kCSmall]) {
+      if (n[kCSmall] <= kSmallCtaMax * ctx->num_sms) {
+        ch(k_small_idct_cta, n[kCSmall], kSmallCtaThreads, 0, g, f,
+           L[kCSmall], n[kCSmall]);
+      } else {
+        ch(k_small_idct, Blocks(3 * n[kCSmall], kSmallIdctThreads),
+           kSmallIdctThreads, 0, g, f, L[kCSmall], n[kCSmall]);
+      }
+    }
     if (n[kC4]) {
-      k_dct4_idct<<<Blocks(3 * n[kC4], kDct4Threads / 8), kDct4Threads, 0,
-                    cls(kC4)>>>(g, f, L[kC4], n[kC4], s.predict_hf);
-      ++ctx->launches;
+      ch(k_dct4_idct, Blocks(3 * n[kC4], kDct4Threads / 8), kDct4Threads, 0,
+         g, f, L[kC4], n[kC4], s.predict_hf);
     }
     if (n[kC32] && ctx->form != PIKGPU_FORM_FP32) {
       // One channel per CTA: four blocks of 32 rows per batch, up to
@@ -725,20 +764,12 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       // without HF prediction reached 3.0e-5 against FP64.
       const int items = 3 * ((n[kC32] + 3) / 4);
       const int grid = std::min(items, ctx->num_sms * ctx->tc_ctas_per_sm);
-      k_square_idct_tc1<32, 3><<<grid, tc::kThreads, 0, cls(kC32)>>>(
-          g, f, L[kC32], n[kC32], s.predict_hf, counters + kWorkIdct32,
-          P<int>(ctx->tc_err));
-      ++ctx->launches;
+      ch(k_square_idct_tc1<32, 3>, grid, tc::kThreads, 0, g, f, L[kC32],
+         n[kC32], s.predict_hf, counters + kWorkIdct32, P<int>(ctx->tc_err));
     } else if (n[kC32]) {
       // One 256-thread CTA per block.
-      k_square_idct<32><<<n[kC32], 256, 0, cls(kC32)>>>(g, f, L[kC32], n[kC32],
-                                                       s.predict_hf);
-      ++ctx->launches;
-    }
-    if (n[kC8]) {
-      k_square_idct_rows<8><<<rows_grid(3 * n[kC8], 8), kSquareThreads, 0,
-                              cls(kC8)>>>(g, f, L[kC8], n[kC8], s.predict_hf);
-      ++ctx->launches;
+      ch(k_square_idct<32>, n[kC32], 256, 0, g, f, L[kC32], n[kC32],
+         s.predict_hf);
     }
     if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
       const int items = (n[kC16] + 7) / 8;
@@ -749,23 +780,19 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
       // carries the bulk of the coefficients (it is added in FP32 outside
       // the tensor cores); frames without it take three terms.
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16 && s.predict_hf) {
-        k_square_idct_tc1<16, 2><<<grid, tc::kThreads, 0, cls(kC16)>>>(
-            g, f, L[kC16], n[kC16], s.predict_hf, counters + kWorkIdct,
-            P<int>(ctx->tc_err));
+        ch(k_square_idct_tc1<16, 2>, grid, tc::kThreads, 0, g, f, L[kC16],
+           n[kC16], s.predict_hf, counters + kWorkIdct, P<int>(ctx->tc_err));
       } else {
-        k_square_idct_tc1<16, 3><<<grid, tc::kThreads, 0, cls(kC16)>>>(
-            g, f, L[kC16], n[kC16], s.predict_hf, counters + kWorkIdct,
-            P<int>(ctx->tc_err));
+        ch(k_square_idct_tc1<16, 3>, grid, tc::kThreads, 0, g, f, L[kC16],
+           n[kC16], s.predict_hf, counters + kWorkIdct, P<int>(ctx->tc_err));
       }
-      ++ctx->launches;
     } else if (n[kC16]) {
-      k_square_idct_rows<16><<<rows_grid(3 * n[kC16], 16), kSquareThreads, 0,
-                               cls(kC16)>>>(g, f, L[kC16], n[kC16],
-                                            s.predict_hf);
-      ++ctx->launches;
+      ch(k_square_idct_rows<16>, rows_grid(3 * n[kC16], 16), kSquareThreads,
+         0, g, f, L[kC16], n[kC16], s.predict_hf);
     }
+    CUDA_TRY(ctx, ch.err);
   }
-  br.Join(1, ctx->kSide);
+  br.Join(1, 1);
   const float* final_in = f.idct;
   Mark(ctx, kTGab1);
   if (s.have_ar) {
@@ -820,73 +847,62 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
         ++ctx->launches;
       }
     }
-    br.Fork(2, ctx->kSide);
+    br.Fork(2, 1);
     auto rows_grid = [](int items, int nn) {
       const int upw = 32 / nn;
       const int warps = (items + upw - 1) / upw;
       return (warps * 32 + kSquareThreads - 1) / kSquareThreads;
     };
-    if (n[kCSmall]) {
-      if (n[kCSmall] <= kSmallCtaMax * ctx->num_sms) {
-        k_small_ar_cta<<<n[kCSmall], kSmallCtaThreads, 0, cls(kCSmall)>>>(
-            g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
-      } else {
-        k_small_ar<<<Blocks(n[kCSmall], kSmallArBlocks), 3 * kSmallArBlocks,
-                     0, cls(kCSmall)>>>(
-            g, f, s, P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
-      }
+    if (n[kC8]) {
+      k_square_ar_rows<8><<<rows_grid(n[kC8], 8), kSquareThreads, 0, st>>>(
+          g, f, s, P<uint32_t>(ctx->active[kC8]), counters + kC8);
       ++ctx->launches;
     }
+    ClassChain ch{br[0], &ctx->launches};
+    if (n[kCSmall]) {
+      if (n[kCSmall] <= kSmallCtaMax * ctx->num_sms) {
+        ch(k_small_ar_cta, n[kCSmall], kSmallCtaThreads, 0, g, f, s,
+           P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
+      } else {
+        ch(k_small_ar, Blocks(n[kCSmall], kSmallArBlocks),
+           3 * kSmallArBlocks, 0, g, f, s,
+           P<uint32_t>(ctx->active[kCSmall]), counters + kCSmall);
+      }
+    }
     if (n[kC4]) {
-      k_dct4_ar<<<Blocks(n[kC4], kDct4ArThreads / 32), kDct4ArThreads, 0,
-                  cls(kC4)>>>(
-          g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
-      ++ctx->launches;
+      ch(k_dct4_ar, Blocks(n[kC4], kDct4ArThreads / 32), kDct4ArThreads, 0,
+         g, f, s, P<uint32_t>(ctx->active[kC4]), counters + kC4);
     }
     if (n[kC32] && ctx->form != PIKGPU_FORM_FP32) {
       // Four blocks per batch; two CTAs per SM (256 tensor-memory columns
       // each); three BF16 terms in both tensor-core forms (see the
       // transforms).
       const int grid = std::min((n[kC32] + 3) / 4, ctx->num_sms * 2);
-      k_square_ar_tc<32, 3><<<grid, tc::kThreads, ArTcSmemBytes<32, 3>(),
-                              cls(kC32)>>>(
-          g, f, s, P<uint32_t>(ctx->active[kC32]), counters + kC32,
-          counters + kWorkAr32, P<int>(ctx->tc_err));
-      ++ctx->launches;
+      ch(k_square_ar_tc<32, 3>, grid, tc::kThreads, ArTcSmemBytes<32, 3>(),
+         g, f, s, P<uint32_t>(ctx->active[kC32]), counters + kC32,
+         counters + kWorkAr32, P<int>(ctx->tc_err));
     } else if (n[kC32]) {
-      k_square_ar<32><<<n[kC32], 256, 0, cls(kC32)>>>(
-          g, f, s, P<uint32_t>(ctx->active[kC32]), counters + kC32);
-      ++ctx->launches;
-    }
-    if (n[kC8]) {
-      k_square_ar_rows<8><<<rows_grid(n[kC8], 8), kSquareThreads, 0,
-                            cls(kC8)>>>(g, f, s, P<uint32_t>(ctx->active[kC8]),
-                                        counters + kC8);
-      ++ctx->launches;
+      ch(k_square_ar<32>, n[kC32], 256, 0, g, f, s,
+         P<uint32_t>(ctx->active[kC32]), counters + kC32);
     }
     if (n[kC16] && ctx->form != PIKGPU_FORM_FP32) {
       const int grid =
           std::min((n[kC16] + 7) / 8, ctx->num_sms * ctx->tc_ctas_per_sm);
       if (ctx->form == PIKGPU_FORM_SPLIT_BF16) {
-        k_square_ar_tc<16, 2><<<grid, tc::kThreads, ArTcSmemBytes<16, 2>(),
-                                cls(kC16)>>>(
-            g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
-            counters + kWorkAr, P<int>(ctx->tc_err));
+        ch(k_square_ar_tc<16, 2>, grid, tc::kThreads, ArTcSmemBytes<16, 2>(),
+           g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
+           counters + kWorkAr, P<int>(ctx->tc_err));
       } else {
-        k_square_ar_tc<16, 3><<<grid, tc::kThreads, ArTcSmemBytes<16, 3>(),
-                                cls(kC16)>>>(
-            g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
-            counters + kWorkAr, P<int>(ctx->tc_err));
+        ch(k_square_ar_tc<16, 3>, grid, tc::kThreads, ArTcSmemBytes<16, 3>(),
+           g, f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16,
+           counters + kWorkAr, P<int>(ctx->tc_err));
       }
-      ++ctx->launches;
     } else if (n[kC16]) {
-      k_square_ar_rows<16><<<rows_grid(n[kC16], 16), kSquareThreads, 0,
-                             cls(kC16)>>>(g, f, s,
-                                          P<uint32_t>(ctx->active[kC16]),
-                                          counters + kC16);
-      ++ctx->launches;
+      ch(k_square_ar_rows<16>, rows_grid(n[kC16], 16), kSquareThreads, 0, g,
+         f, s, P<uint32_t>(ctx->active[kC16]), counters + kC16);
     }
-    br.Join(2, ctx->kSide);
+    CUDA_TRY(ctx, ch.err);
+    br.Join(2, 1);
     final_in = f.filt;
   } else {
     Mark(ctx, kTEpf);

@@ -1005,6 +1005,8 @@ template <int N>
 __global__ void __launch_bounds__(256)
     k_square_idct(Geo g, DevFrame f, const uint32_t* list, int count,
                   int predict_hf) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   constexpr int NN = N * N;
   constexpr int NB = NN >= 256 ? 1 : 256 / NN;
   __shared__ float s_a[NN], s_b[NN];
@@ -1079,6 +1081,8 @@ constexpr int kDct4Threads = 128;
 __global__ void __launch_bounds__(kDct4Threads)
     k_dct4_idct(Geo g, DevFrame f, const uint32_t* list, int count,
                 int predict_hf) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   constexpr int kUnits = kDct4Threads / 8;
   __shared__ float s_t[kUnits][2][2][4][5];  // per unit: [sy][sx][row][col]
   const int unit = threadIdx.x >> 3, j = threadIdx.x & 7;
@@ -1529,6 +1533,8 @@ __device__ void SmallForwardPar(int type, int c, int e, float (*px)[64],
 // (k_small_idct: throughput, for frames with many).
 __global__ void __launch_bounds__(kSmallCtaThreads)
     k_small_idct_cta(Geo g, DevFrame f, const uint32_t* list, int count) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   __shared__ float s_co[3][64], s_px[3][64];
   __shared__ float s_aux[3][4];
   const int c = threadIdx.x >> 6, e = threadIdx.x & 63;
@@ -1550,6 +1556,8 @@ __global__ void __launch_bounds__(kSmallCtaThreads)
 constexpr int kSmallIdctThreads = 64;
 __global__ void __launch_bounds__(kSmallIdctThreads)
     k_small_idct(Geo g, DevFrame f, const uint32_t* list, int count) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   __shared__ float s_in[kSmallIdctThreads][65];
   __shared__ float s_out[kSmallIdctThreads][65];
   const int lane = threadIdx.x & 31, w0 = threadIdx.x & ~31;
@@ -1685,6 +1693,8 @@ template <int N>
 __global__ void __launch_bounds__(256)
     k_square_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
                 const int* count_ptr) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   constexpr int NN = N * N;
   constexpr int NB = NN >= 256 ? 1 : 256 / NN;
   constexpr int cov = N / 8;
@@ -1770,6 +1780,8 @@ constexpr int kDct4ArThreads = 128;
 __global__ void __launch_bounds__(kDct4ArThreads)
     k_dct4_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
               const int* count_ptr) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   constexpr int kWarps = kDct4ArThreads / 32;
   const int count = *count_ptr;
   if (int(blockIdx.x) * kWarps >= count) return;  // whole CTA
@@ -2032,6 +2044,8 @@ __device__ void SmallForward(int type, const float* px, int ps, float* co) {
 __global__ void __launch_bounds__(kSmallCtaThreads)
     k_small_ar_cta(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
                    const int* count_ptr) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   if (int(blockIdx.x) >= *count_ptr) return;  // whole CTA
   __shared__ float s_px[3][64], s_co[3][64], s_r[3][64];
   __shared__ float s_aux[3][4];
@@ -2084,6 +2098,8 @@ constexpr int kSmallArBlocks = 32;
 __global__ void __launch_bounds__(3 * kSmallArBlocks)
     k_small_ar(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
                const int* count_ptr) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   __shared__ float s_ratio[3][kSmallArBlocks][65];
   const int count = *count_ptr;
   if (int(blockIdx.x) * kSmallArBlocks >= count) return;  // whole CTA

@@ -99,6 +99,8 @@ template <int N>
 __global__ void __launch_bounds__(kSquareThreads)
     k_square_idct_rows(Geo g, DevFrame f, const uint32_t* list, int count,
                        int predict_hf) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   using namespace square;
   constexpr int UPW = 32 / N;  // units per warp
   constexpr int cov = N / 8;
@@ -201,6 +203,8 @@ template <int N>
 __global__ void __launch_bounds__(kSquareThreads)
     k_square_ar_rows(Geo g, DevFrame f, FrameScalars s, const uint32_t* list,
                      const int* count_ptr) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   using namespace square;
   constexpr int UPW = 32 / N;
   constexpr int cov = N / 8;

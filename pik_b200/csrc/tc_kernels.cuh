@@ -354,6 +354,8 @@ template <int N, int S>
 __global__ void __launch_bounds__(tc::kThreads, N == 16 ? 4 : 2)
     k_square_ar_tc(Geo g, DevFrame f, FrameScalars sc, const uint32_t* list,
                    const int* count_ptr, int* work, int* err) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   using namespace tc;
   constexpr int BPB = 128 / N;
   constexpr int cov = N / 8;
@@ -545,6 +547,8 @@ template <int N, int S>
 __global__ void __launch_bounds__(tc::kThreads, N == 16 ? 8 : 4)
     k_square_idct_tc1(Geo g, DevFrame f, const uint32_t* list, int count,
                       int predict_hf, int* work, int* err) {
+  PdlLaunchDependents();
+  PdlTail pdl_tail;
   using namespace tc;
   using square::CoefRowOffset;
   static_assert(N == 16 || N == 32, "DCT16X16 or DCT32X32");
