@@ -614,11 +614,10 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
       epf_smem + 3 * (TH + 8) * kEpfGRow);
   uint32_t* sa = epf_smem + 3 * (TH + 8) * kEpfGRow + 3 * (TH + 10) * kEpfTS;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sa + 3 * (TH + 8) * kEpfAligned);
+  PdlLaunchDependents();  // the active-block pass may start on free SMs
   const int tiles_x = (w + kEpfW - 1) / kEpfW;
   const int x0 = (blockIdx.x % tiles_x) * kEpfW;
   const int y0 = (blockIdx.x / tiles_x) * TH;
-  float amin, mul, stretch;
-  GuideParams(mm, &amin, &mul, &stretch);
   const uint32_t tile_s = tc::SmemU32(tile), mbar_s = tc::SmemU32(mbar);
   const bool tma = use_tma && EpfInterior<TH>(w, h, x0, y0) &&
                    (tile_s & 127u) == 0;
@@ -642,6 +641,12 @@ __global__ void __launch_bounds__(16 * TH, TH == 16 ? 3 : 2)
   } else {
     EpfStage<TH>(in, w, h, x0, y0, tile, threadIdx.x);
   }
+  // The input is complete before the min/max pass starts; the guide range
+  // in `mm` is that pass's output (the previous kernel on the stream, under
+  // a programmatic dependent launch still running until here).
+  PdlWait();
+  float amin, mul, stretch;
+  GuideParams(mm, &amin, &mul, &stretch);
   const int sig = EpfLaneSigma(sgs, stretch, w, h, x0, y0);
   if (tma) {
     __syncthreads();  // the mbarrier is initialised before anyone waits

@@ -66,6 +66,14 @@ struct PdlTail {
     asm volatile("griddepcontrol.wait;" ::: "memory");
   }
 };
+// On the main stream, kernels that read their predecessor's output (the
+// EPF reads the guide range of the min/max pass, the active-block pass the
+// EPF's sigma) may also be launched that way: they call PdlWait before the
+// first such read, and what comes before it (staging the frame's tile, say)
+// overlaps the predecessor's last CTAs.
+__device__ __forceinline__ void PdlWait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
 
 // Frame geometry.
 struct Geo {

@@ -462,6 +462,28 @@ void Mark(pikgpu_ctx* ctx, int i) {
   if (ctx->profile) cudaEventRecord(ctx->ev[i], ctx->stream);
 }
 
+// Launches `kernel` on `st`; with `pdl`, as a programmatic dependent of the
+// kernel before it on the stream
+// (cudaLaunchAttributeProgrammaticStreamSerialization): it may then start
+// once every CTA of that kernel has begun (PdlLaunchDependents), and it
+// orders itself after that kernel's completion with griddepcontrol.wait
+// (PdlWait or PdlTail in the kernel).
+template <typename... KArgs, typename... Args>
+cudaError_t LaunchPdl(bool pdl, void (*kernel)(KArgs...), int grid, int block,
+                      size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr = {};
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? &attr : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // The frame EPF or the DC EPF: the min/max of the guide source is expected
 // in `mm` already. `sgs`: where the per-block sigma comes from (computed in
 // the kernel); `dco`: the DC image's clamped output instead of `out`.
@@ -518,7 +540,7 @@ void EpfLaunch(cudaStream_t st, int num_sms, int form, const float* in,
                const float* guide_src, int gab, int w, int h,
                const uint32_t* mm, const EpfSigma& sgs, float* out,
                const uint8_t* guide_ovr, const EpfDc& dco, int* err,
-               uint32_t polls = tc::kMaxPolls) {
+               uint32_t polls = tc::kMaxPolls, bool pdl = false) {
   // Images that fill fewer than two CTAs per SM with 32-row tiles (the DC
   // image) take 8-row tiles: four times the CTAs, a quarter of the latency.
   const bool small = Blocks(w, kEpfW) * Blocks(h, kEpfH) < 2 * num_sms;
@@ -529,27 +551,28 @@ void EpfLaunch(cudaStream_t st, int num_sms, int form, const float* in,
   CUtensorMap map;
   memset(&map, 0, sizeof(map));
   const int tma = err && EpfTileMap(&map, in, w, h, th) ? 1 : 0;
+  // Errors of the launch surface through cudaGetLastError.
   if (small) {
     if (fma) {
-      k_epf_box<true, 8><<<grid(8), 16 * 8, EpfSmemBytes(8), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
-          err, polls);
+      LaunchPdl(pdl, k_epf_box<true, 8>, grid(8), 16 * 8, EpfSmemBytes(8), st,
+                in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map,
+                tma, err, polls);
     } else {
-      k_epf_box<false, 8><<<grid(8), 16 * 8, EpfSmemBytes(8), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
-          err, polls);
+      LaunchPdl(pdl, k_epf_box<false, 8>, grid(8), 16 * 8, EpfSmemBytes(8),
+                st, in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco,
+                map, tma, err, polls);
     }
   } else {
     if (fma) {
       // 16-row tiles of 256 threads, three CTAs per SM: the cx-major loop
       // of these forms needs ~85 registers.
-      k_epf_box<true, 16><<<grid(16), 16 * 16, EpfSmemBytes(16), st>>>(
-          in, guide_src, guide_ovr, gab, w, h, mm, sgs, out, dco, map, tma,
-          err, polls);
+      LaunchPdl(pdl, k_epf_box<true, 16>, grid(16), 16 * 16,
+                EpfSmemBytes(16), st, in, guide_src, guide_ovr, gab, w, h, mm,
+                sgs, out, dco, map, tma, err, polls);
     } else {
-      k_epf_box<false, kEpfH><<<grid(kEpfH), kEpfThreads, kEpfSmemBytes,
-                                st>>>(in, guide_src, guide_ovr, gab, w, h, mm,
-                                      sgs, out, dco, map, tma, err, polls);
+      LaunchPdl(pdl, k_epf_box<false, kEpfH>, grid(kEpfH), kEpfThreads,
+                kEpfSmemBytes, st, in, guide_src, guide_ovr, gab, w, h, mm,
+                sgs, out, dco, map, tma, err, polls);
     }
   }
 }
@@ -600,17 +623,8 @@ struct ClassChain {
   template <typename... KArgs, typename... Args>
   void operator()(void (*kernel)(KArgs...), int grid, int block, size_t smem,
                   Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr = {};
-    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr.val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = started ? &attr : nullptr;
-    cfg.numAttrs = started ? 1 : 0;
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+    const cudaError_t e =
+        LaunchPdl(started, kernel, grid, block, smem, st, args...);
     if (e != cudaSuccess && err == cudaSuccess) err = e;
     started = true;
     ++*launches;
@@ -801,6 +815,12 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     // here only its min/max), or the IDCT output itself (sharpened guide,
     // or no gaborish).
     const int gab = s.use_sharpened ? 0 : s.gaborish;
+    // The clamp tape starts empty (written by the clamp kernels only).
+    if (f.clamp_tape) cudaMemsetAsync(f.clamp_tape, 0, nac, st);
+    // The EPF, and after it the active-block pass, as programmatic
+    // dependents of the kernel before each (LaunchPdl) when nothing else
+    // lies between them on the stream (no per-group events, no stage copy).
+    const bool pdl = !ctx->profile && !ctx->keep_stages;
     if (gab) {
       const int warps = Blocks(g.PW, 128) * Blocks(g.PH, kGmmRows);
       k_gaborish_minmax<<<dim3(Blocks(warps, 8), 3), 256, 0, st>>>(
@@ -821,7 +841,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     EpfLaunch(st, ctx->num_sms, ctx->form, f.idct, f.idct, gab, g.PW, g.PH,
               mm, sgs, f.filt,
               ctx->use_guide_ovr ? P<uint8_t>(ctx->guide_ovr) : nullptr,
-              EpfDc{}, P<int>(ctx->tc_err), ctx->tc_polls);
+              EpfDc{}, P<int>(ctx->tc_err), ctx->tc_polls, pdl);
     ++ctx->launches;
     if (ctx->keep_stages) {
       cudaMemcpyAsync(ctx->dbg_epf.p, f.filt, sizeof(float) * 3 * npx,
@@ -829,7 +849,6 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
     }
     Mark(ctx, kTAr);
     // Only blocks the EPF filtered need the clamp (see k_active_blocks).
-    if (f.clamp_tape) cudaMemsetAsync(f.clamp_tape, 0, nac, st);
     // Every class's filtered blocks in one pass (main stream), then the
     // classes' clamps, the ones with few blocks first (see the transforms).
     {
@@ -842,8 +861,8 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
         total += n[k];
       }
       if (total) {
-        k_active_blocks<<<Blocks(total, 256), 256, 0, st>>>(g, sig, f.acs, cl,
-                                                            counters);
+        CUDA_TRY(ctx, LaunchPdl(pdl, k_active_blocks, Blocks(total, 256), 256,
+                                0, st, g, sig, f.acs, cl, counters));
         ++ctx->launches;
       }
     }

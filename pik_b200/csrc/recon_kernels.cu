@@ -305,6 +305,7 @@ __global__ void k_frame_init(uint32_t* mm, int* counters, int n) {
 
 __global__ void __launch_bounds__(256)
     k_minmax(const float* planes, size_t n, uint32_t* mm) {
+  PdlLaunchDependents();  // the EPF may start on free SMs
   __shared__ uint32_t s_lo[8], s_hi[8];
   const int c = blockIdx.y;
   const float* p = planes + size_t(c) * n;

@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(kSquareThreads)
 __global__ void k_active_blocks(Geo g, const int32_t* sigma,
                                 const uint8_t* acs, ClassLists cl,
                                 int* counters) {
+  PdlWait();  // the EPF's sigma
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int k = 0;
   while (k < kMaxClasses && i >= cl.n[k]) i -= cl.n[k++];

@@ -179,6 +179,7 @@ constexpr int kGmmRows = 8;
 __global__ void __launch_bounds__(256, 3)
     k_gaborish_minmax(const float* in, int w, int h, int strength,
                       uint32_t* mm) {
+  PdlLaunchDependents();  // the EPF may start on free SMs
   constexpr int R = kGmmRows;
   __shared__ uint32_t s_lo[8], s_hi[8];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
