@@ -236,7 +236,9 @@ int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
  *  KEEP_STAGES: keep the dequantised AC, EPF and pre-opsin planes for
  *               pikgpu_get_stage (costs extra device memory and copies);
  *  PROFILE:     time each kernel group with CUDA events
- *               (pikgpu_last_kernel_times);
+ *               (pikgpu_last_kernel_times); every kernel then runs on one
+ *               stream after the one before it (no concurrent branches, no
+ *               programmatic dependent launches, no graph replay);
  *  FORM:        PIKGPU_FORM_FP32 (default): every stage in FP32 on the CUDA
  *               cores in the reference's operation order;
  *               PIKGPU_FORM_SPLIT_BF16: the 16x16 and 32x32 transforms
@@ -257,7 +259,10 @@ int pikgpu_validate(const pikgpu_frame_params* params, char* msg,
  *               device buffers, outputs and stream all unchanged -- the
  *               coefficients and side information may differ), the launch
  *               sequence is captured once into a CUDA graph and replayed
- *               as one launch; 0: every call launches its ~30 kernels. */
+ *               as one launch; 0: every call launches its 17 or so kernels.
+ *               Either way some kernels are programmatic dependent launches
+ *               of the kernel before them on their stream: they may start
+ *               while it finishes, ordered by griddepcontrol in the kernels. */
 #define PIKGPU_OPT_KEEP_STAGES 1
 #define PIKGPU_OPT_PROFILE 2
 #define PIKGPU_OPT_FORM 3

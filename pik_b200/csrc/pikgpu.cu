@@ -618,13 +618,14 @@ struct Branches {
 struct ClassChain {
   cudaStream_t st;
   int* launches;
+  bool pdl;  // false: ordinary launches, each after the one before
   bool started = false;
   cudaError_t err = cudaSuccess;
   template <typename... KArgs, typename... Args>
   void operator()(void (*kernel)(KArgs...), int grid, int block, size_t smem,
                   Args... args) {
     const cudaError_t e =
-        LaunchPdl(started, kernel, grid, block, smem, st, args...);
+        LaunchPdl(pdl && started, kernel, grid, block, smem, st, args...);
     if (e != cudaSuccess && err == cudaSuccess) err = e;
     started = true;
     ++*launches;
@@ -757,7 +758,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
                               st>>>(g, f, L[kC8], n[kC8], s.predict_hf);
       ++ctx->launches;
     }
-    ClassChain ch{br[0], &ctx->launches};
+    ClassChain ch{br[0], &ctx->launches, !ctx->profile};
     if (n[kCSmall]) {
       if (n[kCSmall] <= kSmallCtaMax * ctx->num_sms) {
         ch(k_small_idct_cta, n[kCSmall], kSmallCtaThreads, 0, g, f,
@@ -877,7 +878,7 @@ int LaunchAll(pikgpu_ctx* ctx, float* lin, size_t lin_stride, uint8_t* rgb8,
           g, f, s, P<uint32_t>(ctx->active[kC8]), counters + kC8);
       ++ctx->launches;
     }
-    ClassChain ch{br[0], &ctx->launches};
+    ClassChain ch{br[0], &ctx->launches, !ctx->profile};
     if (n[kCSmall]) {
       if (n[kCSmall] <= kSmallCtaMax * ctx->num_sms) {
         ch(k_small_ar_cta, n[kCSmall], kSmallCtaThreads, 0, g, f, s,
