@@ -285,7 +285,7 @@ def batch_frames(n=64):
 def batch_main(args):
     """Total MP/s of 64 frames of uneven sizes: one replay of the batch's
     captured CUDA graph per step, against the same 64 frames reconstructed
-    by per-image calls (each a synchronous sequence of ~30 launches)."""
+    by per-image calls (each a synchronous sequence of 17 or so launches)."""
     import torch
     from pik_b200 import native
     ws, rank, local = dist_env()
@@ -833,7 +833,7 @@ def main():
 
     ms, launches, clk = time_device(args.form, sample_clocks=True)
     value = ws * px / (ms * 1e-3) / 1e6
-    # The same without graph replay: every step launches its ~30 kernels.
+    # The same without graph replay: every step launches its 17 kernels.
     ms_direct = time_device(args.form, graphs=False)[0]
     # The other forms on the same frame, for the form comparison.
     forms = {args.form: ms}

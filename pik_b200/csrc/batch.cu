@@ -4,7 +4,7 @@
 // once into one CUDA graph, one branch per frame (forked from and joined to
 // the batch stream through events), and the graph is replayed. Frames that
 // are too small to fill the GPU then run side by side, and the CPU cost of
-// the frames' ~30 launches each is paid once at capture instead of on every
+// the frames' 17 or so launches each is paid once at capture instead of on every
 // call. The graph depends on each frame's geometry, block lists, options and
 // output pointers; any change re-captures it on the next call.
 // Included by pikgpu.cu (uses the context internals and LaunchAll).
